@@ -1,0 +1,147 @@
+"""ctypes binding of libexfemus_b200.so (the C ABI declared in include/exfemus_b200.h)."""
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libexfemus_b200.so")
+
+EXF_OK = 0
+EXF_ERR_ARG = 1
+EXF_ERR_CUDA = 2
+EXF_ERR_STATE = 3
+EXF_ERR_DIVERGED = 4
+EXF_ERR_NOT_CONVERGED = 5
+EXF_ERR_SINGULAR = 6
+EXF_ERR_NOMEM = 7
+EXF_ERR_UNSUPPORTED = 8
+
+KIND_T = 0
+KIND_NS = 1
+BC_HEAT_DIRICHLET = 1
+BC_CAVITY = 2
+BC_CHANNEL = 3
+BC_BOUSS_NS = 4
+BC_BOUSS_T = 5
+SMOOTH_GS = 0
+SMOOTH_VANKA = 1
+PREC_FP64 = 0
+PREC_MIXED = 1
+
+
+class ExfMeshDesc(C.Structure):
+    _fields_ = [("dim", C.c_int), ("nlev", C.c_int), ("n0", C.c_int * 3), ("box", C.c_double * 6),
+                ("device", C.c_int)]
+
+
+class ExfPhys(C.Structure):
+    _fields_ = [("inv_re", C.c_double), ("inv_prdl", C.c_double), ("rho", C.c_double),
+                ("rhocp", C.c_double), ("inv_dt", C.c_double), ("penalty", C.c_double),
+                ("upwind_ns", C.c_double), ("upwind_t", C.c_double), ("ifr", C.c_double),
+                ("dirg", C.c_double * 3), ("buoy", C.c_double)]
+
+
+class ExfMgParams(C.Structure):
+    _fields_ = [("eps", C.c_double), ("max_cycles", C.c_int), ("gamma", C.c_int),
+                ("nu_pre", C.c_int), ("nu_post", C.c_int), ("double_below_top", C.c_int),
+                ("smoother", C.c_int), ("omega", C.c_double), ("corr_damp", C.c_double),
+                ("cond_corr", C.c_int), ("reverse_colours", C.c_int), ("precision", C.c_int),
+                ("use_graph", C.c_int)]
+
+
+class ExfSolveStats(C.Structure):
+    _fields_ = [("cycles", C.c_int), ("converged", C.c_int), ("rel_res", C.c_double),
+                ("bnorm", C.c_double), ("seconds", C.c_double), ("hist", C.c_double * 256)]
+
+
+class ExfError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__("exfemus_b200 error %d: %s" % (code, msg))
+        self.code = code
+
+
+_L = None
+
+# (name, restype, argtypes) of every exported entry point
+_P = C.c_void_p
+_I = C.c_int
+_IP = C.POINTER(C.c_int)
+_DP = C.POINTER(C.c_double)
+_LP = C.POINTER(C.c_long)
+SIGNATURES = [
+    ("exf_last_error", C.c_char_p, []),
+    ("exf_version", C.c_char_p, []),
+    ("exf_mesh_create", _I, [C.POINTER(ExfMeshDesc), C.POINTER(_P)]),
+    ("exf_mesh_destroy", _I, [_P]),
+    ("exf_mesh_info", _I, [_P, _I, _IP, _IP, _IP]),
+    ("exf_mesh_get_xyz", _I, [_P, _DP]),
+    ("exf_mesh_get_conn", _I, [_P, _I, _IP, _IP, _IP]),
+    ("exf_sys_create", _I, [_P, _I, C.POINTER(_P)]),
+    ("exf_sys_destroy", _I, [_P]),
+    ("exf_sys_ndof", _I, [_P, _I, _IP]),
+    ("exf_sys_get_node_dof", _I, [_P, _I, _IP]),
+    ("exf_sys_bc_preset", _I, [_P, _I]),
+    ("exf_sys_set_bc", _I, [_P, _IP, _IP]),
+    ("exf_sys_get_bc", _I, [_P, _IP, _IP]),
+    ("exf_sys_nnz", _I, [_P, _I, _LP]),
+    ("exf_sys_get_pattern", _I, [_P, _I, _IP, _IP]),
+    ("exf_sys_get_prol", _I, [_P, _I, _LP, _IP, _IP, _DP]),
+    ("exf_sys_get_rest", _I, [_P, _I, _LP, _IP, _IP, _DP]),
+    ("exf_sys_get_colours", _I, [_P, _I, _IP, _IP]),
+    ("exf_sys_couple", _I, [_P, _P]),
+    ("exf_sys_set_xold", _I, [_P, _DP]),
+    ("exf_sys_get_xold", _I, [_P, _DP]),
+    ("exf_sys_set_x", _I, [_P, _DP]),
+    ("exf_sys_get_x", _I, [_P, _DP]),
+    ("exf_sys_xold_update", _I, [_P]),
+    ("exf_sys_set_source", _I, [_P, _DP]),
+    ("exf_sys_set_rhs", _I, [_P, _DP]),
+    ("exf_sys_get_rhs", _I, [_P, _DP]),
+    ("exf_gen_mat_rhs", _I, [_P, C.POINTER(ExfPhys), _I, _I]),
+    ("exf_assemble_all", _I, [_P, C.POINTER(ExfPhys)]),
+    ("exf_get_matrix", _I, [_P, _I, _DP]),
+    ("exf_set_matrix", _I, [_P, _I, _DP]),
+    ("exf_mg_solve", _I, [_P, C.POINTER(ExfMgParams), C.POINTER(ExfSolveStats)]),
+    ("exf_resid", _I, [_P, _I, _DP, _DP, _DP]),
+    ("exf_restrict", _I, [_P, _I, _DP, _DP]),
+    ("exf_prolong", _I, [_P, _I, _DP, _DP]),
+    ("exf_smooth", _I, [_P, _I, C.POINTER(ExfMgParams), _I, _DP, _DP]),
+    ("exf_coarse_solve", _I, [_P, _DP, _DP]),
+    ("exf_sys_transpose", _I, [_P]),
+    ("exf_adjoint_forward", _I, [_P, C.POINTER(ExfPhys), C.POINTER(ExfMgParams), C.POINTER(ExfSolveStats)]),
+    ("exf_adjoint_backward", _I, [_P, C.POINTER(ExfPhys), C.POINTER(ExfMgParams), _DP, _DP, _DP,
+                                  C.POINTER(ExfSolveStats)]),
+    ("exf_time_op", _I, [_P, _I, _I, C.POINTER(ExfMgParams), C.POINTER(ExfPhys), _I, _DP]),
+    ("exf_sync", _I, [_P]),
+]
+
+
+def load():
+    """Load the CUDA library; raises if it has not been built (there is no fallback)."""
+    global _L
+    if _L is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError("libexfemus_b200.so not built: run python -m exfemus_b200.build")
+        L = C.CDLL(LIB_PATH)
+        for name, res, args in SIGNATURES:
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _L = L
+    return _L
+
+
+def check(rc):
+    if rc != EXF_OK:
+        msg = load().exf_last_error().decode(errors="replace")
+        raise ExfError(rc, msg)
+    return rc
+
+
+def dptr(a):
+    return a.ctypes.data_as(_DP)
+
+
+def iptr(a):
+    return a.ctypes.data_as(_IP)

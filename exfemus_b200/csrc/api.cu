@@ -1,0 +1,917 @@
+// api.cu -- the C ABI: meshes, systems (one per equation, like an MGSolBase object),
+// assembly dispatch, and the multigrid driver (MGSolve/MGStep) on device-resident state.
+//
+// Multigrid (src/MGSolverBase.C:163-289): recursive cycle with gamma coarse visits,
+// sweeps doubled below the top level, damped coarse correction (0.95 in the reference,
+// optionally conditional as in the reference), exact coarse solve.  The stop test is the
+// relative residual ||b-Ax||/||b|| of the top level.  Mixed precision: the residual,
+// solution update and coarse solve are FP64; the V-cycle (smoother, residuals, transfers)
+// runs on FP32 copies of the level matrices (defect correction).
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "exf_internal.h"
+
+namespace exf {
+
+static thread_local char g_err[512] = "";
+void set_error(const char *fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_err, sizeof(g_err), fmt, ap);
+  va_end(ap);
+}
+
+static inline unsigned nblk(long n, int bs) { return (unsigned)((n + bs - 1) / bs); }
+
+// ------------------------------------------------- NB <-> DOF-level CSR values
+__global__ void k_nb_to_csr(int N, int NL, int d, int ns, const int *qq_ptr, const int *ql_ptr, long nqq, long nql,
+                            long nqqL, const double *vv, const double *vp, const double *pv, const double *pp,
+                            const int *rowptr, double *out, int dir) {
+  long r = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  long nq = (long)d * N;
+  long nrow = nq + (ns ? NL : 0);
+  if (r >= nrow) return;
+  long o = rowptr[r];
+  double *vvw = const_cast<double *>(vv), *vpw = const_cast<double *>(vp), *pvw = const_cast<double *>(pv),
+         *ppw = const_cast<double *>(pp);
+  if (r < nq) {
+    int a = (int)(r / N), n = (int)(r % N);
+    for (int b = 0; b < d; b++)
+      for (int k = qq_ptr[n]; k < qq_ptr[n + 1]; k++, o++) {
+        long idx = (long)(a * d + b) * nqq + k;
+        if (dir == 0) out[o] = vv[idx];
+        else vvw[idx] = out[o];
+      }
+    if (ns)
+      for (int k = ql_ptr[n]; k < ql_ptr[n + 1]; k++, o++) {
+        long idx = (long)a * nql + k;
+        if (dir == 0) out[o] = vp[idx];
+        else vpw[idx] = out[o];
+      }
+  } else {
+    int m = (int)(r - nq);
+    for (int b = 0; b < d; b++)
+      for (int k = qq_ptr[m]; k < qq_ptr[m + 1]; k++, o++) {
+        long idx = (long)b * nqqL + k;
+        if (dir == 0) out[o] = pv[idx];
+        else pvw[idx] = out[o];
+      }
+    for (int k = ql_ptr[m]; k < ql_ptr[m + 1]; k++, o++) {
+      if (dir == 0) out[o] = pp[k];
+      else ppw[k] = out[o];
+    }
+  }
+}
+
+static int nb_csr(exf_sys *s, int lev, double *d_vals, int dir) {
+  SysLevel &L = s->L[lev];
+  k_nb_to_csr<<<nblk(L.ndof, 256), 256, 0, s->stream>>>(L.N, L.NL, s->nv2, s->nv1, L.qq_ptr.p, L.ql_ptr.p, L.nqq,
+                                                         L.nql, L.nqqL, L.A.vv.p, L.A.vp.p, L.A.pv.p, L.A.pp.p,
+                                                         L.csr_ptr.p, d_vals, dir);
+  EXF_LAUNCH_CHECK();
+  return EXF_OK;
+}
+int csr_values(exf_sys *s, int lev, double *d_out) { return nb_csr(s, lev, d_out, 0); }
+int csr_set_values(exf_sys *s, int lev, const double *d_in) { return nb_csr(s, lev, const_cast<double *>(d_in), 1); }
+
+__global__ void k_d2f(const double *a, float *b, long n) {
+  long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) b[i] = (float)a[i];
+}
+int sync_fp32(exf_sys *s, int lev) {
+  SysLevel &L = s->L[lev];
+  auto cp = [&](const DBuf<double> &a, DBuf<float> &b) {
+    if (a.p && b.p) k_d2f<<<nblk(a.n, 256), 256, 0, s->stream>>>(a.p, b.p, a.n);
+  };
+  cp(L.A.vv, L.A32.vv);
+  cp(L.A.vp, L.A32.vp);
+  cp(L.A.pv, L.A32.pv);
+  cp(L.A.pp, L.A32.pp);
+  EXF_LAUNCH_CHECK();
+  return EXF_OK;
+}
+
+// ----------------------------------------------------------------- transpose
+// block (n,m) of A^T = block (m,n) of A transposed; B^T <-> B through gidx
+__global__ void k_tpos(const int *qq_ptr, const int *qq_col, int N, int *tpos) {
+  int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= N) return;
+  for (int k = qq_ptr[n]; k < qq_ptr[n + 1]; k++) {
+    int m = qq_col[k];
+    int lo = qq_ptr[m], hi = qq_ptr[m + 1];
+    while (lo < hi) {
+      int mid = (lo + hi) >> 1;
+      if (qq_col[mid] < n) lo = mid + 1;
+      else hi = mid;
+    }
+    tpos[k] = lo;
+  }
+}
+__global__ void k_tpos_l(const int *ql_ptr, const int *ql_col, int NL, int *tpos) {
+  int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= NL) return;
+  for (int k = ql_ptr[n]; k < ql_ptr[n + 1]; k++) {
+    int m = ql_col[k];
+    int lo = ql_ptr[m], hi = ql_ptr[m + 1];
+    while (lo < hi) {
+      int mid = (lo + hi) >> 1;
+      if (ql_col[mid] < n) lo = mid + 1;
+      else hi = mid;
+    }
+    tpos[k] = lo;
+  }
+}
+__global__ void k_transpose_vv(const double *src, double *dst, const int *tpos, long nqq, int d) {
+  long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nqq) return;
+  long t = tpos[k];
+  for (int a = 0; a < d; a++)
+    for (int b = 0; b < d; b++) dst[(long)(a * d + b) * nqq + k] = src[(long)(b * d + a) * nqq + t];
+}
+__global__ void k_transpose_bp(const double *vp, const double *pv, double *vp_t, double *pv_t, const int *gidx,
+                               long nql, long nqqL, int d) {
+  long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nqqL) return;
+  long g = gidx[k];
+  for (int a = 0; a < d; a++) {
+    pv_t[(long)a * nqqL + k] = vp[(long)a * nql + g];
+    vp_t[(long)a * nql + g] = pv[(long)a * nqqL + k];
+  }
+}
+__global__ void k_transpose_pp(const double *src, double *dst, const int *tpos, long n) {
+  long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < n) dst[k] = src[tpos[k]];
+}
+
+int transpose_level(exf_sys *s, int lev) {
+  SysLevel &L = s->L[lev];
+  cudaStream_t st = s->stream;
+  const int d = s->nv2;
+  DBuf<int> tpos;
+  EXF_TRY(tpos.alloc(L.nqq));
+  k_tpos<<<nblk(L.N, 128), 128, 0, st>>>(L.qq_ptr.p, L.qq_col.p, L.N, tpos.p);
+  DBuf<double> vv;
+  EXF_TRY(vv.alloc(L.A.vv.n));
+  k_transpose_vv<<<nblk(L.nqq, 256), 256, 0, st>>>(L.A.vv.p, vv.p, tpos.p, L.nqq, d);
+  EXF_CUDA(cudaMemcpyAsync(L.A.vv.p, vv.p, L.A.vv.n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+  if (s->nv1) {
+    DBuf<double> vp, pv, pp;
+    DBuf<int> tl;
+    EXF_TRY(vp.alloc(L.A.vp.n));
+    EXF_TRY(pv.alloc(L.A.pv.n));
+    EXF_TRY(pp.alloc(L.A.pp.n));
+    EXF_TRY(tl.alloc(L.nllL));
+    EXF_TRY(vp.zero(st));
+    k_transpose_bp<<<nblk(L.nqqL, 256), 256, 0, st>>>(L.A.vp.p, L.A.pv.p, vp.p, pv.p, L.gidx.p, L.nql, L.nqqL, d);
+    k_tpos_l<<<nblk(L.NL, 128), 128, 0, st>>>(L.ql_ptr.p, L.ql_col.p, L.NL, tl.p);
+    k_transpose_pp<<<nblk(L.nllL, 256), 256, 0, st>>>(L.A.pp.p, pp.p, tl.p, L.nllL);
+    EXF_CUDA(cudaMemcpyAsync(L.A.vp.p, vp.p, L.A.vp.n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    EXF_CUDA(cudaMemcpyAsync(L.A.pv.p, pv.p, L.A.pv.n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    EXF_CUDA(cudaMemcpyAsync(L.A.pp.p, pp.p, L.A.pp.n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    EXF_CUDA(cudaStreamSynchronize(st));
+  }
+  EXF_LAUNCH_CHECK();
+  EXF_CUDA(cudaStreamSynchronize(st));
+  return sync_fp32(s, lev);
+}
+
+// ------------------------------------------------------------ multigrid
+// MGStep (src/MGSolverBase.C:212-289) for value type T on the vectors VT of each level.
+// rest/crest of the reference are kept on the device when cond_corr is requested.
+template <class T>
+static T *lvx(SysLevel &L);
+template <>
+double *lvx<double>(SysLevel &L) { return L.x.p; }
+template <>
+float *lvx<float>(SysLevel &L) { return L.x32.p; }
+template <class T>
+static T *lvb(SysLevel &L);
+template <>
+double *lvb<double>(SysLevel &L) { return L.b.p; }
+template <>
+float *lvb<float>(SysLevel &L) { return L.b32.p; }
+template <class T>
+static T *lvr(SysLevel &L);
+template <>
+double *lvr<double>(SysLevel &L) { return L.r.p; }
+template <>
+float *lvr<float>(SysLevel &L) { return L.r32.p; }
+
+template <class T>
+static int mg_step(exf_sys *s, int lev, const exf_mg_params *p, bool final_resid, double *d_norm_out) {
+  SysLevel &L = s->L[lev];
+  T *x = lvx<T>(L), *b = lvb<T>(L), *r = lvr<T>(L);
+  const int top = s->nlev - 1;
+  if (lev == 0) {
+    EXF_TRY(coarse_apply<T>(s, b, x));
+    if (final_resid) EXF_TRY(spmv_resid<T>(s, 0, x, b, r, d_norm_out));
+    return EXF_OK;
+  }
+  const int mul = (p->double_below_top && lev < top) ? 2 : 1;
+  EXF_TRY(smooth<T>(s, lev, p, p->nu_pre * mul, x, b));
+  EXF_TRY(spmv_resid<T>(s, lev, x, b, r, nullptr));
+  SysLevel &C = s->L[lev - 1];
+  EXF_TRY(restrict_op<T>(s, lev - 1, r, lvb<T>(C)));
+  EXF_CUDA(cudaMemsetAsync(lvx<T>(C), 0, C.ndof * sizeof(T), s->stream));
+  for (int g = 0; g < p->gamma; g++) EXF_TRY(mg_step<T>(s, lev - 1, p, false, nullptr));
+  EXF_TRY(prolong_add<T>(s, lev, lvx<T>(C), x, p->corr_damp));
+  EXF_TRY(smooth<T>(s, lev, p, p->nu_post * mul, x, b));
+  if (final_resid) EXF_TRY(spmv_resid<T>(s, lev, x, b, r, d_norm_out));
+  return EXF_OK;
+}
+
+// FP64 cycle on the top level: returns ||b - A x||^2 in *d_relres
+int vcycle_fp64(exf_sys *s, const exf_mg_params *p, double *d_norm2) {
+  EXF_TRY(mg_step<double>(s, s->nlev - 1, p, true, d_norm2));
+  return gauge_shift(s, s->L[s->nlev - 1].x.p);
+}
+
+// mixed: r64 = b - A x (already in L.r), cast, FP32 cycle, x += e
+int vcycle_mixed(exf_sys *s, const exf_mg_params *p) {
+  SysLevel &T = s->L[s->nlev - 1];
+  EXF_TRY(cast_d2f(s->stream, T.r.p, T.b32.p, T.ndof));
+  EXF_CUDA(cudaMemsetAsync(T.x32.p, 0, T.ndof * sizeof(float), s->stream));
+  EXF_TRY(mg_step<float>(s, s->nlev - 1, p, false, nullptr));
+  EXF_TRY(add_f2d(s->stream, T.x32.p, T.x.p, T.ndof));
+  return gauge_shift(s, T.x.p);
+}
+
+}  // namespace exf
+
+using namespace exf;
+
+// ===================================================================== C ABI
+extern "C" {
+
+const char *exf_last_error(void) { return g_err; }
+const char *exf_version(void) { return "exfemus_b200 1.0 (sm_100a)"; }
+
+int exf_mesh_create(const exf_mesh_desc *desc, exf_mesh **out) {
+  if (!desc || !out || (desc->dim != 2 && desc->dim != 3) || desc->nlev < 1 || desc->nlev > 12) {
+    set_error("exf_mesh_create: bad descriptor");
+    return EXF_ERR_ARG;
+  }
+  for (int d = 0; d < desc->dim; d++)
+    if (desc->n0[d] < 1) {
+      set_error("exf_mesh_create: n0 must be >= 1");
+      return EXF_ERR_ARG;
+    }
+  EXF_CUDA(cudaSetDevice(desc->device));
+  exf_mesh *m = new exf_mesh();
+  m->dim = desc->dim;
+  m->nlev = desc->nlev;
+  m->device = desc->device;
+  for (int d = 0; d < 3; d++) m->n0[d] = desc->n0[d];
+  for (int d = 0; d < 6; d++) m->box[d] = desc->box[d];
+  int rc = build_mesh_host(m);
+  if (rc != EXF_OK) {
+    delete m;
+    return rc;
+  }
+  *out = m;
+  return EXF_OK;
+}
+
+int exf_mesh_destroy(exf_mesh *m) {
+  delete m;
+  return EXF_OK;
+}
+
+int exf_mesh_info(const exf_mesh *m, int lev, int *nnodes, int *nel, int *nvert0) {
+  if (!m || lev < 0 || lev >= m->nlev) {
+    set_error("exf_mesh_info: bad level");
+    return EXF_ERR_ARG;
+  }
+  if (nnodes) *nnodes = m->lev[lev].nnodes;
+  if (nel) *nel = m->lev[lev].nel;
+  if (nvert0) *nvert0 = m->nvert0;
+  return EXF_OK;
+}
+
+int exf_mesh_get_xyz(const exf_mesh *m, double *xyz) {
+  if (!m || !xyz) return EXF_ERR_ARG;
+  memcpy(xyz, m->xyz.data(), m->xyz.size() * sizeof(double));
+  return EXF_OK;
+}
+
+int exf_mesh_get_conn(const exf_mesh *m, int lev, int *conn, int *neigh, int *colour) {
+  if (!m || lev < 0 || lev >= m->nlev) return EXF_ERR_ARG;
+  const MeshLevel &ml = m->lev[lev];
+  if (conn) memcpy(conn, ml.conn.data(), ml.conn.size() * sizeof(int));
+  if (neigh) memcpy(neigh, ml.neigh.data(), ml.neigh.size() * sizeof(int));
+  if (colour) memcpy(colour, ml.colour.data(), ml.colour.size() * sizeof(int));
+  return EXF_OK;
+}
+
+static int sys_upload_bc(exf_sys *s) {
+  int ntd = (int)s->bc0.size();
+  EXF_CUDA(cudaMemcpyAsync(s->d_bc0.p, s->bc0.data(), ntd * sizeof(int), cudaMemcpyHostToDevice, s->stream));
+  EXF_CUDA(cudaMemcpyAsync(s->d_bc1.p, s->bc1.data(), ntd * sizeof(int), cudaMemcpyHostToDevice, s->stream));
+  EXF_TRY(update_rmask(s));
+  // pressure gauge: first pressure node flagged Dirichlet (bc0 == 0)
+  s->gauge_node = -1;
+  if (s->kind == EXF_KIND_NS) {
+    SysLevel &T = s->L[s->nlev - 1];
+    for (int i = 0; i < T.NL; i++)
+      if (s->bc0[(size_t)s->nv2 * T.N + i] == 0) {
+        s->gauge_node = i;
+        break;
+      }
+  }
+  SysLevel &L0 = s->L[0];
+  std::vector<double> gm(L0.ndof, 1.);
+  if (s->gauge_node >= 0 && s->gauge_node < L0.NL) gm[(size_t)s->nv2 * L0.N + s->gauge_node] = 0.;
+  EXF_TRY(s->gmask0.alloc(L0.ndof));
+  EXF_CUDA(cudaMemcpyAsync(s->gmask0.p, gm.data(), gm.size() * sizeof(double), cudaMemcpyHostToDevice, s->stream));
+  EXF_CUDA(cudaStreamSynchronize(s->stream));
+  s->coarse_ok = 0;
+  return EXF_OK;
+}
+
+int exf_sys_create(exf_mesh *m, int kind, exf_sys **out) {
+  if (!m || !out || (kind != EXF_KIND_T && kind != EXF_KIND_NS)) {
+    set_error("exf_sys_create: bad argument");
+    return EXF_ERR_ARG;
+  }
+  EXF_CUDA(cudaSetDevice(m->device));
+  exf_sys *s = new exf_sys();
+  s->mesh = m;
+  s->kind = kind;
+  s->dim = m->dim;
+  s->nlev = m->nlev;
+  s->nv2 = kind == EXF_KIND_T ? 1 : m->dim;
+  s->nv1 = kind == EXF_KIND_T ? 0 : 1;
+  s->nvars = s->nv2 + s->nv1;
+  if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreate(&s->ev0) != cudaSuccess || cudaEventCreate(&s->ev1) != cudaSuccess) {
+    set_error("exf_sys_create: stream/event creation failed");
+    delete s;
+    return EXF_ERR_CUDA;
+  }
+  s->L.resize(s->nlev);
+  // MGSolDA::init_dof (src/MGSolverDA.C:880-951): host copy of _node_dof for the ABI
+  s->node_dof.resize(s->nlev);
+  for (int l = 0; l < s->nlev; l++) {
+    int N = m->lev[l].nnodes, NL = l > 0 ? m->lev[l - 1].nnodes : m->nvert0;
+    std::vector<int> &nd = s->node_dof[l];
+    nd.assign((size_t)s->nvars * m->ntop, -1);
+    int cnt = 0;
+    for (int v = 0; v < s->nv2; v++)
+      for (int k = 0; k < N; k++) nd[k + (size_t)v * m->ntop] = cnt++;
+    for (int v = 0; v < s->nv1; v++)
+      for (int k = 0; k < NL; k++) nd[k + (size_t)(s->nv2 + v) * m->ntop] = cnt++;
+  }
+  int rc = build_patterns(s);
+  if (rc == EXF_OK) rc = build_colours(s);
+  if (rc == EXF_OK) rc = build_transfers(s);
+  int ntd = rc == EXF_OK ? s->L[s->nlev - 1].ndof : 0;
+  if (rc == EXF_OK) {
+    s->bc0.assign(ntd, 1);
+    s->bc1.assign(ntd, 1);
+    rc = s->d_bc0.alloc(ntd);
+    if (rc == EXF_OK) rc = s->d_bc1.alloc(ntd);
+    if (rc == EXF_OK) rc = s->xold.alloc(ntd);
+    if (rc == EXF_OK) rc = s->xold.zero(s->stream);
+    if (rc == EXF_OK) rc = s->src_qe.alloc(m->lev[s->nlev - 1].nel);
+    if (rc == EXF_OK) rc = s->src_qe.zero(s->stream);
+    if (rc == EXF_OK) rc = s->red.out.alloc(16);
+    if (rc == EXF_OK) rc = sys_upload_bc(s);
+  }
+  if (rc != EXF_OK) {
+    exf_sys_destroy(s);
+    return rc;
+  }
+  *out = s;
+  return EXF_OK;
+}
+
+int exf_sys_destroy(exf_sys *s) {
+  if (!s) return EXF_OK;
+  for (int k = 0; k < 2; k++)
+    if (s->graph[k]) cudaGraphExecDestroy(s->graph[k]);
+  if (s->stream) cudaStreamSynchronize(s->stream);
+  s->L.clear();
+  if (s->ev0) cudaEventDestroy(s->ev0);
+  if (s->ev1) cudaEventDestroy(s->ev1);
+  if (s->stream) cudaStreamDestroy(s->stream);
+  delete s;
+  return EXF_OK;
+}
+
+#define CHECK_SYS(s)                      \
+  do {                                    \
+    if (!(s)) {                           \
+      set_error("null system handle");    \
+      return EXF_ERR_ARG;                 \
+    }                                     \
+  } while (0)
+#define CHECK_LEV(s, lev)                                 \
+  do {                                                    \
+    CHECK_SYS(s);                                         \
+    if ((lev) < 0 || (lev) >= (s)->nlev) {                \
+      set_error("level %d out of range", (int)(lev));     \
+      return EXF_ERR_ARG;                                 \
+    }                                                     \
+  } while (0)
+
+int exf_sys_ndof(const exf_sys *s, int lev, int *ndof) {
+  CHECK_LEV(s, lev);
+  *ndof = s->L[lev].ndof;
+  return EXF_OK;
+}
+
+int exf_sys_get_node_dof(const exf_sys *s, int lev, int *node_dof) {
+  CHECK_LEV(s, lev);
+  memcpy(node_dof, s->node_dof[lev].data(), s->node_dof[lev].size() * sizeof(int));
+  return EXF_OK;
+}
+
+// bc_read presets: flags are functions of the node coordinates (GenBc_loop,
+// src/MGSolverDA.C:781-865; User_NS.C bc_read)
+int exf_sys_bc_preset(exf_sys *s, int preset) {
+  CHECK_SYS(s);
+  exf_mesh *m = s->mesh;
+  const int top = s->nlev - 1, dim = m->dim;
+  const SysLevel &T = s->L[top];
+  std::fill(s->bc0.begin(), s->bc0.end(), 1);
+  std::fill(s->bc1.begin(), s->bc1.end(), 1);
+  if (preset < 1 || preset > 5) {
+    set_error("unknown bc preset %d", preset);
+    return EXF_ERR_ARG;
+  }
+  for (int n = 0; n < m->ntop; n++) {
+    const int *p = &m->lat[3 * n];
+    int lo[3], hi[3], onb = 0;
+    for (int d = 0; d < 3; d++) {
+      lo[d] = d < dim && p[d] == 0;
+      hi[d] = d < dim && p[d] == m->L[d] - 1;
+      onb |= lo[d] | hi[d];
+    }
+    if (!onb) continue;  // interior nodes keep (1,1) (bc_intern_read)
+    for (int v = 0; v < s->nvars; v++) {
+      const bool quad = v < s->nv2;
+      if (!quad && n >= T.NL) continue;
+      const size_t dof = quad ? (size_t)v * T.N + n : (size_t)s->nv2 * T.N + n;
+      int b0 = 1, b1 = 0;
+      switch (preset) {
+        case EXF_BC_HEAT_DIRICHLET:
+          b0 = 0;
+          b1 = 0;
+          break;
+        case EXF_BC_CAVITY:
+          if (quad) {
+            b0 = 0;
+            b1 = (v == 0 && hi[1] && !lo[0] && !hi[0]) ? 4 : 0;
+          } else if (n == 0) {
+            b0 = 0;  // pressure gauge node
+          }
+          break;
+        case EXF_BC_CHANNEL:
+          if (quad) {
+            int wall = lo[1] || hi[1] || lo[2] || hi[2];
+            if (wall || lo[0]) {
+              b0 = 0;
+              b1 = (v == 0 && lo[0] && !wall) ? 4 : 0;
+            }
+          }
+          break;
+        case EXF_BC_BOUSS_NS:
+          if (quad) {
+            b0 = 0;
+            b1 = 0;
+          } else if (n == 0) {
+            b0 = 0;
+          }
+          break;
+        case EXF_BC_BOUSS_T:
+          if (lo[0]) {
+            b0 = 0;
+            b1 = 1;
+          } else if (hi[0]) {
+            b0 = 0;
+            b1 = 0;
+          }
+          break;
+      }
+      s->bc0[dof] = b0;
+      s->bc1[dof] = b1;
+    }
+  }
+  return sys_upload_bc(s);
+}
+
+int exf_sys_set_bc(exf_sys *s, const int *bc0, const int *bc1) {
+  CHECK_SYS(s);
+  if (!bc0 || !bc1) return EXF_ERR_ARG;
+  memcpy(s->bc0.data(), bc0, s->bc0.size() * sizeof(int));
+  memcpy(s->bc1.data(), bc1, s->bc1.size() * sizeof(int));
+  return sys_upload_bc(s);
+}
+
+int exf_sys_get_bc(const exf_sys *s, int *bc0, int *bc1) {
+  CHECK_SYS(s);
+  if (bc0) memcpy(bc0, s->bc0.data(), s->bc0.size() * sizeof(int));
+  if (bc1) memcpy(bc1, s->bc1.data(), s->bc1.size() * sizeof(int));
+  return EXF_OK;
+}
+
+int exf_sys_nnz(const exf_sys *s, int lev, long *nnz) {
+  CHECK_LEV(s, lev);
+  *nnz = s->L[lev].nnz;
+  return EXF_OK;
+}
+
+int exf_sys_get_pattern(exf_sys *s, int lev, int *rowptr, int *col) {
+  CHECK_LEV(s, lev);
+  SysLevel &L = s->L[lev];
+  if (rowptr)
+    EXF_CUDA(cudaMemcpyAsync(rowptr, L.csr_ptr.p, (L.ndof + 1) * sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+  if (col) EXF_CUDA(cudaMemcpyAsync(col, L.csr_col.p, L.nnz * sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+  EXF_CUDA(cudaStreamSynchronize(s->stream));
+  return EXF_OK;
+}
+
+// expand a node-level transfer to DOF level: row (a, node) -> columns (a, node')
+static void expand_transfer(const exf_sys *s, const Transfer &Tq, const Transfer &Tl, int nrow_q, int ncol_q,
+                            int nrow_l, int ncol_l, const double *mask, std::vector<int> &ptr,
+                            std::vector<int> &col, std::vector<double> &val) {
+  ptr.assign(1, 0);
+  col.clear();
+  val.clear();
+  int row = 0;
+  for (int a = 0; a < s->nv2; a++)
+    for (int i = 0; i < nrow_q; i++, row++) {
+      for (int q = Tq.h_ptr[i]; q < Tq.h_ptr[i + 1]; q++) {
+        col.push_back(a * ncol_q + Tq.h_col[q]);
+        val.push_back(Tq.h_val[q] * (mask ? mask[row] : 1.));
+      }
+      ptr.push_back((int)col.size());
+    }
+  if (s->nv1)
+    for (int i = 0; i < nrow_l; i++, row++) {
+      for (int q = Tl.h_ptr[i]; q < Tl.h_ptr[i + 1]; q++) {
+        col.push_back(s->nv2 * ncol_q + Tl.h_col[q]);
+        val.push_back(Tl.h_val[q] * (mask ? mask[row] : 1.));
+      }
+      ptr.push_back((int)col.size());
+    }
+}
+
+int exf_sys_get_prol(exf_sys *s, int lev, long *nnz, int *rowptr, int *col, double *val) {
+  CHECK_LEV(s, lev);
+  if (lev == 0) {
+    set_error("no prolongation into level 0");
+    return EXF_ERR_ARG;
+  }
+  const SysLevel &F = s->L[lev], &C = s->L[lev - 1];
+  std::vector<int> p, c;
+  std::vector<double> v;
+  expand_transfer(s, F.Pq, F.Pl, F.N, C.N, F.NL, C.NL, nullptr, p, c, v);
+  if (nnz) *nnz = (long)c.size();
+  if (rowptr) memcpy(rowptr, p.data(), p.size() * sizeof(int));
+  if (col) memcpy(col, c.data(), c.size() * sizeof(int));
+  if (val) memcpy(val, v.data(), v.size() * sizeof(double));
+  return EXF_OK;
+}
+
+int exf_sys_get_rest(exf_sys *s, int lev, long *nnz, int *rowptr, int *col, double *val) {
+  CHECK_LEV(s, lev);
+  if (lev == s->nlev - 1) {
+    set_error("no restriction from above the top level");
+    return EXF_ERR_ARG;
+  }
+  const SysLevel &C = s->L[lev], &F = s->L[lev + 1];
+  std::vector<double> mask(C.ndof);
+  EXF_CUDA(cudaMemcpyAsync(mask.data(), C.rmask.p, C.ndof * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+  EXF_CUDA(cudaStreamSynchronize(s->stream));
+  std::vector<int> p, c;
+  std::vector<double> v;
+  expand_transfer(s, C.Rq, C.Rl, C.N, F.N, C.NL, F.NL, mask.data(), p, c, v);
+  if (nnz) *nnz = (long)c.size();
+  if (rowptr) memcpy(rowptr, p.data(), p.size() * sizeof(int));
+  if (col) memcpy(col, c.data(), c.size() * sizeof(int));
+  if (val) memcpy(val, v.data(), v.size() * sizeof(double));
+  return EXF_OK;
+}
+
+int exf_sys_get_colours(exf_sys *s, int lev, int *ncolours, int *colour_of_item) {
+  CHECK_LEV(s, lev);
+  SysLevel &L = s->L[lev];
+  if (ncolours) *ncolours = L.ncolour;
+  if (colour_of_item)
+    EXF_CUDA(cudaMemcpyAsync(colour_of_item, L.item_colour.p, L.item_colour.n * sizeof(int), cudaMemcpyDeviceToHost,
+                             s->stream));
+  EXF_CUDA(cudaStreamSynchronize(s->stream));
+  return EXF_OK;
+}
+
+int exf_sys_couple(exf_sys *s, exf_sys *other) {
+  CHECK_SYS(s);
+  if (other && other->mesh != s->mesh) {
+    set_error("coupled systems must share the mesh");
+    return EXF_ERR_ARG;
+  }
+  s->other = other;
+  return EXF_OK;
+}
+
+static int h2d(exf_sys *s, double *d, const double *h, size_t n) {
+  if (!h) return EXF_ERR_ARG;
+  EXF_CUDA(cudaMemcpyAsync(d, h, n * sizeof(double), cudaMemcpyHostToDevice, s->stream));
+  EXF_CUDA(cudaStreamSynchronize(s->stream));
+  return EXF_OK;
+}
+static int d2h(exf_sys *s, double *h, const double *d, size_t n) {
+  if (!h) return EXF_ERR_ARG;
+  EXF_CUDA(cudaMemcpyAsync(h, d, n * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+  EXF_CUDA(cudaStreamSynchronize(s->stream));
+  return EXF_OK;
+}
+
+int exf_sys_set_xold(exf_sys *s, const double *x) {
+  CHECK_SYS(s);
+  return h2d(s, s->xold.p, x, s->xold.n);
+}
+int exf_sys_get_xold(exf_sys *s, double *x) {
+  CHECK_SYS(s);
+  return d2h(s, x, s->xold.p, s->xold.n);
+}
+int exf_sys_set_x(exf_sys *s, const double *x) {
+  CHECK_SYS(s);
+  SysLevel &T = s->L[s->nlev - 1];
+  return h2d(s, T.x.p, x, T.ndof);
+}
+int exf_sys_get_x(exf_sys *s, double *x) {
+  CHECK_SYS(s);
+  SysLevel &T = s->L[s->nlev - 1];
+  return d2h(s, x, T.x.p, T.ndof);
+}
+int exf_sys_xold_update(exf_sys *s) {
+  CHECK_SYS(s);
+  SysLevel &T = s->L[s->nlev - 1];
+  EXF_CUDA(cudaMemcpyAsync(s->xold.p, T.x.p, T.ndof * sizeof(double), cudaMemcpyDeviceToDevice, s->stream));
+  return EXF_OK;
+}
+int exf_sys_set_source(exf_sys *s, const double *qe) {
+  CHECK_SYS(s);
+  return h2d(s, s->src_qe.p, qe, s->src_qe.n);
+}
+int exf_sys_set_rhs(exf_sys *s, const double *b) {
+  CHECK_SYS(s);
+  SysLevel &T = s->L[s->nlev - 1];
+  return h2d(s, T.b.p, b, T.ndof);
+}
+int exf_sys_get_rhs(exf_sys *s, double *b) {
+  CHECK_SYS(s);
+  SysLevel &T = s->L[s->nlev - 1];
+  return d2h(s, b, T.b.p, T.ndof);
+}
+
+int exf_gen_mat_rhs(exf_sys *s, const exf_phys *ph, int lev, int mode) {
+  CHECK_LEV(s, lev);
+  if (!ph || (mode != 0 && mode != 1)) return EXF_ERR_ARG;
+  if (s->kind == EXF_KIND_NS && s->mesh->dim == 3 && s->nv2 != 3) return EXF_ERR_STATE;
+  // a natural side with nonzero NS boundary flag would need the Neumann branch
+  if (s->kind == EXF_KIND_NS) {
+    const SysLevel &T = s->L[s->nlev - 1];
+    for (size_t i = 0; i < (size_t)s->nv2 * T.N; i++)
+      if (s->bc0[i] != 0 && s->bc1[i] != 0 && s->bc1[i] != 1) {
+        set_error("NS Neumann/traction flags are not supported (dof %zu flag %d)", i, s->bc1[i]);
+        return EXF_ERR_UNSUPPORTED;
+      }
+  }
+  EXF_TRY(assemble_level(s, ph, lev, mode));
+  EXF_TRY(sync_fp32(s, lev));
+  if (lev == 0) s->coarse_ok = 0;
+  s->assembled = 1;
+  return EXF_OK;
+}
+
+int exf_assemble_all(exf_sys *s, const exf_phys *ph) {
+  CHECK_SYS(s);
+  EXF_TRY(exf_gen_mat_rhs(s, ph, s->nlev - 1, 1));
+  for (int l = 0; l < s->nlev - 1; l++) EXF_TRY(exf_gen_mat_rhs(s, ph, l, 0));
+  return EXF_OK;
+}
+
+int exf_get_matrix(exf_sys *s, int lev, double *val) {
+  CHECK_LEV(s, lev);
+  SysLevel &L = s->L[lev];
+  DBuf<double> d;
+  EXF_TRY(d.alloc(L.nnz));
+  EXF_TRY(csr_values(s, lev, d.p));
+  return d2h(s, val, d.p, L.nnz);
+}
+
+int exf_set_matrix(exf_sys *s, int lev, const double *val) {
+  CHECK_LEV(s, lev);
+  SysLevel &L = s->L[lev];
+  DBuf<double> d;
+  EXF_TRY(d.alloc(L.nnz));
+  EXF_TRY(h2d(s, d.p, val, L.nnz));
+  EXF_TRY(csr_set_values(s, lev, d.p));
+  EXF_TRY(sync_fp32(s, lev));
+  EXF_CUDA(cudaStreamSynchronize(s->stream));
+  if (lev == 0) s->coarse_ok = 0;
+  s->assembled = 1;
+  return EXF_OK;
+}
+
+int exf_sys_transpose(exf_sys *s) {
+  CHECK_SYS(s);
+  for (int l = 0; l < s->nlev; l++) EXF_TRY(transpose_level(s, l));
+  s->coarse_ok = 0;
+  s->transposed ^= 1;
+  return EXF_OK;
+}
+
+// ------------------------------------------------------------------ solve
+static int read_scalar(exf_sys *s, const double *d, double *h) {
+  EXF_CUDA(cudaMemcpyAsync(h, d, sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+  EXF_CUDA(cudaStreamSynchronize(s->stream));
+  return EXF_OK;
+}
+
+int exf_mg_solve(exf_sys *s, const exf_mg_params *p, exf_solve_stats *st) {
+  CHECK_SYS(s);
+  if (!p || !st) return EXF_ERR_ARG;
+  if (!s->assembled) {
+    set_error("exf_mg_solve before assembly");
+    return EXF_ERR_STATE;
+  }
+  if (p->gamma < 1 || p->nu_pre < 0 || p->nu_post < 0 || p->max_cycles < 0) return EXF_ERR_ARG;
+  if (p->cond_corr) {
+    set_error("conditional coarse correction is not implemented on the device");
+    return EXF_ERR_UNSUPPORTED;
+  }
+  memset(st, 0, sizeof(*st));
+  SysLevel &T = s->L[s->nlev - 1];
+  double *dnb = s->red.out.p, *dnr = s->red.out.p + 1;
+  if (!s->coarse_ok) EXF_TRY(coarse_factor(s));
+  EXF_CUDA(cudaEventRecord(s->ev0, s->stream));
+  EXF_TRY(norm2(s, T.b.p, T.ndof, dnb));
+  double bn2 = 0.;
+  EXF_TRY(read_scalar(s, dnb, &bn2));
+  double bn = sqrt(bn2);
+  st->bnorm = bn;
+  const double den = bn > 0. ? bn : 1.;
+  // initial residual
+  EXF_TRY(spmv_resid<double>(s, s->nlev - 1, T.x.p, T.b.p, T.r.p, dnr));
+  double r2 = 0.;
+  EXF_TRY(read_scalar(s, dnr, &r2));
+  double rel = sqrt(r2) / den;
+  st->rel_res = rel;
+  int rc = EXF_OK;
+  while (rel > p->eps && st->cycles < p->max_cycles) {
+    if (p->precision == EXF_PREC_MIXED) {
+      EXF_TRY(vcycle_mixed(s, p));
+      EXF_TRY(spmv_resid<double>(s, s->nlev - 1, T.x.p, T.b.p, T.r.p, dnr));
+    } else {
+      EXF_TRY(vcycle_fp64(s, p, dnr));
+    }
+    EXF_TRY(read_scalar(s, dnr, &r2));
+    rel = sqrt(r2) / den;
+    if (st->cycles < 256) st->hist[st->cycles] = rel;
+    st->cycles++;
+    st->rel_res = rel;
+    if (!std::isfinite(rel)) {
+      rc = EXF_ERR_DIVERGED;
+      set_error("multigrid diverged at cycle %d", st->cycles);
+      break;
+    }
+  }
+  if (p->precision != EXF_PREC_MIXED) {
+    // the FP64 cycle leaves the residual of the pre-gauge iterate in T.r; the residual is
+    // invariant under the pressure shift, so rel stands.
+  }
+  EXF_CUDA(cudaEventRecord(s->ev1, s->stream));
+  EXF_CUDA(cudaEventSynchronize(s->ev1));
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, s->ev0, s->ev1);
+  st->seconds = ms * 1e-3;
+  st->converged = rel <= p->eps;
+  if (rc == EXF_OK && !st->converged) {
+    set_error("not converged: rel %.3e after %d cycles", rel, st->cycles);
+    rc = EXF_ERR_NOT_CONVERGED;
+  }
+  return rc;
+}
+
+int exf_resid(exf_sys *s, int lev, const double *x, const double *b, double *r) {
+  CHECK_LEV(s, lev);
+  SysLevel &L = s->L[lev];
+  DBuf<double> dx, db, dr;
+  EXF_TRY(dx.alloc(L.ndof));
+  EXF_TRY(db.alloc(L.ndof));
+  EXF_TRY(dr.alloc(L.ndof));
+  EXF_TRY(h2d(s, dx.p, x, L.ndof));
+  if (b) EXF_TRY(h2d(s, db.p, b, L.ndof));
+  EXF_TRY(spmv_resid<double>(s, lev, dx.p, b ? db.p : nullptr, dr.p, nullptr));
+  return d2h(s, r, dr.p, L.ndof);
+}
+
+int exf_restrict(exf_sys *s, int lev, const double *r_fine, double *b_coarse) {
+  CHECK_LEV(s, lev);
+  if (lev >= s->nlev - 1) return EXF_ERR_ARG;
+  SysLevel &C = s->L[lev], &F = s->L[lev + 1];
+  DBuf<double> df, dc;
+  EXF_TRY(df.alloc(F.ndof));
+  EXF_TRY(dc.alloc(C.ndof));
+  EXF_TRY(h2d(s, df.p, r_fine, F.ndof));
+  EXF_TRY(restrict_op<double>(s, lev, df.p, dc.p));
+  return d2h(s, b_coarse, dc.p, C.ndof);
+}
+
+int exf_prolong(exf_sys *s, int lev, const double *x_coarse, double *y_fine) {
+  CHECK_LEV(s, lev);
+  if (lev == 0) return EXF_ERR_ARG;
+  SysLevel &F = s->L[lev], &C = s->L[lev - 1];
+  DBuf<double> df, dc;
+  EXF_TRY(df.alloc(F.ndof));
+  EXF_TRY(dc.alloc(C.ndof));
+  EXF_TRY(h2d(s, dc.p, x_coarse, C.ndof));
+  EXF_TRY(prolong_add<double>(s, lev, dc.p, df.p, 0.));
+  return d2h(s, y_fine, df.p, F.ndof);
+}
+
+int exf_smooth(exf_sys *s, int lev, const exf_mg_params *p, int nsweeps, double *x, const double *b) {
+  CHECK_LEV(s, lev);
+  if (!p || nsweeps < 0) return EXF_ERR_ARG;
+  SysLevel &L = s->L[lev];
+  DBuf<double> dx, db;
+  EXF_TRY(dx.alloc(L.ndof));
+  EXF_TRY(db.alloc(L.ndof));
+  EXF_TRY(h2d(s, dx.p, x, L.ndof));
+  EXF_TRY(h2d(s, db.p, b, L.ndof));
+  EXF_TRY(smooth<double>(s, lev, p, nsweeps, dx.p, db.p));
+  return d2h(s, x, dx.p, L.ndof);
+}
+
+int exf_coarse_solve(exf_sys *s, const double *b, double *x) {
+  CHECK_SYS(s);
+  SysLevel &L = s->L[0];
+  DBuf<double> dx, db;
+  EXF_TRY(dx.alloc(L.ndof));
+  EXF_TRY(db.alloc(L.ndof));
+  EXF_TRY(h2d(s, db.p, b, L.ndof));
+  EXF_TRY(coarse_apply<double>(s, db.p, dx.p));
+  return d2h(s, x, dx.p, L.ndof);
+}
+
+// device time of one operation class, averaged over reps launches (CUDA events on the
+// system stream, after one untimed warm-up)
+int exf_time_op(exf_sys *s, int what, int lev, const exf_mg_params *p, const exf_phys *ph, int reps,
+                double *avg_ms) {
+  CHECK_LEV(s, lev);
+  if (!p || !avg_ms || reps < 1) return EXF_ERR_ARG;
+  if (what == 2 && !ph) return EXF_ERR_ARG;
+  if (what != 2 && !s->assembled) return EXF_ERR_STATE;
+  if (!s->coarse_ok && what == 3) EXF_TRY(coarse_factor(s));
+  SysLevel &L = s->L[lev];
+  const bool f32 = p->precision == EXF_PREC_MIXED;
+  auto once = [&]() -> int {
+    switch (what) {
+      case 0:
+        return f32 ? spmv_resid<float>(s, lev, L.x32.p, L.b32.p, L.r32.p, nullptr)
+                   : spmv_resid<double>(s, lev, L.x.p, L.b.p, L.r.p, nullptr);
+      case 1:
+        return f32 ? smooth<float>(s, lev, p, 1, L.x32.p, L.b32.p) : smooth<double>(s, lev, p, 1, L.x.p, L.b.p);
+      case 2:
+        for (int l = s->nlev - 1; l >= 0; l--) EXF_TRY(assemble_level(s, ph, l, l == s->nlev - 1 ? 1 : 0));
+        return EXF_OK;
+      case 3: {
+        SysLevel &T = s->L[s->nlev - 1];
+        if (f32) {
+          EXF_TRY(spmv_resid<double>(s, s->nlev - 1, T.x.p, T.b.p, T.r.p, s->red.out.p + 1));
+          return vcycle_mixed(s, p);
+        }
+        return vcycle_fp64(s, p, s->red.out.p + 1);
+      }
+      default:
+        set_error("exf_time_op: unknown operation %d", what);
+        return EXF_ERR_ARG;
+    }
+  };
+  EXF_TRY(once());
+  EXF_CUDA(cudaEventRecord(s->ev0, s->stream));
+  for (int i = 0; i < reps; i++) EXF_TRY(once());
+  EXF_CUDA(cudaEventRecord(s->ev1, s->stream));
+  EXF_CUDA(cudaEventSynchronize(s->ev1));
+  float ms = 0.f;
+  EXF_CUDA(cudaEventElapsedTime(&ms, s->ev0, s->ev1));
+  *avg_ms = ms / reps;
+  if (what == 2)
+    for (int l = 0; l < s->nlev; l++) EXF_TRY(sync_fp32(s, l));
+  return EXF_OK;
+}
+
+int exf_sync(exf_sys *s) {
+  CHECK_SYS(s);
+  EXF_CUDA(cudaStreamSynchronize(s->stream));
+  return EXF_OK;
+}
+
+}  // extern "C"

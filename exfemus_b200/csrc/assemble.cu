@@ -1,0 +1,546 @@
+// assemble.cu -- element-batched Q2 (heat) and Q2-Q1 Taylor-Hood (Navier-Stokes)
+// assembly into the node-block matrix (GenMatRhs).
+//
+// One CTA per element of the current colour; elements of one colour share no node,
+// so every matrix/rhs entry they touch is written by exactly one CTA: the scatter is a
+// plain read-add-write, needs no atomics, and the summation order is fixed by the
+// colour order (results are deterministic).  Geometry, shape tables and per-Gauss-point
+// coefficients live in shared memory; each thread owns (i,j) node pairs and integrates
+// every variable block of that pair over the Gauss points.
+//
+// Restates MGSolT::GenMatRhs (template_appl/nse/SRC/MGSolverT.C:93-525) and
+// MGSolNS::GenMatRhs (template_appl/nse/SRC/MGSolverNS.C:108-717), NS_EQUATIONS==1:
+//   velocity blocks  (MGSolverNS.C:401-433), B^T (:438-452), B (:458-489),
+//   upwind f = UP*rho*0.5*(coth Pe - 1/Pe)*h/|v| (:336-339),
+//   rhs (:381-388), Dirichlet penalty Ipenalty = det_side*penalty (:531-601),
+//   heat: MGSolverT.C volume block and Dirichlet/Robin boundary blocks.
+#include <cmath>
+#include <vector>
+
+#include "exf_internal.h"
+#include "fe_topology.h"
+
+namespace exf {
+
+template <int DIM>
+struct FE {
+  static constexpr int NEN = DIM == 2 ? 9 : 27;
+  static constexpr int NVX = DIM == 2 ? 4 : 8;
+  static constexpr int NQ = DIM == 2 ? 9 : 27;
+  static constexpr int NSIDE = DIM == 2 ? 4 : 6;
+  static constexpr int NSN = DIM == 2 ? 3 : 9;
+  static constexpr int NSQ = DIM == 2 ? 3 : 9;
+};
+
+// reference-element tables, built once on the host (src/MGFE.C:195-945)
+template <int DIM>
+struct FETab {
+  double w[FE<DIM>::NQ];
+  double phi[FE<DIM>::NQ][FE<DIM>::NEN];
+  double dphi[FE<DIM>::NQ][FE<DIM>::NEN][DIM];
+  double psi[FE<DIM>::NQ][FE<DIM>::NVX];
+  double sw[FE<DIM>::NSQ];
+  double sphi[FE<DIM>::NSQ][FE<DIM>::NSN];
+  double sdphi[FE<DIM>::NSQ][FE<DIM>::NSN][DIM - 1];
+};
+
+static double lag1(int a, double x) {
+  if (a == 0) return .5 * x * (x - 1.);
+  if (a == 2) return .5 * x * (x + 1.);
+  return 1. - x * x;
+}
+static double dlag1(int a, double x) {
+  if (a == 0) return x - .5;
+  if (a == 2) return x + .5;
+  return -2. * x;
+}
+static double lin1(int a, double x) { return a == 0 ? .5 * (1. - x) : .5 * (1. + x); }
+
+template <int DIM>
+static void fill_tab(FETab<DIM> &t) {
+  const double g[3] = {-sqrt(3. / 5.), 0., sqrt(3. / 5.)};
+  const double gw[3] = {5. / 9., 8. / 9., 5. / 9.};
+  using F = FE<DIM>;
+  for (int q = 0; q < F::NQ; q++) {
+    int iq[3];
+    if (DIM == 2) {
+      iq[0] = q / 3;
+      iq[1] = q % 3;
+      iq[2] = 1;
+    } else {
+      iq[0] = q / 9;
+      iq[1] = (q / 3) % 3;
+      iq[2] = q % 3;
+    }
+    double xi[3] = {g[iq[0]], g[iq[1]], DIM == 3 ? g[iq[2]] : 0.};
+    t.w[q] = gw[iq[0]] * gw[iq[1]] * (DIM == 3 ? gw[iq[2]] : 1.);
+    for (int s = 0; s < F::NEN; s++) {
+      const int *abc = DIM == 2 ? Q9_ABC[s] : H27_ABC[s];
+      double v = 1.;
+      for (int d = 0; d < DIM; d++) v *= lag1(abc[d], xi[d]);
+      t.phi[q][s] = v;
+      for (int k = 0; k < DIM; k++) {
+        double dv = 1.;
+        for (int d = 0; d < DIM; d++) dv *= (d == k) ? dlag1(abc[d], xi[d]) : lag1(abc[d], xi[d]);
+        t.dphi[q][s][k] = dv;
+      }
+    }
+    for (int s = 0; s < F::NVX; s++) {
+      const int *abc = DIM == 2 ? Q9_ABC[s] : H27_ABC[s];
+      double v = 1.;
+      for (int d = 0; d < DIM; d++) v *= lin1(abc[d], xi[d]);
+      t.psi[q][s] = v;
+    }
+  }
+  const int sdim = DIM - 1;
+  for (int q = 0; q < F::NSQ; q++) {
+    int iq[2];
+    if (sdim == 1) {
+      iq[0] = q;
+      iq[1] = 1;
+    } else {
+      iq[0] = q / 3;
+      iq[1] = q % 3;
+    }
+    double xi[2] = {g[iq[0]], g[iq[1]]};
+    t.sw[q] = gw[iq[0]] * (sdim == 2 ? gw[iq[1]] : 1.);
+    for (int s = 0; s < F::NSN; s++) {
+      int abc[2];
+      if (sdim == 1) {
+        abc[0] = s == 0 ? 0 : (s == 1 ? 2 : 1);
+        abc[1] = 1;
+      } else {
+        abc[0] = Q9_ABC[s][0];
+        abc[1] = Q9_ABC[s][1];
+      }
+      double v = 1.;
+      for (int d = 0; d < sdim; d++) v *= lag1(abc[d], xi[d]);
+      t.sphi[q][s] = v;
+      for (int k = 0; k < sdim; k++) {
+        double dv = 1.;
+        for (int d = 0; d < sdim; d++) dv *= (d == k) ? dlag1(abc[d], xi[d]) : lag1(abc[d], xi[d]);
+        t.sdphi[q][s][k] = dv;
+      }
+    }
+  }
+}
+
+struct SideTab {
+  int nodes[6][9];
+  int dir[6][3];
+};
+
+template <int DIM>
+struct AsmArgs {
+  const FETab<DIM> *tab;
+  SideTab side;
+  const int *elist;      // elements of this colour
+  int nel_c;
+  const int *conn, *neigh;
+  const double *xyz;     // [dim][ntop]
+  int ntop;
+  int N, NL, Ntop;       // level Q2 nodes, level Q1 nodes, top Q2 nodes
+  const int *bc0, *bc1;  // top-level flags
+  const double *xold;    // own x_old (top)
+  const double *vel;     // coupled NS x_old (top) for T, or null
+  int vel_Ntop;
+  const double *temp;    // coupled T x_old (top) for NS buoyancy, or null
+  const double *qe;      // per top element source (T), or null
+  const int *qq_ptr, *ql_ptr;
+  const uint8_t *pos_qq, *pos_ql;
+  long nqq, nql, nqqL;
+  double *vv, *vp, *pv, *pp;
+  double *rhs;           // level rhs or null (mode 0)
+  exf_phys ph;
+  int kind;
+};
+
+template <int DIM>
+__device__ double jac_sur(const FETab<DIM> *t, int q, const double (*xb)[9]) {
+  if (DIM == 2) {
+    double dx = 0, dy = 0;
+    for (int s = 0; s < 3; s++) {
+      dx += xb[0][s] * t->sdphi[q][s][0];
+      dy += xb[1][s] * t->sdphi[q][s][0];
+    }
+    return sqrt(dx * dx + dy * dy);
+  } else {
+    double a[3] = {0, 0, 0}, b[3] = {0, 0, 0};
+    for (int s = 0; s < 9; s++)
+      for (int d = 0; d < 3; d++) {
+        a[d] += xb[d][s] * t->sdphi[q][s][0];
+        b[d] += xb[d][s] * t->sdphi[q][s][DIM - 2];
+      }
+    double c0 = a[1] * b[2] - a[2] * b[1], c1 = a[2] * b[0] - a[0] * b[2], c2 = a[0] * b[1] - a[1] * b[0];
+    return sqrt(c0 * c0 + c1 * c1 + c2 * c2);
+  }
+}
+
+template <int DIM, int NT>
+__global__ void __launch_bounds__(NT) k_assemble(AsmArgs<DIM> A, int mode) {
+  using F = FE<DIM>;
+  constexpr int NEN = F::NEN, NVX = F::NVX, NQ = F::NQ;
+  const int tid = threadIdx.x;
+  const int e = A.elist[blockIdx.x];
+  const bool ns = A.kind == EXF_KIND_NS;
+  const int nv2 = ns ? DIM : 1;
+
+  __shared__ int s_conn[NEN];
+  __shared__ double s_xx[DIM][NEN];
+  __shared__ int s_bcv[DIM + 1][NEN];
+  __shared__ int s_bcb[DIM + 1][NEN];
+  __shared__ double s_uold[DIM + 1][NEN];
+  __shared__ double s_vold[DIM][NEN];
+  __shared__ double s_told[NEN];
+  __shared__ double s_phi[NQ][NEN];
+  __shared__ double s_dphi[NQ][NEN][DIM];
+  __shared__ double s_psi[NQ][NVX];
+  __shared__ double s_ij[NQ][DIM * DIM];
+  __shared__ double s_JxW[NQ];
+  __shared__ double s_cM[NQ];          // JxW*rho*inv_dt (NS) or JxW*rhocp*inv_dt (T)
+  __shared__ double s_cA[NQ][DIM];     // JxW*rho*v_k
+  __shared__ double s_cL[NQ][DIM];     // JxW*rho*(nu + f_k v_k^2)
+  __shared__ double s_cT[NQ][DIM * DIM];  // JxW*rho*(nu + f_a v_a v_b)
+  __shared__ double s_cR[NQ][DIM];     // rhs coefficient per component
+  __shared__ double s_h[DIM];
+
+  const FETab<DIM> *t = A.tab;
+  // ---- element data (get_el_dof_bc, get_el_sol)
+  for (int k = tid; k < NEN; k += NT) {
+    int nd = A.conn[(long)e * NEN + k];
+    s_conn[k] = nd;
+    for (int d = 0; d < DIM; d++) s_xx[d][k] = A.xyz[nd + (long)d * A.ntop];
+    for (int v = 0; v < nv2; v++) {
+      long td = (long)v * A.Ntop + nd;
+      s_bcv[v][k] = A.bc0[td];
+      s_bcb[v][k] = A.bc1[td];
+      s_uold[v][k] = A.xold ? A.xold[td] : 0.;
+    }
+    if (ns && k < NVX) {
+      long td = (long)nv2 * A.Ntop + nd;
+      s_bcv[DIM][k] = A.bc0[td];
+      s_bcb[DIM][k] = A.bc1[td];
+      s_uold[DIM][k] = A.xold ? A.xold[td] : 0.;
+    }
+    for (int d = 0; d < DIM; d++) {
+      if (ns) s_vold[d][k] = s_uold[d][k];
+      else s_vold[d][k] = A.vel ? A.vel[nd + (long)d * A.vel_Ntop] : 0.;
+    }
+    if (ns) s_told[k] = A.temp ? A.temp[nd] : 0.;
+    else s_told[k] = s_uold[0][k];
+  }
+  for (int i = tid; i < NQ * NEN; i += NT) (&s_phi[0][0])[i] = (&t->phi[0][0])[i];
+  for (int i = tid; i < NQ * NVX; i += NT) (&s_psi[0][0])[i] = (&t->psi[0][0])[i];
+  __syncthreads();
+  if (tid < DIM) {
+    const int v2 = DIM == 2 ? 2 : 6, v3 = DIM == 2 ? 3 : 7;
+    double h = fabs(s_xx[tid][v2] - s_xx[tid][0]);
+    double h1 = fabs(s_xx[tid][v3] - s_xx[tid][1]);
+    s_h[tid] = h < h1 ? h1 : h;
+  }
+  __syncthreads();
+  // ---- per Gauss point: Jacobian (src/MGFE.C:1066-1170), fields, coefficients
+  const exf_phys &ph = A.ph;
+  const double diff_t = ph.inv_prdl * ph.inv_re;
+  const double q_e = (!ns && A.qe) ? A.qe[e] : 0.;
+  for (int q = tid; q < NQ; q += NT) {
+    double J[DIM][DIM];
+    for (int a = 0; a < DIM; a++)
+      for (int b = 0; b < DIM; b++) {
+        double sum = 0.;
+        for (int s = 0; s < NEN; s++) sum += s_xx[a][s] * t->dphi[q][s][b];
+        J[a][b] = sum;
+      }
+    double det, inv[DIM][DIM];  // inv[b][a] = dxi_b/dx_a
+    if (DIM == 2) {
+      det = J[0][0] * J[1][1] - J[1][0] * J[0][1];
+      double id = 1. / det;
+      inv[0][0] = J[1][1] * id;
+      inv[0][1] = -J[0][1] * id;
+      inv[1][0] = -J[1][0] * id;
+      inv[1][1] = J[0][0] * id;
+    } else {
+      const int o = DIM - 1;  // keeps indices in range for DIM==2 instantiations
+      det = J[0][0] * (J[1][1] * J[o][o] - J[1][o] * J[o][1]) - J[0][1] * (J[1][0] * J[o][o] - J[1][o] * J[o][0]) +
+            J[0][o] * (J[1][0] * J[o][1] - J[1][1] * J[o][0]);
+      double id = 1. / det;
+      inv[0][0] = (J[1][1] * J[o][o] - J[1][o] * J[o][1]) * id;
+      inv[0][1] = (J[0][o] * J[o][1] - J[0][1] * J[o][o]) * id;
+      inv[0][o] = (J[0][1] * J[1][o] - J[0][o] * J[1][1]) * id;
+      inv[1][0] = (J[1][o] * J[o][0] - J[1][0] * J[o][o]) * id;
+      inv[1][1] = (J[0][0] * J[o][o] - J[0][o] * J[o][0]) * id;
+      inv[1][o] = (J[0][o] * J[1][0] - J[0][0] * J[1][o]) * id;
+      inv[o][0] = (J[1][0] * J[o][1] - J[1][1] * J[o][0]) * id;
+      inv[o][1] = (J[0][1] * J[o][0] - J[0][0] * J[o][1]) * id;
+      inv[o][o] = (J[0][0] * J[1][1] - J[0][1] * J[1][0]) * id;
+    }
+    for (int i = 0; i < DIM; i++)
+      for (int j = 0; j < DIM; j++) s_ij[q][j + i * DIM] = inv[j][i];
+    double JxW = det * t->w[q];
+    s_JxW[q] = JxW;
+    double vg[DIM], mod = 1e-20, tg = 0.;
+    for (int d = 0; d < DIM; d++) {
+      double sum = 0.;
+      for (int k = 0; k < NEN; k++) sum += s_phi[q][k] * s_vold[d][k];
+      vg[d] = sum;
+      mod += sum * sum;
+    }
+    for (int k = 0; k < NEN; k++) tg += s_phi[q][k] * s_told[k];
+    mod = sqrt(mod);
+    double f[DIM];
+    if (ns) {
+      for (int d = 0; d < DIM; d++) {
+        double pe = 0.5 * mod * s_h[d] / ph.inv_re;
+        f[d] = ph.upwind_ns * ph.rho * 0.5 * (1. / tanh(pe) - 1. / pe) * s_h[d] / mod;
+      }
+      s_cM[q] = JxW * ph.rho * ph.inv_dt;
+      for (int a = 0; a < DIM; a++) {
+        s_cA[q][a] = JxW * ph.rho * vg[a];
+        s_cL[q][a] = JxW * ph.rho * (ph.inv_re + f[a] * vg[a] * vg[a]);
+        for (int b = 0; b < DIM; b++) s_cT[q][a * DIM + b] = JxW * ph.rho * (ph.inv_re + f[a] * vg[a] * vg[b]);
+        s_cR[q][a] = JxW * (ph.rho * vg[a] * ph.inv_dt + ph.rho * ph.ifr * ph.dirg[a] + ph.buoy * tg * ph.dirg[a]);
+      }
+    } else {
+      for (int d = 0; d < DIM; d++) {
+        if (A.vel) {
+          double pe = 0.5 * mod * s_h[d] / diff_t;
+          f[d] = ph.upwind_t * ph.rhocp * 0.5 * (1. / tanh(pe) - 1. / pe) * s_h[d] / mod;
+        } else {
+          f[d] = 0.;
+        }
+      }
+      s_cM[q] = JxW * ph.rhocp * ph.inv_dt;
+      for (int a = 0; a < DIM; a++) {
+        s_cA[q][a] = JxW * ph.rhocp * vg[a];
+        s_cL[q][a] = JxW * (diff_t + f[a] * vg[a] * vg[a]);
+      }
+      s_cR[q][0] = JxW * (ph.rhocp * tg * ph.inv_dt + q_e);
+    }
+  }
+  __syncthreads();
+  // global shape derivatives (get_dphi_gl_g, src/MGFE.C:1496-1520)
+  for (int p = tid; p < NQ * NEN; p += NT) {
+    int q = p / NEN, s = p % NEN;
+    for (int i = 0; i < DIM; i++) {
+      double sum = 0.;
+      for (int j = 0; j < DIM; j++) sum += s_ij[q][j + i * DIM] * t->dphi[q][s][j];
+      s_dphi[q][s][i] = sum;
+    }
+  }
+  __syncthreads();
+
+  // ---- volume integrals, node pairs (i,j)
+  const int *qq_ptr = A.qq_ptr;
+  for (int p = tid; p < NEN * NEN; p += NT) {
+    const int i = p / NEN, j = p % NEN;
+    const int ni = s_conn[i];
+    const long blk = qq_ptr[ni] + A.pos_qq[((long)e * NEN + i) * NEN + j];
+    if (!ns) {
+      double K = 0.;
+#pragma unroll 3
+      for (int q = 0; q < NQ; q++) {
+        const double pi = s_phi[q][i], pj = s_phi[q][j];
+        double adv = 0., lap = 0.;
+        for (int k = 0; k < DIM; k++) {
+          const double gj = s_dphi[q][j][k];
+          adv += s_cA[q][k] * gj;
+          lap += s_cL[q][k] * gj * s_dphi[q][i][k];
+        }
+        K += pi * (s_cM[q] * pj + adv) + lap;
+      }
+      A.vv[blk] += s_bcv[0][i] * K;
+    } else {
+      double M = 0., T[DIM * DIM];
+      for (int k = 0; k < DIM * DIM; k++) T[k] = 0.;
+#pragma unroll 3
+      for (int q = 0; q < NQ; q++) {
+        const double pi = s_phi[q][i], pj = s_phi[q][j];
+        double gj[DIM], gi[DIM], adv = 0., lap = 0.;
+        for (int k = 0; k < DIM; k++) {
+          gj[k] = s_dphi[q][j][k];
+          gi[k] = s_dphi[q][i][k];
+          adv += s_cA[q][k] * gj[k];
+          lap += s_cL[q][k] * gj[k] * gi[k];
+        }
+        M += pi * (s_cM[q] * pj + adv) + lap;
+        for (int a = 0; a < DIM; a++) {
+          const double ga = s_dphi[q][j][a];
+          for (int b = 0; b < DIM; b++) T[a * DIM + b] += s_cT[q][a * DIM + b] * ga * gi[b];
+        }
+      }
+      for (int a = 0; a < DIM; a++) {
+        const double bcv = s_bcv[a][i];
+        for (int b = 0; b < DIM; b++) {
+          double v = T[a * DIM + b] + (a == b ? M : 0.);
+          A.vv[(long)(a * DIM + b) * A.nqq + blk] += bcv * v;
+        }
+      }
+    }
+  }
+  if (ns) {
+    // E_b(iv, j) = sum_q JxW psi_iv d_b phi_j : B^T (velocity rows) and B (pressure rows)
+    for (int p = tid; p < NVX * NEN; p += NT) {
+      const int iv = p / NEN, j = p % NEN;
+      double E[DIM];
+      for (int b = 0; b < DIM; b++) E[b] = 0.;
+      for (int q = 0; q < NQ; q++) {
+        const double w = s_JxW[q] * s_psi[q][iv];
+        for (int b = 0; b < DIM; b++) E[b] += w * s_dphi[q][j][b];
+      }
+      // B^T: row (a, node j), column pressure vertex iv
+      const int nj = s_conn[j];
+      const long kq = A.ql_ptr[nj] + A.pos_ql[((long)e * NEN + j) * NVX + iv];
+      for (int a = 0; a < DIM; a++) A.vp[(long)a * A.nql + kq] += s_bcv[a][j] * (-E[a]);
+      // B: pressure row iv, column (b, node j)
+      const int niv = s_conn[iv];
+      const long kp = qq_ptr[niv] + A.pos_qq[((long)e * NEN + iv) * NEN + j];
+      for (int b = 0; b < DIM; b++) A.pv[(long)b * A.nqqL + kp] += ph.rho * E[b];
+    }
+  }
+  // rhs
+  if (mode == 1) {
+    for (int p = tid; p < nv2 * NEN; p += NT) {
+      const int a = p / NEN, i = p % NEN;
+      double F = 0.;
+      for (int q = 0; q < NQ; q++) F += s_phi[q][i] * s_cR[q][a];
+      A.rhs[(long)a * A.N + s_conn[i]] += s_bcv[a][i] * F;
+    }
+  }
+  __syncthreads();
+
+  // ---- boundary sides: Dirichlet penalty (and Robin for T), one side at a time
+  for (int sd = 0; sd < F::NSIDE; sd++) {
+    if (A.neigh[(long)e * F::NSIDE + sd] != -1) continue;
+    const int *sur = A.side.nodes[sd];
+    const int last = sur[F::NSN - 1];
+    double xb[DIM][9];
+    for (int k = 0; k < F::NSN; k++)
+      for (int d = 0; d < DIM; d++) xb[d][k] = s_xx[d][sur[k]];
+    const double det = jac_sur<DIM>(t, F::NSQ - 1, xb);
+    const double ipen = det * ph.penalty;
+    double nrm[3];
+    for (int d = 0; d < 3; d++) nrm[d] = (double)A.side.dir[sd][d];
+    for (int p = tid; p < nv2 * F::NSN; p += NT) {
+      const int a = p / F::NSN, k = p % F::NSN;
+      const int lv = sur[k];
+      const int nlv = s_conn[lv];
+      const long blk = qq_ptr[nlv] + A.pos_qq[((long)e * NEN + lv) * NEN + lv];
+      if (s_bcv[a][last] == 0) {
+        if (!ns) {
+          const int bc_beta = s_bcb[0][last] % 2;
+          A.vv[blk] += ipen;
+          if (mode == 1) A.rhs[nlv] += bc_beta * ipen * s_uold[0][lv];
+        } else {
+          const int bs = s_bcb[a][lv];
+          const int bc_rhs = (bs & 4) >> 2, bc_tg = (bs & 2) >> 1, bc_n = bs % 2;
+          double vdn = 0.;
+          for (int d = 0; d < DIM; d++) vdn += nrm[d] * s_uold[d][lv];
+          A.vv[(long)(a * DIM + a) * A.nqq + blk] +=
+              ((1 - bc_n) * (1 - bc_tg) + bc_tg) * ipen + ipen * nrm[a] * nrm[a] * (bc_n - bc_tg);
+          for (int b = a + 1; b < DIM; b++)
+            A.vv[(long)(a * DIM + b) * A.nqq + blk] += ipen * nrm[b] * nrm[a] * (bc_n - bc_tg);
+          if (mode == 1)
+            A.rhs[(long)a * A.N + nlv] +=
+                bc_rhs * ipen *
+                ((1 - bc_n) * (1 - bc_tg) * s_uold[a][lv] + bc_n * vdn * nrm[a] +
+                 bc_tg * (s_uold[a][lv] - vdn * nrm[a]));
+        }
+      } else if (!ns && s_bcb[0][last] != 0) {
+        // Robin: k dT/dn = -h T; the constant terms of the reference are zero
+        const int bs = s_bcb[0][lv];
+        const int bc_alpha = (bs & 2) >> 1;
+        const double bv = s_bcv[0][lv];
+        for (int j = 0; j < F::NSN; j++) {
+          double v = 0.;
+          for (int q = 0; q < F::NSQ; q++) v += jac_sur<DIM>(t, q, xb) * t->sw[q] * t->sphi[q][k] * t->sphi[q][j];
+          const long bj = qq_ptr[nlv] + A.pos_qq[((long)e * NEN + lv) * NEN + sur[j]];
+          A.vv[bj] += bv * bc_alpha * diff_t * v;
+        }
+      }
+    }
+    __syncthreads();
+  }
+}
+
+template <int DIM>
+static int assemble_dim(exf_sys *s, const exf_phys *ph, int lev, int mode) {
+  static FETab<DIM> *d_tab = nullptr;
+  static int tab_dev = -1;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (!d_tab || tab_dev != dev) {
+    FETab<DIM> h;
+    fill_tab<DIM>(h);
+    EXF_CUDA(cudaMalloc(&d_tab, sizeof(FETab<DIM>)));
+    EXF_CUDA(cudaMemcpy(d_tab, &h, sizeof(FETab<DIM>), cudaMemcpyHostToDevice));
+    tab_dev = dev;
+  }
+  exf_mesh *m = s->mesh;
+  SysLevel &L = s->L[lev];
+  const MeshLevel &ml = m->lev[lev];
+  const int top = s->nlev - 1;
+  cudaStream_t st = s->stream;
+  AsmArgs<DIM> a;
+  a.tab = d_tab;
+  for (int sd = 0; sd < FE<DIM>::NSIDE; sd++) {
+    for (int k = 0; k < FE<DIM>::NSN; k++) a.side.nodes[sd][k] = DIM == 2 ? Q9_SIDE[sd][k] : H27_FACE[sd][k];
+    for (int d = 0; d < 3; d++) a.side.dir[sd][d] = DIM == 2 ? Q9_SIDE_DIR[sd][d] : H27_FACE_DIR[sd][d];
+  }
+  a.conn = ml.d_conn.p;
+  a.neigh = ml.d_neigh.p;
+  a.xyz = m->d_xyz.p;
+  a.ntop = m->ntop;
+  a.N = L.N;
+  a.NL = L.NL;
+  a.Ntop = s->L[top].N;
+  a.bc0 = s->d_bc0.p;
+  a.bc1 = s->d_bc1.p;
+  a.xold = s->xold.p;
+  a.vel = nullptr;
+  a.temp = nullptr;
+  a.vel_Ntop = s->L[top].N;
+  if (s->other && s->kind == EXF_KIND_T && s->other->kind == EXF_KIND_NS) {
+    a.vel = s->other->xold.p;
+    a.vel_Ntop = s->other->L[top].N;
+  }
+  if (s->other && s->kind == EXF_KIND_NS && s->other->kind == EXF_KIND_T) a.temp = s->other->xold.p;
+  a.qe = (lev == top && s->kind == EXF_KIND_T) ? s->src_qe.p : nullptr;
+  a.qq_ptr = L.qq_ptr.p;
+  a.ql_ptr = L.ql_ptr.p;
+  a.pos_qq = L.pos_qq.p;
+  a.pos_ql = L.pos_ql.p;
+  a.nqq = L.nqq;
+  a.nql = L.nql;
+  a.nqqL = L.nqqL;
+  a.vv = L.A.vv.p;
+  a.vp = L.A.vp.p;
+  a.pv = L.A.pv.p;
+  a.pp = L.A.pp.p;
+  a.rhs = mode == 1 ? L.b.p : nullptr;
+  a.ph = *ph;
+  a.kind = s->kind;
+  EXF_TRY(L.A.vv.zero(st));
+  if (s->nv1) {
+    EXF_TRY(L.A.vp.zero(st));
+    EXF_TRY(L.A.pv.zero(st));
+    EXF_TRY(L.A.pp.zero(st));
+  }
+  if (mode == 1) EXF_TRY(L.b.zero(st));
+  constexpr int NT = DIM == 2 ? 128 : 256;
+  for (int c = 0; c < 8; c++) {
+    int n = ml.ecol_off[c + 1] - ml.ecol_off[c];
+    if (n == 0) continue;
+    a.elist = ml.d_elist.p + ml.ecol_off[c];
+    a.nel_c = n;
+    k_assemble<DIM, NT><<<n, NT, 0, st>>>(a, mode);
+    EXF_LAUNCH_CHECK();
+  }
+  return EXF_OK;
+}
+
+int assemble_level(exf_sys *s, const exf_phys *ph, int lev, int mode) {
+  if (s->mesh->dim == 2) return assemble_dim<2>(s, ph, lev, mode);
+  return assemble_dim<3>(s, ph, lev, mode);
+}
+
+}  // namespace exf

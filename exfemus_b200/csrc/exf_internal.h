@@ -1,0 +1,225 @@
+// exf_internal.h -- internal data structures of the B200 assembly + multigrid library.
+//
+// HBM layout per level (one equation system):
+//   node pattern   qq_ptr/qq_col (Q2 node -> sorted Q2 neighbour nodes),
+//                  ql_ptr/ql_col (Q2 node -> sorted Q1 neighbour nodes)
+//   values         node-block planar arrays ("NB" layout): for d velocity components
+//                  vv[(a*d+b)*nqq + k]  velocity row comp a, column comp b, block k
+//                  vp[a*nql + k]        velocity row comp a, pressure column (B^T)
+//                  pv[b*nqqL + k]       pressure row, velocity column comp b (B)
+//                  pp[k]                pressure-pressure (k < ql_ptr[NL])
+//                  one index per block instead of one per entry; planes make every
+//                  warp load contiguous.  The reference's DOF-level CSR (all four
+//                  blocks qq/ql/lq/ll, sorted columns) is produced from it on demand.
+//   vectors        DOF order of MGSolDA::init_dof: component-major Q2 variables, then
+//                  the Q1 variable on the first NL nodes.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/exfemus_b200.h"
+
+namespace exf {
+
+void set_error(const char *fmt, ...);
+
+#define EXF_CUDA(call)                                                                 \
+  do {                                                                                 \
+    cudaError_t e__ = (call);                                                          \
+    if (e__ != cudaSuccess) {                                                          \
+      exf::set_error("%s:%d %s: %s", __FILE__, __LINE__, #call, cudaGetErrorString(e__)); \
+      return EXF_ERR_CUDA;                                                             \
+    }                                                                                  \
+  } while (0)
+
+#define EXF_LAUNCH_CHECK()                                                             \
+  do {                                                                                 \
+    cudaError_t e__ = cudaGetLastError();                                              \
+    if (e__ != cudaSuccess) {                                                          \
+      exf::set_error("%s:%d launch: %s", __FILE__, __LINE__, cudaGetErrorString(e__)); \
+      return EXF_ERR_CUDA;                                                             \
+    }                                                                                  \
+  } while (0)
+
+#define EXF_TRY(expr)          \
+  do {                         \
+    int rc__ = (expr);         \
+    if (rc__ != EXF_OK) return rc__; \
+  } while (0)
+
+// device buffer with RAII
+template <class T>
+struct DBuf {
+  T *p = nullptr;
+  size_t n = 0;
+  DBuf() = default;
+  DBuf(const DBuf &) = delete;
+  DBuf &operator=(const DBuf &) = delete;
+  DBuf(DBuf &&o) noexcept : p(o.p), n(o.n) {
+    o.p = nullptr;
+    o.n = 0;
+  }
+  DBuf &operator=(DBuf &&o) noexcept {
+    if (this != &o) {
+      release();
+      p = o.p;
+      n = o.n;
+      o.p = nullptr;
+      o.n = 0;
+    }
+    return *this;
+  }
+  ~DBuf() { release(); }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  int alloc(size_t count) {
+    release();
+    if (count == 0) count = 1;
+    if (cudaMalloc(&p, count * sizeof(T)) != cudaSuccess) {
+      cudaGetLastError();
+      set_error("cudaMalloc of %zu bytes failed", count * sizeof(T));
+      return EXF_ERR_NOMEM;
+    }
+    n = count;
+    return EXF_OK;
+  }
+  int zero(cudaStream_t s) { return cudaMemsetAsync(p, 0, n * sizeof(T), s) == cudaSuccess ? EXF_OK : EXF_ERR_CUDA; }
+};
+
+struct MeshLevel {
+  int nnodes = 0, nel = 0, ne[3] = {1, 1, 1};
+  std::vector<int> conn, neigh, colour;   // host copies
+  DBuf<int> d_conn, d_neigh;
+  DBuf<int> d_elist;                      // elements sorted by colour
+  int ecol_off[9] = {0};
+};
+
+}  // namespace exf
+
+struct exf_mesh {
+  int dim = 2, nlev = 1, nen = 9, nvx = 4, nsides = 4, nsn = 3;
+  int n0[3] = {1, 1, 1}, L[3] = {1, 1, 1};
+  int ntop = 0, nvert0 = 0;
+  int device = 0;
+  double box[6] = {0, 1, 0, 1, 0, 1};
+  std::vector<int> lat;       // [ntop*3]
+  std::vector<double> xyz;    // [dim*ntop]
+  std::vector<exf::MeshLevel> lev;
+  exf::DBuf<double> d_xyz;
+  exf::DBuf<int> d_lat;
+};
+
+namespace exf {
+
+template <class T>
+struct LevelVals {
+  DBuf<T> vv, vp, pv, pp;
+};
+
+// node-level transfer operator (CSR) applied per variable component
+struct Transfer {
+  int nrow = 0;
+  DBuf<int> ptr, col;
+  DBuf<double> val;
+  DBuf<float> val32;
+  std::vector<int> h_ptr, h_col;
+  std::vector<double> h_val;
+};
+
+struct SysLevel {
+  int N = 0, NL = 0, ndof = 0, nel = 0;
+  long nqq = 0, nql = 0, nqqL = 0, nllL = 0, nnz = 0;
+  DBuf<int> qq_ptr, qq_col, ql_ptr, ql_col;
+  DBuf<int> diag_pos;    // [N] absolute block index of n in qq(n)
+  DBuf<int> gidx;        // [nqqL] for pressure-row block k: index into vp of G(., n_k; m)
+  DBuf<uint8_t> pos_qq;  // [nel*nen*nen]
+  DBuf<uint8_t> pos_ql;  // [nel*nen*nvx]
+  DBuf<int> csr_ptr, csr_col;  // DOF-level CSR (built on device)
+  // smoother colouring: items = DOFs (T) or pressure nodes (NS), grouped by colour
+  int ncolour = 0;
+  std::vector<int> col_off;    // [ncolour+1]
+  DBuf<int> col_items;
+  DBuf<int> item_colour;
+  LevelVals<double> A;
+  LevelVals<float> A32;
+  // transfers: Pq/Pl from level-1 to this level (fine rows), Rq/Rl from this level+1
+  Transfer Pq, Pl, Rq, Rl;
+  DBuf<double> rmask;    // [ndof] restriction row mask (bc0 % 2 of the top DOF)
+  // vectors
+  DBuf<double> x, b, r, dx;
+  DBuf<float> x32, b32, r32, dx32;
+  DBuf<double> vanka_dp;  // per pressure node correction scratch
+  DBuf<float> vanka_dp32;
+};
+
+struct Partials {
+  DBuf<double> part;   // per-block partial sums
+  DBuf<double> out;    // reduced scalars
+  int nblk = 0;
+};
+
+}  // namespace exf
+
+struct exf_sys {
+  exf_mesh *mesh = nullptr;
+  int kind = 0, nv2 = 1, nv1 = 0, nvars = 1, nlev = 1, dim = 2;
+  cudaStream_t stream = nullptr;
+  std::vector<std::vector<int>> node_dof;   // host, [nvars*ntop] per level
+  std::vector<int> bc0, bc1;                // top-level DOFs (host)
+  exf::DBuf<int> d_bc0, d_bc1;
+  std::vector<exf::SysLevel> L;
+  exf::DBuf<double> xold, src_qe, rhs_top;  // top-level fields
+  exf::DBuf<double> coarse_inv;             // dense inverse of the (gauged) coarsest matrix
+  exf::DBuf<double> coarse_work;            // Gauss-Jordan work [n x 2n]
+  exf::DBuf<int> coarse_piv;
+  exf::DBuf<double> gmask0;                 // coarse gauge mask (0 at gauge DOFs)
+  int coarse_ok = 0;
+  int gauge_node = -1;                      // top-level pressure gauge node (-1 none)
+  int assembled = 0;
+  int transposed = 0;
+  exf_sys *other = nullptr;                 // coupled system (T <- NS velocity, NS <- T)
+  exf::Partials red;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  // captured V-cycle graphs (per precision)
+  cudaGraphExec_t graph[2] = {nullptr, nullptr};
+  unsigned long long graph_key[2] = {0, 0};
+};
+
+namespace exf {
+// kernels / launchers implemented in the .cu files
+int build_mesh_host(exf_mesh *m);
+int build_patterns(exf_sys *s);
+int build_transfers(exf_sys *s);
+int update_rmask(exf_sys *s);
+int build_colours(exf_sys *s);
+int assemble_level(exf_sys *s, const exf_phys *ph, int lev, int mode);
+int sync_fp32(exf_sys *s, int lev);
+int csr_values(exf_sys *s, int lev, double *d_out);         // NB -> CSR order (device)
+int csr_set_values(exf_sys *s, int lev, const double *d_in);
+int coarse_factor(exf_sys *s);
+int transpose_level(exf_sys *s, int lev);
+
+// solver primitives (templated on value type; launched on s->stream)
+template <class T>
+int spmv_resid(exf_sys *s, int lev, const T *x, const T *b, T *r, double *d_norm2);
+template <class T>
+int restrict_op(exf_sys *s, int lev_c, const T *r_f, T *b_c);
+template <class T>
+int prolong_add(exf_sys *s, int lev_f, const T *x_c, T *x_f, double damp);
+template <class T>
+int smooth(exf_sys *s, int lev, const exf_mg_params *p, int nsweeps, T *x, const T *b);
+template <class T>
+int coarse_apply(exf_sys *s, const T *b, T *x);
+int gauge_shift(exf_sys *s, double *x);
+int cast_d2f(cudaStream_t st, const double *a, float *b, long n);
+int add_f2d(cudaStream_t st, const float *a, double *b, long n);
+int norm2(exf_sys *s, const double *v, long n, double *d_out);
+int vcycle_fp64(exf_sys *s, const exf_mg_params *p, double *d_relres);
+int vcycle_mixed(exf_sys *s, const exf_mg_params *p);
+}  // namespace exf

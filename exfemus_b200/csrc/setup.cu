@@ -1,0 +1,512 @@
+// setup.cu -- one-time integer work on the device: node patterns, the DOF-level CSR
+// pattern, element->slot maps, smoother colouring, and the transfer operators.
+//
+// Reference: the sparsity pattern is gencase's compute_mat_qq (union of the nodes of
+// every element containing a node, USER_APPL/gencase/src/MGGenCase.C:1781-1862) read by
+// MGSolDA::ReadMatrix (src/MGSolverDA.C:1785-2009) into LASPACK rows, which LASPACK
+// sorts before the first product (contrib/laspack/operats.c:813).  Here the rows are
+// built sorted; every result is independent of thread scheduling.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+
+#include "exf_internal.h"
+#include "fe_topology.h"
+
+namespace exf {
+
+// ------------------------------------------------------------------ exclusive scan
+// in-place exclusive scan of n ints, returns total in *total (host)
+__global__ void k_scan_tiles(int *a, long n, int *tile_sum) {
+  __shared__ int s[1024];
+  long i = (long)blockIdx.x * 1024 + threadIdx.x;
+  int v = i < n ? a[i] : 0;
+  s[threadIdx.x] = v;
+  __syncthreads();
+  for (int off = 1; off < 1024; off <<= 1) {
+    int t = threadIdx.x >= off ? s[threadIdx.x - off] : 0;
+    __syncthreads();
+    s[threadIdx.x] += t;
+    __syncthreads();
+  }
+  if (i < n) a[i] = s[threadIdx.x] - v;
+  if (threadIdx.x == 1023) tile_sum[blockIdx.x] = s[1023];
+}
+__global__ void k_scan_sums(int *tile_sum, int ntiles, int *total) {
+  if (threadIdx.x == 0) {
+    int run = 0;
+    for (int t = 0; t < ntiles; t++) {
+      int v = tile_sum[t];
+      tile_sum[t] = run;
+      run += v;
+    }
+    *total = run;
+  }
+}
+__global__ void k_scan_add(int *a, long n, const int *tile_sum) {
+  long i = (long)blockIdx.x * 1024 + threadIdx.x;
+  if (i < n) a[i] += tile_sum[blockIdx.x];
+}
+
+static int exclusive_scan(int *d, long n, int *total, cudaStream_t st) {
+  long ntiles = (n + 1023) / 1024;
+  DBuf<int> ts, tot;
+  EXF_TRY(ts.alloc(ntiles));
+  EXF_TRY(tot.alloc(1));
+  k_scan_tiles<<<ntiles, 1024, 0, st>>>(d, n, ts.p);
+  k_scan_sums<<<1, 32, 0, st>>>(ts.p, (int)ntiles, tot.p);
+  k_scan_add<<<ntiles, 1024, 0, st>>>(d, n, ts.p);
+  EXF_LAUNCH_CHECK();
+  EXF_CUDA(cudaMemcpyAsync(total, tot.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+  EXF_CUDA(cudaStreamSynchronize(st));
+  return EXF_OK;
+}
+
+// ------------------------------------------------------------- node incidence
+__global__ void k_count_incidence(const int *conn, long nentries, int *cnt) {
+  long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < nentries) atomicAdd(&cnt[conn[i]], 1);
+}
+__global__ void k_fill_incidence(const int *conn, long nentries, int nen, const int *ptr, int *fill, int *elist) {
+  long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < nentries) {
+    int n = conn[i];
+    int slot = atomicAdd(&fill[n], 1);
+    elist[ptr[n] + slot] = (int)(i / nen);
+  }
+}
+// sort each node's element list (<= 8 entries): makes the lists schedule-independent
+__global__ void k_sort_incidence(const int *ptr, int *elist, int N) {
+  int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= N) return;
+  int b = ptr[n], e = ptr[n + 1];
+  for (int i = b + 1; i < e; i++) {
+    int v = elist[i], j = i - 1;
+    while (j >= b && elist[j] > v) {
+      elist[j + 1] = elist[j];
+      j--;
+    }
+    elist[j + 1] = v;
+  }
+}
+
+// sorted-unique insertion into a small local list
+__device__ __forceinline__ int insert_unique(int *lst, int cnt, int v, int cap) {
+  int lo = 0, hi = cnt;
+  while (lo < hi) {
+    int mid = (lo + hi) >> 1;
+    if (lst[mid] < v) lo = mid + 1;
+    else hi = mid;
+  }
+  if (lo < cnt && lst[lo] == v) return cnt;
+  if (cnt >= cap) return cnt + 1;  // overflow: reported by the caller, never written
+  for (int k = cnt; k > lo; k--) lst[k] = lst[k - 1];
+  lst[lo] = v;
+  return cnt + 1;
+}
+
+// node pattern: union of the nodes (qq) and of the vertices (ql) of the elements
+// containing each node.  pass 0 writes counts, pass 1 writes the sorted lists.
+template <int NEN, int NVX, int MAXQ, int MAXL>
+__global__ void k_node_pattern(const int *conn, const int *eptr, const int *elist, int N, int pass, int *qq_cnt,
+                               int *ql_cnt, const int *qq_ptr, const int *ql_ptr, int *qq_col, int *ql_col,
+                               int *bad) {
+  int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= N) return;
+  int lq[MAXQ], ll[MAXL];
+  int cq = 0, cl = 0;
+  for (int k = eptr[n]; k < eptr[n + 1]; k++) {
+    const int *c = conn + (long)elist[k] * NEN;
+    for (int j = 0; j < NEN; j++) cq = min(insert_unique(lq, cq, c[j], MAXQ), MAXQ + 1);
+    for (int j = 0; j < NVX; j++) cl = min(insert_unique(ll, cl, c[j], MAXL), MAXL + 1);
+  }
+  if (cq > MAXQ || cl > MAXL) {  // not a structured quad9/hex27 hierarchy
+    atomicExch(bad, 1);
+    cq = min(cq, MAXQ);
+    cl = min(cl, MAXL);
+  }
+  if (pass == 0) {
+    qq_cnt[n] = cq;
+    ql_cnt[n] = cl;
+  } else {
+    for (int j = 0; j < cq; j++) qq_col[qq_ptr[n] + j] = lq[j];
+    for (int j = 0; j < cl; j++) ql_col[ql_ptr[n] + j] = ll[j];
+  }
+}
+
+__device__ __forceinline__ int bsearch_dev(const int *a, int lo, int hi, int v) {
+  // returns index in [lo,hi) with a[idx]==v, or -1
+  while (lo < hi) {
+    int mid = (lo + hi) >> 1;
+    int x = a[mid];
+    if (x == v) return mid;
+    if (x < v) lo = mid + 1;
+    else hi = mid;
+  }
+  return -1;
+}
+
+__global__ void k_diag_pos(const int *qq_ptr, const int *qq_col, int N, int *diag) {
+  int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n < N) diag[n] = bsearch_dev(qq_col, qq_ptr[n], qq_ptr[n + 1], n);
+}
+
+// element slot maps: pos_qq[e][i][j] = position of node j in qq(node i) (relative),
+// pos_ql[e][i][jv] = position of vertex jv in ql(node i)
+__global__ void k_elem_pos(const int *conn, int nel, int nen, int nvx, const int *qq_ptr, const int *qq_col,
+                           const int *ql_ptr, const int *ql_col, uint8_t *pos_qq, uint8_t *pos_ql, int *bad) {
+  long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long)nel * nen) return;
+  long e = t / nen;
+  int i = (int)(t % nen);
+  const int *c = conn + e * nen;
+  int ni = c[i];
+  for (int j = 0; j < nen; j++) {
+    int p = bsearch_dev(qq_col, qq_ptr[ni], qq_ptr[ni + 1], c[j]);
+    if (p < 0) atomicExch(bad, 1);
+    pos_qq[(e * nen + i) * nen + j] = (uint8_t)(p - qq_ptr[ni]);
+  }
+  for (int j = 0; j < nvx; j++) {
+    int p = bsearch_dev(ql_col, ql_ptr[ni], ql_ptr[ni + 1], c[j]);
+    if (p < 0) atomicExch(bad, 1);
+    pos_ql[(e * nen + i) * nvx + j] = (uint8_t)(p - ql_ptr[ni]);
+  }
+}
+
+// for the pressure row of Q1 node m and its block k (velocity node n_k): index of the
+// B^T entry (row n_k, pressure column m) inside vp
+__global__ void k_gidx(const int *qq_ptr, const int *qq_col, const int *ql_ptr, const int *ql_col, int NL, int *gidx,
+                       int *bad) {
+  int m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= NL) return;
+  for (int k = qq_ptr[m]; k < qq_ptr[m + 1]; k++) {
+    int n = qq_col[k];
+    int p = bsearch_dev(ql_col, ql_ptr[n], ql_ptr[n + 1], m);
+    if (p < 0) atomicExch(bad, 1);
+    gidx[k] = p;
+  }
+}
+
+// DOF-level CSR: row (a,n) = [b*N + qq(n)] for b < nv2, then [nv2*N + ql(n)]
+__global__ void k_csr_rowlen(const int *qq_ptr, const int *ql_ptr, int N, int NL, int nv2, int nv1, int *rowlen) {
+  long r = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  long nrow = (long)nv2 * N + (long)nv1 * NL;
+  if (r >= nrow) return;
+  int n = r < (long)nv2 * N ? (int)(r % N) : (int)(r - (long)nv2 * N);
+  rowlen[r] = nv2 * (qq_ptr[n + 1] - qq_ptr[n]) + nv1 * (ql_ptr[n + 1] - ql_ptr[n]);
+}
+__global__ void k_csr_fill(const int *qq_ptr, const int *qq_col, const int *ql_ptr, const int *ql_col, int N, int NL,
+                           int nv2, int nv1, const int *rowptr, int *col) {
+  long r = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  long nrow = (long)nv2 * N + (long)nv1 * NL;
+  if (r >= nrow) return;
+  int n = r < (long)nv2 * N ? (int)(r % N) : (int)(r - (long)nv2 * N);
+  int o = rowptr[r];
+  for (int b = 0; b < nv2; b++)
+    for (int k = qq_ptr[n]; k < qq_ptr[n + 1]; k++) col[o++] = b * N + qq_col[k];
+  if (nv1)
+    for (int k = ql_ptr[n]; k < ql_ptr[n + 1]; k++) col[o++] = nv2 * N + ql_col[k];
+}
+
+static inline unsigned nblk(long n, int bs) { return (unsigned)((n + bs - 1) / bs); }
+
+int build_patterns(exf_sys *s) {
+  exf_mesh *m = s->mesh;
+  cudaStream_t st = s->stream;
+  const int nen = m->nen, nvx = m->nvx;
+  for (int l = 0; l < s->nlev; l++) {
+    SysLevel &L = s->L[l];
+    const MeshLevel &ml = m->lev[l];
+    L.N = ml.nnodes;
+    L.NL = l > 0 ? m->lev[l - 1].nnodes : m->nvert0;
+    L.nel = ml.nel;
+    L.ndof = s->nv2 * L.N + s->nv1 * L.NL;
+    long nent = (long)ml.nel * nen;
+    DBuf<int> eptr, fill, elist;
+    EXF_TRY(eptr.alloc(L.N + 1));
+    EXF_TRY(fill.alloc(L.N));
+    EXF_TRY(elist.alloc(nent));
+    EXF_TRY(eptr.zero(st));
+    EXF_TRY(fill.zero(st));
+    k_count_incidence<<<nblk(nent, 256), 256, 0, st>>>(ml.d_conn.p, nent, eptr.p);
+    EXF_LAUNCH_CHECK();
+    int tot = 0;
+    EXF_TRY(exclusive_scan(eptr.p, L.N + 1, &tot, st));
+    k_fill_incidence<<<nblk(nent, 256), 256, 0, st>>>(ml.d_conn.p, nent, nen, eptr.p, fill.p, elist.p);
+    k_sort_incidence<<<nblk(L.N, 256), 256, 0, st>>>(eptr.p, elist.p, L.N);
+    EXF_LAUNCH_CHECK();
+    DBuf<int> bad;
+    EXF_TRY(bad.alloc(1));
+    EXF_TRY(bad.zero(st));
+    EXF_TRY(L.qq_ptr.alloc(L.N + 1));
+    EXF_TRY(L.ql_ptr.alloc(L.N + 1));
+    EXF_TRY(L.qq_ptr.zero(st));
+    EXF_TRY(L.ql_ptr.zero(st));
+    auto launch_pattern = [&](int pass) {
+      if (m->dim == 2)
+        k_node_pattern<9, 4, 25, 9><<<nblk(L.N, 128), 128, 0, st>>>(
+            ml.d_conn.p, eptr.p, elist.p, L.N, pass, L.qq_ptr.p, L.ql_ptr.p, L.qq_ptr.p, L.ql_ptr.p, L.qq_col.p,
+            L.ql_col.p, bad.p);
+      else
+        k_node_pattern<27, 8, 125, 27><<<nblk(L.N, 128), 128, 0, st>>>(
+            ml.d_conn.p, eptr.p, elist.p, L.N, pass, L.qq_ptr.p, L.ql_ptr.p, L.qq_ptr.p, L.ql_ptr.p, L.qq_col.p,
+            L.ql_col.p, bad.p);
+    };
+    launch_pattern(0);
+    EXF_LAUNCH_CHECK();
+    int nqq = 0, nql = 0;
+    EXF_TRY(exclusive_scan(L.qq_ptr.p, L.N + 1, &nqq, st));
+    EXF_TRY(exclusive_scan(L.ql_ptr.p, L.N + 1, &nql, st));
+    L.nqq = nqq;
+    L.nql = nql;
+    EXF_TRY(L.qq_col.alloc(nqq));
+    EXF_TRY(L.ql_col.alloc(nql));
+    launch_pattern(1);
+    EXF_LAUNCH_CHECK();
+    int hq = 0, hl = 0;
+    EXF_CUDA(cudaMemcpyAsync(&hq, L.qq_ptr.p + L.NL, sizeof(int), cudaMemcpyDeviceToHost, st));
+    EXF_CUDA(cudaMemcpyAsync(&hl, L.ql_ptr.p + L.NL, sizeof(int), cudaMemcpyDeviceToHost, st));
+    EXF_CUDA(cudaStreamSynchronize(st));
+    L.nqqL = hq;
+    L.nllL = hl;
+    // derived maps
+    EXF_TRY(L.diag_pos.alloc(L.N));
+    k_diag_pos<<<nblk(L.N, 256), 256, 0, st>>>(L.qq_ptr.p, L.qq_col.p, L.N, L.diag_pos.p);
+    EXF_TRY(L.pos_qq.alloc((size_t)ml.nel * nen * nen));
+    EXF_TRY(L.pos_ql.alloc((size_t)ml.nel * nen * nvx));
+    k_elem_pos<<<nblk(nent, 128), 128, 0, st>>>(ml.d_conn.p, ml.nel, nen, nvx, L.qq_ptr.p, L.qq_col.p, L.ql_ptr.p,
+                                                L.ql_col.p, L.pos_qq.p, L.pos_ql.p, bad.p);
+    if (s->nv1) {
+      EXF_TRY(L.gidx.alloc(L.nqqL));
+      k_gidx<<<nblk(L.NL, 128), 128, 0, st>>>(L.qq_ptr.p, L.qq_col.p, L.ql_ptr.p, L.ql_col.p, L.NL, L.gidx.p,
+                                              bad.p);
+    }
+    EXF_LAUNCH_CHECK();
+    // DOF CSR
+    long nrow = L.ndof;
+    EXF_TRY(L.csr_ptr.alloc(nrow + 1));
+    EXF_TRY(L.csr_ptr.zero(st));
+    k_csr_rowlen<<<nblk(nrow, 256), 256, 0, st>>>(L.qq_ptr.p, L.ql_ptr.p, L.N, L.NL, s->nv2, s->nv1,
+                                                  L.csr_ptr.p);
+    EXF_LAUNCH_CHECK();
+    int nnz = 0;
+    EXF_TRY(exclusive_scan(L.csr_ptr.p, nrow + 1, &nnz, st));
+    L.nnz = nnz;
+    EXF_TRY(L.csr_col.alloc(nnz));
+    k_csr_fill<<<nblk(nrow, 256), 256, 0, st>>>(L.qq_ptr.p, L.qq_col.p, L.ql_ptr.p, L.ql_col.p, L.N, L.NL, s->nv2,
+                                                s->nv1, L.csr_ptr.p, L.csr_col.p);
+    EXF_LAUNCH_CHECK();
+    int hbad = 0;
+    EXF_CUDA(cudaMemcpyAsync(&hbad, bad.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    EXF_CUDA(cudaStreamSynchronize(st));
+    if (hbad) {
+      set_error("pattern build: inconsistent node pattern on level %d", l);
+      return EXF_ERR_STATE;
+    }
+    // values
+    const int d = s->nv2;
+    EXF_TRY(L.A.vv.alloc((size_t)d * d * L.nqq));
+    EXF_TRY(L.A32.vv.alloc((size_t)d * d * L.nqq));
+    if (s->nv1) {
+      EXF_TRY(L.A.vp.alloc((size_t)d * L.nql));
+      EXF_TRY(L.A.pv.alloc((size_t)d * L.nqqL));
+      EXF_TRY(L.A.pp.alloc(L.nllL));
+      EXF_TRY(L.A32.vp.alloc((size_t)d * L.nql));
+      EXF_TRY(L.A32.pv.alloc((size_t)d * L.nqqL));
+      EXF_TRY(L.A32.pp.alloc(L.nllL));
+    }
+    // vectors
+    EXF_TRY(L.x.alloc(L.ndof));
+    EXF_TRY(L.b.alloc(L.ndof));
+    EXF_TRY(L.r.alloc(L.ndof));
+    EXF_TRY(L.dx.alloc(L.ndof));
+    EXF_TRY(L.x32.alloc(L.ndof));
+    EXF_TRY(L.b32.alloc(L.ndof));
+    EXF_TRY(L.r32.alloc(L.ndof));
+    EXF_TRY(L.dx32.alloc(L.ndof));
+    EXF_TRY(L.rmask.alloc(L.ndof));
+    EXF_TRY(L.x.zero(st));
+    EXF_TRY(L.x32.zero(st));
+    EXF_TRY(L.dx.zero(st));
+    EXF_TRY(L.dx32.zero(st));
+    if (s->nv1) {
+      EXF_TRY(L.vanka_dp.alloc(L.NL));
+      EXF_TRY(L.vanka_dp32.alloc(L.NL));
+    }
+  }
+  return EXF_OK;
+}
+
+// --------------------------------------------------------------- colouring
+// T (Gauss-Seidel): item = node, colour = lattice index of level l mod 3 per axis;
+// two nodes of one colour never share an element.  NS (Vanka): item = pressure node,
+// colour = vertex index mod 3 per axis; the velocity stars of one colour are disjoint.
+__global__ void k_item_colour(const int *lat, int nitem, int step, int dim, int *colour) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nitem) return;
+  int c = 0, mul = 1;
+  for (int d = 0; d < dim; d++) {
+    c += ((lat[3 * i + d] / step) % 3) * mul;
+    mul *= 3;
+  }
+  colour[i] = c;
+}
+
+int build_colours(exf_sys *s) {
+  exf_mesh *m = s->mesh;
+  cudaStream_t st = s->stream;
+  for (int l = 0; l < s->nlev; l++) {
+    SysLevel &L = s->L[l];
+    int sl = 1 << (m->nlev - 1 - l);
+    int nitem = s->kind == EXF_KIND_T ? L.N : L.NL;
+    int step = s->kind == EXF_KIND_T ? sl : 2 * sl;
+    EXF_TRY(L.item_colour.alloc(nitem));
+    k_item_colour<<<nblk(nitem, 256), 256, 0, st>>>(m->d_lat.p, nitem, step, m->dim, L.item_colour.p);
+    EXF_LAUNCH_CHECK();
+    std::vector<int> col(nitem);
+    EXF_CUDA(cudaMemcpyAsync(col.data(), L.item_colour.p, nitem * sizeof(int), cudaMemcpyDeviceToHost, st));
+    EXF_CUDA(cudaStreamSynchronize(st));
+    L.ncolour = m->dim == 2 ? 9 : 27;
+    L.col_off.assign(L.ncolour + 1, 0);
+    for (int i = 0; i < nitem; i++) L.col_off[col[i] + 1]++;
+    for (int c = 0; c < L.ncolour; c++) L.col_off[c + 1] += L.col_off[c];
+    std::vector<int> items(nitem), pos(L.col_off.begin(), L.col_off.end() - 1);
+    for (int i = 0; i < nitem; i++) items[pos[col[i]]++] = i;
+    EXF_TRY(L.col_items.alloc(nitem));
+    EXF_CUDA(cudaMemcpyAsync(L.col_items.p, items.data(), nitem * sizeof(int), cudaMemcpyHostToDevice, st));
+    EXF_CUDA(cudaStreamSynchronize(st));
+  }
+  return EXF_OK;
+}
+
+// ---------------------------------------------------------------- transfers
+// 1D Lagrange bases on {-1,0,+1} and the linear basis on {-1,+1} (src/MGFE.C:252-263)
+static double lag1(int a, double x) {
+  if (a == 0) return .5 * x * (x - 1.);
+  if (a == 2) return .5 * x * (x + 1.);
+  return 1. - x * x;
+}
+static double lin1(int a, double x) { return a == 0 ? .5 * (1. - x) : .5 * (1. + x); }
+
+// Prolongation rows: the fine node's row holds the parent element's shape functions at
+// the node, |v| > 1e-8 kept, columns sorted (gencase compute_prol_qq,
+// MGGenCase.C:2308-2393; the values equal the embedding matrices of
+// src/MGGeomEl.C:182-600).  Restriction = transposed prolongation, |v| > 1e-6
+// (compute_res_qq, MGGenCase.C:2452-2569).  Both are node-level; every variable
+// component uses the same node operator (no inter-variable coupling).
+static void build_prol_host(const exf_mesh *m, int l, bool quad, Transfer &P) {
+  const int dim = m->dim, nen = m->nen, nvx = m->nvx;
+  const MeshLevel &fl = m->lev[l], &cl = m->lev[l - 1];
+  int nrow = quad ? fl.nnodes : cl.nnodes;  // Q1 nodes of level l = Q2 nodes of level l-1
+  int s_f = 1 << (m->nlev - 1 - l), s_c = 2 * s_f;
+  std::vector<int> own(fl.nnodes, -1);
+  for (int e = 0; e < fl.nel; e++)
+    for (int k = 0; k < nen; k++) {
+      int nd = fl.conn[(size_t)e * nen + k];
+      if (own[nd] < 0) own[nd] = e;
+    }
+  P.nrow = nrow;
+  P.h_ptr.assign(nrow + 1, 0);
+  P.h_col.clear();
+  P.h_val.clear();
+  for (int i = 0; i < nrow; i++) {
+    int e = own[i];
+    int ex[3] = {e % fl.ne[0], (e / fl.ne[0]) % fl.ne[1], e / (fl.ne[0] * fl.ne[1])};
+    int pe[3] = {ex[0] >> 1, ex[1] >> 1, ex[2] >> 1};
+    int pel = (pe[2] * cl.ne[1] + pe[1]) * cl.ne[0] + pe[0];
+    const int *pc = &cl.conn[(size_t)pel * nen];
+    double xi[3] = {0, 0, 0};
+    for (int d = 0; d < dim; d++) xi[d] = -1. + (double)(m->lat[3 * i + d] - 2 * pe[d] * s_c) / (double)s_c;
+    std::vector<std::pair<int, double>> ent;
+    int nsh = quad ? nen : nvx;
+    for (int kj = 0; kj < nsh; kj++) {
+      const int *abc = dim == 2 ? Q9_ABC[kj] : H27_ABC[kj];
+      double v = 1.;
+      for (int d = 0; d < dim; d++) v *= quad ? lag1(abc[d], xi[d]) : lin1(abc[d], xi[d]);
+      if (fabs(v) > 1e-8) ent.push_back({pc[kj], v});
+    }
+    std::sort(ent.begin(), ent.end());
+    for (auto &pv : ent) {
+      P.h_col.push_back(pv.first);
+      P.h_val.push_back(pv.second);
+    }
+    P.h_ptr[i + 1] = (int)P.h_col.size();
+  }
+}
+
+static void transpose_host(const Transfer &P, int ncol, Transfer &R) {
+  R.nrow = ncol;
+  R.h_ptr.assign(ncol + 1, 0);
+  for (int i = 0; i < P.nrow; i++)
+    for (int q = P.h_ptr[i]; q < P.h_ptr[i + 1]; q++)
+      if (fabs(P.h_val[q]) > 1e-6) R.h_ptr[P.h_col[q] + 1]++;
+  for (int i = 0; i < ncol; i++) R.h_ptr[i + 1] += R.h_ptr[i];
+  R.h_col.assign(R.h_ptr[ncol], 0);
+  R.h_val.assign(R.h_ptr[ncol], 0.);
+  std::vector<int> fill(R.h_ptr.begin(), R.h_ptr.end() - 1);
+  for (int i = 0; i < P.nrow; i++)
+    for (int q = P.h_ptr[i]; q < P.h_ptr[i + 1]; q++)
+      if (fabs(P.h_val[q]) > 1e-6) {
+        int c = P.h_col[q];
+        R.h_col[fill[c]] = i;
+        R.h_val[fill[c]] = P.h_val[q];
+        fill[c]++;
+      }
+}
+
+static int upload_transfer(Transfer &T) {
+  EXF_TRY(T.ptr.alloc(T.h_ptr.size()));
+  EXF_TRY(T.col.alloc(T.h_col.size()));
+  EXF_TRY(T.val.alloc(T.h_val.size()));
+  EXF_TRY(T.val32.alloc(T.h_val.size()));
+  std::vector<float> v32(T.h_val.begin(), T.h_val.end());
+  EXF_CUDA(cudaMemcpy(T.ptr.p, T.h_ptr.data(), T.h_ptr.size() * sizeof(int), cudaMemcpyHostToDevice));
+  if (!T.h_col.empty()) {
+    EXF_CUDA(cudaMemcpy(T.col.p, T.h_col.data(), T.h_col.size() * sizeof(int), cudaMemcpyHostToDevice));
+    EXF_CUDA(cudaMemcpy(T.val.p, T.h_val.data(), T.h_val.size() * sizeof(double), cudaMemcpyHostToDevice));
+    EXF_CUDA(cudaMemcpy(T.val32.p, v32.data(), v32.size() * sizeof(float), cudaMemcpyHostToDevice));
+  }
+  return EXF_OK;
+}
+
+int build_transfers(exf_sys *s) {
+  exf_mesh *m = s->mesh;
+  for (int l = 1; l < s->nlev; l++) {
+    SysLevel &F = s->L[l];
+    SysLevel &C = s->L[l - 1];
+    build_prol_host(m, l, true, F.Pq);
+    EXF_TRY(upload_transfer(F.Pq));
+    transpose_host(F.Pq, C.N, C.Rq);
+    EXF_TRY(upload_transfer(C.Rq));
+    if (s->nv1) {
+      build_prol_host(m, l, false, F.Pl);
+      EXF_TRY(upload_transfer(F.Pl));
+      transpose_host(F.Pl, C.NL, C.Rl);
+      EXF_TRY(upload_transfer(C.Rl));
+    }
+  }
+  return EXF_OK;
+}
+
+// restriction row mask: bc[0][top dof] % 2 (src/MGSolverDA.C:2423-2425)
+__global__ void k_rmask(const int *bc0, int N, int NL, int Ntop, int nv2, int nv1, double *mask) {
+  long r = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  long nrow = (long)nv2 * N + (long)nv1 * NL;
+  if (r >= nrow) return;
+  long td;
+  if (r < (long)nv2 * N) td = (r / N) * (long)Ntop + (r % N);
+  else td = (long)nv2 * Ntop + (r - (long)nv2 * N);
+  mask[r] = (double)(bc0[td] % 2);
+}
+
+int update_rmask(exf_sys *s) {
+  int Ntop = s->L[s->nlev - 1].N;
+  for (int l = 0; l < s->nlev; l++) {
+    SysLevel &L = s->L[l];
+    k_rmask<<<nblk(L.ndof, 256), 256, 0, s->stream>>>(s->d_bc0.p, L.N, L.NL, Ntop, s->nv2, s->nv1, L.rmask.p);
+    EXF_LAUNCH_CHECK();
+  }
+  return EXF_OK;
+}
+
+}  // namespace exf

@@ -1,0 +1,333 @@
+"""Host-side mirror of exFEMuS's MGSolBase / MGSolDA interface over the C ABI.
+
+Method names follow the reference (include/MGSolverBase.h:118-361): MGDofBcOp,
+GenBc, GenMatRhs(time, Level, mode), MGSolve(Eps, MaxIter, Gamma, Nc_pre, Nc_coarse,
+Nc_post), MGStep, MGTimeStep(time).  Errors raise ExfError with the library message
+(the reference aborts; the C ABI returns a status).  Everything runs on the GPU; there
+is no CPU path.
+"""
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from ._lib import (ExfMeshDesc, ExfMgParams, ExfPhys, ExfSolveStats, check, dptr, iptr, load)
+
+
+def phys(**kw):
+    """Physics parameters with the reference defaults (UP_WIND_NS=0.1, UP_WIND_T=1)."""
+    p = ExfPhys()
+    p.inv_re, p.inv_prdl, p.rho, p.rhocp = 1.0, 1.0, 1.0, 1.0
+    p.inv_dt, p.penalty = 0.0, 1.0
+    p.upwind_ns, p.upwind_t = 0.1, 1.0
+    p.ifr, p.buoy = 0.0, 0.0
+    for k, v in kw.items():
+        if k == "dirg":
+            for i, x in enumerate(v):
+                p.dirg[i] = x
+        else:
+            setattr(p, k, v)
+    return p
+
+
+def mg_params(**kw):
+    """Multigrid parameters (MGSolve defaults of the reference where they apply)."""
+    p = ExfMgParams()
+    p.eps, p.max_cycles, p.gamma = 1e-10, 100, 1
+    p.nu_pre, p.nu_post, p.double_below_top = 2, 2, 1
+    p.smoother, p.omega, p.corr_damp = _lib.SMOOTH_GS, 0.4, 0.95
+    p.cond_corr, p.reverse_colours, p.precision, p.use_graph = 0, 0, _lib.PREC_FP64, 0
+    for k, v in kw.items():
+        setattr(p, k, v)
+    return p
+
+
+class Mesh:
+    """Structured multilevel quad9/hex27 hierarchy (MGMesh analogue)."""
+
+    def __init__(self, dim, nlev, n0, box, device=0):
+        L = load()
+        d = ExfMeshDesc()
+        d.dim, d.nlev, d.device = dim, nlev, device
+        n0 = list(n0) + [1] * (3 - len(n0))
+        box = list(box) + [0.0] * (6 - len(box))
+        for i in range(3):
+            d.n0[i] = n0[i]
+        for i in range(6):
+            d.box[i] = box[i]
+        h = C.c_void_p()
+        check(L.exf_mesh_create(C.byref(d), C.byref(h)))
+        self.h, self.L, self.dim, self.nlev = h, L, dim, nlev
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.exf_mesh_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def info(self, lev):
+        a, b, c = C.c_int(), C.c_int(), C.c_int()
+        check(self.L.exf_mesh_info(self.h, lev, C.byref(a), C.byref(b), C.byref(c)))
+        return a.value, b.value, c.value
+
+    def nnodes(self, lev):
+        return self.info(lev)[0]
+
+    def nel(self, lev):
+        return self.info(lev)[1]
+
+    @property
+    def nvert0(self):
+        return self.info(0)[2]
+
+    @property
+    def ntop(self):
+        return self.nnodes(self.nlev - 1)
+
+    @property
+    def nen(self):
+        return 9 if self.dim == 2 else 27
+
+    def xyz(self):
+        a = np.zeros(self.dim * self.ntop)
+        check(self.L.exf_mesh_get_xyz(self.h, dptr(a)))
+        return a.reshape(self.dim, self.ntop)
+
+    def conn(self, lev):
+        ne = self.nel(lev)
+        ns = 4 if self.dim == 2 else 6
+        c = np.zeros(ne * self.nen, np.int32)
+        nb = np.zeros(ne * ns, np.int32)
+        col = np.zeros(ne, np.int32)
+        check(self.L.exf_mesh_get_conn(self.h, lev, iptr(c), iptr(nb), iptr(col)))
+        return c.reshape(ne, self.nen), nb.reshape(ne, ns), col
+
+
+class MGSolBase:
+    """One equation system on the GPU (MGSolBase/MGSolDA analogue)."""
+
+    kind = None
+
+    def __init__(self, mesh, kind=None):
+        self.L = load()
+        self.mesh = mesh
+        if kind is not None:
+            self.kind = kind
+        h = C.c_void_p()
+        check(self.L.exf_sys_create(mesh.h, self.kind, C.byref(h)))  # init_dof + pattern (MGDofBcOp)
+        self.h = h
+        self.nlev = mesh.nlev
+        self.nvars = 1 if self.kind == _lib.KIND_T else mesh.dim + 1
+        self.phys = phys()
+        self._keep = None
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.exf_sys_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    # ---- DOF / operators
+    def MGDofBcOp(self, preset=None):
+        if preset is not None:
+            self.GenBc(preset)
+
+    def ndof(self, lev):
+        n = C.c_int()
+        check(self.L.exf_sys_ndof(self.h, lev, C.byref(n)))
+        return n.value
+
+    @property
+    def ntop_dof(self):
+        return self.ndof(self.nlev - 1)
+
+    def node_dof(self, lev):
+        a = np.zeros(self.nvars * self.mesh.ntop, np.int32)
+        check(self.L.exf_sys_get_node_dof(self.h, lev, iptr(a)))
+        return a
+
+    def GenBc(self, preset):
+        check(self.L.exf_sys_bc_preset(self.h, preset))
+
+    def set_bc(self, bc0, bc1):
+        bc0 = np.ascontiguousarray(bc0, np.int32)
+        bc1 = np.ascontiguousarray(bc1, np.int32)
+        check(self.L.exf_sys_set_bc(self.h, iptr(bc0), iptr(bc1)))
+
+    def bc(self):
+        n = self.ntop_dof
+        b0 = np.zeros(n, np.int32)
+        b1 = np.zeros(n, np.int32)
+        check(self.L.exf_sys_get_bc(self.h, iptr(b0), iptr(b1)))
+        return b0, b1
+
+    def nnz(self, lev):
+        v = C.c_long()
+        check(self.L.exf_sys_nnz(self.h, lev, C.byref(v)))
+        return v.value
+
+    def pattern(self, lev):
+        rp = np.zeros(self.ndof(lev) + 1, np.int32)
+        col = np.zeros(self.nnz(lev), np.int32)
+        check(self.L.exf_sys_get_pattern(self.h, lev, iptr(rp), iptr(col)))
+        return rp, col
+
+    def _transfer(self, fn, lev, nrow):
+        nnz = C.c_long()
+        check(fn(self.h, lev, C.byref(nnz), None, None, None))
+        rp = np.zeros(nrow + 1, np.int32)
+        col = np.zeros(nnz.value, np.int32)
+        val = np.zeros(nnz.value)
+        check(fn(self.h, lev, C.byref(nnz), iptr(rp), iptr(col), dptr(val)))
+        return rp, col, val
+
+    def prol(self, lev):  # Prl[lev]: level lev-1 -> lev (ReadProl)
+        return self._transfer(self.L.exf_sys_get_prol, lev, self.ndof(lev))
+
+    def rest(self, lev):  # Rst[lev]: level lev+1 -> lev (ReadRest)
+        return self._transfer(self.L.exf_sys_get_rest, lev, self.ndof(lev))
+
+    def colours(self, lev):
+        nitem = self.mesh.nnodes(lev) if self.kind == _lib.KIND_T else (
+            self.mesh.nnodes(lev - 1) if lev > 0 else self.mesh.nvert0)
+        out = np.zeros(nitem, np.int32)
+        nc = C.c_int()
+        check(self.L.exf_sys_get_colours(self.h, lev, C.byref(nc), iptr(out)))
+        return nc.value, out
+
+    def couple(self, other):
+        check(self.L.exf_sys_couple(self.h, other.h if other is not None else None))
+
+    # ---- fields
+    def set_xold(self, x):
+        x = np.ascontiguousarray(x, np.float64)
+        check(self.L.exf_sys_set_xold(self.h, dptr(x)))
+
+    def xold(self):
+        x = np.zeros(self.ntop_dof)
+        check(self.L.exf_sys_get_xold(self.h, dptr(x)))
+        return x
+
+    def set_x(self, x):
+        x = np.ascontiguousarray(x, np.float64)
+        check(self.L.exf_sys_set_x(self.h, dptr(x)))
+
+    def x(self):
+        x = np.zeros(self.ntop_dof)
+        check(self.L.exf_sys_get_x(self.h, dptr(x)))
+        return x
+
+    def xold_update(self):
+        check(self.L.exf_sys_xold_update(self.h))
+
+    def set_source(self, qe):
+        qe = np.ascontiguousarray(qe, np.float64)
+        check(self.L.exf_sys_set_source(self.h, dptr(qe)))
+
+    def set_rhs(self, b):
+        b = np.ascontiguousarray(b, np.float64)
+        check(self.L.exf_sys_set_rhs(self.h, dptr(b)))
+
+    def rhs(self):
+        b = np.zeros(self.ntop_dof)
+        check(self.L.exf_sys_get_rhs(self.h, dptr(b)))
+        return b
+
+    # ---- assembly (GenMatRhs)
+    def GenMatRhs(self, time, Level, mode):
+        del time  # steady / pseudo-time: the time level enters through phys.inv_dt
+        check(self.L.exf_gen_mat_rhs(self.h, C.byref(self.phys), Level, mode))
+
+    def assemble_all(self):
+        check(self.L.exf_assemble_all(self.h, C.byref(self.phys)))
+
+    def matrix(self, lev):
+        v = np.zeros(self.nnz(lev))
+        check(self.L.exf_get_matrix(self.h, lev, dptr(v)))
+        return v
+
+    def set_matrix(self, lev, v):
+        v = np.ascontiguousarray(v, np.float64)
+        check(self.L.exf_set_matrix(self.h, lev, dptr(v)))
+
+    def csr(self, lev):
+        rp, col = self.pattern(lev)
+        return rp, col, self.matrix(lev)
+
+    def transpose(self):
+        check(self.L.exf_sys_transpose(self.h))
+
+    # ---- solve (MGSolve / MGStep)
+    def solve(self, params):
+        st = ExfSolveStats()
+        rc = self.L.exf_mg_solve(self.h, C.byref(params), C.byref(st))
+        if rc not in (_lib.EXF_OK, _lib.EXF_ERR_NOT_CONVERGED):
+            check(rc)
+        return st
+
+    def MGSolve(self, Eps, MaxIter, Gamma=1, Nc_pre=8, Nc_coarse=40, Nc_post=8, **kw):
+        del Nc_coarse  # the coarsest level is solved directly
+        p = mg_params(eps=Eps, max_cycles=MaxIter, gamma=Gamma, nu_pre=Nc_pre, nu_post=Nc_post,
+                      smoother=_lib.SMOOTH_VANKA if self.kind == _lib.KIND_NS else _lib.SMOOTH_GS, **kw)
+        return self.solve(p)
+
+    def MGTimeStep(self, time, params):
+        """GenMatRhs(top,1) + GenMatRhs(L<top,0) + MGSolve + x_old update (MGSolverNS.C:722-750)."""
+        del time
+        self.assemble_all()
+        st = self.solve(params)
+        self.xold_update()
+        return st
+
+    # ---- unit operations on host arrays
+    def resid(self, lev, x, b=None):
+        """r = b - A x on level lev (NumericVectorM::resid); with b=None returns A x."""
+        r = np.zeros(self.ndof(lev))
+        x = np.ascontiguousarray(x, np.float64)
+        bb = None if b is None else np.ascontiguousarray(b, np.float64)
+        check(self.L.exf_resid(self.h, lev, dptr(x), None if bb is None else dptr(bb), dptr(r)))
+        return r
+
+    def spmv(self, lev, x):
+        return self.resid(lev, x, None)
+
+    def restrict(self, lev, r_fine):
+        out = np.zeros(self.ndof(lev))
+        r_fine = np.ascontiguousarray(r_fine, np.float64)
+        check(self.L.exf_restrict(self.h, lev, dptr(r_fine), dptr(out)))
+        return out
+
+    def prolong(self, lev, x_coarse):
+        out = np.zeros(self.ndof(lev))
+        x_coarse = np.ascontiguousarray(x_coarse, np.float64)
+        check(self.L.exf_prolong(self.h, lev, dptr(x_coarse), dptr(out)))
+        return out
+
+    def smooth(self, lev, params, nsweeps, x, b):
+        x = np.array(x, dtype=np.float64)
+        b = np.ascontiguousarray(b, np.float64)
+        check(self.L.exf_smooth(self.h, lev, C.byref(params), nsweeps, dptr(x), dptr(b)))
+        return x
+
+    def coarse_solve(self, b):
+        x = np.zeros(self.ndof(0))
+        b = np.ascontiguousarray(b, np.float64)
+        check(self.L.exf_coarse_solve(self.h, dptr(b), dptr(x)))
+        return x
+
+    def sync(self):
+        check(self.L.exf_sync(self.h))
+
+
+class MGSolT(MGSolBase):
+    """Temperature equation (MGSolT, template_appl/nse/SRC/MGSolverT.h)."""
+    kind = _lib.KIND_T
+
+
+class MGSolNS(MGSolBase):
+    """Coupled Navier-Stokes, Taylor-Hood Q2-Q1 (MGSolNS, NS_EQUATIONS==1)."""
+    kind = _lib.KIND_NS

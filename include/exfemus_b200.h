@@ -1,0 +1,188 @@
+/*
+ * exfemus_b200.h -- C ABI of the B200 assembly + geometric-multigrid library.
+ *
+ * The library replaces the LASPACK backend of exFEMuS's MGSolBase/MGSolDA path:
+ * element assembly (GenMatRhs), the level operators (ReadMatrix/ReadProl/ReadRest),
+ * and the multigrid solve (MGSolve/MGStep with its smoothers and coarse solve) run on
+ * one GPU.  Host code passes plain pointers and sizes; every call returns an EXF_*
+ * status and never aborts.  A mesh owns the structured multilevel hierarchy; a system
+ * (one per equation, like one MGSolBase object) owns its DOF map, boundary flags,
+ * level matrices, transfer operators and vectors in device memory.  One CUDA stream
+ * per system; a system is not thread-safe, independent systems are.
+ *
+ * Reference interfaces replaced (paths within danieleunibo/exfemus):
+ *   include/MGSolverBase.h:118-361   MGSolBase (MGDofBcOp, GenMatRhs, MGSolve, MGStep)
+ *   include/MGSolverDA.h             MGSolDA   (init_dof, GenBc, init, ReadProl, ReadRest)
+ *   contrib/matrix/sparse_matrixM.h  SparseMatrixM / SparseMMatrixM handles
+ *   contrib/matrix/numeric_vectorM.h:292-293  NumericVectorM::resid / matrix_mult
+ *   contrib/matrix/linear_solverM.h:84-157    LinearSolverM::solve / adjoint_solve
+ */
+#ifndef EXFEMUS_B200_H
+#define EXFEMUS_B200_H
+
+#if defined(__GNUC__)
+#define EXF_API __attribute__((visibility("default")))
+#else
+#define EXF_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- status */
+#define EXF_OK 0
+#define EXF_ERR_ARG 1           /* bad argument (null handle, size, level)          */
+#define EXF_ERR_CUDA 2          /* CUDA runtime error (message in exf_last_error)   */
+#define EXF_ERR_STATE 3         /* call order violated (e.g. solve before assembly) */
+#define EXF_ERR_DIVERGED 4      /* NaN/Inf residual during the multigrid solve      */
+#define EXF_ERR_NOT_CONVERGED 5 /* max_cycles reached above the tolerance           */
+#define EXF_ERR_SINGULAR 6      /* zero pivot in the coarsest direct factorisation  */
+#define EXF_ERR_NOMEM 7         /* device allocation failed                         */
+#define EXF_ERR_UNSUPPORTED 8   /* boundary flag or option not implemented         */
+
+/* system kinds: MGSolT (one quadratic variable) and coupled MGSolNS (NS_EQUATIONS==1:
+ * dim quadratic velocity components + one linear pressure) */
+#define EXF_KIND_T 0
+#define EXF_KIND_NS 1
+
+/* boundary-condition presets: the per-node bc_read rules of the workloads */
+#define EXF_BC_HEAT_DIRICHLET 1  /* T = 0 on every wall                              */
+#define EXF_BC_CAVITY 2          /* no-slip, u = 1 on the lid interior, p gauge node 0 */
+#define EXF_BC_CHANNEL 3         /* inlet x=0 prescribed, no-slip walls, natural outlet */
+#define EXF_BC_BOUSS_NS 4        /* no-slip on all walls, p gauge node 0             */
+#define EXF_BC_BOUSS_T 5         /* T prescribed on x=0 and x=1, adiabatic y walls   */
+
+/* smoothers */
+#define EXF_SMOOTH_GS 0          /* multi-colour Gauss-Seidel (scalar systems)      */
+#define EXF_SMOOTH_VANKA 1       /* multi-colour pressure-node Vanka (NS)           */
+
+/* precision of the V-cycle */
+#define EXF_PREC_FP64 0          /* everything FP64                                 */
+#define EXF_PREC_MIXED 1         /* FP32 V-cycle inside FP64 defect correction      */
+
+typedef struct {
+  int dim;          /* 2 (quad9/quad4) or 3 (hex27/hex8)                          */
+  int nlev;         /* geometric levels                                            */
+  int n0[3];        /* elements per direction on level 0                           */
+  double box[6];    /* x0,x1,y0,y1,z0,z1                                           */
+  int device;       /* CUDA device ordinal                                         */
+} exf_mesh_desc;
+
+typedef struct {
+  double inv_re;    /* _IRe (viscosity); heat diffusivity = inv_prdl*inv_re        */
+  double inv_prdl;  /* _IPrdl                                                      */
+  double rho;       /* density factor                                              */
+  double rhocp;     /* rho*cp                                                      */
+  double inv_dt;    /* 1/dt of the mass term (0 = steady)                          */
+  double penalty;   /* Dirichlet penalty scale: Ipenalty = det_side*penalty        */
+  double upwind_ns; /* UP_WIND_NS                                                  */
+  double upwind_t;  /* UP_WIND_T                                                   */
+  double ifr;       /* _IFr                                                        */
+  double dirg[3];   /* _dirg                                                       */
+  double buoy;      /* Boussinesq source coefficient: f += buoy*T*dirg             */
+} exf_phys;
+
+typedef struct {
+  double eps;          /* stop when ||b-Ax||/||b|| <= eps                          */
+  int max_cycles;
+  int gamma;           /* cycles per coarse visit (1 = V)                          */
+  int nu_pre, nu_post; /* smoothing sweeps                                         */
+  int double_below_top;/* 1: sweeps doubled below the top level (MGStep)           */
+  int smoother;        /* EXF_SMOOTH_*                                             */
+  double omega;        /* Vanka damping                                            */
+  double corr_damp;    /* coarse-correction factor (reference 0.95)                */
+  int cond_corr;       /* 1: reference's conditional coarse correction             */
+  int reverse_colours; /* 1: colours swept in reverse order                        */
+  int precision;       /* EXF_PREC_*                                               */
+  int use_graph;       /* 1: replay each V-cycle from a captured CUDA graph        */
+} exf_mg_params;
+
+typedef struct {
+  int cycles;
+  int converged;
+  double rel_res;
+  double bnorm;
+  double seconds;      /* device time of the solve (CUDA events on the system stream) */
+  double hist[256];    /* relative residual after each cycle                       */
+} exf_solve_stats;
+
+typedef struct exf_mesh exf_mesh;
+typedef struct exf_sys exf_sys;
+
+EXF_API const char *exf_last_error(void);
+EXF_API const char *exf_version(void);
+
+/* --- mesh: structured multilevel hierarchy (the restated gencase output) ------------
+ * replaces MGMesh::read_c (src/MGMesh.C:493-908) for generated boxes */
+EXF_API int exf_mesh_create(const exf_mesh_desc *desc, exf_mesh **out);
+EXF_API int exf_mesh_destroy(exf_mesh *m);
+EXF_API int exf_mesh_info(const exf_mesh *m, int lev, int *nnodes, int *nel, int *nvert0);
+EXF_API int exf_mesh_get_xyz(const exf_mesh *m, double *xyz);               /* [dim][ntop]    */
+EXF_API int exf_mesh_get_conn(const exf_mesh *m, int lev, int *conn, int *neigh, int *colour);
+
+/* --- system: MGSolBase::MGDofBcOp (src/MGSolverBase.C:139-159) --------------------- */
+EXF_API int exf_sys_create(exf_mesh *m, int kind, exf_sys **out);      /* init_dof + pattern   */
+EXF_API int exf_sys_destroy(exf_sys *s);
+EXF_API int exf_sys_ndof(const exf_sys *s, int lev, int *ndof);
+EXF_API int exf_sys_get_node_dof(const exf_sys *s, int lev, int *node_dof);   /* _node_dof[L] */
+EXF_API int exf_sys_bc_preset(exf_sys *s, int preset);                     /* GenBc            */
+EXF_API int exf_sys_set_bc(exf_sys *s, const int *bc0, const int *bc1);
+EXF_API int exf_sys_get_bc(const exf_sys *s, int *bc0, int *bc1);
+EXF_API int exf_sys_nnz(const exf_sys *s, int lev, long *nnz);
+EXF_API int exf_sys_get_pattern(exf_sys *s, int lev, int *rowptr, int *col); /* ReadMatrix    */
+/* transfer operators; pass NULL arrays to query nnz only */
+EXF_API int exf_sys_get_prol(exf_sys *s, int lev, long *nnz, int *rowptr, int *col, double *val);
+EXF_API int exf_sys_get_rest(exf_sys *s, int lev, long *nnz, int *rowptr, int *col, double *val);
+EXF_API int exf_sys_get_colours(exf_sys *s, int lev, int *ncolours, int *colour_of_item);
+/* coupling: T reads the NS velocity, NS reads T for buoyancy (get_el_sol of the
+ * other equation, src/MGSolverBase.C:336-354) */
+EXF_API int exf_sys_couple(exf_sys *s, exf_sys *other);
+
+/* --- fields (host buffers) ---------------------------------------------------------- */
+EXF_API int exf_sys_set_xold(exf_sys *s, const double *xold);   /* x_old[top]             */
+EXF_API int exf_sys_get_xold(exf_sys *s, double *xold);
+EXF_API int exf_sys_set_x(exf_sys *s, const double *x);         /* x[top]                 */
+EXF_API int exf_sys_get_x(exf_sys *s, double *x);
+EXF_API int exf_sys_xold_update(exf_sys *s);                    /* x_old[top] = x[top]    */
+EXF_API int exf_sys_set_source(exf_sys *s, const double *qe);   /* per top-level element  */
+EXF_API int exf_sys_set_rhs(exf_sys *s, const double *b);
+EXF_API int exf_sys_get_rhs(exf_sys *s, double *b);
+
+/* --- assembly: GenMatRhs (MGSolverNS.C:108-717, MGSolverT.C:93-525) ----------------- */
+EXF_API int exf_gen_mat_rhs(exf_sys *s, const exf_phys *ph, int lev, int mode);
+EXF_API int exf_assemble_all(exf_sys *s, const exf_phys *ph);   /* top mode 1, others mode 0 */
+EXF_API int exf_get_matrix(exf_sys *s, int lev, double *val);   /* values in pattern order  */
+EXF_API int exf_set_matrix(exf_sys *s, int lev, const double *val);
+
+/* --- solve: MGSolve / MGStep (src/MGSolverBase.C:163-289) on device state ------------- */
+EXF_API int exf_mg_solve(exf_sys *s, const exf_mg_params *p, exf_solve_stats *st);
+/* unit-level operations on host buffers (NumericVectorM::resid / matrix_mult);
+ * exf_resid with b == NULL returns r = A x */
+EXF_API int exf_resid(exf_sys *s, int lev, const double *x, const double *b, double *r);
+EXF_API int exf_restrict(exf_sys *s, int lev, const double *r_fine, double *b_coarse); /* lev = coarse */
+EXF_API int exf_prolong(exf_sys *s, int lev, const double *x_coarse, double *y_fine);  /* lev = fine   */
+EXF_API int exf_smooth(exf_sys *s, int lev, const exf_mg_params *p, int nsweeps, double *x, const double *b);
+EXF_API int exf_coarse_solve(exf_sys *s, const double *b, double *x);
+EXF_API int exf_sys_transpose(exf_sys *s);                      /* A[L] <- A[L]^T, all levels */
+
+/* --- discrete adjoint of the T solve (LinearSolverM::adjoint_solve semantics) ------------
+ * forward: assemble all levels with the current x_old/sources and solve A T = b.
+ * backward: solve A^T lambda = dJ/dT on the transposed hierarchy (colours reversed) and
+ * return dJ/dq_e (per top element) and dJ/dg (per top DOF: derivative with respect to
+ * the Dirichlet data value held in x_old at Dirichlet DOFs). */
+EXF_API int exf_adjoint_forward(exf_sys *s, const exf_phys *ph, const exf_mg_params *p, exf_solve_stats *st);
+EXF_API int exf_adjoint_backward(exf_sys *s, const exf_phys *ph, const exf_mg_params *p, const double *djdx,
+                         double *djdq, double *djdg, exf_solve_stats *st);
+
+/* --- timing of one kernel class on device-resident data (CUDA events) -----------------
+ * what: 0 = SpMV residual, 1 = smoother sweep, 2 = assembly (all levels), 3 = V-cycle;
+ * avg_ms = average duration per launch group over reps, precision per exf_mg_params */
+EXF_API int exf_time_op(exf_sys *s, int what, int lev, const exf_mg_params *p, const exf_phys *ph, int reps,
+                double *avg_ms);
+EXF_API int exf_sync(exf_sys *s);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -321,6 +321,12 @@ static void fe_init(fe_tab *t, int dim) {
   }
 }
 
+void or_side_table(int dim, int *out) {
+  int ns = dim == 2 ? 4 : 6, nn = dim == 2 ? 3 : 9;
+  for (int s = 0; s < ns; s++)
+    for (int k = 0; k < nn; k++) out[s * nn + k] = dim == 2 ? Q9_SIDE[s][k] : H27_FACE[s][k];
+}
+
 void or_fe_tables(int dim, double *phi_q, double *dphi_q, double *phi_l, double *w) {
   fe_tab t;
   fe_init(&t, dim);

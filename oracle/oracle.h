@@ -110,6 +110,8 @@ void or_smooth(or_sys *s, int lev, const or_mg_params *p, int nsweeps, double *x
 
 /* FE tables (for golden checks): Q2/Q1 shape values at the Gauss points. */
 void or_fe_tables(int dim, double *phi_q, double *dphi_q, double *phi_l, double *w);
+/* side -> local node table (the restated _surf_top) */
+void or_side_table(int dim, int *out);
 
 #ifdef __cplusplus
 }

@@ -87,6 +87,7 @@ def oracle_lib():
         L.or_coarse_solve.argtypes = [P, dp, dp]
         L.or_smooth.argtypes = [P, I, C.POINTER(OrMgParams), I, dp, dp]
         L.or_fe_tables.argtypes = [I, dp, dp, dp, dp]
+        L.or_side_table.argtypes = [I, ip]
         _LIB = L
     return _LIB
 

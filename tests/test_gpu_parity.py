@@ -1,0 +1,181 @@
+"""GPU parity against the CPU oracle through the C ABI (needs a B200).
+
+Integer work (mesh tables, DOF maps, boundary flags, sparsity pattern, colouring,
+transfer operators) must be bit-exact; FP64 matrix and rhs entries within 1e-12
+relative; solver operations within 1e-12; solutions within 1e-9 relative L2.
+"""
+import numpy as np
+import pytest
+
+import exfemus_b200 as ex
+from exfemus_b200 import _lib
+
+from conftest import or_mg, rel
+from gpu_cases import CASES, make
+
+pytestmark = pytest.mark.gpu
+
+NAMES = list(CASES)
+
+
+@pytest.fixture(scope="module", params=NAMES)
+def case(request, oracle_mod, gpu_lib):
+    c = make(request.param, oracle_mod)
+    c["name"] = request.param
+    return c
+
+
+def test_mesh_tables_bit_exact(case):
+    gm, om = case["gm"], case["om"]
+    assert np.array_equal(gm.xyz(), om.xyz())
+    for lev in range(case["nlev"]):
+        gc, gn, gcol = gm.conn(lev)
+        oc, on, ocol = om.conn(lev)
+        assert np.array_equal(gc, oc) and np.array_equal(gn, on) and np.array_equal(gcol, ocol)
+
+
+def test_dof_map_and_bc_bit_exact(case):
+    gs, os_ = case["gs"], case["os"]
+    for lev in range(case["nlev"]):
+        assert gs.ndof(lev) == os_.ndof(lev)
+        assert np.array_equal(gs.node_dof(lev), os_.node_dof(lev))
+    g0, g1 = gs.bc()
+    o0, o1 = os_.bc()
+    assert np.array_equal(g0, o0) and np.array_equal(g1, o1)
+
+
+def test_pattern_bit_exact(case):
+    for lev in range(case["nlev"]):
+        grp, gcol = case["gs"].pattern(lev)
+        orp, ocol = case["os"].pattern(lev)
+        assert np.array_equal(grp, orp) and np.array_equal(gcol, ocol)
+
+
+def test_colouring_bit_exact(case):
+    for lev in range(case["nlev"]):
+        gn, gc = case["gs"].colours(lev)
+        on, oc = case["os"].colours(lev)
+        assert gn == on and np.array_equal(gc, oc)
+
+
+def test_transfers_bit_exact(case):
+    gs, os_ = case["gs"], case["os"]
+    for lev in range(1, case["nlev"]):
+        for a, b in zip(gs.prol(lev), os_.prol(lev)):
+            assert np.array_equal(a, b)
+    for lev in range(case["nlev"] - 1):
+        for a, b in zip(gs.rest(lev), os_.rest(lev)):
+            assert np.array_equal(a, b)
+
+
+def _assemble_both(case):
+    gs, os_ = case["gs"], case["os"]
+    gs.assemble_all()
+    os_.assemble_all(case["oph"], xold=case["xold"], qe=case["qe"])
+
+
+def test_assembly_matches_oracle(case):
+    _assemble_both(case)
+    gs, os_ = case["gs"], case["os"]
+    for lev in range(case["nlev"]):
+        g, o = gs.matrix(lev), os_.matrix(lev)
+        assert np.abs(g - o).max() <= 1e-12 * np.abs(o).max(), (lev, np.abs(g - o).max())
+    g, o = gs.rhs(), os_.rhs()
+    assert np.abs(g - o).max() <= 1e-12 * max(np.abs(o).max(), 1e-300)
+
+
+def test_solver_operations_match_oracle(case):
+    _assemble_both(case)
+    gs, os_ = case["gs"], case["os"]
+    rng = np.random.default_rng(3)
+    top = case["nlev"] - 1
+    for lev in range(case["nlev"]):
+        x = rng.standard_normal(gs.ndof(lev))
+        assert rel(gs.spmv(lev, x), os_.spmv(lev, x)) < 1e-13
+    for lev in range(top):
+        r = rng.standard_normal(gs.ndof(lev + 1))
+        rp, col, val = os_.rest(lev)
+        import scipy.sparse as sp
+        R = sp.csr_matrix((val, col, rp), shape=(os_.ndof(lev), os_.ndof(lev + 1)))
+        assert rel(gs.restrict(lev, r), R @ r) < 1e-14
+        xc = rng.standard_normal(gs.ndof(lev))
+        rp, col, val = os_.prol(lev + 1)
+        P = sp.csr_matrix((val, col, rp), shape=(os_.ndof(lev + 1), os_.ndof(lev)))
+        assert rel(gs.prolong(lev + 1, xc), P @ xc) < 1e-14
+
+
+def test_smoother_sweep_matches_oracle(case, oracle_mod):
+    _assemble_both(case)
+    gs, os_ = case["gs"], case["os"]
+    rng = np.random.default_rng(5)
+    ns = case["kind"] == 1
+    smoother = _lib.SMOOTH_VANKA if ns else _lib.SMOOTH_GS
+    for rev in (0, 1):
+        for lev in range(1, case["nlev"]):
+            x = rng.standard_normal(gs.ndof(lev))
+            b = rng.standard_normal(gs.ndof(lev))
+            gp = ex.mg_params(smoother=smoother, omega=0.4, reverse_colours=rev)
+            op = or_mg(oracle_mod, smoother=1 if ns else 0, omega=0.4, reverse_colours=rev)
+            xg = gs.smooth(lev, gp, 2, x, b)
+            xo = os_.smooth(lev, op, 2, x, b)
+            assert rel(xg, xo) < 1e-12, (lev, rev, rel(xg, xo))
+
+
+def test_coarse_direct_solve(case):
+    _assemble_both(case)
+    gs, os_ = case["gs"], case["os"]
+    b = np.random.default_rng(9).standard_normal(gs.ndof(0))
+    assert rel(gs.coarse_solve(b), os_.coarse_solve(b)) < 1e-10
+
+
+def test_multigrid_fp64_matches_oracle_per_cycle(case, oracle_mod):
+    _assemble_both(case)
+    gs, os_ = case["gs"], case["os"]
+    ns = case["kind"] == 1
+    nu = (3, 3) if ns else (2, 2)
+    gp = ex.mg_params(eps=1e-11, max_cycles=80, nu_pre=nu[0], nu_post=nu[1],
+                      smoother=_lib.SMOOTH_VANKA if ns else _lib.SMOOTH_GS, omega=0.4)
+    op = or_mg(oracle_mod, eps=1e-11, max_cycles=80, nu_pre=nu[0], nu_post=nu[1], smoother=1 if ns else 0,
+               omega=0.4)
+    x0 = case["xold"]
+    gs.set_x(x0)
+    st = gs.solve(gp)
+    xo, sto = os_.mg_solve(op, x0=x0)
+    assert st.converged and sto.converged
+    assert st.cycles == sto.cycles
+    hist_g = np.array(st.hist[:st.cycles])
+    hist_o = np.array(sto.hist[:sto.cycles])
+    assert np.all(np.abs(hist_g - hist_o) <= 1e-6 * hist_o + 1e-14)
+    assert rel(gs.x(), xo) < 1e-9
+
+
+def test_mixed_precision_matches_fp64_oracle(case, oracle_mod):
+    _assemble_both(case)
+    gs, os_ = case["gs"], case["os"]
+    ns = case["kind"] == 1
+    nu = (3, 3) if ns else (2, 2)
+    gp = ex.mg_params(eps=1e-12, max_cycles=120, nu_pre=nu[0], nu_post=nu[1],
+                      smoother=_lib.SMOOTH_VANKA if ns else _lib.SMOOTH_GS, omega=0.4,
+                      precision=_lib.PREC_MIXED)
+    op = or_mg(oracle_mod, eps=1e-13, max_cycles=150, nu_pre=nu[0], nu_post=nu[1], smoother=1 if ns else 0,
+               omega=0.4)
+    x0 = case["xold"]
+    gs.set_x(x0)
+    st = gs.solve(gp)
+    xo, sto = os_.mg_solve(op, x0=x0)
+    assert st.converged and st.rel_res <= 1e-12
+    assert rel(gs.x(), xo) < 1e-9
+
+
+def test_solve_is_deterministic(case):
+    _assemble_both(case)
+    gs = case["gs"]
+    ns = case["kind"] == 1
+    outs = []
+    for _ in range(2):
+        gs.set_x(case["xold"])
+        gs.solve(ex.mg_params(eps=1e-10, max_cycles=60, nu_pre=3 if ns else 2, nu_post=3 if ns else 2,
+                              smoother=_lib.SMOOTH_VANKA if ns else _lib.SMOOTH_GS, omega=0.4,
+                              precision=_lib.PREC_MIXED))
+        outs.append(gs.x())
+    assert np.array_equal(outs[0], outs[1])
