@@ -1,0 +1,393 @@
+"""Benchmark of the assembly + geometric-multigrid path on the 3D Taylor-Hood channel.
+
+Workload (channel3d): 4x1x1 box, hex27 velocity / hex8 pressure, 64x16x16 fine elements,
+4 levels (8x2x2 coarsest), mu = 0.01 (Re 100), parabolic inlet, no-slip walls, natural
+outlet.  One step = one Picard step: assembly of every level (GenMatRhs) + the
+mixed-precision multigrid solve to ||b-Ax||/||b|| <= 1e-10 + x_old update.  Data are
+synthetic (generated mesh and fields); the fine matrix (~1 GB FP64) exceeds L2, so every
+timed iteration streams from HBM.
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+N > 1 runs N independent replicas (one per GPU; the path does not shard), the time is the
+max over ranks.  --impl reference times the CPU path (the oracle restatement of the
+reference's MGSolve/MGStep with the same smoother, single core) on rank 0.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "secs to 1e-10 rel residual, mixed vs FP64 on GPU; V-cycle DOF/s; assembly Melem/s"
+WORKLOAD = "channel3d"
+# V-cycles the FP64 algorithm needs on the first Picard system of channel3d (identical
+# iterates on CPU and GPU, checked per cycle by the parity tests); used to scale the
+# bounded CPU sample to seconds-to-1e-10.
+CPU_CYCLES_TO_TOL = 32
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default=WORKLOAD)
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--mode", default="bench", choices=["bench", "vcycle"],
+                    help="vcycle: assemble once and run one mixed and one FP64 V-cycle (profiling case)")
+    return ap.parse_args()
+
+
+def dist_setup(backend):
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group(backend=backend, timeout=datetime.timedelta(seconds=600))
+    return ws, rank, local
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.th = threading.Thread(target=self._read, daemon=True)
+            self.th.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.th.join(timeout=2)
+        sm = [float(r[1]) for r in self.rows if len(r) >= 9 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) >= 9 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in self.rows:
+            if len(r) >= 9:
+                for k, n in enumerate(names):
+                    if r[5 + k].lower().startswith("active"):
+                        reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def read_traffic():
+    """dram bytes per launch of the top kernel from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", "vanka_channel3d_traffic.txt")
+    out = {}
+    if os.path.exists(path):
+        for line in open(path):
+            if "=" in line and not line.startswith("#"):
+                k, v = line.split("=", 1)
+                try:
+                    out[k.strip()] = float(v)
+                except ValueError:
+                    pass
+    return out
+
+
+def measured_peak():
+    try:
+        d = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        return float(d["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def cpu_reference(w_over=None, ncycles=1, assemble=True):
+    """Oracle (restated MGSolve/MGStep, FP64, one core) on the channel3d system."""
+    import oracle
+    from exfemus_b200 import workloads
+    from exfemus_b200._lib import BC_CHANNEL
+    oracle.build()
+    w = dict(workloads.WORKLOADS[WORKLOAD])
+    if w_over:
+        w.update(w_over)
+    m = oracle.OrMesh(w["dim"], w["nlev"], w["n0"], w["box"])
+    s = oracle.OrSys(m, 1)
+    s.bc_preset(BC_CHANNEL)
+    top = w["nlev"] - 1
+    x0 = workloads.ns_initial(w, m.xyz(), m.ntop, s.ndof(top))
+    ph = oracle.OrPhys()
+    ph.inv_re = w["phys"]["inv_re"]
+    ph.inv_prdl = ph.rho = ph.rhocp = ph.penalty = 1.0
+    ph.upwind_ns, ph.upwind_t = 0.1, 1.0
+    t0 = time.perf_counter()
+    s.assemble_all(ph, xold=x0)
+    t_asm = time.perf_counter() - t0
+    mp = oracle.OrMgParams()
+    mp.eps, mp.max_cycles, mp.gamma, mp.nu_pre, mp.nu_post = 1e-30, ncycles, 1, 3, 3
+    mp.double_below_top, mp.smoother, mp.omega, mp.corr_damp = 1, 1, workloads.VANKA_OMEGA, 0.95
+    t0 = time.perf_counter()
+    s.mg_solve(mp, x0=x0)
+    t_cyc = (time.perf_counter() - t0) / ncycles
+    nel = sum(m.nel(l) for l in range(w["nlev"]))
+    return dict(t_asm=t_asm, t_cycle=t_cyc, nel=nel, ndof=s.ndof(top), sys=s, mp=mp, x0=x0)
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return
+    import oracle
+    oracle.build()
+    ref = cpu_reference(ncycles=1)
+    s, mp, x0 = ref["sys"], ref["mp"], ref["x0"]
+    for _ in range(args.warmup):
+        s.mg_solve(mp, x0=x0)
+    times = []
+    t_all = time.perf_counter()
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        s.mg_solve(mp, x0=x0)
+        times.append(time.perf_counter() - t0)
+    wall = time.perf_counter() - t_all
+    t_cycle = float(np.mean(times))
+    value = t_cycle * CPU_CYCLES_TO_TOL
+    sample = ("one FP64 V-cycle (3/3 Vanka sweeps, doubled below the top, direct coarse solve) of the "
+              "first Picard system per step, x %d cycles to 1e-10; assembly of all levels %.2f s" %
+              (CPU_CYCLES_TO_TOL, ref["t_asm"]))
+    line = {"metric": METRIC, "value": value, "unit": "s", "impl": "reference", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * wall / args.steps,
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": {"workload": WORKLOAD, "mesh": "64x16x16 hex27/hex8, 4 levels",
+                                            "ndof": ref["ndof"]},
+            "cpu_baseline": {"value": value, "unit": "s", "cores": 1, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "assembly_melem_per_s": ref["nel"] / ref["t_asm"] / 1e6,
+            "vcycle_dof_per_s": ref["ndof"] / t_cycle}
+    print(json.dumps(line), flush=True)
+
+
+def run_vcycle(args, local):
+    """One assembly and one V-cycle per precision on the workload (kernel profiling)."""
+    import exfemus_b200 as ex
+    from exfemus_b200 import _lib
+    case = ex.make_case(args.workload, device=local)
+    ns = case["NS"]
+    ns.assemble_all()
+    for prec in (_lib.PREC_MIXED, _lib.PREC_FP64):
+        p = case["mg_NS"]
+        p.precision, p.max_cycles = prec, 1
+        st = ns.solve(p)
+        print("precision %d: 1 cycle, rel %.3e, %.3f ms" % (prec, st.rel_res, st.seconds * 1e3), flush=True)
+
+
+def run_ours(args, ws, rank, local):
+    import exfemus_b200 as ex
+    from exfemus_b200 import _lib
+
+    L = ex.load()
+    if args.mode == "vcycle":
+        return run_vcycle(args, local)
+    case = ex.make_case(args.workload, device=local)
+    w = case["w"]
+    ns = case["NS"]
+    top = w["nlev"] - 1
+    mg_mixed = case["mg_NS"]
+    mg_mixed.precision = _lib.PREC_MIXED
+    mg_mixed.eps = 1e-10
+    mg_fp64 = ex.mg_params(**{f[0]: getattr(mg_mixed, f[0]) for f in mg_mixed._fields_})
+    mg_fp64.precision = _lib.PREC_FP64
+
+    def picard_step():
+        ns.assemble_all()
+        st = ns.solve(mg_mixed)
+        if not st.converged:
+            raise RuntimeError("solve did not converge: rel %.3e after %d cycles" % (st.rel_res, st.cycles))
+        ns.xold_update()
+        return st
+
+    for _ in range(args.warmup):
+        picard_step()
+    ns.sync()
+    barrier(ws)
+    clocks = ClockSampler(local)
+    clocks.start()
+    n0 = L.exf_launch_count()
+    _lib.check(L.exf_event_record(ns.h, 0))
+    solve_s, cycles = [], []
+    for _ in range(args.steps):
+        st = picard_step()
+        solve_s.append(st.seconds)
+        cycles.append(st.cycles)
+    _lib.check(L.exf_event_record(ns.h, 1))
+    ns.sync()
+    import ctypes as C
+    msv = C.c_double()
+    _lib.check(L.exf_event_elapsed(ns.h, 0, 1, C.byref(msv)))
+    launches = L.exf_launch_count() - n0
+    clk = clocks.stop()
+    step_ms = msv.value / args.steps
+    secs_mixed = float(np.mean(solve_s))
+    secs_mixed_max = max_over_ranks(ws, secs_mixed)
+    step_ms = max_over_ranks(ws, step_ms)
+
+    # mixed vs FP64 on the next Picard system, same initial guess
+    ns.assemble_all()
+    x0 = ns.x()
+    res = {}
+    sols = {}
+    for name, p in (("fp64", mg_fp64), ("mixed", mg_mixed)):
+        ts = []
+        for _ in range(2):
+            ns.set_x(x0)
+            st = ns.solve(p)
+            ts.append(st.seconds)
+            res[name + "_cycles"] = st.cycles
+        res[name] = float(np.mean(ts))
+        sols[name] = ns.x()
+    tight = ex.mg_params(**{f[0]: getattr(mg_fp64, f[0]) for f in mg_fp64._fields_})
+    tight.eps, tight.max_cycles = 1e-13, 400
+    ns.set_x(x0)
+    ns.solve(tight)
+    x_ref = ns.x()
+    err_mixed = float(np.linalg.norm(sols["mixed"] - x_ref) / np.linalg.norm(x_ref))
+    err_fp64 = float(np.linalg.norm(sols["fp64"] - x_ref) / np.linalg.norm(x_ref))
+    ns.set_x(sols["mixed"])
+
+    # kernel-level figures (device-resident, CUDA events on the system stream)
+    tv = C.c_double()
+    _lib.check(L.exf_time_op(ns.h, 3, top, C.byref(mg_mixed), C.byref(ns.phys), 3, C.byref(tv)))
+    vcycle_ms = tv.value
+    _lib.check(L.exf_time_op(ns.h, 2, top, C.byref(mg_mixed), C.byref(ns.phys), 3, C.byref(tv)))
+    asm_ms = tv.value
+    _lib.check(L.exf_time_op(ns.h, 1, top, C.byref(mg_mixed), C.byref(ns.phys), 5, C.byref(tv)))
+    sweep_ms = tv.value
+    _lib.check(L.exf_time_op(ns.h, 0, top, C.byref(mg_mixed), C.byref(ns.phys), 20, C.byref(tv)))
+    spmv32_ms = tv.value
+    _lib.check(L.exf_time_op(ns.h, 0, top, C.byref(mg_fp64), C.byref(ns.phys), 20, C.byref(tv)))
+    spmv64_ms = tv.value
+    b_spmv32, b_sweep32 = C.c_double(), C.c_double()
+    _lib.check(L.exf_level_bytes(ns.h, top, _lib.PREC_MIXED, C.byref(b_spmv32), C.byref(b_sweep32)))
+    b_spmv64, dummy = C.c_double(), C.c_double()
+    _lib.check(L.exf_level_bytes(ns.h, top, _lib.PREC_FP64, C.byref(b_spmv64), C.byref(dummy)))
+    ndof = ns.ntop_dof
+    nel = sum(case["mesh"].nel(l) for l in range(w["nlev"]))
+    peak, peak_kind = measured_peak()
+    achieved = b_sweep32.value / (sweep_ms * 1e-3) / 1e9
+    tr = read_traffic()
+
+    # end to end through the public API with host buffers (pinned) and host results
+    import torch
+    xo_host = torch.empty(ndof, dtype=torch.float64).pin_memory()
+    xo_host.numpy()[:] = ns.xold()
+    out_host = torch.empty(ndof, dtype=torch.float64).pin_memory()
+    e2e = []
+    for _ in range(args.e2e_steps):
+        _lib.check(L.exf_event_record(ns.h, 2))
+        _lib.check(L.exf_sys_set_xold(ns.h, _lib.dptr(xo_host.numpy())))
+        ns.assemble_all()
+        st = ns.solve(mg_mixed)
+        _lib.check(L.exf_sys_get_x(ns.h, _lib.dptr(out_host.numpy())))
+        _lib.check(L.exf_event_record(ns.h, 3))
+        _lib.check(L.exf_event_elapsed(ns.h, 2, 3, C.byref(tv)))
+        e2e.append(tv.value * 1e-3)
+    e2e_s = max_over_ranks(ws, float(np.mean(e2e)))
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        ref = cpu_reference(ncycles=1)
+        cpu = {"value": ref["t_cycle"] * res["fp64_cycles"], "unit": "s", "cores": 1, "kind": "port",
+               "sample": "oracle FP64 restatement, one V-cycle of the first Picard system (%.2f s) x %d cycles "
+                         "the identical GPU FP64 path needed; CPU assembly of all levels %.2f s"
+                         % (ref["t_cycle"], res["fp64_cycles"], ref["t_asm"])}
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": secs_mixed_max, "unit": "s", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 V-cycle / f64 defect correction", "data": "synthetic",
+            "config": {"workload": args.workload, "mesh": "64x16x16 hex27/hex8, 4 levels (8x2x2 coarsest)",
+                       "ndof": ndof, "nnz_fine": ns.nnz(top), "picard_step": "assembly all levels + mixed solve "
+                       "to 1e-10 + x_old update", "l2": "inputs larger than L2 (fine matrix %.2f GB FP64)"
+                       % (b_spmv64.value / 1e9), "parallelism": "replicas" if ws > 1 else "single GPU"},
+            "secs_fp64": res["fp64"], "secs_mixed": res["mixed"], "speedup_mixed_vs_fp64": res["fp64"] / res["mixed"],
+            "cycles_fp64": res["fp64_cycles"], "cycles_mixed": res["mixed_cycles"],
+            "err_mixed_vs_fp64_1e-13": err_mixed, "err_fp64_1e-10_vs_fp64_1e-13": err_fp64,
+            "vcycle_dof_per_s": ndof / (vcycle_ms * 1e-3), "vcycle_ms": vcycle_ms,
+            "assembly_melem_per_s": nel / (asm_ms * 1e-3) / 1e6, "assembly_ms": asm_ms,
+            "spmv_fp32_gbs": b_spmv32.value / (spmv32_ms * 1e-3) / 1e9,
+            "spmv_fp64_gbs": b_spmv64.value / (spmv64_ms * 1e-3) / 1e9,
+            "roofline": {"kernel": "k_vanka_patch+k_vanka_apply (FP32 sweep, fine level)", "bound": "hbm",
+                         "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "peak_kind": peak_kind, "algorithmic_bytes": b_sweep32.value, "sweep_ms": sweep_ms,
+                         "traffic": tr.get("dram_bytes_per_sweep")},
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": ndof * 8, "d2h_bytes_per_step": ndof * 8,
+                    "what": "host x_old -> GenMatRhs all levels -> mixed MGSolve to 1e-10 -> host x"},
+            "gpu_launches": int(launches),
+            "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+
+
+def barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(ws, v):
+    if ws == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        ws, rank, local = dist_setup("gloo")
+        run_reference(args, rank)
+    else:
+        ws, rank, local = dist_setup("nccl")
+        if ws > 1:
+            import torch
+            torch.cuda.set_device(local)
+        run_ours(args, ws, rank, local)
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -17,6 +17,8 @@
 namespace exf {
 
 static thread_local char g_err[512] = "";
+static unsigned long long g_launches = 0;
+void count_launch(int n) { __atomic_add_fetch(&g_launches, (unsigned long long)n, __ATOMIC_RELAXED); }
 void set_error(const char *fmt, ...) {
   va_list ap;
   va_start(ap, fmt);
@@ -84,7 +86,10 @@ __global__ void k_d2f(const double *a, float *b, long n) {
 int sync_fp32(exf_sys *s, int lev) {
   SysLevel &L = s->L[lev];
   auto cp = [&](const DBuf<double> &a, DBuf<float> &b) {
-    if (a.p && b.p) k_d2f<<<nblk(a.n, 256), 256, 0, s->stream>>>(a.p, b.p, a.n);
+    if (a.p && b.p) {
+      k_d2f<<<nblk(a.n, 256), 256, 0, s->stream>>>(a.p, b.p, a.n);
+      EXF_COUNT(1);
+    }
   };
   cp(L.A.vv, L.A32.vv);
   cp(L.A.vp, L.A32.vp);
@@ -247,6 +252,23 @@ using namespace exf;
 extern "C" {
 
 const char *exf_last_error(void) { return g_err; }
+long long exf_launch_count(void) { return (long long)__atomic_load_n(&g_launches, __ATOMIC_RELAXED); }
+
+int exf_event_record(exf_sys *s, int slot) {
+  if (!s || slot < 0 || slot >= 8) return EXF_ERR_ARG;
+  if (!s->user_ev[slot]) EXF_CUDA(cudaEventCreate(&s->user_ev[slot]));
+  EXF_CUDA(cudaEventRecord(s->user_ev[slot], s->stream));
+  return EXF_OK;
+}
+
+int exf_event_elapsed(exf_sys *s, int a, int b, double *ms) {
+  if (!s || !ms || a < 0 || a >= 8 || b < 0 || b >= 8 || !s->user_ev[a] || !s->user_ev[b]) return EXF_ERR_ARG;
+  EXF_CUDA(cudaEventSynchronize(s->user_ev[b]));
+  float f = 0.f;
+  EXF_CUDA(cudaEventElapsedTime(&f, s->user_ev[a], s->user_ev[b]));
+  *ms = f;
+  return EXF_OK;
+}
 const char *exf_version(void) { return "exfemus_b200 1.0 (sm_100a)"; }
 
 int exf_mesh_create(const exf_mesh_desc *desc, exf_mesh **out) {
@@ -394,6 +416,8 @@ int exf_sys_destroy(exf_sys *s) {
     if (s->graph[k]) cudaGraphExecDestroy(s->graph[k]);
   if (s->stream) cudaStreamSynchronize(s->stream);
   s->L.clear();
+  for (int k = 0; k < 8; k++)
+    if (s->user_ev[k]) cudaEventDestroy(s->user_ev[k]);
   if (s->ev0) cudaEventDestroy(s->ev0);
   if (s->ev1) cudaEventDestroy(s->ev1);
   if (s->stream) cudaStreamDestroy(s->stream);
@@ -905,6 +929,48 @@ int exf_time_op(exf_sys *s, int what, int lev, const exf_mg_params *p, const exf
   *avg_ms = ms / reps;
   if (what == 2)
     for (int l = 0; l < s->nlev; l++) EXF_TRY(sync_fp32(s, l));
+  return EXF_OK;
+}
+
+// algorithmic bytes of one level operation in the node-block layout (value bytes vb):
+// spmv   every block once (d*d values + one index), every B/B^T entry once, row pointers,
+//        x read, r written, b read;
+// sweep  one Vanka sweep: each pressure patch reads the rows of every velocity node of its
+//        star (the colour schedule re-reads a node once per star containing it), its own
+//        pressure row, b and x of its DOFs and writes x; a Gauss-Seidel sweep reads A once.
+int exf_level_bytes(exf_sys *s, int lev, int precision, double *spmv_bytes, double *sweep_bytes) {
+  CHECK_LEV(s, lev);
+  SysLevel &L = s->L[lev];
+  const double vb = precision == EXF_PREC_MIXED ? 4. : 8.;
+  const int d = s->nv2;
+  std::vector<int> qp(L.N + 1), lp(L.N + 1), qc(L.nqq);
+  EXF_CUDA(cudaMemcpy(qp.data(), L.qq_ptr.p, (L.N + 1) * sizeof(int), cudaMemcpyDeviceToHost));
+  EXF_CUDA(cudaMemcpy(lp.data(), L.ql_ptr.p, (L.N + 1) * sizeof(int), cudaMemcpyDeviceToHost));
+  EXF_CUDA(cudaMemcpy(qc.data(), L.qq_col.p, L.nqq * sizeof(int), cudaMemcpyDeviceToHost));
+  auto vrow = [&](int n) {  // bytes of the d velocity rows of node n
+    return (double)(qp[n + 1] - qp[n]) * (d * d * vb + 4.) + (double)(lp[n + 1] - lp[n]) * (d * vb + 4.) + 8.;
+  };
+  auto prow = [&](int m) {
+    return (double)(qp[m + 1] - qp[m]) * (d * vb) + (double)(lp[m + 1] - lp[m]) * vb + 4.;
+  };
+  double A = 0.;
+  for (int n = 0; n < L.N; n++) A += vrow(n);
+  if (s->nv1)
+    for (int m = 0; m < L.NL; m++) A += prow(m);
+  const double vec = (double)L.ndof * vb;
+  if (spmv_bytes) *spmv_bytes = A + 3. * vec;
+  if (sweep_bytes) {
+    if (s->kind == EXF_KIND_T) {
+      *sweep_bytes = A + 3. * vec;
+    } else {
+      double B = 0.;
+      for (int m = 0; m < L.NL; m++) {
+        for (int k = qp[m]; k < qp[m + 1]; k++) B += vrow(qc[k]) + 3. * d * vb;  // rows + b, x read/write
+        B += prow(m) + 3. * vb;
+      }
+      *sweep_bytes = B;
+    }
+  }
   return EXF_OK;
 }
 

@@ -534,6 +534,7 @@ static int assemble_dim(exf_sys *s, const exf_phys *ph, int lev, int mode) {
     a.nel_c = n;
     k_assemble<DIM, NT><<<n, NT, 0, st>>>(a, mode);
     EXF_LAUNCH_CHECK();
+    EXF_COUNT(1);
   }
   return EXF_OK;
 }

@@ -25,6 +25,8 @@
 namespace exf {
 
 void set_error(const char *fmt, ...);
+void count_launch(int n);  // kernels launched by the library (all streams)
+#define EXF_COUNT(n) exf::count_launch(n)
 
 #define EXF_CUDA(call)                                                                 \
   do {                                                                                 \
@@ -186,6 +188,7 @@ struct exf_sys {
   exf_sys *other = nullptr;                 // coupled system (T <- NS velocity, NS <- T)
   exf::Partials red;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  cudaEvent_t user_ev[8] = {nullptr};
   // captured V-cycle graphs (per precision)
   cudaGraphExec_t graph[2] = {nullptr, nullptr};
   unsigned long long graph_key[2] = {0, 0};

@@ -168,9 +168,11 @@ static int launch_spmv(exf_sys *s, int lev, const T *x, const T *b, T *r, double
       L.N, L.NL, L.qq_ptr.p, L.qq_col.p, L.ql_ptr.p, L.ql_col.p, L.nqq, L.nql, L.nqqL, VT<T>::vv(L), VT<T>::vp(L),
       VT<T>::pv(L), VT<T>::pp(L), x, b, r, d_norm2 ? s->red.part.p : nullptr);
   EXF_LAUNCH_CHECK();
+  EXF_COUNT(1);
   if (d_norm2) {
     k_reduce_partials<<<1, 1024, 0, s->stream>>>(s->red.part.p, grid, d_norm2);
     EXF_LAUNCH_CHECK();
+    EXF_COUNT(1);
   }
   return EXF_OK;
 }
@@ -218,6 +220,7 @@ int restrict_op(exf_sys *s, int lev_c, const T *r_f, T *b_c) {
       s->nv2, s->nv1, C.N, C.NL, F.N, C.Rq.ptr.p, C.Rq.col.p, VT<T>::pq(C.Rq), s->nv1 ? C.Rl.ptr.p : nullptr,
       s->nv1 ? C.Rl.col.p : nullptr, s->nv1 ? VT<T>::pq(C.Rl) : nullptr, C.rmask.p, r_f, b_c);
   EXF_LAUNCH_CHECK();
+  EXF_COUNT(1);
   return EXF_OK;
 }
 template int restrict_op<double>(exf_sys *, int, const double *, double *);
@@ -258,6 +261,7 @@ static int prolong_impl(exf_sys *s, int lev_f, const T *x_c, T *x_f, double damp
       s->nv2, s->nv1, F.N, F.NL, C.N, F.Pq.ptr.p, F.Pq.col.p, VT<T>::pq(F.Pq), s->nv1 ? F.Pl.ptr.p : nullptr,
       s->nv1 ? F.Pl.col.p : nullptr, s->nv1 ? VT<T>::pq(F.Pl) : nullptr, x_c, x_f, (T)damp, overwrite, cond);
   EXF_LAUNCH_CHECK();
+  EXF_COUNT(1);
   return EXF_OK;
 }
 template <class T>
@@ -445,6 +449,7 @@ static int vanka_sweep(exf_sys *s, int lev, const exf_mg_params *p, T *x, const 
         VT<T>::vv(L), VT<T>::vp(L), VT<T>::pv(L), VT<T>::pp(L), x, b, dx, (T)p->omega);
     k_vanka_apply<T, D, NT><<<n, NT, 0, s->stream>>>(items, L.N, L.qq_ptr.p, L.qq_col.p, dx, x);
     EXF_LAUNCH_CHECK();
+    EXF_COUNT(2);
   }
   return EXF_OK;
 }
@@ -460,6 +465,7 @@ static int gs_sweep(exf_sys *s, int lev, const exf_mg_params *p, T *x, const T *
     k_gs_colour<T, LPR><<<nblk((long)n * LPR, 256), 256, 0, s->stream>>>(
         L.col_items.p + L.col_off[c], n, L.qq_ptr.p, L.qq_col.p, L.diag_pos.p, VT<T>::vv(L), b, x);
     EXF_LAUNCH_CHECK();
+    EXF_COUNT(1);
   }
   return EXF_OK;
 }
@@ -603,6 +609,7 @@ int coarse_apply(exf_sys *s, const T *b, T *x) {
   const int n = s->L[0].ndof;
   k_coarse_gemv<T><<<nblk(n, 8), 256, 0, s->stream>>>(s->coarse_inv.p, n, s->gmask0.p, b, x);
   EXF_LAUNCH_CHECK();
+  EXF_COUNT(1);
   return EXF_OK;
 }
 template int coarse_apply<double>(exf_sys *, const double *, double *);
@@ -620,11 +627,13 @@ __global__ void k_add_f2d(const float *a, double *b, long n) {
 int cast_d2f(cudaStream_t st, const double *a, float *b, long n) {
   k_cast_d2f<<<nblk(n, 256), 256, 0, st>>>(a, b, n);
   EXF_LAUNCH_CHECK();
+  EXF_COUNT(1);
   return EXF_OK;
 }
 int add_f2d(cudaStream_t st, const float *a, double *b, long n) {
   k_add_f2d<<<nblk(n, 256), 256, 0, st>>>(a, b, n);
   EXF_LAUNCH_CHECK();
+  EXF_COUNT(1);
   return EXF_OK;
 }
 
@@ -642,6 +651,7 @@ int norm2(exf_sys *s, const double *v, long n, double *d_out) {
   k_norm2_part<256><<<grid, 256, 0, s->stream>>>(v, n, s->red.part.p);
   k_reduce_partials<<<1, 1024, 0, s->stream>>>(s->red.part.p, grid, d_out);
   EXF_LAUNCH_CHECK();
+  EXF_COUNT(2);
   return EXF_OK;
 }
 
@@ -658,6 +668,7 @@ int gauge_shift(exf_sys *s, double *x) {
   k_gauge_read<<<1, 1, 0, s->stream>>>(p, s->gauge_node, s->red.out.p + 8);
   k_gauge_sub<<<nblk(T.NL, 256), 256, 0, s->stream>>>(p, T.NL, s->red.out.p + 8);
   EXF_LAUNCH_CHECK();
+  EXF_COUNT(2);
   return EXF_OK;
 }
 

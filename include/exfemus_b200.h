@@ -181,6 +181,13 @@ EXF_API int exf_adjoint_backward(exf_sys *s, const exf_phys *ph, const exf_mg_pa
 EXF_API int exf_time_op(exf_sys *s, int what, int lev, const exf_mg_params *p, const exf_phys *ph, int reps,
                 double *avg_ms);
 EXF_API int exf_sync(exf_sys *s);
+/* device-side timing marks on the system stream (8 slots) and the number of kernels the
+ * library has launched so far (all systems) */
+EXF_API int exf_event_record(exf_sys *s, int slot);
+EXF_API int exf_event_elapsed(exf_sys *s, int slot_a, int slot_b, double *ms);
+EXF_API long long exf_launch_count(void);
+/* algorithmic bytes of one residual (spmv) and one smoother sweep on level lev */
+EXF_API int exf_level_bytes(exf_sys *s, int lev, int precision, double *spmv_bytes, double *sweep_bytes);
 
 #ifdef __cplusplus
 }
