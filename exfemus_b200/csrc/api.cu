@@ -753,6 +753,75 @@ int exf_sys_transpose(exf_sys *s) {
 }
 
 // ------------------------------------------------------------------ solve
+// one outer cycle; leaves ||b - A x||^2 of the top level in *dnr
+static int cycle_body(exf_sys *s, const exf_mg_params *p, double *dnr) {
+  SysLevel &T = s->L[s->nlev - 1];
+  if (p->precision == EXF_PREC_MIXED) {
+    EXF_TRY(vcycle_mixed(s, p));
+    return spmv_resid<double>(s, s->nlev - 1, T.x.p, T.b.p, T.r.p, dnr);
+  }
+  return vcycle_fp64(s, p, dnr);
+}
+
+static unsigned long long params_key(const exf_mg_params *p) {
+  unsigned long long h = 1469598103934665603ull;
+  auto mix = [&](unsigned long long v) {
+    h ^= v;
+    h *= 1099511628211ull;
+  };
+  mix((unsigned long long)p->gamma);
+  mix((unsigned long long)p->nu_pre);
+  mix((unsigned long long)p->nu_post);
+  mix((unsigned long long)p->double_below_top);
+  mix((unsigned long long)p->smoother);
+  unsigned long long w, c;
+  memcpy(&w, &p->omega, 8);
+  memcpy(&c, &p->corr_damp, 8);
+  mix(w);
+  mix(c);
+  mix((unsigned long long)p->reverse_colours);
+  mix((unsigned long long)p->precision);
+  return h | 1ull;
+}
+
+static int cycle_graph(exf_sys *s, const exf_mg_params *p, double *dnr) {
+  const int gi = p->precision == EXF_PREC_MIXED ? 1 : 0;
+  const unsigned long long key = params_key(p);
+  if (!s->graph[gi] || s->graph_key[gi] != key || s->graph_epoch[gi] != s->buf_epoch) {
+    if (s->graph[gi]) {
+      cudaGraphExecDestroy(s->graph[gi]);
+      s->graph[gi] = nullptr;
+    }
+    cudaGraph_t g = nullptr;
+    const long long c0 = exf_launch_count();
+    EXF_CUDA(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+    int rc = cycle_body(s, p, dnr);
+    cudaError_t e = cudaStreamEndCapture(s->stream, &g);
+    if (rc != EXF_OK) {
+      if (g) cudaGraphDestroy(g);
+      return rc;
+    }
+    if (e != cudaSuccess) {
+      set_error("graph capture failed: %s", cudaGetErrorString(e));
+      return EXF_ERR_CUDA;
+    }
+    e = cudaGraphInstantiate(&s->graph[gi], g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+      set_error("graph instantiation failed: %s", cudaGetErrorString(e));
+      s->graph[gi] = nullptr;
+      return EXF_ERR_CUDA;
+    }
+    s->graph_key[gi] = key;
+    s->graph_epoch[gi] = s->buf_epoch;
+    s->graph_launches[gi] = exf_launch_count() - c0;
+    count_launch(-(int)s->graph_launches[gi]);  // captured, not executed
+  }
+  EXF_CUDA(cudaGraphLaunch(s->graph[gi], s->stream));
+  count_launch((int)s->graph_launches[gi]);
+  return EXF_OK;
+}
+
 static int read_scalar(exf_sys *s, const double *d, double *h) {
   EXF_CUDA(cudaMemcpyAsync(h, d, sizeof(double), cudaMemcpyDeviceToHost, s->stream));
   EXF_CUDA(cudaStreamSynchronize(s->stream));
@@ -790,11 +859,12 @@ int exf_mg_solve(exf_sys *s, const exf_mg_params *p, exf_solve_stats *st) {
   st->rel_res = rel;
   int rc = EXF_OK;
   while (rel > p->eps && st->cycles < p->max_cycles) {
-    if (p->precision == EXF_PREC_MIXED) {
-      EXF_TRY(vcycle_mixed(s, p));
-      EXF_TRY(spmv_resid<double>(s, s->nlev - 1, T.x.p, T.b.p, T.r.p, dnr));
+    // the first cycle runs eagerly (it sizes every scratch buffer); later cycles replay a
+    // captured CUDA graph of the whole cycle when use_graph is set
+    if (p->use_graph && st->cycles > 0) {
+      EXF_TRY(cycle_graph(s, p, dnr));
     } else {
-      EXF_TRY(vcycle_fp64(s, p, dnr));
+      EXF_TRY(cycle_body(s, p, dnr));
     }
     EXF_TRY(read_scalar(s, dnr, &r2));
     rel = sqrt(r2) / den;
@@ -806,10 +876,6 @@ int exf_mg_solve(exf_sys *s, const exf_mg_params *p, exf_solve_stats *st) {
       set_error("multigrid diverged at cycle %d", st->cycles);
       break;
     }
-  }
-  if (p->precision != EXF_PREC_MIXED) {
-    // the FP64 cycle leaves the residual of the pre-gauge iterate in T.r; the residual is
-    // invariant under the pressure shift, so rel stands.
   }
   EXF_CUDA(cudaEventRecord(s->ev1, s->stream));
   EXF_CUDA(cudaEventSynchronize(s->ev1));

@@ -148,16 +148,17 @@ struct SysLevel {
   std::vector<int> col_off;    // [ncolour+1]
   DBuf<int> col_items;
   DBuf<int> item_colour;
+  // Vanka: velocity nodes of the stars of each colour's patches, patch by patch
+  std::vector<int> vrow_off;   // [ncolour+1]
+  DBuf<int> vrows;
   LevelVals<double> A;
   LevelVals<float> A32;
   // transfers: Pq/Pl from level-1 to this level (fine rows), Rq/Rl from this level+1
   Transfer Pq, Pl, Rq, Rl;
   DBuf<double> rmask;    // [ndof] restriction row mask (bc0 % 2 of the top DOF)
   // vectors
-  DBuf<double> x, b, r, dx;
+  DBuf<double> x, b, r, dx;     // dx: smoother scratch (Vanka star-row residuals)
   DBuf<float> x32, b32, r32, dx32;
-  DBuf<double> vanka_dp;  // per pressure node correction scratch
-  DBuf<float> vanka_dp32;
 };
 
 struct Partials {
@@ -192,6 +193,9 @@ struct exf_sys {
   // captured V-cycle graphs (per precision)
   cudaGraphExec_t graph[2] = {nullptr, nullptr};
   unsigned long long graph_key[2] = {0, 0};
+  long long graph_launches[2] = {0, 0};
+  unsigned buf_epoch = 1;                   // bumped when a buffer baked into a graph moves
+  unsigned graph_epoch[2] = {0, 0};
 };
 
 namespace exf {

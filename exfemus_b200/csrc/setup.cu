@@ -329,10 +329,6 @@ int build_patterns(exf_sys *s) {
     EXF_TRY(L.x32.zero(st));
     EXF_TRY(L.dx.zero(st));
     EXF_TRY(L.dx32.zero(st));
-    if (s->nv1) {
-      EXF_TRY(L.vanka_dp.alloc(L.NL));
-      EXF_TRY(L.vanka_dp32.alloc(L.NL));
-    }
   }
   return EXF_OK;
 }
@@ -375,6 +371,25 @@ int build_colours(exf_sys *s) {
     EXF_TRY(L.col_items.alloc(nitem));
     EXF_CUDA(cudaMemcpyAsync(L.col_items.p, items.data(), nitem * sizeof(int), cudaMemcpyHostToDevice, st));
     EXF_CUDA(cudaStreamSynchronize(st));
+    if (s->kind == EXF_KIND_NS) {
+      // star rows of every colour: the velocity nodes of pressure row m (qq(m)), patch by
+      // patch; stars of one colour are disjoint, so each node appears once per colour
+      std::vector<int> qp(L.N + 1), qc(L.nqq);
+      EXF_CUDA(cudaMemcpy(qp.data(), L.qq_ptr.p, (L.N + 1) * sizeof(int), cudaMemcpyDeviceToHost));
+      EXF_CUDA(cudaMemcpy(qc.data(), L.qq_col.p, L.nqq * sizeof(int), cudaMemcpyDeviceToHost));
+      std::vector<int> rows;
+      L.vrow_off.assign(L.ncolour + 1, 0);
+      for (int c = 0; c < L.ncolour; c++) {
+        L.vrow_off[c] = (int)rows.size();
+        for (int t = L.col_off[c]; t < L.col_off[c + 1]; t++) {
+          int mm = items[t];
+          for (int k = qp[mm]; k < qp[mm + 1]; k++) rows.push_back(qc[k]);
+        }
+      }
+      L.vrow_off[L.ncolour] = (int)rows.size();
+      EXF_TRY(L.vrows.alloc(rows.size()));
+      EXF_CUDA(cudaMemcpy(L.vrows.p, rows.data(), rows.size() * sizeof(int), cudaMemcpyHostToDevice));
+    }
   }
   return EXF_OK;
 }

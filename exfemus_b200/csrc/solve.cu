@@ -31,7 +31,6 @@ struct VT<double> {
   static double *b(SysLevel &L) { return L.b.p; }
   static double *r(SysLevel &L) { return L.r.p; }
   static double *dx(SysLevel &L) { return L.dx.p; }
-  static double *dp(SysLevel &L) { return L.vanka_dp.p; }
 };
 template <>
 struct VT<float> {
@@ -44,7 +43,6 @@ struct VT<float> {
   static float *b(SysLevel &L) { return L.b32.p; }
   static float *r(SysLevel &L) { return L.r32.p; }
   static float *dx(SysLevel &L) { return L.dx32.p; }
-  static float *dp(SysLevel &L) { return L.vanka_dp32.p; }
 };
 
 // ------------------------------------------------------------ reductions
@@ -72,6 +70,7 @@ static int ensure_partials(exf_sys *s, int nblk_needed) {
   if (s->red.nblk < nblk_needed) {
     EXF_TRY(s->red.part.alloc(nblk_needed));
     s->red.nblk = nblk_needed;
+    s->buf_epoch++;
   }
   if (!s->red.out.p) EXF_TRY(s->red.out.alloc(16));
   return EXF_OK;
@@ -305,35 +304,28 @@ __global__ void k_gs_colour(const int *__restrict__ items, int nitems, const int
 // approximated by its diagonal the local saddle system is solved in closed form:
 //   dp = (sum_j D_mj r_j/a_jj - r_m) / (sum_j D_mj G_jm/a_jj - c_mm)
 //   du_j = (r_j - G_jm dp)/a_jj ;  x += omega*(du, dp)
-// Phase 1 (this kernel) computes every patch correction of one colour from the iterate at
-// the start of the colour and stores it in dx; phase 2 applies it.  Patches of one colour
-// are disjoint, so the sweep is deterministic and independent of scheduling.
-template <class T, int D, int NT, int KMAX>
+// Per colour: (1) the residual of every velocity row in the colour's stars is computed
+// from the iterate at the start of the colour (a masked SpMV over disjoint stars, fully
+// parallel); (2) one CTA per patch forms the closed-form solve (warp shuffles + a fixed
+// reduction order) and writes its own star.  A patch's pressure row only reads its own
+// star and pressures of other colours, so (2) needs no further synchronisation and the
+// sweep is deterministic.
+template <class T, int D, int LPR, int NT>
 __global__ void __launch_bounds__(NT)
-    k_vanka_patch(const int *__restrict__ items, int N, const int *__restrict__ qq_ptr,
-                  const int *__restrict__ qq_col, const int *__restrict__ ql_ptr, const int *__restrict__ ql_col,
-                  const int *__restrict__ diag_pos, const int *__restrict__ gidx, long nqq, long nql, long nqqL,
-                  const T *__restrict__ vv, const T *__restrict__ vp, const T *__restrict__ pv,
-                  const T *__restrict__ pp, const T *__restrict__ x, const T *__restrict__ b, T *__restrict__ dx,
-                  T omega) {
-  __shared__ T s_r[KMAX][D];
-  __shared__ T s_a[KMAX][D];
-  __shared__ T s_g[KMAX][D];
-  __shared__ double s_red[2][NT / 32];
-  __shared__ double s_dp;
-  const int m = items[blockIdx.x];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  constexpr int NW = NT / 32;
-  const int k0 = qq_ptr[m];
-  const int K = min(qq_ptr[m + 1] - k0, KMAX);  // structured hierarchies never exceed KMAX
-  double S = 0., Tt = 0.;
-  // residual of every velocity row in the patch, one warp per velocity node
-  for (int kk = warp; kk < K; kk += NW) {
-    const int n = qq_col[k0 + kk];
-    T acc[D];
+    k_vanka_rows(const int *__restrict__ rows, int nrows, int N, const int *__restrict__ qq_ptr,
+                 const int *__restrict__ qq_col, const int *__restrict__ ql_ptr, const int *__restrict__ ql_col,
+                 long nqq, long nql, const T *__restrict__ vv, const T *__restrict__ vp, const T *__restrict__ x,
+                 const T *__restrict__ b, T *__restrict__ res) {
+  const int lane = threadIdx.x % LPR;
+  const long g = ((long)blockIdx.x * NT + threadIdx.x) / LPR;
+  const bool valid = g < nrows;
+  const int n = valid ? rows[g] : 0;
+  T acc[D];
 #pragma unroll
-    for (int a = 0; a < D; a++) acc[a] = T(0);
-    for (int k = qq_ptr[n] + lane; k < qq_ptr[n + 1]; k += 32) {
+  for (int a = 0; a < D; a++) acc[a] = T(0);
+  if (valid) {
+    const int k0 = qq_ptr[n], k1 = qq_ptr[n + 1];
+    for (int k = k0 + lane; k < k1; k += LPR) {
       const int c = qq_col[k];
       T xb[D];
 #pragma unroll
@@ -343,111 +335,107 @@ __global__ void __launch_bounds__(NT)
 #pragma unroll
         for (int bb = 0; bb < D; bb++) acc[a] += vv[(long)(a * D + bb) * nqq + k] * xb[bb];
     }
-    for (int k = ql_ptr[n] + lane; k < ql_ptr[n + 1]; k += 32) {
+    const int l0 = ql_ptr[n], l1 = ql_ptr[n + 1];
+    for (int k = l0 + lane; k < l1; k += LPR) {
       const T p = x[(long)D * N + ql_col[k]];
 #pragma unroll
       for (int a = 0; a < D; a++) acc[a] += vp[(long)a * nql + k] * p;
     }
-#pragma unroll
-    for (int a = 0; a < D; a++)
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) acc[a] += __shfl_down_sync(0xffffffffu, acc[a], o);
-    if (lane == 0) {
-      const int dpos = diag_pos[n];
-      const int gk = gidx[k0 + kk];
-#pragma unroll
-      for (int a = 0; a < D; a++) {
-        const T r = b[(long)a * N + n] - acc[a];
-        const T aa = vv[(long)(a * D + a) * nqq + dpos];
-        const T g = vp[(long)a * nql + gk];
-        const T dd = pv[(long)a * nqqL + k0 + kk];
-        s_r[kk][a] = r;
-        s_a[kk][a] = aa;
-        s_g[kk][a] = g;
-        S += (double)(dd * g / aa);
-        Tt += (double)(dd * r / aa);
-      }
-    }
   }
-  // pressure row residual and diagonal (warp 0)
-  double rp = 0., cpp = 0.;
-  if (warp == 0) {
-    T acc = T(0);
-    for (int k = k0 + lane; k < k0 + K; k += 32) {
-      const int nn = qq_col[k];
 #pragma unroll
-      for (int bb = 0; bb < D; bb++) acc += pv[(long)bb * nqqL + k] * x[(long)bb * N + nn];
-    }
-    T cd = T(0);
-    for (int k = ql_ptr[m] + lane; k < ql_ptr[m + 1]; k += 32) {
-      const int c = ql_col[k];
-      acc += pp[k] * x[(long)D * N + c];
-      if (c == m) cd = pp[k];
-    }
+  for (int a = 0; a < D; a++)
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      acc += __shfl_down_sync(0xffffffffu, acc, o);
-      cd += __shfl_down_sync(0xffffffffu, cd, o);
-    }
-    if (lane == 0) {
-      rp = (double)(b[(long)D * N + m] - acc);
-      cpp = (double)cd;
-    }
+    for (int o = LPR / 2; o > 0; o >>= 1) acc[a] += __shfl_down_sync(0xffffffffu, acc[a], o, LPR);
+  if (valid && lane == 0) {
+#pragma unroll
+    for (int a = 0; a < D; a++) res[(long)a * N + n] = b[(long)a * N + n] - acc[a];
   }
-  if (lane == 0) {
-    s_red[0][warp] = S;
-    s_red[1][warp] = Tt;
-  }
+}
+
+template <int NT>
+__device__ __forceinline__ void block_sum4(double v[4], double (*sh)[NT / 32]) {
+#pragma unroll
+  for (int i = 0; i < 4; i++)
+    for (int o = 16; o > 0; o >>= 1) v[i] += __shfl_down_sync(0xffffffffu, v[i], o);
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l == 0)
+    for (int i = 0; i < 4; i++) sh[i][w] = v[i];
   __syncthreads();
-  if (threadIdx.x == 0) {
-    double St = 0., TT = 0.;
-    for (int w = 0; w < NW; w++) {
-      St += s_red[0][w];
-      TT += s_red[1][w];
-    }
-    St -= cpp;
-    TT -= rp;
-    s_dp = fabs(St) > 1e-300 ? TT / St : 0.;
+  for (int i = 0; i < 4; i++) {
+    double r = 0.;
+    for (int k = 0; k < NT / 32; k++) r += sh[i][k];
+    v[i] = r;
   }
-  __syncthreads();
-  const T dp = (T)s_dp;
+}
+
+template <class T, int D, int NT, int KMAX>
+__global__ void __launch_bounds__(NT)
+    k_vanka_solve(const int *__restrict__ items, int N, const int *__restrict__ qq_ptr,
+                  const int *__restrict__ qq_col, const int *__restrict__ ql_ptr, const int *__restrict__ ql_col,
+                  const int *__restrict__ diag_pos, const int *__restrict__ gidx, long nqq, long nql, long nqqL,
+                  const T *__restrict__ vv, const T *__restrict__ vp, const T *__restrict__ pv,
+                  const T *__restrict__ pp, T *__restrict__ x, const T *__restrict__ b, const T *__restrict__ res,
+                  T omega) {
+  __shared__ T s_r[KMAX * D];
+  __shared__ T s_ia[KMAX * D];
+  __shared__ T s_g[KMAX * D];
+  __shared__ double s_red[4][NT / 32];
+  const int m = items[blockIdx.x];
+  const int k0 = qq_ptr[m];
+  const int K = min(qq_ptr[m + 1] - k0, KMAX);  // structured hierarchies never exceed KMAX
+  // v[0] = sum D G/a, v[1] = sum D r/a, v[2] = pressure-row product, v[3] = c_mm
+  double v[4] = {0., 0., 0., 0.};
   for (int t = threadIdx.x; t < K * D; t += NT) {
     const int kk = t / D, a = t % D;
     const int n = qq_col[k0 + kk];
-    dx[(long)a * N + n] = omega * (s_r[kk][a] - s_g[kk][a] * dp) / s_a[kk][a];
+    const T r = res[(long)a * N + n];
+    const T ia = T(1) / vv[(long)(a * D + a) * nqq + diag_pos[n]];
+    const T g = vp[(long)a * nql + gidx[k0 + kk]];
+    const T dd = pv[(long)a * nqqL + k0 + kk];
+    s_r[t] = r;
+    s_ia[t] = ia;
+    s_g[t] = g;
+    v[0] += (double)(dd * g * ia);
+    v[1] += (double)(dd * r * ia);
+    v[2] += (double)(dd * x[(long)a * N + n]);
   }
-  if (threadIdx.x == 0) dx[(long)D * N + m] = omega * dp;
-}
-
-template <class T, int D, int NT>
-__global__ void __launch_bounds__(NT)
-    k_vanka_apply(const int *__restrict__ items, int N, const int *__restrict__ qq_ptr,
-                  const int *__restrict__ qq_col, const T *__restrict__ dx, T *__restrict__ x) {
-  const int m = items[blockIdx.x];
-  const int k0 = qq_ptr[m], K = qq_ptr[m + 1] - k0;
+  for (int k = ql_ptr[m] + threadIdx.x; k < ql_ptr[m + 1]; k += NT) {
+    const int c = ql_col[k];
+    v[2] += (double)(pp[k] * x[(long)D * N + c]);
+    if (c == m) v[3] += (double)pp[k];
+  }
+  block_sum4<NT>(v, s_red);  // ends with every thread holding the totals
+  const double rp = (double)b[(long)D * N + m] - v[2];
+  const double St = v[0] - v[3], Tt = v[1] - rp;
+  const double dp = fabs(St) > 1e-300 ? Tt / St : 0.;
+  const T dpt = (T)dp;
   for (int t = threadIdx.x; t < K * D; t += NT) {
     const int kk = t / D, a = t % D;
     const long idx = (long)a * N + qq_col[k0 + kk];
-    x[idx] += dx[idx];
+    x[idx] += omega * (s_r[t] - s_g[t] * dpt) * s_ia[t];
   }
-  if (threadIdx.x == 0) x[(long)D * N + m] += dx[(long)D * N + m];
+  if (threadIdx.x == 0) x[(long)D * N + m] += omega * dpt;
 }
 
 template <class T, int D>
 static int vanka_sweep(exf_sys *s, int lev, const exf_mg_params *p, T *x, const T *b) {
   SysLevel &L = s->L[lev];
-  constexpr int NT = D == 3 ? 256 : 128;
+  constexpr int NTS = D == 3 ? 128 : 64;
   constexpr int KMAX = D == 3 ? 125 : 25;
-  T *dx = VT<T>::dx(L);
+  constexpr int LPR = D == 3 ? 32 : 16;
+  constexpr int NTR = 256;
+  T *res = VT<T>::dx(L);
   for (int cc = 0; cc < L.ncolour; cc++) {
     const int c = p->reverse_colours ? L.ncolour - 1 - cc : cc;
     const int n = L.col_off[c + 1] - L.col_off[c];
     if (n == 0) continue;
-    const int *items = L.col_items.p + L.col_off[c];
-    k_vanka_patch<T, D, NT, KMAX><<<n, NT, 0, s->stream>>>(
-        items, L.N, L.qq_ptr.p, L.qq_col.p, L.ql_ptr.p, L.ql_col.p, L.diag_pos.p, L.gidx.p, L.nqq, L.nql, L.nqqL,
-        VT<T>::vv(L), VT<T>::vp(L), VT<T>::pv(L), VT<T>::pp(L), x, b, dx, (T)p->omega);
-    k_vanka_apply<T, D, NT><<<n, NT, 0, s->stream>>>(items, L.N, L.qq_ptr.p, L.qq_col.p, dx, x);
+    const int nr = L.vrow_off[c + 1] - L.vrow_off[c];
+    k_vanka_rows<T, D, LPR, NTR><<<nblk((long)nr * LPR, NTR), NTR, 0, s->stream>>>(
+        L.vrows.p + L.vrow_off[c], nr, L.N, L.qq_ptr.p, L.qq_col.p, L.ql_ptr.p, L.ql_col.p, L.nqq, L.nql,
+        VT<T>::vv(L), VT<T>::vp(L), x, b, res);
+    k_vanka_solve<T, D, NTS, KMAX><<<n, NTS, 0, s->stream>>>(
+        L.col_items.p + L.col_off[c], L.N, L.qq_ptr.p, L.qq_col.p, L.ql_ptr.p, L.ql_col.p, L.diag_pos.p, L.gidx.p,
+        L.nqq, L.nql, L.nqqL, VT<T>::vv(L), VT<T>::vp(L), VT<T>::pv(L), VT<T>::pp(L), x, b, res, (T)p->omega);
     EXF_LAUNCH_CHECK();
     EXF_COUNT(2);
   }
@@ -576,7 +564,10 @@ int coarse_factor(exf_sys *s) {
     k_gj_elim<<<grid, 256, 0, st>>>(W, n, k, colk.p);
   }
   EXF_LAUNCH_CHECK();
-  EXF_TRY(s->coarse_inv.alloc((size_t)n * n));
+  if (s->coarse_inv.n != (size_t)n * n) {
+    EXF_TRY(s->coarse_inv.alloc((size_t)n * n));
+    s->buf_epoch++;
+  }
   k_extract_inv<<<n, 128, 0, st>>>(W, n, s->coarse_inv.p);
   EXF_LAUNCH_CHECK();
   int hbad = 0;
