@@ -365,12 +365,12 @@ def barrier(ws):
         dist.barrier()
 
 
-def max_over_ranks(ws, v):
+def max_over_ranks(ws, v, device="cuda"):
     if ws == 1:
         return v
     import torch
     import torch.distributed as dist
-    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    t = torch.tensor([v], dtype=torch.float64, device=device)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 

@@ -96,7 +96,7 @@ int sync_fp32(exf_sys *s, int lev) {
   cp(L.A.pv, L.A32.pv);
   cp(L.A.pp, L.A32.pp);
   EXF_LAUNCH_CHECK();
-  return EXF_OK;
+  return vanka_prep(s, lev);
 }
 
 // ----------------------------------------------------------------- transpose

@@ -148,9 +148,15 @@ struct SysLevel {
   std::vector<int> col_off;    // [ncolour+1]
   DBuf<int> col_items;
   DBuf<int> item_colour;
-  // Vanka: velocity nodes of the stars of each colour's patches, patch by patch
+  // Vanka: velocity nodes of the stars of each colour's patches, patch by patch; entry
+  // g of vrows is the (patch, star node) pair g, so per-entry data is stored compactly
   std::vector<int> vrow_off;   // [ncolour+1]
   DBuf<int> vrows;
+  DBuf<int> pstart;            // [NL] first vrows entry of each patch (by pressure node)
+  DBuf<double> vk64, pk64;     // per entry*D: {1/a, D/a, G/a}; per patch: {S, c_mm}
+  DBuf<float> vk32, pk32;
+  DBuf<double> vres64;         // compact star-row residuals [nvrows*D] + pressure rows [NL]
+  DBuf<float> vres32;
   LevelVals<double> A;
   LevelVals<float> A32;
   // transfers: Pq/Pl from level-1 to this level (fine rows), Rq/Rl from this level+1
@@ -206,7 +212,8 @@ int build_transfers(exf_sys *s);
 int update_rmask(exf_sys *s);
 int build_colours(exf_sys *s);
 int assemble_level(exf_sys *s, const exf_phys *ph, int lev, int mode);
-int sync_fp32(exf_sys *s, int lev);
+int sync_fp32(exf_sys *s, int lev);  // FP32 copy + smoother coefficients after a matrix change
+int vanka_prep(exf_sys *s, int lev);
 int csr_values(exf_sys *s, int lev, double *d_out);         // NB -> CSR order (device)
 int csr_set_values(exf_sys *s, int lev, const double *d_in);
 int coarse_factor(exf_sys *s);

@@ -378,17 +378,28 @@ int build_colours(exf_sys *s) {
       EXF_CUDA(cudaMemcpy(qp.data(), L.qq_ptr.p, (L.N + 1) * sizeof(int), cudaMemcpyDeviceToHost));
       EXF_CUDA(cudaMemcpy(qc.data(), L.qq_col.p, L.nqq * sizeof(int), cudaMemcpyDeviceToHost));
       std::vector<int> rows;
+      std::vector<int> pst(L.NL, 0);
       L.vrow_off.assign(L.ncolour + 1, 0);
       for (int c = 0; c < L.ncolour; c++) {
         L.vrow_off[c] = (int)rows.size();
         for (int t = L.col_off[c]; t < L.col_off[c + 1]; t++) {
           int mm = items[t];
+          pst[mm] = (int)rows.size();
           for (int k = qp[mm]; k < qp[mm + 1]; k++) rows.push_back(qc[k]);
         }
       }
       L.vrow_off[L.ncolour] = (int)rows.size();
       EXF_TRY(L.vrows.alloc(rows.size()));
       EXF_CUDA(cudaMemcpy(L.vrows.p, rows.data(), rows.size() * sizeof(int), cudaMemcpyHostToDevice));
+      EXF_TRY(L.pstart.alloc(L.NL));
+      EXF_CUDA(cudaMemcpy(L.pstart.p, pst.data(), pst.size() * sizeof(int), cudaMemcpyHostToDevice));
+      const size_t ne = rows.size() * (size_t)s->nv2;
+      EXF_TRY(L.vk64.alloc(3 * ne));
+      EXF_TRY(L.vk32.alloc(3 * ne));
+      EXF_TRY(L.pk64.alloc(2 * (size_t)L.NL));
+      EXF_TRY(L.pk32.alloc(2 * (size_t)L.NL));
+      EXF_TRY(L.vres64.alloc(ne + L.NL));
+      EXF_TRY(L.vres32.alloc(ne + L.NL));
     }
   }
   return EXF_OK;

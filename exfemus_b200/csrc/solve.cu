@@ -8,6 +8,9 @@
 // All kernels are templated on the value type: FP64 for the plain path and the outer
 // defect correction, FP32 (storage and accumulation) for the mixed-precision V-cycle.
 // Reductions are two-stage with a fixed order, so every result is bitwise reproducible.
+#include <cooperative_groups.h>
+
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <vector>
@@ -76,6 +79,50 @@ static int ensure_partials(exf_sys *s, int nblk_needed) {
   return EXF_OK;
 }
 
+// acc[a] += sum over the node row n of the d x d blocks times x (and B^T times p);
+// two blocks per lane in flight
+template <class T, int D, int LPR, bool PRESSURE>
+__device__ __forceinline__ void node_row_dot(int n, int lane, int N, const int *__restrict__ qq_ptr,
+                                             const int *__restrict__ qq_col, const int *__restrict__ ql_ptr,
+                                             const int *__restrict__ ql_col, long nqq, long nql,
+                                             const T *__restrict__ vv, const T *__restrict__ vp,
+                                             const T *__restrict__ x, T acc[D]) {
+  const int k0 = qq_ptr[n], k1 = qq_ptr[n + 1];
+  int k = k0 + lane;
+  for (; k + LPR < k1; k += 2 * LPR) {
+    const int c0 = qq_col[k], c1 = qq_col[k + LPR];
+    T v0[D * D], v1[D * D], x0[D], x1[D];
+#pragma unroll
+    for (int q = 0; q < D * D; q++) {
+      v0[q] = vv[(long)q * nqq + k];
+      v1[q] = vv[(long)q * nqq + k + LPR];
+    }
+#pragma unroll
+    for (int bb = 0; bb < D; bb++) {
+      x0[bb] = x[(long)bb * N + c0];
+      x1[bb] = x[(long)bb * N + c1];
+    }
+#pragma unroll
+    for (int a = 0; a < D; a++)
+#pragma unroll
+      for (int bb = 0; bb < D; bb++) acc[a] += v0[a * D + bb] * x0[bb] + v1[a * D + bb] * x1[bb];
+  }
+  if (k < k1) {
+    const int c0 = qq_col[k];
+#pragma unroll
+    for (int a = 0; a < D; a++)
+#pragma unroll
+      for (int bb = 0; bb < D; bb++) acc[a] += vv[(long)(a * D + bb) * nqq + k] * x[(long)bb * N + c0];
+  }
+  if (PRESSURE) {
+    for (int kp = ql_ptr[n] + lane; kp < ql_ptr[n + 1]; kp += LPR) {
+      const T p = x[(long)D * N + ql_col[kp]];
+#pragma unroll
+      for (int a = 0; a < D; a++) acc[a] += vp[(long)a * nql + kp] * p;
+    }
+  }
+}
+
 // ------------------------------------------------------------------ SpMV
 // row groups: g < N -> Q2 node g (d outputs), g >= N -> Q1 node g-N (1 output).
 // LPR lanes per row group; the node-block index k is shared by the d*d planes.
@@ -97,26 +144,7 @@ __global__ void __launch_bounds__(NT)
 #pragma unroll
   for (int a = 0; a < D; a++) acc[a] = T(0);
   if (vel) {
-    const int n = (int)g;
-    const int k0 = qq_ptr[n], k1 = qq_ptr[n + 1];
-    for (int k = k0 + lane; k < k1; k += LPR) {
-      const int m = qq_col[k];
-      T xb[D];
-#pragma unroll
-      for (int bb = 0; bb < D; bb++) xb[bb] = x[(long)bb * N + m];
-#pragma unroll
-      for (int a = 0; a < D; a++)
-#pragma unroll
-        for (int bb = 0; bb < D; bb++) acc[a] += vv[(long)(a * D + bb) * nqq + k] * xb[bb];
-    }
-    if (NS) {
-      const int l0 = ql_ptr[n], l1 = ql_ptr[n + 1];
-      for (int k = l0 + lane; k < l1; k += LPR) {
-        const T p = x[(long)D * N + ql_col[k]];
-#pragma unroll
-        for (int a = 0; a < D; a++) acc[a] += vp[(long)a * nql + k] * p;
-      }
-    }
+    node_row_dot<T, D, LPR, NS>((int)g, lane, N, qq_ptr, qq_col, ql_ptr, ql_col, nqq, nql, vv, vp, x, acc);
   } else if (prs) {
     const int m = (int)(g - N);
     const int k0 = qq_ptr[m], k1 = qq_ptr[m + 1];
@@ -289,13 +317,12 @@ __global__ void k_gs_colour(const int *__restrict__ items, int nitems, const int
   const bool valid = g < nitems;  // all lanes reach the shuffles
   const int n = valid ? items[g] : 0;
   const int dp = valid ? diag_pos[n] : 0;
-  T acc = T(0);
-  if (valid)
-    for (int k = qq_ptr[n] + lane; k < qq_ptr[n + 1]; k += LPR)
-      if (k != dp) acc += vv[k] * x[qq_col[k]];
+  T acc[1] = {T(0)};
+  if (valid) node_row_dot<T, 1, LPR, false>(n, lane, 0, qq_ptr, qq_col, nullptr, nullptr, 0, 0, vv, nullptr, x, acc);
 #pragma unroll
-  for (int o = LPR / 2; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o, LPR);
-  if (valid && lane == 0) x[n] = (b[n] - acc) / vv[dp];
+  for (int o = LPR / 2; o > 0; o >>= 1) acc[0] += __shfl_down_sync(0xffffffffu, acc[0], o, LPR);
+  // the row product included the diagonal term; remove it (x[n] is not updated yet)
+  if (valid && lane == 0) x[n] = (b[n] - (acc[0] - vv[dp] * x[n])) / vv[dp];
 }
 
 // --------------------------------------------------------------- Vanka
@@ -304,141 +331,187 @@ __global__ void k_gs_colour(const int *__restrict__ items, int nitems, const int
 // approximated by its diagonal the local saddle system is solved in closed form:
 //   dp = (sum_j D_mj r_j/a_jj - r_m) / (sum_j D_mj G_jm/a_jj - c_mm)
 //   du_j = (r_j - G_jm dp)/a_jj ;  x += omega*(du, dp)
-// Per colour: (1) the residual of every velocity row in the colour's stars is computed
-// from the iterate at the start of the colour (a masked SpMV over disjoint stars, fully
-// parallel); (2) one CTA per patch forms the closed-form solve (warp shuffles + a fixed
-// reduction order) and writes its own star.  A patch's pressure row only reads its own
-// star and pressures of other colours, so (2) needs no further synchronisation and the
-// sweep is deterministic.
+// After every assembly k_vanka_prep stores, per (patch, star DOF), {1/a_jj, D_mj/a_jj,
+// G_jm/a_jj} contiguously in patch order, and per patch the Schur denominator.
+// Per colour: (1) k_vanka_rows computes the residual of every velocity row in the
+// colour's stars and of the patches' pressure rows from the iterate at the start of the
+// colour (a masked SpMV over disjoint stars, fully parallel, residuals written in patch
+// order); (2) k_vanka_solve, one CTA per patch, reduces the Schur numerator with warp
+// shuffles in a fixed order and writes its own star.  Stars of one colour are disjoint,
+// so the sweep is deterministic and independent of scheduling.
+
 template <class T, int D, int LPR, int NT>
 __global__ void __launch_bounds__(NT)
-    k_vanka_rows(const int *__restrict__ rows, int nrows, int N, const int *__restrict__ qq_ptr,
-                 const int *__restrict__ qq_col, const int *__restrict__ ql_ptr, const int *__restrict__ ql_col,
-                 long nqq, long nql, const T *__restrict__ vv, const T *__restrict__ vp, const T *__restrict__ x,
-                 const T *__restrict__ b, T *__restrict__ res) {
+    k_vanka_rows(const int *__restrict__ rows, int nrows, int gbase, const int *__restrict__ items, int npatch,
+                 int N, const int *__restrict__ qq_ptr, const int *__restrict__ qq_col,
+                 const int *__restrict__ ql_ptr, const int *__restrict__ ql_col, long nqq, long nql, long nqqL,
+                 const T *__restrict__ vv, const T *__restrict__ vp, const T *__restrict__ pv,
+                 const T *__restrict__ pp, const T *__restrict__ x, const T *__restrict__ b, T *__restrict__ res,
+                 long pres_off) {
   const int lane = threadIdx.x % LPR;
   const long g = ((long)blockIdx.x * NT + threadIdx.x) / LPR;
-  const bool valid = g < nrows;
-  const int n = valid ? rows[g] : 0;
+  const bool vel = g < nrows;
+  const bool prs = !vel && g < (long)nrows + npatch;
   T acc[D];
 #pragma unroll
   for (int a = 0; a < D; a++) acc[a] = T(0);
-  if (valid) {
-    const int k0 = qq_ptr[n], k1 = qq_ptr[n + 1];
-    for (int k = k0 + lane; k < k1; k += LPR) {
+  int node = 0;
+  if (vel) {
+    node = rows[g];
+    node_row_dot<T, D, LPR, true>(node, lane, N, qq_ptr, qq_col, ql_ptr, ql_col, nqq, nql, vv, vp, x, acc);
+  } else if (prs) {
+    node = items[g - nrows];
+    for (int k = qq_ptr[node] + lane; k < qq_ptr[node + 1]; k += LPR) {
       const int c = qq_col[k];
-      T xb[D];
 #pragma unroll
-      for (int bb = 0; bb < D; bb++) xb[bb] = x[(long)bb * N + c];
-#pragma unroll
-      for (int a = 0; a < D; a++)
-#pragma unroll
-        for (int bb = 0; bb < D; bb++) acc[a] += vv[(long)(a * D + bb) * nqq + k] * xb[bb];
+      for (int bb = 0; bb < D; bb++) acc[0] += pv[(long)bb * nqqL + k] * x[(long)bb * N + c];
     }
-    const int l0 = ql_ptr[n], l1 = ql_ptr[n + 1];
-    for (int k = l0 + lane; k < l1; k += LPR) {
-      const T p = x[(long)D * N + ql_col[k]];
-#pragma unroll
-      for (int a = 0; a < D; a++) acc[a] += vp[(long)a * nql + k] * p;
-    }
+    for (int k = ql_ptr[node] + lane; k < ql_ptr[node + 1]; k += LPR) acc[0] += pp[k] * x[(long)D * N + ql_col[k]];
   }
 #pragma unroll
   for (int a = 0; a < D; a++)
 #pragma unroll
     for (int o = LPR / 2; o > 0; o >>= 1) acc[a] += __shfl_down_sync(0xffffffffu, acc[a], o, LPR);
-  if (valid && lane == 0) {
+  if (lane == 0) {
+    if (vel) {
 #pragma unroll
-    for (int a = 0; a < D; a++) res[(long)a * N + n] = b[(long)a * N + n] - acc[a];
+      for (int a = 0; a < D; a++) res[(gbase + g) * D + a] = b[(long)a * N + node] - acc[a];
+    } else if (prs) {
+      res[pres_off + node] = b[(long)D * N + node] - acc[0];
+    }
   }
 }
 
-template <int NT>
-__device__ __forceinline__ void block_sum4(double v[4], double (*sh)[NT / 32]) {
-#pragma unroll
-  for (int i = 0; i < 4; i++)
-    for (int o = 16; o > 0; o >>= 1) v[i] += __shfl_down_sync(0xffffffffu, v[i], o);
-  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-  if (l == 0)
-    for (int i = 0; i < 4; i++) sh[i][w] = v[i];
-  __syncthreads();
-  for (int i = 0; i < 4; i++) {
-    double r = 0.;
-    for (int k = 0; k < NT / 32; k++) r += sh[i][k];
-    v[i] = r;
-  }
-}
-
-template <class T, int D, int NT, int KMAX>
-__global__ void __launch_bounds__(NT)
-    k_vanka_solve(const int *__restrict__ items, int N, const int *__restrict__ qq_ptr,
-                  const int *__restrict__ qq_col, const int *__restrict__ ql_ptr, const int *__restrict__ ql_col,
-                  const int *__restrict__ diag_pos, const int *__restrict__ gidx, long nqq, long nql, long nqqL,
-                  const T *__restrict__ vv, const T *__restrict__ vp, const T *__restrict__ pv,
-                  const T *__restrict__ pp, T *__restrict__ x, const T *__restrict__ b, const T *__restrict__ res,
-                  T omega) {
-  __shared__ T s_r[KMAX * D];
-  __shared__ T s_ia[KMAX * D];
-  __shared__ T s_g[KMAX * D];
-  __shared__ double s_red[4][NT / 32];
-  const int m = items[blockIdx.x];
-  const int k0 = qq_ptr[m];
-  const int K = min(qq_ptr[m + 1] - k0, KMAX);  // structured hierarchies never exceed KMAX
-  // v[0] = sum D G/a, v[1] = sum D r/a, v[2] = pressure-row product, v[3] = c_mm
-  double v[4] = {0., 0., 0., 0.};
-  for (int t = threadIdx.x; t < K * D; t += NT) {
+// per (patch, star DOF): {1/a, D/a, G/a}; per patch: {sum D G / a - c_mm, c_mm}
+template <int D>
+__global__ void k_vanka_prep(int NL, const int *__restrict__ pstart, const int *__restrict__ qq_ptr,
+                             const int *__restrict__ qq_col, const int *__restrict__ ql_ptr,
+                             const int *__restrict__ ql_col, const int *__restrict__ diag_pos,
+                             const int *__restrict__ gidx, long nqq, long nql, long nqqL, const double *vv,
+                             const double *vp, const double *pv, const double *pp, double *vk64, float *vk32,
+                             double *pk64, float *pk32) {
+  const int m = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+  if (m >= NL) return;  // one warp per patch, uniform per warp
+  const int k0 = qq_ptr[m], K = qq_ptr[m + 1] - k0;
+  const long g0 = pstart[m];
+  double S = 0.;
+  for (int t = lane; t < K * D; t += 32) {
     const int kk = t / D, a = t % D;
     const int n = qq_col[k0 + kk];
-    const T r = res[(long)a * N + n];
-    const T ia = T(1) / vv[(long)(a * D + a) * nqq + diag_pos[n]];
-    const T g = vp[(long)a * nql + gidx[k0 + kk]];
-    const T dd = pv[(long)a * nqqL + k0 + kk];
-    s_r[t] = r;
-    s_ia[t] = ia;
-    s_g[t] = g;
-    v[0] += (double)(dd * g * ia);
-    v[1] += (double)(dd * r * ia);
-    v[2] += (double)(dd * x[(long)a * N + n]);
+    const double ia = 1. / vv[(long)(a * D + a) * nqq + diag_pos[n]];
+    const double dd = pv[(long)a * nqqL + k0 + kk];
+    const double gg = vp[(long)a * nql + gidx[k0 + kk]];
+    const long e = 3 * ((g0 + kk) * D + a);
+    vk64[e] = ia;
+    vk64[e + 1] = dd * ia;
+    vk64[e + 2] = gg * ia;
+    vk32[e] = (float)ia;
+    vk32[e + 1] = (float)(dd * ia);
+    vk32[e + 2] = (float)(gg * ia);
+    S += dd * gg * ia;
   }
-  for (int k = ql_ptr[m] + threadIdx.x; k < ql_ptr[m + 1]; k += NT) {
-    const int c = ql_col[k];
-    v[2] += (double)(pp[k] * x[(long)D * N + c]);
-    if (c == m) v[3] += (double)pp[k];
+  double cmm = 0.;
+  for (int k = ql_ptr[m] + lane; k < ql_ptr[m + 1]; k += 32)
+    if (ql_col[k] == m) cmm += pp[k];
+  for (int o = 16; o > 0; o >>= 1) {
+    S += __shfl_down_sync(0xffffffffu, S, o);
+    cmm += __shfl_down_sync(0xffffffffu, cmm, o);
   }
-  block_sum4<NT>(v, s_red);  // ends with every thread holding the totals
-  const double rp = (double)b[(long)D * N + m] - v[2];
-  const double St = v[0] - v[3], Tt = v[1] - rp;
-  const double dp = fabs(St) > 1e-300 ? Tt / St : 0.;
-  const T dpt = (T)dp;
+  if (lane == 0) {
+    pk64[2 * m] = S - cmm;
+    pk64[2 * m + 1] = cmm;
+    pk32[2 * m] = (float)(S - cmm);
+    pk32[2 * m + 1] = (float)cmm;
+  }
+}
+
+template <class T, int D, int NT>
+__global__ void __launch_bounds__(NT)
+    k_vanka_solve(const int *__restrict__ items, int N, const int *__restrict__ qq_ptr,
+                  const int *__restrict__ vrows, const int *__restrict__ pstart, const T *__restrict__ vk,
+                  const T *__restrict__ pk, const T *__restrict__ res, long pres_off, T *__restrict__ x, T omega) {
+  __shared__ double s_red[NT / 32];
+  const int m = items[blockIdx.x];
+  const int K = qq_ptr[m + 1] - qq_ptr[m];
+  const long g0 = pstart[m];
+  const T *rr = res + g0 * D;
+  const T *w = vk + 3 * g0 * D;
+  double tsum = 0.;
+  for (int t = threadIdx.x; t < K * D; t += NT) tsum += (double)(w[3 * t + 1] * rr[t]);
+  for (int o = 16; o > 0; o >>= 1) tsum += __shfl_down_sync(0xffffffffu, tsum, o);
+  if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = tsum;
+  __syncthreads();
+  double Tt = 0.;
+  for (int k = 0; k < NT / 32; k++) Tt += s_red[k];
+  const double St = (double)pk[2 * m];
+  Tt -= (double)res[pres_off + m];
+  const T dp = (T)(fabs(St) > 1e-300 ? Tt / St : 0.);
   for (int t = threadIdx.x; t < K * D; t += NT) {
     const int kk = t / D, a = t % D;
-    const long idx = (long)a * N + qq_col[k0 + kk];
-    x[idx] += omega * (s_r[t] - s_g[t] * dpt) * s_ia[t];
+    const long idx = (long)a * N + vrows[g0 + kk];
+    x[idx] += omega * (rr[t] * w[3 * t] - w[3 * t + 2] * dp);
   }
-  if (threadIdx.x == 0) x[(long)D * N + m] += omega * dpt;
+  if (threadIdx.x == 0) x[(long)D * N + m] += omega * dp;
 }
+
+template <class T>
+struct VK;
+template <>
+struct VK<double> {
+  static const double *vk(const SysLevel &L) { return L.vk64.p; }
+  static const double *pk(const SysLevel &L) { return L.pk64.p; }
+  static double *res(SysLevel &L) { return L.vres64.p; }
+};
+template <>
+struct VK<float> {
+  static const float *vk(const SysLevel &L) { return L.vk32.p; }
+  static const float *pk(const SysLevel &L) { return L.pk32.p; }
+  static float *res(SysLevel &L) { return L.vres32.p; }
+};
 
 template <class T, int D>
 static int vanka_sweep(exf_sys *s, int lev, const exf_mg_params *p, T *x, const T *b) {
   SysLevel &L = s->L[lev];
   constexpr int NTS = D == 3 ? 128 : 64;
-  constexpr int KMAX = D == 3 ? 125 : 25;
   constexpr int LPR = D == 3 ? 32 : 16;
   constexpr int NTR = 256;
-  T *res = VT<T>::dx(L);
+  T *res = VK<T>::res(L);
+  const long pres_off = (long)L.vrow_off[L.ncolour] * D;
   for (int cc = 0; cc < L.ncolour; cc++) {
     const int c = p->reverse_colours ? L.ncolour - 1 - cc : cc;
     const int n = L.col_off[c + 1] - L.col_off[c];
     if (n == 0) continue;
     const int nr = L.vrow_off[c + 1] - L.vrow_off[c];
-    k_vanka_rows<T, D, LPR, NTR><<<nblk((long)nr * LPR, NTR), NTR, 0, s->stream>>>(
-        L.vrows.p + L.vrow_off[c], nr, L.N, L.qq_ptr.p, L.qq_col.p, L.ql_ptr.p, L.ql_col.p, L.nqq, L.nql,
-        VT<T>::vv(L), VT<T>::vp(L), x, b, res);
-    k_vanka_solve<T, D, NTS, KMAX><<<n, NTS, 0, s->stream>>>(
-        L.col_items.p + L.col_off[c], L.N, L.qq_ptr.p, L.qq_col.p, L.ql_ptr.p, L.ql_col.p, L.diag_pos.p, L.gidx.p,
-        L.nqq, L.nql, L.nqqL, VT<T>::vv(L), VT<T>::vp(L), VT<T>::pv(L), VT<T>::pp(L), x, b, res, (T)p->omega);
+    const int *items = L.col_items.p + L.col_off[c];
+    k_vanka_rows<T, D, LPR, NTR><<<nblk((long)(nr + n) * LPR, NTR), NTR, 0, s->stream>>>(
+        L.vrows.p + L.vrow_off[c], nr, L.vrow_off[c], items, n, L.N, L.qq_ptr.p, L.qq_col.p, L.ql_ptr.p,
+        L.ql_col.p, L.nqq, L.nql, L.nqqL, VT<T>::vv(L), VT<T>::vp(L), VT<T>::pv(L), VT<T>::pp(L), x, b, res,
+        pres_off);
+    k_vanka_solve<T, D, NTS><<<n, NTS, 0, s->stream>>>(items, L.N, L.qq_ptr.p, L.vrows.p, L.pstart.p,
+                                                        VK<T>::vk(L), VK<T>::pk(L), res, pres_off, x,
+                                                        (T)p->omega);
     EXF_LAUNCH_CHECK();
     EXF_COUNT(2);
   }
+  return EXF_OK;
+}
+
+int vanka_prep(exf_sys *s, int lev) {
+  if (s->kind != EXF_KIND_NS) return EXF_OK;
+  SysLevel &L = s->L[lev];
+  const unsigned grid = nblk(L.NL, 4);
+  if (s->dim == 2)
+    k_vanka_prep<2><<<grid, 128, 0, s->stream>>>(L.NL, L.pstart.p, L.qq_ptr.p, L.qq_col.p, L.ql_ptr.p,
+                                                  L.ql_col.p, L.diag_pos.p, L.gidx.p, L.nqq, L.nql, L.nqqL,
+                                                  L.A.vv.p, L.A.vp.p, L.A.pv.p, L.A.pp.p, L.vk64.p, L.vk32.p,
+                                                  L.pk64.p, L.pk32.p);
+  else
+    k_vanka_prep<3><<<grid, 128, 0, s->stream>>>(L.NL, L.pstart.p, L.qq_ptr.p, L.qq_col.p, L.ql_ptr.p,
+                                                  L.ql_col.p, L.diag_pos.p, L.gidx.p, L.nqq, L.nql, L.nqqL,
+                                                  L.A.vv.p, L.A.vp.p, L.A.pv.p, L.A.pp.p, L.vk64.p, L.vk32.p,
+                                                  L.pk64.p, L.pk32.p);
+  EXF_LAUNCH_CHECK();
+  EXF_COUNT(1);
   return EXF_OK;
 }
 
@@ -475,100 +548,161 @@ template int smooth<double>(exf_sys *, int, const exf_mg_params *, int, double *
 template int smooth<float>(exf_sys *, int, const exf_mg_params *, int, float *, const float *);
 
 // -------------------------------------------------- coarsest direct solve
-// Gauss-Jordan with partial pivoting on [A0 | I] gives A0^{-1} once per assembly; each
-// coarse solve is then one dense GEMV in FP64.  Pressure-gauge rows become identity rows
-// in the factored copy (the enclosed-flow pressure level is otherwise free).
+// In-place Gauss-Jordan inversion with partial pivoting, once per assembly, in ONE
+// cooperative kernel (two grid-wide barriers per pivot).  Pivot rows are not swapped:
+// step k pivots on the largest |a_ik| among unused rows p_k, which leaves
+// W[p_k][j] = A0^{-1}[k][p_j]; the extraction kernel undoes the permutation.  Each coarse
+// solve is then one dense GEMV in FP64.  Pressure-gauge rows become identity rows in the
+// factored copy (the enclosed-flow pressure level is otherwise free).  Ties in the pivot
+// search go to the smallest row index, so the factorisation is deterministic.
 __global__ void k_dense_from_csr(const int *ptr, const int *col, const double *val, int n, double *W) {
   int i = blockIdx.x;
-  for (int k = ptr[i] + threadIdx.x; k < ptr[i + 1]; k += blockDim.x) W[(long)i * 2 * n + col[k]] = val[k];
-  for (int j = threadIdx.x; j < n; j += blockDim.x) W[(long)i * 2 * n + n + j] = (i == j) ? 1. : 0.;
+  for (int j = threadIdx.x; j < n; j += blockDim.x) W[(long)i * n + j] = 0.;
+  __syncthreads();
+  for (int k = ptr[i] + threadIdx.x; k < ptr[i + 1]; k += blockDim.x) W[(long)i * n + col[k]] = val[k];
 }
 __global__ void k_gauge_rows(double *W, int n, const double *gmask) {
   int i = blockIdx.x;
   if (gmask[i] != 0.) return;
-  for (int j = threadIdx.x; j < 2 * n; j += blockDim.x) W[(long)i * 2 * n + j] = (j == i) ? 1. : 0.;
+  for (int j = threadIdx.x; j < n; j += blockDim.x) W[(long)i * n + j] = (j == i) ? 1. : 0.;
 }
-// pivot step k: one CTA selects the pivot, swaps, scales row k, stashes column k
-__global__ void k_gj_pivot(double *W, int n, int k, double *colk, int *bad) {
-  __shared__ double sv[1024];
-  __shared__ int si[1024];
-  const int t = threadIdx.x;
-  double best = -1.;
-  int bi = k;
-  for (int i = k + t; i < n; i += blockDim.x) {
-    double v = fabs(W[(long)i * 2 * n + k]);
-    if (v > best) {
-      best = v;
-      bi = i;
-    }
+
+__device__ __forceinline__ void argmax_merge(double &v, int &i, double v2, int i2) {
+  if (v2 > v || (v2 == v && i2 >= 0 && (i < 0 || i2 < i))) {
+    v = v2;
+    i = i2;
   }
-  sv[t] = best;
-  si[t] = bi;
+}
+
+template <int NT>
+__device__ void block_argmax(double v, int i, double *sv, int *si, double *bm, int *bi) {
+  for (int o = 16; o > 0; o >>= 1) {
+    double v2 = __shfl_down_sync(0xffffffffu, v, o);
+    int i2 = __shfl_down_sync(0xffffffffu, i, o);
+    argmax_merge(v, i, v2, i2);
+  }
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l == 0) {
+    sv[w] = v;
+    si[w] = i;
+  }
   __syncthreads();
-  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
-    if (t < o) {
-      if (sv[t + o] > sv[t] || (sv[t + o] == sv[t] && si[t + o] < si[t])) {
-        sv[t] = sv[t + o];
-        si[t] = si[t + o];
-      }
+  if (threadIdx.x == 0) {
+    double bv = -1.;
+    int bidx = -1;
+    for (int k = 0; k < NT / 32; k++) argmax_merge(bv, bidx, sv[k], si[k]);
+    bm[blockIdx.x] = bv;
+    bi[blockIdx.x] = bidx;
+  }
+  __syncthreads();
+}
+
+template <int NT>
+__global__ void __launch_bounds__(NT)
+    k_gj_coop(double *W, int n, int *pivrow, double *colk, double *rowp, double *bm, int *bi, int *used, int *bad) {
+  namespace cg = cooperative_groups;
+  cg::grid_group grid = cg::this_grid();
+  __shared__ double sv[NT / 32];
+  __shared__ int si[NT / 32];
+  __shared__ int s_p;
+  const long gt = (long)blockIdx.x * NT + threadIdx.x;
+  const long nth = (long)gridDim.x * NT;
+  // candidates for column 0
+  {
+    double v = -1.;
+    int idx = -1;
+    for (long i = gt; i < n; i += nth) argmax_merge(v, idx, fabs(W[i * n]), (int)i);
+    block_argmax<NT>(v, idx, sv, si, bm, bi);
+  }
+  grid.sync();
+  for (int k = 0; k < n; k++) {
+    // phase A: every block selects the same pivot row and stashes row p and column k
+    if (threadIdx.x == 0) {
+      double bv = -1.;
+      int bidx = -1;
+      for (int b = 0; b < (int)gridDim.x; b++) argmax_merge(bv, bidx, bm[b], bi[b]);
+      s_p = bidx;
     }
     __syncthreads();
-  }
-  const int p = si[0];
-  const double pv = W[(long)p * 2 * n + k];
-  if (t == 0 && pv == 0.) *bad = 1;
-  __syncthreads();
-  if (p != k)
-    for (int j = t; j < 2 * n; j += blockDim.x) {
-      double a = W[(long)k * 2 * n + j];
-      W[(long)k * 2 * n + j] = W[(long)p * 2 * n + j];
-      W[(long)p * 2 * n + j] = a;
+    const int p = s_p;
+    if (p < 0) {  // every remaining row is zero in this column: singular
+      if (gt == 0) *bad = 1;
+      return;     // uniform across the grid: every block took the same branch
     }
-  __syncthreads();
-  const double inv = pv != 0. ? 1. / pv : 0.;
-  for (int j = t; j < 2 * n; j += blockDim.x) W[(long)k * 2 * n + j] *= inv;
-  for (int i = t; i < n; i += blockDim.x) colk[i] = (i == k) ? 0. : W[(long)i * 2 * n + k];
+    if (gt == 0) {
+      pivrow[k] = p;
+      used[p] = 1;
+      if (W[(long)p * n + k] == 0.) *bad = 1;
+    }
+    for (long t = gt; t < n; t += nth) {
+      rowp[t] = W[(long)p * n + t];
+      colk[t] = W[t * n + k];
+    }
+    grid.sync();
+    // phase B: update every entry, collect pivot candidates of column k+1
+    const double piv = rowp[k];
+    const double inv = piv != 0. ? 1. / piv : 0.;
+    double v = -1.;
+    int idx = -1;
+    const long nn = (long)n * n;
+    for (long e = gt; e < nn; e += nth) {
+      const int i = (int)(e / n), j = (int)(e % n);
+      double a;
+      if (i == p) a = (j == k) ? inv : rowp[j] * inv;
+      else if (j == k) a = -colk[i] * inv;
+      else a = W[e] - colk[i] * rowp[j] * inv;
+      W[e] = a;
+      if (j == k + 1 && i != p && !used[i]) argmax_merge(v, idx, fabs(a), i);
+    }
+    block_argmax<NT>(v, idx, sv, si, bm, bi);
+    grid.sync();
+  }
 }
-__global__ void k_gj_elim(double *W, int n, int k, const double *colk) {
-  const int i = blockIdx.y;
-  const double f = colk[i];
-  if (f == 0.) return;
-  for (int j = k + blockIdx.x * blockDim.x + threadIdx.x; j < 2 * n; j += gridDim.x * blockDim.x)
-    W[(long)i * 2 * n + j] -= f * W[(long)k * 2 * n + j];
-}
-__global__ void k_extract_inv(const double *W, int n, double *inv) {
-  int i = blockIdx.x;
-  for (int j = threadIdx.x; j < n; j += blockDim.x) inv[(long)i * n + j] = W[(long)i * 2 * n + n + j];
+
+// inv[k][p_j] = W[p_k][j]
+__global__ void k_extract_inv(const double *W, int n, const int *pivrow, double *inv) {
+  const int k = blockIdx.x;
+  const int pk = pivrow[k];
+  for (int j = threadIdx.x; j < n; j += blockDim.x) inv[(long)k * n + pivrow[j]] = W[(long)pk * n + j];
 }
 
 int coarse_factor(exf_sys *s) {
   SysLevel &L = s->L[0];
   const int n = L.ndof;
   cudaStream_t st = s->stream;
-  DBuf<double> vals, colk;
-  DBuf<int> bad;
+  DBuf<double> vals, colk, rowp, bm;
+  DBuf<int> bad, pivrow, used, bi;
   EXF_TRY(vals.alloc(L.nnz));
   EXF_TRY(csr_values(s, 0, vals.p));
-  EXF_TRY(s->coarse_work.alloc((size_t)n * 2 * n));
-  EXF_TRY(s->coarse_work.zero(st));
+  EXF_TRY(s->coarse_work.alloc((size_t)n * n));
   EXF_TRY(colk.alloc(n));
+  EXF_TRY(rowp.alloc(n));
+  EXF_TRY(pivrow.alloc(n));
+  EXF_TRY(used.alloc(n));
+  EXF_TRY(used.zero(st));
   EXF_TRY(bad.alloc(1));
   EXF_TRY(bad.zero(st));
   double *W = s->coarse_work.p;
   k_dense_from_csr<<<n, 128, 0, st>>>(L.csr_ptr.p, L.csr_col.p, vals.p, n, W);
   k_gauge_rows<<<n, 128, 0, st>>>(W, n, s->gmask0.p);
   EXF_LAUNCH_CHECK();
-  for (int k = 0; k < n; k++) {
-    k_gj_pivot<<<1, 1024, 0, st>>>(W, n, k, colk.p, bad.p);
-    dim3 grid((unsigned)std::min<long>(8, nblk(2 * n - k, 256)), n);
-    k_gj_elim<<<grid, 256, 0, st>>>(W, n, k, colk.p);
-  }
-  EXF_LAUNCH_CHECK();
+  constexpr int NT = 256;
+  int dev = 0, nsm = 0, per_sm = 0;
+  EXF_CUDA(cudaGetDevice(&dev));
+  EXF_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  EXF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_gj_coop<NT>, NT, 0));
+  long want = ((long)n * n + NT - 1) / NT;
+  int grid = (int)std::min<long>(std::max(1, nsm * std::min(per_sm, 2)), std::max<long>(1, want));
+  EXF_TRY(bm.alloc(grid));
+  EXF_TRY(bi.alloc(grid));
+  void *args[] = {&W, (void *)&n, &pivrow.p, &colk.p, &rowp.p, &bm.p, &bi.p, &used.p, &bad.p};
+  EXF_CUDA(cudaLaunchCooperativeKernel((void *)k_gj_coop<NT>, grid, NT, args, 0, st));
+  EXF_COUNT(3);
   if (s->coarse_inv.n != (size_t)n * n) {
     EXF_TRY(s->coarse_inv.alloc((size_t)n * n));
     s->buf_epoch++;
   }
-  k_extract_inv<<<n, 128, 0, st>>>(W, n, s->coarse_inv.p);
+  k_extract_inv<<<n, 128, 0, st>>>(W, n, pivrow.p, s->coarse_inv.p);
   EXF_LAUNCH_CHECK();
   int hbad = 0;
   EXF_CUDA(cudaMemcpyAsync(&hbad, bad.p, sizeof(int), cudaMemcpyDeviceToHost, st));

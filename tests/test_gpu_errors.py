@@ -1,0 +1,87 @@
+"""Failure detection on the device path, injected on the host (needs a B200): every
+failure comes back as a status code with a message and the context stays usable.
+No test faults, traps or hangs the GPU."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import exfemus_b200 as ex
+from exfemus_b200 import _lib
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture()
+def heat(gpu_lib):
+    m = ex.Mesh(2, 3, (4, 4), (0, 1, 0, 1))
+    t = ex.MGSolT(m)
+    t.GenBc(_lib.BC_HEAT_DIRICHLET)
+    t.set_source(np.ones(m.nel(2)))
+    return t
+
+
+def _solve_rc(t, **kw):
+    st = _lib.ExfSolveStats()
+    p = ex.mg_params(**kw)
+    return _lib.load().exf_mg_solve(t.h, C.byref(p), C.byref(st)), st
+
+
+def test_solve_before_assembly_is_a_state_error(heat):
+    rc, _ = _solve_rc(heat)
+    assert rc == _lib.EXF_ERR_STATE
+
+
+def test_nan_in_rhs_reports_divergence_and_context_survives(heat):
+    heat.assemble_all()
+    b = heat.rhs()
+    b[7] = np.nan
+    heat.set_rhs(b)
+    rc, st = _solve_rc(heat, max_cycles=5)
+    assert rc == _lib.EXF_ERR_DIVERGED
+    assert b"diverged" in _lib.load().exf_last_error()
+    heat.assemble_all()  # the same context keeps working
+    rc, st = _solve_rc(heat)
+    assert rc == _lib.EXF_OK and st.converged
+
+
+def test_cycle_limit_reports_not_converged(heat):
+    heat.assemble_all()
+    heat.set_x(np.zeros(heat.ntop_dof))
+    rc, st = _solve_rc(heat, max_cycles=1, eps=1e-14)
+    assert rc == _lib.EXF_ERR_NOT_CONVERGED and st.cycles == 1
+
+
+def test_bad_arguments(heat):
+    L = _lib.load()
+    n = C.c_int()
+    assert L.exf_sys_ndof(heat.h, 99, C.byref(n)) == _lib.EXF_ERR_ARG
+    rc, _ = _solve_rc(heat, cond_corr=1)
+    assert rc in (_lib.EXF_ERR_STATE, _lib.EXF_ERR_UNSUPPORTED)
+    heat.assemble_all()
+    rc, _ = _solve_rc(heat, cond_corr=1)
+    assert rc == _lib.EXF_ERR_UNSUPPORTED
+
+
+def test_unsupported_ns_traction_flag(gpu_lib):
+    m = ex.Mesh(2, 2, (2, 2), (0, 1, 0, 1))
+    ns = ex.MGSolNS(m)
+    ns.GenBc(_lib.BC_CHANNEL if False else _lib.BC_CAVITY)
+    b0, b1 = ns.bc()
+    i = int(np.where(b0[:m.ntop] == 1)[0][0])
+    b1[i] = 2  # tangential-traction flag on a natural velocity DOF
+    ns.set_bc(b0, b1)
+    with pytest.raises(_lib.ExfError) as e:
+        ns.assemble_all()
+    assert e.value.code == _lib.EXF_ERR_UNSUPPORTED
+
+
+def test_graph_and_eager_cycles_agree_bitwise(heat):
+    heat.assemble_all()
+    xs = []
+    for g in (0, 1):
+        heat.set_x(np.zeros(heat.ntop_dof))
+        st = heat.solve(ex.mg_params(use_graph=g, precision=_lib.PREC_MIXED))
+        assert st.converged
+        xs.append(heat.x())
+    assert np.array_equal(xs[0], xs[1])
