@@ -220,7 +220,7 @@ static int mg_step(exf_sys *s, int lev, const exf_mg_params *p, bool final_resid
   EXF_TRY(spmv_resid<T>(s, lev, x, b, r, nullptr));
   SysLevel &C = s->L[lev - 1];
   EXF_TRY(restrict_op<T>(s, lev - 1, r, lvb<T>(C)));
-  EXF_CUDA(cudaMemsetAsync(lvx<T>(C), 0, C.ndof * sizeof(T), s->stream));
+  EXF_TRY(zero_vec<T>(s->stream, lvx<T>(C), C.ndof));
   for (int g = 0; g < p->gamma; g++) EXF_TRY(mg_step<T>(s, lev - 1, p, false, nullptr));
   EXF_TRY(prolong_add<T>(s, lev, lvx<T>(C), x, p->corr_damp));
   EXF_TRY(smooth<T>(s, lev, p, p->nu_post * mul, x, b));
@@ -238,7 +238,7 @@ int vcycle_fp64(exf_sys *s, const exf_mg_params *p, double *d_norm2) {
 int vcycle_mixed(exf_sys *s, const exf_mg_params *p) {
   SysLevel &T = s->L[s->nlev - 1];
   EXF_TRY(cast_d2f(s->stream, T.r.p, T.b32.p, T.ndof));
-  EXF_CUDA(cudaMemsetAsync(T.x32.p, 0, T.ndof * sizeof(float), s->stream));
+  EXF_TRY(zero_vec<float>(s->stream, T.x32.p, T.ndof));
   EXF_TRY(mg_step<float>(s, s->nlev - 1, p, false, nullptr));
   EXF_TRY(add_f2d(s->stream, T.x32.p, T.x.p, T.ndof));
   return gauge_shift(s, T.x.p);
@@ -858,6 +858,11 @@ int exf_mg_solve(exf_sys *s, const exf_mg_params *p, exf_solve_stats *st) {
   double rel = sqrt(r2) / den;
   st->rel_res = rel;
   int rc = EXF_OK;
+  if (!std::isfinite(rel) || !std::isfinite(bn)) {
+    set_error("multigrid diverged: non-finite initial residual or rhs");
+    rc = EXF_ERR_DIVERGED;
+    rel = p->eps;  // skip the cycle loop
+  }
   while (rel > p->eps && st->cycles < p->max_cycles) {
     // the first cycle runs eagerly (it sizes every scratch buffer); later cycles replay a
     // captured CUDA graph of the whole cycle when use_graph is set
@@ -882,7 +887,7 @@ int exf_mg_solve(exf_sys *s, const exf_mg_params *p, exf_solve_stats *st) {
   float ms = 0.f;
   cudaEventElapsedTime(&ms, s->ev0, s->ev1);
   st->seconds = ms * 1e-3;
-  st->converged = rel <= p->eps;
+  st->converged = rc == EXF_OK && rel <= p->eps;
   if (rc == EXF_OK && !st->converged) {
     set_error("not converged: rel %.3e after %d cycles", rel, st->cycles);
     rc = EXF_ERR_NOT_CONVERGED;

@@ -52,6 +52,29 @@ void count_launch(int n);  // kernels launched by the library (all streams)
     if (rc__ != EXF_OK) return rc__; \
   } while (0)
 
+// Programmatic dependent launch: kernels of the multigrid chain are launched with
+// programmatic stream serialisation so the next launch is set up while the previous grid
+// drains; every such kernel starts with EXF_PDL_WAIT (griddepcontrol.wait), before its
+// first global read, so it still observes all writes of the preceding grid.  Launched
+// without the attribute the wait is a no-op.
+#define EXF_PDL_WAIT() asm volatile("griddepcontrol.wait;" ::: "memory")
+
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
+                              Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...);
+}
+
 // device buffer with RAII
 template <class T>
 struct DBuf {
@@ -232,6 +255,8 @@ template <class T>
 int coarse_apply(exf_sys *s, const T *b, T *x);
 int gauge_shift(exf_sys *s, double *x);
 int cast_d2f(cudaStream_t st, const double *a, float *b, long n);
+template <class T>
+int zero_vec(cudaStream_t st, T *a, long n);
 int add_f2d(cudaStream_t st, const float *a, double *b, long n);
 int norm2(exf_sys *s, const double *v, long n, double *d_out);
 int vcycle_fp64(exf_sys *s, const exf_mg_params *p, double *d_relres);

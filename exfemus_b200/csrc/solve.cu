@@ -62,6 +62,7 @@ __device__ __forceinline__ double block_sum(double v, double *sh) {
   return r;
 }
 __global__ void k_reduce_partials(const double *part, int n, double *out) {
+  EXF_PDL_WAIT();
   __shared__ double sh[32];
   double v = 0.;
   for (int i = threadIdx.x; i < n; i += blockDim.x) v += part[i];
@@ -133,6 +134,7 @@ __global__ void __launch_bounds__(NT)
                  const T *__restrict__ vv, const T *__restrict__ vp, const T *__restrict__ pv,
                  const T *__restrict__ pp, const T *__restrict__ x, const T *__restrict__ b, T *__restrict__ r,
                  double *__restrict__ part) {
+  EXF_PDL_WAIT();
   __shared__ double sh[32];
   const int lane = threadIdx.x % LPR;
   const long g = ((long)blockIdx.x * NT + threadIdx.x) / LPR;
@@ -191,14 +193,12 @@ static int launch_spmv(exf_sys *s, int lev, const T *x, const T *b, T *r, double
   long ngroups = (long)L.N + (NS ? L.NL : 0);
   unsigned grid = nblk(ngroups * LPR, NT);
   if (d_norm2) EXF_TRY(ensure_partials(s, grid));
-  k_spmv_resid<T, D, LPR, NS, NT><<<grid, NT, 0, s->stream>>>(
-      L.N, L.NL, L.qq_ptr.p, L.qq_col.p, L.ql_ptr.p, L.ql_col.p, L.nqq, L.nql, L.nqqL, VT<T>::vv(L), VT<T>::vp(L),
-      VT<T>::pv(L), VT<T>::pp(L), x, b, r, d_norm2 ? s->red.part.p : nullptr);
-  EXF_LAUNCH_CHECK();
+  EXF_CUDA(launch_pdl(k_spmv_resid<T, D, LPR, NS, NT>, dim3(grid), dim3(NT), 0, s->stream, L.N, L.NL, L.qq_ptr.p,
+                      L.qq_col.p, L.ql_ptr.p, L.ql_col.p, L.nqq, L.nql, L.nqqL, VT<T>::vv(L), VT<T>::vp(L),
+                      VT<T>::pv(L), VT<T>::pp(L), x, b, r, d_norm2 ? s->red.part.p : nullptr));
   EXF_COUNT(1);
   if (d_norm2) {
-    k_reduce_partials<<<1, 1024, 0, s->stream>>>(s->red.part.p, grid, d_norm2);
-    EXF_LAUNCH_CHECK();
+    EXF_CUDA(launch_pdl(k_reduce_partials, dim3(1), dim3(1024), 0, s->stream, s->red.part.p, (int)grid, d_norm2));
     EXF_COUNT(1);
   }
   return EXF_OK;
@@ -222,6 +222,7 @@ __global__ void k_restrict(int nv2, int nv1, int Nc, int NLc, int Nf, const int 
                            const int *__restrict__ rl_ptr, const int *__restrict__ rl_col,
                            const T *__restrict__ rl_val, const double *__restrict__ mask, const T *__restrict__ rf,
                            T *__restrict__ bc) {
+  EXF_PDL_WAIT();
   long row = (long)blockIdx.x * blockDim.x + threadIdx.x;
   long nq = (long)nv2 * Nc;
   if (row >= nq + (long)nv1 * NLc) return;
@@ -243,10 +244,9 @@ int restrict_op(exf_sys *s, int lev_c, const T *r_f, T *b_c) {
   SysLevel &C = s->L[lev_c];
   SysLevel &F = s->L[lev_c + 1];
   long nrow = C.ndof;
-  k_restrict<T><<<nblk(nrow, 256), 256, 0, s->stream>>>(
-      s->nv2, s->nv1, C.N, C.NL, F.N, C.Rq.ptr.p, C.Rq.col.p, VT<T>::pq(C.Rq), s->nv1 ? C.Rl.ptr.p : nullptr,
-      s->nv1 ? C.Rl.col.p : nullptr, s->nv1 ? VT<T>::pq(C.Rl) : nullptr, C.rmask.p, r_f, b_c);
-  EXF_LAUNCH_CHECK();
+  EXF_CUDA(launch_pdl(k_restrict<T>, dim3(nblk(nrow, 256)), dim3(256), 0, s->stream, s->nv2, s->nv1, C.N, C.NL, F.N,
+                      C.Rq.ptr.p, C.Rq.col.p, VT<T>::pq(C.Rq), s->nv1 ? C.Rl.ptr.p : nullptr,
+                      s->nv1 ? C.Rl.col.p : nullptr, s->nv1 ? VT<T>::pq(C.Rl) : nullptr, C.rmask.p, r_f, b_c));
   EXF_COUNT(1);
   return EXF_OK;
 }
@@ -260,6 +260,7 @@ __global__ void k_prolong(int nv2, int nv1, int Nf, int NLf, int Nc, const int *
                           const int *__restrict__ pl_ptr, const int *__restrict__ pl_col,
                           const T *__restrict__ pl_val, const T *__restrict__ xc, T *__restrict__ xf, T damp,
                           int overwrite, const double *cond_rest) {
+  EXF_PDL_WAIT();
   if (cond_rest && !(cond_rest[1] < cond_rest[0])) return;
   long row = (long)blockIdx.x * blockDim.x + threadIdx.x;
   long nq = (long)nv2 * Nf;
@@ -284,10 +285,10 @@ static int prolong_impl(exf_sys *s, int lev_f, const T *x_c, T *x_f, double damp
   SysLevel &F = s->L[lev_f];
   SysLevel &C = s->L[lev_f - 1];
   long nrow = F.ndof;
-  k_prolong<T><<<nblk(nrow, 256), 256, 0, s->stream>>>(
-      s->nv2, s->nv1, F.N, F.NL, C.N, F.Pq.ptr.p, F.Pq.col.p, VT<T>::pq(F.Pq), s->nv1 ? F.Pl.ptr.p : nullptr,
-      s->nv1 ? F.Pl.col.p : nullptr, s->nv1 ? VT<T>::pq(F.Pl) : nullptr, x_c, x_f, (T)damp, overwrite, cond);
-  EXF_LAUNCH_CHECK();
+  EXF_CUDA(launch_pdl(k_prolong<T>, dim3(nblk(nrow, 256)), dim3(256), 0, s->stream, s->nv2, s->nv1, F.N, F.NL, C.N,
+                      F.Pq.ptr.p, F.Pq.col.p, VT<T>::pq(F.Pq), s->nv1 ? F.Pl.ptr.p : nullptr,
+                      s->nv1 ? F.Pl.col.p : nullptr, s->nv1 ? VT<T>::pq(F.Pl) : nullptr, x_c, x_f, (T)damp, overwrite,
+                      cond));
   EXF_COUNT(1);
   return EXF_OK;
 }
@@ -312,6 +313,7 @@ template <class T, int LPR>
 __global__ void k_gs_colour(const int *__restrict__ items, int nitems, const int *__restrict__ qq_ptr,
                             const int *__restrict__ qq_col, const int *__restrict__ diag_pos,
                             const T *__restrict__ vv, const T *__restrict__ b, T *x) {
+  EXF_PDL_WAIT();
   const int lane = threadIdx.x % LPR;
   const long g = ((long)blockIdx.x * blockDim.x + threadIdx.x) / LPR;
   const bool valid = g < nitems;  // all lanes reach the shuffles
@@ -348,6 +350,7 @@ __global__ void __launch_bounds__(NT)
                  const T *__restrict__ vv, const T *__restrict__ vp, const T *__restrict__ pv,
                  const T *__restrict__ pp, const T *__restrict__ x, const T *__restrict__ b, T *__restrict__ res,
                  long pres_off) {
+  EXF_PDL_WAIT();
   const int lane = threadIdx.x % LPR;
   const long g = ((long)blockIdx.x * NT + threadIdx.x) / LPR;
   const bool vel = g < nrows;
@@ -430,6 +433,7 @@ __global__ void __launch_bounds__(NT)
     k_vanka_solve(const int *__restrict__ items, int N, const int *__restrict__ qq_ptr,
                   const int *__restrict__ vrows, const int *__restrict__ pstart, const T *__restrict__ vk,
                   const T *__restrict__ pk, const T *__restrict__ res, long pres_off, T *__restrict__ x, T omega) {
+  EXF_PDL_WAIT();
   __shared__ double s_red[NT / 32];
   const int m = items[blockIdx.x];
   const int K = qq_ptr[m + 1] - qq_ptr[m];
@@ -483,14 +487,12 @@ static int vanka_sweep(exf_sys *s, int lev, const exf_mg_params *p, T *x, const 
     if (n == 0) continue;
     const int nr = L.vrow_off[c + 1] - L.vrow_off[c];
     const int *items = L.col_items.p + L.col_off[c];
-    k_vanka_rows<T, D, LPR, NTR><<<nblk((long)(nr + n) * LPR, NTR), NTR, 0, s->stream>>>(
-        L.vrows.p + L.vrow_off[c], nr, L.vrow_off[c], items, n, L.N, L.qq_ptr.p, L.qq_col.p, L.ql_ptr.p,
-        L.ql_col.p, L.nqq, L.nql, L.nqqL, VT<T>::vv(L), VT<T>::vp(L), VT<T>::pv(L), VT<T>::pp(L), x, b, res,
-        pres_off);
-    k_vanka_solve<T, D, NTS><<<n, NTS, 0, s->stream>>>(items, L.N, L.qq_ptr.p, L.vrows.p, L.pstart.p,
-                                                        VK<T>::vk(L), VK<T>::pk(L), res, pres_off, x,
-                                                        (T)p->omega);
-    EXF_LAUNCH_CHECK();
+    EXF_CUDA(launch_pdl(k_vanka_rows<T, D, LPR, NTR>, dim3(nblk((long)(nr + n) * LPR, NTR)), dim3(NTR), 0, s->stream,
+                        L.vrows.p + L.vrow_off[c], nr, L.vrow_off[c], items, n, L.N, L.qq_ptr.p, L.qq_col.p,
+                        L.ql_ptr.p, L.ql_col.p, L.nqq, L.nql, L.nqqL, VT<T>::vv(L), VT<T>::vp(L), VT<T>::pv(L),
+                        VT<T>::pp(L), x, b, res, pres_off));
+    EXF_CUDA(launch_pdl(k_vanka_solve<T, D, NTS>, dim3(n), dim3(NTS), 0, s->stream, items, L.N, L.qq_ptr.p,
+                        L.vrows.p, L.pstart.p, VK<T>::vk(L), VK<T>::pk(L), res, pres_off, x, (T)p->omega));
     EXF_COUNT(2);
   }
   return EXF_OK;
@@ -523,9 +525,8 @@ static int gs_sweep(exf_sys *s, int lev, const exf_mg_params *p, T *x, const T *
     const int c = p->reverse_colours ? L.ncolour - 1 - cc : cc;
     const int n = L.col_off[c + 1] - L.col_off[c];
     if (n == 0) continue;
-    k_gs_colour<T, LPR><<<nblk((long)n * LPR, 256), 256, 0, s->stream>>>(
-        L.col_items.p + L.col_off[c], n, L.qq_ptr.p, L.qq_col.p, L.diag_pos.p, VT<T>::vv(L), b, x);
-    EXF_LAUNCH_CHECK();
+    EXF_CUDA(launch_pdl(k_gs_colour<T, LPR>, dim3(nblk((long)n * LPR, 256)), dim3(256), 0, s->stream,
+                        L.col_items.p + L.col_off[c], n, L.qq_ptr.p, L.qq_col.p, L.diag_pos.p, VT<T>::vv(L), b, x));
     EXF_COUNT(1);
   }
   return EXF_OK;
@@ -720,6 +721,7 @@ int coarse_factor(exf_sys *s) {
 template <class T>
 __global__ void k_coarse_gemv(const double *__restrict__ inv, int n, const double *__restrict__ gmask,
                               const T *__restrict__ b, T *__restrict__ x) {
+  EXF_PDL_WAIT();
   const int row = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5), lane = threadIdx.x & 31;
   if (row >= n) return;
   double acc = 0.;
@@ -732,8 +734,8 @@ template <class T>
 int coarse_apply(exf_sys *s, const T *b, T *x) {
   if (!s->coarse_ok) EXF_TRY(coarse_factor(s));
   const int n = s->L[0].ndof;
-  k_coarse_gemv<T><<<nblk(n, 8), 256, 0, s->stream>>>(s->coarse_inv.p, n, s->gmask0.p, b, x);
-  EXF_LAUNCH_CHECK();
+  EXF_CUDA(launch_pdl(k_coarse_gemv<T>, dim3(nblk(n, 8)), dim3(256), 0, s->stream, s->coarse_inv.p, n, s->gmask0.p,
+                      b, x));
   EXF_COUNT(1);
   return EXF_OK;
 }
@@ -741,29 +743,45 @@ template int coarse_apply<double>(exf_sys *, const double *, double *);
 template int coarse_apply<float>(exf_sys *, const float *, float *);
 
 // ---------------------------------------------------------- vector helpers
+template <class T>
+__global__ void k_zero(T *a, long n) {
+  EXF_PDL_WAIT();
+  long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) a[i] = T(0);
+}
+template <class T>
+int zero_vec(cudaStream_t st, T *a, long n) {
+  EXF_CUDA(launch_pdl(k_zero<T>, dim3(nblk(n, 256)), dim3(256), 0, st, a, n));
+  EXF_COUNT(1);
+  return EXF_OK;
+}
+template int zero_vec<double>(cudaStream_t, double *, long);
+template int zero_vec<float>(cudaStream_t, float *, long);
+
 __global__ void k_cast_d2f(const double *a, float *b, long n) {
+  EXF_PDL_WAIT();
   long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) b[i] = (float)a[i];
 }
 __global__ void k_add_f2d(const float *a, double *b, long n) {
+  EXF_PDL_WAIT();
   long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) b[i] += (double)a[i];
 }
 int cast_d2f(cudaStream_t st, const double *a, float *b, long n) {
-  k_cast_d2f<<<nblk(n, 256), 256, 0, st>>>(a, b, n);
-  EXF_LAUNCH_CHECK();
+  EXF_CUDA(launch_pdl(k_cast_d2f, dim3(nblk(n, 256)), dim3(256), 0, st, a, b, n));
   EXF_COUNT(1);
   return EXF_OK;
 }
 int add_f2d(cudaStream_t st, const float *a, double *b, long n) {
-  k_add_f2d<<<nblk(n, 256), 256, 0, st>>>(a, b, n);
-  EXF_LAUNCH_CHECK();
+  EXF_CUDA(launch_pdl(k_add_f2d, dim3(nblk(n, 256)), dim3(256), 0, st, a, b, n));
   EXF_COUNT(1);
   return EXF_OK;
 }
 
 template <int NT>
 __global__ void k_norm2_part(const double *v, long n, double *part) {
+  EXF_PDL_WAIT();
   __shared__ double sh[32];
   double acc = 0.;
   for (long i = (long)blockIdx.x * NT + threadIdx.x; i < n; i += (long)gridDim.x * NT) acc += v[i] * v[i];
@@ -781,8 +799,10 @@ int norm2(exf_sys *s, const double *v, long n, double *d_out) {
 }
 
 // pressure gauge: p -= p[gauge] on the top level
-__global__ void k_gauge_read(const double *x, long idx, double *out) { *out = x[idx]; }
+__global__ void k_gauge_read(const double *x, long idx, double *out) {
+  EXF_PDL_WAIT(); *out = x[idx]; }
 __global__ void k_gauge_sub(double *p, int n, const double *v) {
+  EXF_PDL_WAIT();
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) p[i] -= *v;
 }
@@ -790,9 +810,10 @@ int gauge_shift(exf_sys *s, double *x) {
   if (s->kind != EXF_KIND_NS || s->gauge_node < 0) return EXF_OK;
   SysLevel &T = s->L[s->nlev - 1];
   double *p = x + (long)s->nv2 * T.N;
-  k_gauge_read<<<1, 1, 0, s->stream>>>(p, s->gauge_node, s->red.out.p + 8);
-  k_gauge_sub<<<nblk(T.NL, 256), 256, 0, s->stream>>>(p, T.NL, s->red.out.p + 8);
-  EXF_LAUNCH_CHECK();
+  EXF_CUDA(launch_pdl(k_gauge_read, dim3(1), dim3(1), 0, s->stream, (const double *)p, (long)s->gauge_node,
+                      s->red.out.p + 8));
+  EXF_CUDA(launch_pdl(k_gauge_sub, dim3(nblk(T.NL, 256)), dim3(256), 0, s->stream, p, T.NL,
+                      (const double *)(s->red.out.p + 8)));
   EXF_COUNT(2);
   return EXF_OK;
 }
