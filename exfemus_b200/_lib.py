@@ -118,6 +118,7 @@ SIGNATURES = [
     ("exf_event_elapsed", _I, [_P, _I, _I, _DP]),
     ("exf_launch_count", C.c_longlong, []),
     ("exf_level_bytes", _I, [_P, _I, _I, _DP, _DP]),
+    ("exf_resid_norm_static", _I, [_P, _I, _P, _P, _P, _P]),
 ]
 
 

@@ -186,6 +186,17 @@ EXF_API int exf_sync(exf_sys *s);
 EXF_API int exf_event_record(exf_sys *s, int slot);
 EXF_API int exf_event_elapsed(exf_sys *s, int slot_a, int slot_b, double *ms);
 EXF_API long long exf_launch_count(void);
+/* Allocation-free residual: r = b - A x on level lev and ||r||^2, for callers that cannot
+ * allocate device memory while they run (the host application owns every allocation,
+ * or memory is reserved before a run).  x, b, r and norm2 are DEVICE buffers owned by the
+ * caller (ndof doubles; norm2 one double).  The norm's per-block partial sums live in a
+ * fixed file-scope device array of 32768 doubles held by every GPU that loads the
+ * library; levels needing more partial sums are rejected with EXF_ERR_ARG.  Nothing is
+ * allocated or freed.  The first call on a device resolves the array's device address,
+ * so make that first call before any stream capture.  All calls share the array: calls
+ * that overlap on the GPU race.  It has no counterpart in the reference. */
+EXF_API int exf_resid_norm_static(exf_sys *s, int lev, const double *x, const double *b, double *r,
+                                  double *norm2);
 /* algorithmic bytes of one residual (spmv) and one smoother sweep on level lev */
 EXF_API int exf_level_bytes(exf_sys *s, int lev, int precision, double *spmv_bytes, double *sweep_bytes);
 
