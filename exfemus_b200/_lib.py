@@ -28,6 +28,9 @@ SMOOTH_GS = 0
 SMOOTH_VANKA = 1
 PREC_FP64 = 0
 PREC_MIXED = 1
+VANKA_AUTO = 0
+VANKA_TILE = 1
+VANKA_ROWS = 2
 
 
 class ExfMeshDesc(C.Structure):
@@ -47,7 +50,7 @@ class ExfMgParams(C.Structure):
                 ("nu_pre", C.c_int), ("nu_post", C.c_int), ("double_below_top", C.c_int),
                 ("smoother", C.c_int), ("omega", C.c_double), ("corr_damp", C.c_double),
                 ("cond_corr", C.c_int), ("reverse_colours", C.c_int), ("precision", C.c_int),
-                ("use_graph", C.c_int)]
+                ("use_graph", C.c_int), ("vanka_kernel", C.c_int)]
 
 
 class ExfSolveStats(C.Structure):

@@ -220,7 +220,7 @@ static int mg_step(exf_sys *s, int lev, const exf_mg_params *p, bool final_resid
   EXF_TRY(spmv_resid<T>(s, lev, x, b, r, nullptr));
   SysLevel &C = s->L[lev - 1];
   EXF_TRY(restrict_op<T>(s, lev - 1, r, lvb<T>(C)));
-  EXF_TRY(zero_vec<T>(s->stream, lvx<T>(C), C.ndof));
+  EXF_TRY(zero_vec<T>(s->stream, lvx<T>(C), sizeof(T) == 4 ? C.len32 : (long)C.ndof));
   for (int g = 0; g < p->gamma; g++) EXF_TRY(mg_step<T>(s, lev - 1, p, false, nullptr));
   EXF_TRY(prolong_add<T>(s, lev, lvx<T>(C), x, p->corr_damp));
   EXF_TRY(smooth<T>(s, lev, p, p->nu_post * mul, x, b));
@@ -237,10 +237,11 @@ int vcycle_fp64(exf_sys *s, const exf_mg_params *p, double *d_norm2) {
 // mixed: r64 = b - A x (already in L.r), cast, FP32 cycle, x += e
 int vcycle_mixed(exf_sys *s, const exf_mg_params *p) {
   SysLevel &T = s->L[s->nlev - 1];
-  EXF_TRY(cast_d2f(s->stream, T.r.p, T.b32.p, T.ndof));
-  EXF_TRY(zero_vec<float>(s->stream, T.x32.p, T.ndof));
+  const int i4 = s->nv1 ? 1 : 0;
+  EXF_TRY(cast_d2f(s->stream, T.r.p, T.b32.p, T.ndof, i4, T.N, s->nv2));
+  EXF_TRY(zero_vec<float>(s->stream, T.x32.p, T.len32));
   EXF_TRY(mg_step<float>(s, s->nlev - 1, p, false, nullptr));
-  EXF_TRY(add_f2d(s->stream, T.x32.p, T.x.p, T.ndof));
+  EXF_TRY(add_f2d(s->stream, T.x32.p, T.x.p, T.ndof, i4, T.N, s->nv2));
   return gauge_shift(s, T.x.p);
 }
 
@@ -367,7 +368,8 @@ int exf_sys_create(exf_mesh *m, int kind, exf_sys **out) {
   s->nv2 = kind == EXF_KIND_T ? 1 : m->dim;
   s->nv1 = kind == EXF_KIND_T ? 0 : 1;
   s->nvars = s->nv2 + s->nv1;
-  if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess ||
+  if (cudaDeviceGetAttribute(&s->nsm, cudaDevAttrMultiProcessorCount, m->device) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaEventCreate(&s->ev0) != cudaSuccess || cudaEventCreate(&s->ev1) != cudaSuccess) {
     set_error("exf_sys_create: stream/event creation failed");
     delete s;
@@ -781,6 +783,7 @@ static unsigned long long params_key(const exf_mg_params *p) {
   mix(c);
   mix((unsigned long long)p->reverse_colours);
   mix((unsigned long long)p->precision);
+  mix((unsigned long long)p->vanka_kernel);
   return h | 1ull;
 }
 

@@ -14,6 +14,7 @@
 //   vectors        DOF order of MGSolDA::init_dof: component-major Q2 variables, then
 //                  the Q1 variable on the first NL nodes.
 #pragma once
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -55,9 +56,16 @@ void count_launch(int n);  // kernels launched by the library (all streams)
 // Programmatic dependent launch: kernels of the multigrid chain are launched with
 // programmatic stream serialisation so the next launch is set up while the previous grid
 // drains; every such kernel starts with EXF_PDL_WAIT (griddepcontrol.wait), before its
-// first global read, so it still observes all writes of the preceding grid.  Launched
-// without the attribute the wait is a no-op.
-#define EXF_PDL_WAIT() asm volatile("griddepcontrol.wait;" ::: "memory")
+// first global read, so it still observes all writes of the preceding grid.  Right after
+// the wait it releases its own dependents (griddepcontrol.launch_dependents): their
+// blocks may then be scheduled onto free SM slots, where they block in their own wait
+// until this grid has completed and its writes are visible.  Launched without the
+// attribute both instructions are no-ops.
+#define EXF_PDL_WAIT()                                                \
+  do {                                                                \
+    asm volatile("griddepcontrol.wait;" ::: "memory");                \
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");   \
+  } while (0)
 
 template <typename... KArgs, typename... Args>
 inline cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
@@ -175,6 +183,14 @@ struct SysLevel {
   // g of vrows is the (patch, star node) pair g, so per-entry data is stored compactly
   std::vector<int> vrow_off;   // [ncolour+1]
   DBuf<int> vrows;
+  DBuf<int4> vrinfo;           // per vrows entry: {node, qq_ptr[node], ql_ptr[node],
+                               //   nqq | nql << 8 | index of the node in its patch's tile << 16}
+  DBuf<int4> pinfo;            // per patch in colour order, two int4: {m, pstart[m], qq_ptr[m],
+                               //   ql_ptr[m]}, {nqq(m), nql(m), lattice coordinates of m packed, 0}
+  int Ll[3] = {1, 1, 1};       // Q2 node lattice of this level
+  DBuf<int> latnode;           // [N] node at each lattice point (x fastest)
+  DBuf<int16_t> tcq, tcl;      // per qq / ql block: column minus row as a 9^d-tile index step
+  bool tile_ok = false;        // every star and row fits the tile kernels (5^d nodes)
   DBuf<int> pstart;            // [NL] first vrows entry of each patch (by pressure node)
   DBuf<double> vk64, pk64;     // per entry*D: {1/a, D/a, G/a}; per patch: {S, c_mm}
   DBuf<float> vk32, pk32;
@@ -182,12 +198,22 @@ struct SysLevel {
   DBuf<float> vres32;
   LevelVals<double> A;
   LevelVals<float> A32;
+  // NS, FP32 smoother only: velocity blocks in FP16 scaled per (node, component) row by
+  // the row's largest magnitude vsc[a*N+n] (entries in [-1,1]; value = stored * vsc).
+  // 3D: per block a 16-byte record of values 0..7 (h16), {column, value 8} (h16cx) and
+  // {value 8, tile step} (h16qc, padded for 16-byte chunk reads); 2D: per block an
+  // 8-byte record of values 0..3 (h16), columns from qq_col
+  DBuf<uint4> h16;
+  DBuf<uint2> h16cx;
+  DBuf<uint32_t> h16qc;
+  DBuf<float> vsc;
   // transfers: Pq/Pl from level-1 to this level (fine rows), Rq/Rl from this level+1
   Transfer Pq, Pl, Rq, Rl;
   DBuf<double> rmask;    // [ndof] restriction row mask (bc0 % 2 of the top DOF)
   // vectors
   DBuf<double> x, b, r, dx;     // dx: smoother scratch (Vanka star-row residuals)
-  DBuf<float> x32, b32, r32, dx32;
+  DBuf<float> x32, b32, r32, dx32;  // NS: node-interleaved float4 per node (4N floats)
+  long len32 = 0;                   // length of the FP32 V-cycle vectors
 };
 
 struct Partials {
@@ -212,6 +238,7 @@ struct exf_sys {
   exf::DBuf<int> coarse_piv;
   exf::DBuf<double> gmask0;                 // coarse gauge mask (0 at gauge DOFs)
   int coarse_ok = 0;
+  int nsm = 148;                             // SMs of the system's device
   int gauge_node = -1;                      // top-level pressure gauge node (-1 none)
   int assembled = 0;
   int transposed = 0;
@@ -254,10 +281,10 @@ int smooth(exf_sys *s, int lev, const exf_mg_params *p, int nsweeps, T *x, const
 template <class T>
 int coarse_apply(exf_sys *s, const T *b, T *x);
 int gauge_shift(exf_sys *s, double *x);
-int cast_d2f(cudaStream_t st, const double *a, float *b, long n);
+int cast_d2f(cudaStream_t st, const double *a, float *b, long n, int i4, int N, int d);
 template <class T>
 int zero_vec(cudaStream_t st, T *a, long n);
-int add_f2d(cudaStream_t st, const float *a, double *b, long n);
+int add_f2d(cudaStream_t st, const float *a, double *b, long n, int i4, int N, int d);
 int norm2(exf_sys *s, const double *v, long n, double *d_out);
 int vcycle_fp64(exf_sys *s, const exf_mg_params *p, double *d_relres);
 int vcycle_mixed(exf_sys *s, const exf_mg_params *p);

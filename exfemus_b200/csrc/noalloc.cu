@@ -18,7 +18,7 @@
 #include "exf_internal.h"
 
 namespace exf {
-template <class T, int D, int LPR, bool NS, int NT>
+template <class T, int D, int LPR, bool NS, int NT, bool I4>
 __global__ void k_spmv_resid(int N, int NL, const int *__restrict__ qq_ptr, const int *__restrict__ qq_col,
                              const int *__restrict__ ql_ptr, const int *__restrict__ ql_col, long nqq, long nql,
                              long nqqL, const T *__restrict__ vv, const T *__restrict__ vp,
@@ -61,7 +61,7 @@ static int resid_norm_static(exf_sys *s, int lev, const double *x, const double 
     g_partials_addr[dev] = static_cast<double *>(ptr);
   }
   double *part = g_partials_addr[dev];
-  k_spmv_resid<double, D, LPR, NS, NT><<<(unsigned)grid, NT, 0, s->stream>>>(
+  k_spmv_resid<double, D, LPR, NS, NT, false><<<(unsigned)grid, NT, 0, s->stream>>>(
       L.N, L.NL, L.qq_ptr.p, L.qq_col.p, L.ql_ptr.p, L.ql_col.p, L.nqq, L.nql, L.nqqL, L.A.vv.p, L.A.vp.p, L.A.pv.p,
       L.A.pp.p, x, b, r, part);
   EXF_LAUNCH_CHECK();

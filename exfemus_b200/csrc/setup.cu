@@ -314,16 +314,24 @@ int build_patterns(exf_sys *s) {
       EXF_TRY(L.A32.vp.alloc((size_t)d * L.nql));
       EXF_TRY(L.A32.pv.alloc((size_t)d * L.nqqL));
       EXF_TRY(L.A32.pp.alloc(L.nllL));
+      EXF_TRY(L.h16.alloc(d == 3 ? (size_t)L.nqq : ((size_t)L.nqq + 1) / 2));
+      if (d == 3) EXF_TRY(L.h16cx.alloc((size_t)L.nqq));
+      if (d == 3) EXF_TRY(L.h16qc.alloc(((size_t)L.nqq + 7) & ~(size_t)3));  // 16-byte chunk reads past the end
+      EXF_TRY(L.vsc.alloc((size_t)d * L.N));
     }
     // vectors
     EXF_TRY(L.x.alloc(L.ndof));
     EXF_TRY(L.b.alloc(L.ndof));
     EXF_TRY(L.r.alloc(L.ndof));
     EXF_TRY(L.dx.alloc(L.ndof));
-    EXF_TRY(L.x32.alloc(L.ndof));
-    EXF_TRY(L.b32.alloc(L.ndof));
-    EXF_TRY(L.r32.alloc(L.ndof));
-    EXF_TRY(L.dx32.alloc(L.ndof));
+    L.len32 = s->nv1 ? 4L * L.N : (long)L.ndof;
+    EXF_TRY(L.x32.alloc(L.len32));
+    EXF_TRY(L.b32.alloc(L.len32));
+    EXF_TRY(L.r32.alloc(L.len32));
+    EXF_TRY(L.dx32.alloc(L.len32));
+    EXF_TRY(L.x32.zero(st));
+    EXF_TRY(L.b32.zero(st));
+    EXF_TRY(L.r32.zero(st));
     EXF_TRY(L.rmask.alloc(L.ndof));
     EXF_TRY(L.x.zero(st));
     EXF_TRY(L.x32.zero(st));
@@ -374,9 +382,48 @@ int build_colours(exf_sys *s) {
     if (s->kind == EXF_KIND_NS) {
       // star rows of every colour: the velocity nodes of pressure row m (qq(m)), patch by
       // patch; stars of one colour are disjoint, so each node appears once per colour
-      std::vector<int> qp(L.N + 1), qc(L.nqq);
+      std::vector<int> qp(L.N + 1), qc(L.nqq), lp(L.N + 1), lc(L.nql);
       EXF_CUDA(cudaMemcpy(qp.data(), L.qq_ptr.p, (L.N + 1) * sizeof(int), cudaMemcpyDeviceToHost));
       EXF_CUDA(cudaMemcpy(qc.data(), L.qq_col.p, L.nqq * sizeof(int), cudaMemcpyDeviceToHost));
+      EXF_CUDA(cudaMemcpy(lp.data(), L.ql_ptr.p, (L.N + 1) * sizeof(int), cudaMemcpyDeviceToHost));
+      EXF_CUDA(cudaMemcpy(lc.data(), L.ql_col.p, L.nql * sizeof(int), cudaMemcpyDeviceToHost));
+      // lattice of this level (Q2 nodes): the node at each lattice point, and the offset of
+      // every block's column from its row node as an index step in a 9^d tile
+      const int dim = m->dim;
+      for (int d = 0; d < 3; d++) L.Ll[d] = d < dim ? 2 * m->lev[l].ne[d] + 1 : 1;
+      if (L.Ll[0] > 2048 || L.Ll[1] > 2048 || L.Ll[2] > 1024) {
+        set_error("build_colours: level lattice %dx%dx%d exceeds the packed patch origin", L.Ll[0], L.Ll[1], L.Ll[2]);
+        return EXF_ERR_UNSUPPORTED;
+      }
+      auto latl = [&](int n, int d) { return d < dim ? m->lat[3 * (size_t)n + d] / sl : 0; };
+      std::vector<int> lnode(L.N);
+      for (int n = 0; n < L.N; n++) lnode[((size_t)latl(n, 2) * L.Ll[1] + latl(n, 1)) * L.Ll[0] + latl(n, 0)] = n;
+      const int tstep[3] = {1, 9, 81};
+      bool far = false;
+      auto tcode = [&](int n, int c) {
+        int v = 0;
+        for (int d = 0; d < dim; d++) {
+          const int dd = latl(c, d) - latl(n, d);
+          if (dd < -2 || dd > 2) far = true;
+          v += dd * tstep[d];
+        }
+        return (int16_t)v;
+      };
+      std::vector<int16_t> tq(L.nqq), tl(L.nql);
+      for (int n = 0; n < L.N; n++) {
+        for (int k = qp[n]; k < qp[n + 1]; k++) tq[k] = tcode(n, qc[k]);
+        for (int k = lp[n]; k < lp[n + 1]; k++) tl[k] = tcode(n, lc[k]);
+      }
+      if (far) {
+        set_error("build_colours: a block couples nodes more than 2 lattice steps apart");
+        return EXF_ERR_UNSUPPORTED;
+      }
+      EXF_TRY(L.latnode.alloc(L.N));
+      EXF_CUDA(cudaMemcpy(L.latnode.p, lnode.data(), L.N * sizeof(int), cudaMemcpyHostToDevice));
+      EXF_TRY(L.tcq.alloc(L.nqq));
+      EXF_CUDA(cudaMemcpy(L.tcq.p, tq.data(), L.nqq * sizeof(int16_t), cudaMemcpyHostToDevice));
+      EXF_TRY(L.tcl.alloc(L.nql));
+      EXF_CUDA(cudaMemcpy(L.tcl.p, tl.data(), L.nql * sizeof(int16_t), cudaMemcpyHostToDevice));
       std::vector<int> rows;
       std::vector<int> pst(L.NL, 0);
       L.vrow_off.assign(L.ncolour + 1, 0);
@@ -393,6 +440,34 @@ int build_colours(exf_sys *s) {
       EXF_CUDA(cudaMemcpy(L.vrows.p, rows.data(), rows.size() * sizeof(int), cudaMemcpyHostToDevice));
       EXF_TRY(L.pstart.alloc(L.NL));
       EXF_CUDA(cudaMemcpy(L.pstart.p, pst.data(), pst.size() * sizeof(int), cudaMemcpyHostToDevice));
+      // row descriptors of the star rows and of the patches (so the sweep kernels start
+      // their row products one dependent load earlier), in colour order
+      std::vector<int4> vri(rows.size()), pin(2 * (size_t)nitem);
+      int kmax = 0, rmax = 0;
+      for (int t = 0; t < nitem; t++) {
+        const int mm = items[t];
+        const int K = qp[mm + 1] - qp[mm];
+        kmax = std::max(kmax, K);
+        for (int g = pst[mm]; g < pst[mm] + K; g++) {
+          const int n = rows[g], nq = qp[n + 1] - qp[n], nl = lp[n + 1] - lp[n];
+          if (nq > 0xff || nl > 0xff) {
+            set_error("build_colours: node row of %d/%d blocks exceeds the packed range", nq, nl);
+            return EXF_ERR_UNSUPPORTED;
+          }
+          rmax = std::max(rmax, nq);
+          int tb = 0;
+          for (int d = 0; d < dim; d++) tb += (latl(n, d) - latl(mm, d) + 4) * tstep[d];
+          vri[g] = make_int4(n, qp[n], lp[n], nq | (nl << 8) | (tb << 16));
+        }
+        pin[2 * t] = make_int4(mm, pst[mm], qp[mm], lp[mm]);
+        pin[2 * t + 1] = make_int4(K, lp[mm + 1] - lp[mm], latl(mm, 0) | (latl(mm, 1) << 11) | (latl(mm, 2) << 22), 0);
+      }
+      const int smax = dim == 3 ? 125 : 25;
+      L.tile_ok = kmax <= smax && rmax <= smax;
+      EXF_TRY(L.vrinfo.alloc(vri.size()));
+      EXF_CUDA(cudaMemcpy(L.vrinfo.p, vri.data(), vri.size() * sizeof(int4), cudaMemcpyHostToDevice));
+      EXF_TRY(L.pinfo.alloc(pin.size()));
+      EXF_CUDA(cudaMemcpy(L.pinfo.p, pin.data(), pin.size() * sizeof(int4), cudaMemcpyHostToDevice));
       const size_t ne = rows.size() * (size_t)s->nv2;
       EXF_TRY(L.vk64.alloc(3 * ne));
       EXF_TRY(L.vk32.alloc(3 * ne));

@@ -13,6 +13,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <type_traits>
 #include <vector>
 
 #include "exf_internal.h"
@@ -80,15 +81,35 @@ static int ensure_partials(exf_sys *s, int nblk_needed) {
   return EXF_OK;
 }
 
+// Vector layouts.  DOF order: component a of node n at a*N + n, pressure of vertex m at
+// D*N + m.  I4 (FP32 Navier-Stokes V-cycle): the node's (u, v, w, p) as one float4 at
+// 4n, so a column gather is one 16-byte load; slot 3 of a non-vertex node stays zero.
+template <bool I4>
+struct Lay {
+  static __device__ __forceinline__ long v(int a, long n, long N) { return I4 ? 4 * n + a : (long)a * N + n; }
+  static __device__ __forceinline__ long p(long m, long N, int D) { return I4 ? 4 * m + 3 : (long)D * N + m; }
+};
+
 // acc[a] += sum over the node row n of the d x d blocks times x (and B^T times p);
 // two blocks per lane in flight
-template <class T, int D, int LPR, bool PRESSURE>
+template <class T, int D, int LPR, bool PRESSURE, bool I4 = false>
 __device__ __forceinline__ void node_row_dot(int n, int lane, int N, const int *__restrict__ qq_ptr,
                                              const int *__restrict__ qq_col, const int *__restrict__ ql_ptr,
                                              const int *__restrict__ ql_col, long nqq, long nql,
                                              const T *__restrict__ vv, const T *__restrict__ vp,
                                              const T *__restrict__ x, T acc[D]) {
   const int k0 = qq_ptr[n], k1 = qq_ptr[n + 1];
+  auto gather = [&](int c, T *xb) {
+    if constexpr (I4) {
+      const float4 v = reinterpret_cast<const float4 *>(x)[c];
+      xb[0] = v.x;
+      if (D > 1) xb[D > 1 ? 1 : 0] = v.y;
+      if (D > 2) xb[D > 2 ? 2 : 0] = v.z;
+    } else {
+#pragma unroll
+      for (int bb = 0; bb < D; bb++) xb[bb] = x[(long)bb * N + c];
+    }
+  };
   int k = k0 + lane;
   for (; k + LPR < k1; k += 2 * LPR) {
     const int c0 = qq_col[k], c1 = qq_col[k + LPR];
@@ -98,26 +119,24 @@ __device__ __forceinline__ void node_row_dot(int n, int lane, int N, const int *
       v0[q] = vv[(long)q * nqq + k];
       v1[q] = vv[(long)q * nqq + k + LPR];
     }
-#pragma unroll
-    for (int bb = 0; bb < D; bb++) {
-      x0[bb] = x[(long)bb * N + c0];
-      x1[bb] = x[(long)bb * N + c1];
-    }
+    gather(c0, x0);
+    gather(c1, x1);
 #pragma unroll
     for (int a = 0; a < D; a++)
 #pragma unroll
       for (int bb = 0; bb < D; bb++) acc[a] += v0[a * D + bb] * x0[bb] + v1[a * D + bb] * x1[bb];
   }
   if (k < k1) {
-    const int c0 = qq_col[k];
+    T x0[D];
+    gather(qq_col[k], x0);
 #pragma unroll
     for (int a = 0; a < D; a++)
 #pragma unroll
-      for (int bb = 0; bb < D; bb++) acc[a] += vv[(long)(a * D + bb) * nqq + k] * x[(long)bb * N + c0];
+      for (int bb = 0; bb < D; bb++) acc[a] += vv[(long)(a * D + bb) * nqq + k] * x0[bb];
   }
   if (PRESSURE) {
     for (int kp = ql_ptr[n] + lane; kp < ql_ptr[n + 1]; kp += LPR) {
-      const T p = x[(long)D * N + ql_col[kp]];
+      const T p = x[Lay<I4>::p(ql_col[kp], N, D)];
 #pragma unroll
       for (int a = 0; a < D; a++) acc[a] += vp[(long)a * nql + kp] * p;
     }
@@ -127,7 +146,7 @@ __device__ __forceinline__ void node_row_dot(int n, int lane, int N, const int *
 // ------------------------------------------------------------------ SpMV
 // row groups: g < N -> Q2 node g (d outputs), g >= N -> Q1 node g-N (1 output).
 // LPR lanes per row group; the node-block index k is shared by the d*d planes.
-template <class T, int D, int LPR, bool NS, int NT>
+template <class T, int D, int LPR, bool NS, int NT, bool I4>
 __global__ void __launch_bounds__(NT)
     k_spmv_resid(int N, int NL, const int *__restrict__ qq_ptr, const int *__restrict__ qq_col,
                  const int *__restrict__ ql_ptr, const int *__restrict__ ql_col, long nqq, long nql, long nqqL,
@@ -146,17 +165,17 @@ __global__ void __launch_bounds__(NT)
 #pragma unroll
   for (int a = 0; a < D; a++) acc[a] = T(0);
   if (vel) {
-    node_row_dot<T, D, LPR, NS>((int)g, lane, N, qq_ptr, qq_col, ql_ptr, ql_col, nqq, nql, vv, vp, x, acc);
+    node_row_dot<T, D, LPR, NS, I4>((int)g, lane, N, qq_ptr, qq_col, ql_ptr, ql_col, nqq, nql, vv, vp, x, acc);
   } else if (prs) {
     const int m = (int)(g - N);
     const int k0 = qq_ptr[m], k1 = qq_ptr[m + 1];
     for (int k = k0 + lane; k < k1; k += LPR) {
       const int nn = qq_col[k];
 #pragma unroll
-      for (int bb = 0; bb < D; bb++) acc[0] += pv[(long)bb * nqqL + k] * x[(long)bb * N + nn];
+      for (int bb = 0; bb < D; bb++) acc[0] += pv[(long)bb * nqqL + k] * x[Lay<I4>::v(bb, nn, N)];
     }
     const int l0 = ql_ptr[m], l1 = ql_ptr[m + 1];
-    for (int k = l0 + lane; k < l1; k += LPR) acc[0] += pp[k] * x[(long)D * N + ql_col[k]];
+    for (int k = l0 + lane; k < l1; k += LPR) acc[0] += pp[k] * x[Lay<I4>::p(ql_col[k], N, D)];
   }
 #pragma unroll
   for (int a = 0; a < D; a++)
@@ -167,13 +186,13 @@ __global__ void __launch_bounds__(NT)
     if (vel) {
 #pragma unroll
       for (int a = 0; a < D; a++) {
-        const long row = (long)a * N + g;
+        const long row = Lay<I4>::v(a, g, N);
         T rv = b ? b[row] - acc[a] : acc[a];
         r[row] = rv;
         nrm += (double)rv * (double)rv;
       }
     } else if (prs) {
-      const long row = (long)D * N + (g - N);
+      const long row = Lay<I4>::p(g - N, N, D);
       T rv = b ? b[row] - acc[0] : acc[0];
       r[row] = rv;
       nrm += (double)rv * (double)rv;
@@ -189,11 +208,12 @@ template <class T, int D, bool NS>
 static int launch_spmv(exf_sys *s, int lev, const T *x, const T *b, T *r, double *d_norm2) {
   SysLevel &L = s->L[lev];
   constexpr int NT = 256;
+  constexpr bool I4 = NS && sizeof(T) == 4;
   constexpr int LPR = D == 3 ? 32 : (NS ? 16 : 8);
   long ngroups = (long)L.N + (NS ? L.NL : 0);
   unsigned grid = nblk(ngroups * LPR, NT);
   if (d_norm2) EXF_TRY(ensure_partials(s, grid));
-  EXF_CUDA(launch_pdl(k_spmv_resid<T, D, LPR, NS, NT>, dim3(grid), dim3(NT), 0, s->stream, L.N, L.NL, L.qq_ptr.p,
+  EXF_CUDA(launch_pdl(k_spmv_resid<T, D, LPR, NS, NT, I4>, dim3(grid), dim3(NT), 0, s->stream, L.N, L.NL, L.qq_ptr.p,
                       L.qq_col.p, L.ql_ptr.p, L.ql_col.p, L.nqq, L.nql, L.nqqL, VT<T>::vv(L), VT<T>::vp(L),
                       VT<T>::pv(L), VT<T>::pp(L), x, b, r, d_norm2 ? s->red.part.p : nullptr));
   EXF_COUNT(1);
@@ -216,7 +236,7 @@ template int spmv_resid<float>(exf_sys *, int, const float *, const float *, flo
 
 // ------------------------------------------------------------ transfers
 // b_c[(a,c)] = mask[(a,c)] * sum_f R[c,f] r_f[(a,f)]   (restriction, rows = coarse DOFs)
-template <class T>
+template <class T, bool I4>
 __global__ void k_restrict(int nv2, int nv1, int Nc, int NLc, int Nf, const int *__restrict__ rq_ptr,
                            const int *__restrict__ rq_col, const T *__restrict__ rq_val,
                            const int *__restrict__ rl_ptr, const int *__restrict__ rl_col,
@@ -227,16 +247,17 @@ __global__ void k_restrict(int nv2, int nv1, int Nc, int NLc, int Nf, const int 
   long nq = (long)nv2 * Nc;
   if (row >= nq + (long)nv1 * NLc) return;
   T acc = T(0);
+  long dst;
   if (row < nq) {
     int a = (int)(row / Nc), c = (int)(row % Nc);
-    const T *src = rf + (long)a * Nf;
-    for (int k = rq_ptr[c]; k < rq_ptr[c + 1]; k++) acc += rq_val[k] * src[rq_col[k]];
+    for (int k = rq_ptr[c]; k < rq_ptr[c + 1]; k++) acc += rq_val[k] * rf[Lay<I4>::v(a, rq_col[k], Nf)];
+    dst = Lay<I4>::v(a, c, Nc);
   } else {
     int c = (int)(row - nq);
-    const T *src = rf + (long)nv2 * Nf;
-    for (int k = rl_ptr[c]; k < rl_ptr[c + 1]; k++) acc += rl_val[k] * src[rl_col[k]];
+    for (int k = rl_ptr[c]; k < rl_ptr[c + 1]; k++) acc += rl_val[k] * rf[Lay<I4>::p(rl_col[k], Nf, nv2)];
+    dst = Lay<I4>::p(c, Nc, nv2);
   }
-  bc[row] = (T)mask[row] * acc;
+  bc[dst] = (T)mask[row] * acc;
 }
 
 template <class T>
@@ -244,7 +265,8 @@ int restrict_op(exf_sys *s, int lev_c, const T *r_f, T *b_c) {
   SysLevel &C = s->L[lev_c];
   SysLevel &F = s->L[lev_c + 1];
   long nrow = C.ndof;
-  EXF_CUDA(launch_pdl(k_restrict<T>, dim3(nblk(nrow, 256)), dim3(256), 0, s->stream, s->nv2, s->nv1, C.N, C.NL, F.N,
+  auto kern = (s->nv1 && sizeof(T) == 4) ? k_restrict<T, true> : k_restrict<T, false>;
+  EXF_CUDA(launch_pdl(kern, dim3(nblk(nrow, 256)), dim3(256), 0, s->stream, s->nv2, s->nv1, C.N, C.NL, F.N,
                       C.Rq.ptr.p, C.Rq.col.p, VT<T>::pq(C.Rq), s->nv1 ? C.Rl.ptr.p : nullptr,
                       s->nv1 ? C.Rl.col.p : nullptr, s->nv1 ? VT<T>::pq(C.Rl) : nullptr, C.rmask.p, r_f, b_c));
   EXF_COUNT(1);
@@ -254,7 +276,7 @@ template int restrict_op<double>(exf_sys *, int, const double *, double *);
 template int restrict_op<float>(exf_sys *, int, const float *, float *);
 
 // x_f[(a,f)] += damp * sum_c P[f,c] x_c[(a,c)]   (damp = 0 -> y = P x overwrite mode)
-template <class T>
+template <class T, bool I4>
 __global__ void k_prolong(int nv2, int nv1, int Nf, int NLf, int Nc, const int *__restrict__ pq_ptr,
                           const int *__restrict__ pq_col, const T *__restrict__ pq_val,
                           const int *__restrict__ pl_ptr, const int *__restrict__ pl_col,
@@ -266,17 +288,18 @@ __global__ void k_prolong(int nv2, int nv1, int Nf, int NLf, int Nc, const int *
   long nq = (long)nv2 * Nf;
   if (row >= nq + (long)nv1 * NLf) return;
   T acc = T(0);
+  long dst;
   if (row < nq) {
     int a = (int)(row / Nf), f = (int)(row % Nf);
-    const T *src = xc + (long)a * Nc;
-    for (int k = pq_ptr[f]; k < pq_ptr[f + 1]; k++) acc += pq_val[k] * src[pq_col[k]];
+    for (int k = pq_ptr[f]; k < pq_ptr[f + 1]; k++) acc += pq_val[k] * xc[Lay<I4>::v(a, pq_col[k], Nc)];
+    dst = Lay<I4>::v(a, f, Nf);
   } else {
     int f = (int)(row - nq);
-    const T *src = xc + (long)nv2 * Nc;
-    for (int k = pl_ptr[f]; k < pl_ptr[f + 1]; k++) acc += pl_val[k] * src[pl_col[k]];
+    for (int k = pl_ptr[f]; k < pl_ptr[f + 1]; k++) acc += pl_val[k] * xc[Lay<I4>::p(pl_col[k], Nc, nv2)];
+    dst = Lay<I4>::p(f, Nf, nv2);
   }
-  if (overwrite) xf[row] = acc;
-  else xf[row] += damp * acc;
+  if (overwrite) xf[dst] = acc;
+  else xf[dst] += damp * acc;
 }
 
 template <class T>
@@ -285,7 +308,8 @@ static int prolong_impl(exf_sys *s, int lev_f, const T *x_c, T *x_f, double damp
   SysLevel &F = s->L[lev_f];
   SysLevel &C = s->L[lev_f - 1];
   long nrow = F.ndof;
-  EXF_CUDA(launch_pdl(k_prolong<T>, dim3(nblk(nrow, 256)), dim3(256), 0, s->stream, s->nv2, s->nv1, F.N, F.NL, C.N,
+  auto kern = (s->nv1 && sizeof(T) == 4) ? k_prolong<T, true> : k_prolong<T, false>;
+  EXF_CUDA(launch_pdl(kern, dim3(nblk(nrow, 256)), dim3(256), 0, s->stream, s->nv2, s->nv1, F.N, F.NL, C.N,
                       F.Pq.ptr.p, F.Pq.col.p, VT<T>::pq(F.Pq), s->nv1 ? F.Pl.ptr.p : nullptr,
                       s->nv1 ? F.Pl.col.p : nullptr, s->nv1 ? VT<T>::pq(F.Pl) : nullptr, x_c, x_f, (T)damp, overwrite,
                       cond));
@@ -335,41 +359,175 @@ __global__ void k_gs_colour(const int *__restrict__ items, int nitems, const int
 //   du_j = (r_j - G_jm dp)/a_jj ;  x += omega*(du, dp)
 // After every assembly k_vanka_prep stores, per (patch, star DOF), {1/a_jj, D_mj/a_jj,
 // G_jm/a_jj} contiguously in patch order, and per patch the Schur denominator.
-// Per colour: (1) k_vanka_rows computes the residual of every velocity row in the
-// colour's stars and of the patches' pressure rows from the iterate at the start of the
-// colour (a masked SpMV over disjoint stars, fully parallel, residuals written in patch
-// order); (2) k_vanka_solve, one CTA per patch, reduces the Schur numerator with warp
-// shuffles in a fixed order and writes its own star.  Stars of one colour are disjoint,
-// so the sweep is deterministic and independent of scheduling.
+// Every residual of a colour is computed from the iterate at the start of the colour;
+// stars of one colour are disjoint, so the sweep is deterministic and independent of
+// scheduling.  Two kernel families do this per colour:
+//  ROWS: k_vanka_rows computes the star-row and pressure-row residuals as a masked SpMV
+//        (LPR lanes per row, residuals written in patch order), then k_vanka_solve (one
+//        CTA per patch) reduces the Schur numerator in a fixed order and updates x.
+//  TILE: one CTA per patch gathers the iterate on the 9^d lattice points around vertex m
+//        (every column of the star rows lies within 4 lattice steps of m) into shared
+//        memory, computes the residuals against that tile (columns addressed by a
+//        precomputed tile step, no dependent global gather), solves, and writes compact
+//        corrections; k_vanka_apply adds them once every patch has read its tile.  The
+//        3D FP32 variant (k_vanka_stream) streams each warp's rows into shared memory
+//        with asynchronous copies.
+// The FP32 smoother reads the velocity blocks in FP16, scaled per (node, component) row
+// by the row's largest magnitude (vsc); the FP64 smoother reads the FP64 blocks.
 
-template <class T, int D, int LPR, int NT>
-__global__ void __launch_bounds__(NT)
-    k_vanka_rows(const int *__restrict__ rows, int nrows, int gbase, const int *__restrict__ items, int npatch,
-                 int N, const int *__restrict__ qq_ptr, const int *__restrict__ qq_col,
-                 const int *__restrict__ ql_ptr, const int *__restrict__ ql_col, long nqq, long nql, long nqqL,
-                 const T *__restrict__ vv, const T *__restrict__ vp, const T *__restrict__ pv,
-                 const T *__restrict__ pp, const T *__restrict__ x, const T *__restrict__ b, T *__restrict__ res,
-                 long pres_off) {
+// Sources of the blocks of a row.  Planar: column in col[k], value q of block k at
+// v[q*stride + k] (NQ values).  Packed16: FP16 row-scaled velocity blocks, one 16-byte
+// record of values 0..7 per block plus {column, value 8} (3D), or one 8-byte record of
+// values 0..3 with the column in col[k] (2D): two loads per block instead of 1 + d*d.
+template <class T, int NQ>
+struct PlanarBlocks {
+  static constexpr bool scaled = false;
+  const int *__restrict__ col;
+  const T *__restrict__ v;
+  long stride;
+  __device__ __forceinline__ void load(long k, int &c, T (&o)[NQ]) const {
+    c = col[k];
+#pragma unroll
+    for (int q = 0; q < NQ; q++) o[q] = v[(long)q * stride + k];
+  }
+};
+
+__device__ __forceinline__ float2 h2f(unsigned w) {
+  __half2 h;
+  memcpy(&h, &w, 4);
+  return __half22float2(h);
+}
+
+template <int D>
+struct Packed16 {
+  static constexpr bool scaled = true;
+  const int *__restrict__ col;
+  const void *__restrict__ h;
+  const uint2 *__restrict__ cx;
+  __device__ __forceinline__ void load(long k, int &c, float (&o)[D * D]) const {
+    float2 f;
+    if constexpr (D == 3) {
+      const uint4 r = reinterpret_cast<const uint4 *>(h)[k];
+      const uint2 e = cx[k];
+      c = (int)e.x;
+      f = h2f(r.x); o[0] = f.x; o[1] = f.y;
+      f = h2f(r.y); o[2] = f.x; o[3] = f.y;
+      f = h2f(r.z); o[4] = f.x; o[5] = f.y;
+      f = h2f(r.w); o[6] = f.x; o[7] = f.y;
+      f = h2f(e.y); o[8] = f.x;
+    } else {
+      const uint2 r = reinterpret_cast<const uint2 *>(h)[k];
+      c = col[k];
+      f = h2f(r.x); o[0] = f.x; o[1] = f.y;
+      f = h2f(r.y); o[2] = f.x; o[3] = f.y;
+    }
+  }
+};
+
+// Row product of one star row (RA = D outputs: d x d blocks and the d planes of vp) or
+// pressure row (RA = 1: the d planes of pv as 1 x d blocks, and pp) by LPR lanes, UNR
+// blocks per lane in flight: all columns and values of a chunk are loaded before the
+// first gather; the pressure couplings (at most LPR per row on these meshes) are loaded
+// up front with them.  rsc undoes a row scaling of the blocks on each lane's sum.
+template <class T, int D, int LPR, int UNR, bool I4, int RA, class BL>
+__device__ __forceinline__ void patch_row_dot(int lane, int N, int k0, int nk, int l0, int nl, const BL &bl,
+                                              const int *__restrict__ ql_col, long lstride,
+                                              const T *__restrict__ lv, const T *__restrict__ x, T acc[D],
+                                              const T (&rsc)[D]) {
+  int lc = -1;
+  T lw[RA];
+  if (lane < nl) {
+    lc = ql_col[l0 + lane];
+#pragma unroll
+    for (int a = 0; a < RA; a++) lw[a] = lv[(long)a * lstride + l0 + lane];
+  }
+  for (int base = 0; base < nk; base += UNR * LPR) {
+    int c[UNR];
+    T v[UNR][RA * D];
+#pragma unroll
+    for (int u = 0; u < UNR; u++) {
+      const int i = base + u * LPR + lane;
+      c[u] = -1;
+      if (i < nk) bl.load(k0 + i, c[u], v[u]);
+    }
+    T xb[UNR][D];
+#pragma unroll
+    for (int u = 0; u < UNR; u++) {
+      if constexpr (I4) {
+        float4 t4 = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (c[u] >= 0) t4 = reinterpret_cast<const float4 *>(x)[c[u]];
+        xb[u][0] = t4.x;
+        if (D > 1) xb[u][D > 1 ? 1 : 0] = t4.y;
+        if (D > 2) xb[u][D > 2 ? 2 : 0] = t4.z;
+      } else {
+#pragma unroll
+        for (int bb = 0; bb < D; bb++) xb[u][bb] = c[u] >= 0 ? x[(long)bb * N + c[u]] : T(0);
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < UNR; u++)
+      if (c[u] >= 0)
+#pragma unroll
+        for (int a = 0; a < RA; a++)
+#pragma unroll
+          for (int bb = 0; bb < D; bb++) acc[a] += v[u][a * D + bb] * xb[u][bb];
+  }
+  if constexpr (BL::scaled) {
+#pragma unroll
+    for (int a = 0; a < RA; a++) acc[a] *= rsc[a];
+  }
+  if (lc >= 0) {
+    const T pval = x[Lay<I4>::p(lc, N, D)];
+#pragma unroll
+    for (int a = 0; a < RA; a++) acc[a] += lw[a] * pval;
+  }
+  for (int i = LPR + lane; i < nl; i += LPR) {  // rows with more than LPR pressure couplings
+    const T pval = x[Lay<I4>::p(ql_col[l0 + i], N, D)];
+#pragma unroll
+    for (int a = 0; a < RA; a++) acc[a] += lv[(long)a * lstride + l0 + i] * pval;
+  }
+}
+
+// ROWS phase 1: residuals of the star rows (g < nrows) and of the patches' pressure
+// rows (g >= nrows), LPR lanes per row, written in patch order.  rinfo per star row:
+// {node, qq_ptr[node], ql_ptr[node], nqq | nql << 8 | tile index << 16}; pinfo per patch
+// (two int4): {m, first star entry, qq_ptr[m], ql_ptr[m]}, {nqq(m), nql(m), lattice, 0}.
+template <class T, int D, int LPR, int NT, bool I4, int UNR, int MINB, class VB>
+__global__ void __launch_bounds__(NT, MINB)
+    k_vanka_rows(const int4 *__restrict__ rinfo, int nrows, int gbase, const int4 *__restrict__ pinfo, int npatch,
+                 int N, VB vb, const T *__restrict__ vsc, const int *__restrict__ qq_col,
+                 const int *__restrict__ ql_col, long nql, long nqqL, const T *__restrict__ vp,
+                 const T *__restrict__ pv, const T *__restrict__ pp, const T *__restrict__ x,
+                 const T *__restrict__ b, T *__restrict__ res, long pres_off) {
   EXF_PDL_WAIT();
   const int lane = threadIdx.x % LPR;
   const long g = ((long)blockIdx.x * NT + threadIdx.x) / LPR;
   const bool vel = g < nrows;
   const bool prs = !vel && g < (long)nrows + npatch;
-  T acc[D];
+  T acc[D], bv[D];
 #pragma unroll
-  for (int a = 0; a < D; a++) acc[a] = T(0);
+  for (int a = 0; a < D; a++) acc[a] = bv[a] = T(0);
   int node = 0;
   if (vel) {
-    node = rows[g];
-    node_row_dot<T, D, LPR, true>(node, lane, N, qq_ptr, qq_col, ql_ptr, ql_col, nqq, nql, vv, vp, x, acc);
-  } else if (prs) {
-    node = items[g - nrows];
-    for (int k = qq_ptr[node] + lane; k < qq_ptr[node + 1]; k += LPR) {
-      const int c = qq_col[k];
+    const int4 ri = rinfo[g];
+    node = ri.x;
+    if (lane == 0) {
 #pragma unroll
-      for (int bb = 0; bb < D; bb++) acc[0] += pv[(long)bb * nqqL + k] * x[(long)bb * N + c];
+      for (int a = 0; a < D; a++) bv[a] = b[Lay<I4>::v(a, node, N)];
     }
-    for (int k = ql_ptr[node] + lane; k < ql_ptr[node + 1]; k += LPR) acc[0] += pp[k] * x[(long)D * N + ql_col[k]];
+    T sc[D];
+#pragma unroll
+    for (int a = 0; a < D; a++) sc[a] = VB::scaled ? vsc[(long)a * N + node] : T(1);
+    patch_row_dot<T, D, LPR, UNR, I4, D>(lane, N, ri.y, ri.w & 0xff, ri.z, (ri.w >> 8) & 0xff, vb, ql_col, nql, vp,
+                                         x, acc, sc);
+  } else if (prs) {
+    const int4 pi = pinfo[2 * (g - nrows)];
+    const int4 pj = pinfo[2 * (g - nrows) + 1];
+    node = pi.x;
+    if (lane == 0) bv[0] = b[Lay<I4>::p(node, N, D)];
+    const T one[D] = {};
+    const PlanarBlocks<T, D> pb{qq_col, pv, nqqL};
+    patch_row_dot<T, D, LPR, UNR, I4, 1>(lane, N, pi.z, pj.x, pi.w, pj.y, pb, ql_col, 0, pp, x, acc, one);
   }
 #pragma unroll
   for (int a = 0; a < D; a++)
@@ -378,9 +536,9 @@ __global__ void __launch_bounds__(NT)
   if (lane == 0) {
     if (vel) {
 #pragma unroll
-      for (int a = 0; a < D; a++) res[(gbase + g) * D + a] = b[(long)a * N + node] - acc[a];
+      for (int a = 0; a < D; a++) res[(gbase + g) * D + a] = bv[a] - acc[a];
     } else if (prs) {
-      res[pres_off + node] = b[(long)D * N + node] - acc[0];
+      res[pres_off + node] = bv[0] - acc[0];
     }
   }
 }
@@ -428,34 +586,71 @@ __global__ void k_vanka_prep(int NL, const int *__restrict__ pstart, const int *
   }
 }
 
-template <class T, int D, int NT>
+// ROWS phase 2: one CTA per patch; every value the update needs (residuals,
+// coefficients, star nodes, current iterate) is loaded in one round before the Schur
+// numerator is reduced (warp shuffles, then the warps in order).  SU entries per thread
+// cover the stars of these meshes; longer stars take the loops after the first round.
+template <class T, int D, int NT, bool I4, int SU>
 __global__ void __launch_bounds__(NT)
-    k_vanka_solve(const int *__restrict__ items, int N, const int *__restrict__ qq_ptr,
-                  const int *__restrict__ vrows, const int *__restrict__ pstart, const T *__restrict__ vk,
+    k_vanka_solve(const int4 *__restrict__ pinfo, int N, const int *__restrict__ vrows, const T *__restrict__ vk,
                   const T *__restrict__ pk, const T *__restrict__ res, long pres_off, T *__restrict__ x, T omega) {
   EXF_PDL_WAIT();
-  __shared__ double s_red[NT / 32];
-  const int m = items[blockIdx.x];
-  const int K = qq_ptr[m + 1] - qq_ptr[m];
-  const long g0 = pstart[m];
+  __shared__ double s_red[NT / 32], s_bc[2];
+  const int4 pi = pinfo[2 * blockIdx.x];
+  const int m = pi.x, KD = pinfo[2 * blockIdx.x + 1].x * D;
+  const long g0 = pi.y;
   const T *rr = res + g0 * D;
   const T *w = vk + 3 * g0 * D;
+  T r_[SU], w0[SU], w1[SU], w2[SU], xv[SU];
+  long ix[SU];
+#pragma unroll
+  for (int u = 0; u < SU; u++) {
+    const int t = threadIdx.x + u * NT;
+    ix[u] = -1;
+    r_[u] = w0[u] = w1[u] = w2[u] = xv[u] = T(0);
+    if (t < KD) {
+      r_[u] = rr[t];
+      w0[u] = w[3 * t];
+      w1[u] = w[3 * t + 1];
+      w2[u] = w[3 * t + 2];
+      ix[u] = Lay<I4>::v(t % D, vrows[g0 + t / D], N);
+    }
+  }
+#pragma unroll
+  for (int u = 0; u < SU; u++)
+    if (ix[u] >= 0) xv[u] = x[ix[u]];
+  T rp = T(0), xp = T(0);
+  double Sd = 0.;
+  if (threadIdx.x == 0) {
+    rp = res[pres_off + m];
+    Sd = (double)pk[2 * m];
+    xp = x[Lay<I4>::p(m, N, D)];
+  }
   double tsum = 0.;
-  for (int t = threadIdx.x; t < K * D; t += NT) tsum += (double)(w[3 * t + 1] * rr[t]);
+#pragma unroll
+  for (int u = 0; u < SU; u++)
+    if (ix[u] >= 0) tsum += (double)(w1[u] * r_[u]);
+  for (int t = threadIdx.x + SU * NT; t < KD; t += NT) tsum += (double)(w[3 * t + 1] * rr[t]);
   for (int o = 16; o > 0; o >>= 1) tsum += __shfl_down_sync(0xffffffffu, tsum, o);
   if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = tsum;
   __syncthreads();
-  double Tt = 0.;
-  for (int k = 0; k < NT / 32; k++) Tt += s_red[k];
-  const double St = (double)pk[2 * m];
-  Tt -= (double)res[pres_off + m];
-  const T dp = (T)(fabs(St) > 1e-300 ? Tt / St : 0.);
-  for (int t = threadIdx.x; t < K * D; t += NT) {
-    const int kk = t / D, a = t % D;
-    const long idx = (long)a * N + vrows[g0 + kk];
+  if (threadIdx.x == 0) {
+    double Tt = 0.;
+    for (int k = 0; k < NT / 32; k++) Tt += s_red[k];
+    s_bc[0] = Tt - (double)rp;
+    s_bc[1] = Sd;
+  }
+  __syncthreads();
+  const double num = s_bc[0], den = s_bc[1];
+  const T dp = (T)(fabs(den) > 1e-300 ? num / den : 0.);
+#pragma unroll
+  for (int u = 0; u < SU; u++)
+    if (ix[u] >= 0) x[ix[u]] = xv[u] + omega * (r_[u] * w0[u] - w2[u] * dp);
+  for (int t = threadIdx.x + SU * NT; t < KD; t += NT) {
+    const long idx = Lay<I4>::v(t % D, vrows[g0 + t / D], N);
     x[idx] += omega * (rr[t] * w[3 * t] - w[3 * t + 2] * dp);
   }
-  if (threadIdx.x == 0) x[(long)D * N + m] += omega * dp;
+  if (threadIdx.x == 0) x[Lay<I4>::p(m, N, D)] = xp + omega * dp;
 }
 
 template <class T>
@@ -473,12 +668,455 @@ struct VK<float> {
   static float *res(SysLevel &L) { return L.vres32.p; }
 };
 
+// ------------------------------------------------- TILE: one CTA per patch
+// Block sources in tile mode: load() fetches a block's raw record, step() and unpack()
+// give the tile step of its column and its values.
+template <int D>
+struct TileBlocks16 {  // FP16 row-scaled; 3D: uint4 + {value 8, step}; 2D: uint2 + step
+  static constexpr bool scaled = true;
+  struct Raw {
+    uint4 r;
+    uint32_t e;
+  };
+  const void *__restrict__ h;
+  const uint32_t *__restrict__ qc;
+  const int16_t *__restrict__ tcq;
+  __device__ __forceinline__ Raw load(long k) const {
+    Raw w;
+    if constexpr (D == 3) {
+      w.r = reinterpret_cast<const uint4 *>(h)[k];
+      w.e = qc[k];
+    } else {
+      const uint2 r2 = reinterpret_cast<const uint2 *>(h)[k];
+      w.r = make_uint4(r2.x, r2.y, 0u, 0u);
+      w.e = (uint32_t)(uint16_t)tcq[k] << 16;
+    }
+    return w;
+  }
+  static __device__ __forceinline__ int step(const Raw &w) { return (int)(int16_t)(w.e >> 16); }
+  static __device__ __forceinline__ void unpack(const Raw &w, float (&o)[D * D]) {
+    float2 f;
+    f = h2f(w.r.x); o[0] = f.x; o[1] = f.y;
+    f = h2f(w.r.y); o[2] = f.x; o[3] = f.y;
+    if constexpr (D == 3) {
+      f = h2f(w.r.z); o[4] = f.x; o[5] = f.y;
+      f = h2f(w.r.w); o[6] = f.x; o[7] = f.y;
+      o[8] = h2f(w.e).x;
+    }
+  }
+};
+template <class T, int NQ>
+struct TileBlocksPlanar {
+  static constexpr bool scaled = false;
+  struct Raw {
+    T v[NQ];
+    int st;
+  };
+  const T *__restrict__ v;
+  long stride;
+  const int16_t *__restrict__ tcq;
+  __device__ __forceinline__ Raw load(long k) const {
+    Raw w;
+    w.st = tcq[k];
+#pragma unroll
+    for (int q = 0; q < NQ; q++) w.v[q] = v[(long)q * stride + k];
+    return w;
+  }
+  static __device__ __forceinline__ int step(const Raw &w) { return w.st; }
+  static __device__ __forceinline__ void unpack(const Raw &w, T (&o)[NQ]) {
+#pragma unroll
+    for (int q = 0; q < NQ; q++) o[q] = w.v[q];
+  }
+};
+
+// Row product against the tile: UNR blocks per lane loaded, then used; the rest of the
+// row (longer than UNR*LPR blocks), the row scale and the pressure couplings (lv planes,
+// tile steps tcl, tile slot 3) in tile_row_finish.
+template <class BL, int UNR>
+struct RowRegs {
+  bool ok[UNR];
+  typename BL::Raw w[UNR];
+};
+
+template <int LPR, int UNR, class BL>
+__device__ __forceinline__ void tile_row_load(int lane, int base, int k0, int nk, const BL &bl, RowRegs<BL, UNR> &R) {
+#pragma unroll
+  for (int u = 0; u < UNR; u++) {
+    const int i = base + u * LPR + lane;
+    R.ok[u] = i < nk;
+    if (R.ok[u]) R.w[u] = bl.load(k0 + i);
+  }
+}
+
+template <class T, int D, int UNR, int RA, class BL>
+__device__ __forceinline__ void tile_row_use(const T (*tile)[4], int tb, const RowRegs<BL, UNR> &R, T acc[RA]) {
+#pragma unroll
+  for (int u = 0; u < UNR; u++)
+    if (R.ok[u]) {
+      T v[RA * D];
+      BL::unpack(R.w[u], v);
+      const T *xt = tile[tb + BL::step(R.w[u])];
+#pragma unroll
+      for (int a = 0; a < RA; a++)
+#pragma unroll
+        for (int bb = 0; bb < D; bb++) acc[a] += v[a * D + bb] * xt[bb];
+    }
+}
+
+template <class T, int D, int LPR, int UNR, int RA, class BL>
+__device__ __forceinline__ void tile_row_finish(int lane, const T (*tile)[4], int tb, int k0, int nk, int l0, int nl,
+                                                const BL &bl, const int16_t *__restrict__ tcl, long lstride,
+                                                const T *__restrict__ lv, T acc[RA], const T (&rsc)[RA]) {
+  for (int base = UNR * LPR; base < nk; base += UNR * LPR) {
+    RowRegs<BL, UNR> R;
+    tile_row_load<LPR, UNR>(lane, base, k0, nk, bl, R);
+    tile_row_use<T, D, UNR, RA>(tile, tb, R, acc);
+  }
+  if constexpr (BL::scaled) {
+#pragma unroll
+    for (int a = 0; a < RA; a++) acc[a] *= rsc[a];
+  }
+  for (int i = lane; i < nl; i += LPR) {
+    const T pval = tile[tb + tcl[l0 + i]][3];
+#pragma unroll
+    for (int a = 0; a < RA; a++) acc[a] += lv[(long)a * lstride + l0 + i] * pval;
+  }
+}
+
+// The iterate on the 9^d tile around the patch vertex whose lattice coordinates are
+// packed in pz (zero outside the mesh, never referenced there).
+template <class T, int D, int NT, bool I4>
+__device__ __forceinline__ void load_tile(T (*tile)[4], int pz, int N, int NL, int L0, int L1, int L2,
+                                          const int *__restrict__ latnode, const T *__restrict__ x) {
+  constexpr int TS = D == 3 ? 729 : 81;
+  const int ox = (pz & 2047) - 4, oy = ((pz >> 11) & 2047) - 4, oz = ((pz >> 22) & 1023) - 4;
+  for (int t = threadIdx.x; t < TS; t += NT) {
+    const int gx = ox + t % 9, gy = oy + (t / 9) % 9, gz = D == 3 ? oz + t / 81 : 0;
+    T q0 = T(0), q1 = T(0), q2 = T(0), q3 = T(0);
+    if (gx >= 0 && gx < L0 && gy >= 0 && gy < L1 && gz >= 0 && gz < L2) {
+      const int n = latnode[((long)gz * L1 + gy) * L0 + gx];
+      if constexpr (I4) {
+        const float4 f = reinterpret_cast<const float4 *>(x)[n];
+        q0 = f.x;
+        q1 = f.y;
+        q2 = f.z;
+        q3 = f.w;
+      } else {
+        q0 = x[n];
+        q1 = x[(long)N + n];
+        if (D == 3) q2 = x[2L * N + n];
+        if (n < NL) q3 = x[(long)D * N + n];
+      }
+    }
+    tile[t][0] = q0;
+    tile[t][1] = q1;
+    tile[t][2] = q2;
+    tile[t][3] = q3;
+  }
+}
+
+// Schur numerator (threads in order, warps in order) and the corrections of one patch
+// from its residuals res[0 .. K*D] (the last one the pressure row)
+template <class T, int D, int NT>
+__device__ __forceinline__ void patch_solve(const T *res, double *red, int K, int m, long g0,
+                                            const T *__restrict__ vk, const T *__restrict__ pk, T *__restrict__ dlt,
+                                            long pres_off, T omega) {
+  constexpr int NW = NT / 32;
+  const int KD = K * D;
+  const T *w = vk + 3 * g0 * D;
+  double tsum = 0.;
+  for (int t = threadIdx.x; t < KD; t += NT) tsum += (double)(w[3 * t + 1] * res[t]);
+  for (int o = 16; o > 0; o >>= 1) tsum += __shfl_down_sync(0xffffffffu, tsum, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = tsum;
+  __syncthreads();
+  double Tt = 0.;
+  for (int k = 0; k < NW; k++) Tt += red[k];
+  Tt -= (double)res[KD];
+  const double Sd = (double)pk[2 * m];
+  const T dp = (T)(fabs(Sd) > 1e-300 ? Tt / Sd : 0.);
+  for (int t = threadIdx.x; t < KD; t += NT) dlt[g0 * D + t] = omega * (res[t] * w[3 * t] - w[3 * t + 2] * dp);
+  if (threadIdx.x == 0) dlt[pres_off + m] = omega * dp;
+}
+
+template <class T, int D, int NT, int LPR, int UNR, bool I4, class BL>
+__global__ void __launch_bounds__(NT)
+    k_vanka_tile(const int4 *__restrict__ pinfo, const int4 *__restrict__ rinfo, int N, int NL, int L0, int L1,
+                 int L2, const int *__restrict__ latnode, BL bl, const T *__restrict__ vsc,
+                 const int16_t *__restrict__ tcq, const int16_t *__restrict__ tcl, long nql, long nqqL,
+                 const T *__restrict__ vp, const T *__restrict__ pv, const T *__restrict__ pp,
+                 const T *__restrict__ vk, const T *__restrict__ pk, const T *__restrict__ x,
+                 const T *__restrict__ b, T *__restrict__ dlt, long pres_off, T omega) {
+  constexpr int TS = D == 3 ? 729 : 81;
+  constexpr int KMAX = D == 3 ? 125 : 25;
+  constexpr int TC = D == 3 ? 364 : 40;  // tile index of the patch vertex
+  constexpr int NW = NT / 32;
+  constexpr int NG = NW * (32 / LPR);    // row groups of the CTA
+  __shared__ T tile[TS][4];
+  __shared__ T res[KMAX * D + 1];
+  __shared__ int4 s_ri[KMAX];
+  __shared__ double red[NW];
+  EXF_PDL_WAIT();
+  const int4 pi = pinfo[2 * blockIdx.x];
+  const int4 pj = pinfo[2 * blockIdx.x + 1];
+  const int m = pi.x, K = pj.x;
+  const long g0 = pi.y;
+  for (int r = threadIdx.x; r < K; r += NT) s_ri[r] = rinfo[g0 + r];
+  load_tile<T, D, NT, I4>(tile, pj.z, N, NL, L0, L1, L2, latnode, x);
+  __syncthreads();
+  // star-row residuals, one row per row group and pass
+  const int lane = threadIdx.x % LPR, grp = threadIdx.x / LPR;
+  const int npass = (K + NG - 1) / NG;
+  for (int ps = 0; ps < npass; ps++) {
+    const int r = ps * NG + grp;
+    int4 ri = make_int4(0, 0, 0, 0);
+    if (r < K) ri = s_ri[r];
+    RowRegs<BL, UNR> R;
+    tile_row_load<LPR, UNR>(lane, 0, ri.y, r < K ? (ri.w & 0xff) : 0, bl, R);
+    T sc[D], bv[D], acc[D];
+#pragma unroll
+    for (int a = 0; a < D; a++) {
+      sc[a] = T(1);
+      bv[a] = acc[a] = T(0);
+      if (r < K) {
+        if (BL::scaled) sc[a] = vsc[(long)a * N + ri.x];
+        if (lane == 0) bv[a] = b[Lay<I4>::v(a, ri.x, N)];
+      }
+    }
+    if (r < K) {
+      tile_row_use<T, D, UNR, D>(tile, ri.w >> 16, R, acc);
+      tile_row_finish<T, D, LPR, UNR, D>(lane, tile, ri.w >> 16, ri.y, ri.w & 0xff, ri.z, (ri.w >> 8) & 0xff, bl,
+                                         tcl, nql, vp, acc, sc);
+    }
+#pragma unroll
+    for (int a = 0; a < D; a++)
+#pragma unroll
+      for (int o = LPR / 2; o > 0; o >>= 1) acc[a] += __shfl_down_sync(0xffffffffu, acc[a], o, LPR);
+    if (lane == 0 && r < K) {
+#pragma unroll
+      for (int a = 0; a < D; a++) res[r * D + a] = bv[a] - acc[a];
+    }
+  }
+  // pressure row of m: one warp
+  if (threadIdx.x < 32) {
+    const int ln = threadIdx.x;
+    T acc[1] = {T(0)};
+    const T one[1] = {T(1)};
+    const TileBlocksPlanar<T, D> pb{pv, nqqL, tcq};
+    tile_row_finish<T, D, 32, 1, 1>(ln, tile, TC, pi.z - 32, K + 32, pi.w, pj.y, pb, tcl, 0, pp, acc, one);
+    for (int o = 16; o > 0; o >>= 1) acc[0] += __shfl_down_sync(0xffffffffu, acc[0], o);
+    if (ln == 0) res[K * D] = b[Lay<I4>::p(m, N, D)] - acc[0];
+  }
+  __syncthreads();
+  patch_solve<T, D, NT>(res, red, K, m, g0, vk, pk, dlt, pres_off, omega);
+}
+
+// --------------------------------------- TILE, 3D FP32: streamed star rows
+// Each warp owns star rows w, w+NW, ... of the patch and streams their FP16 records
+// (16-byte values + 4-byte {value 8, tile step}) into a per-warp ring of SLOTS
+// shared-memory slots with asynchronous copies (cp.async), SLOTS-1 rows ahead of the row
+// it computes, so the bytes in flight do not depend on registers; the small per-row data
+// (row scales, right-hand side, pressure couplings) is loaded one row ahead into
+// registers.  Waits are cp.async.wait_group on the thread's own copies (no spinning).
+#define EXF_ST_ROWMAX 128  // records per slot (star rows have at most 125 blocks)
+#define EXF_ST_QMAX 136    // 4-byte words per slot: 125 blocks + alignment slack, 16-byte multiple
+
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+template <int NT, int SLOTS>
+struct StreamSmem {
+  float tile[729][4];
+  float res[125 * 3 + 1];
+  int4 ri[125];
+  double red[NT / 32];
+  uint4 h[NT / 32][SLOTS][EXF_ST_ROWMAX];
+  uint32_t q[NT / 32][SLOTS][EXF_ST_QMAX];
+};
+
+template <int NT, int SLOTS>
+__global__ void __launch_bounds__(NT)
+    k_vanka_stream(const int4 *__restrict__ pinfo, const int4 *__restrict__ rinfo, int N, int L0, int L1, int L2,
+                   const int *__restrict__ latnode, const uint4 *__restrict__ h16, const uint32_t *__restrict__ h16qc,
+                   const float *__restrict__ vsc, const int16_t *__restrict__ tcq, const int16_t *__restrict__ tcl,
+                   long nql, long nqqL, const float *__restrict__ vp, const float *__restrict__ pv,
+                   const float *__restrict__ pp, const float *__restrict__ vk, const float *__restrict__ pk,
+                   const float *__restrict__ x, const float *__restrict__ b, float *__restrict__ dlt, long pres_off,
+                   float omega) {
+  constexpr int NW = NT / 32;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  StreamSmem<NT, SLOTS> &S = *reinterpret_cast<StreamSmem<NT, SLOTS> *>(smem_raw);
+  EXF_PDL_WAIT();
+  const int4 pi = pinfo[2 * blockIdx.x];
+  const int4 pj = pinfo[2 * blockIdx.x + 1];
+  const int m = pi.x, K = pj.x;
+  const long g0 = pi.y;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int nmine = K > warp ? (K - warp + NW - 1) / NW : 0;  // star rows of this warp
+  for (int r = threadIdx.x; r < K; r += NT) S.ri[r] = rinfo[g0 + r];
+  __syncthreads();
+  // copies of the i-th row of this warp into slot i % SLOTS (the 4-byte records as the
+  // aligned 16-byte chunks that cover them)
+  auto issue = [&](int i) {
+    const int4 ri = S.ri[warp + i * NW];
+    const int k0 = ri.y, nk = ri.w & 0xff;
+    const int sl = i % SLOTS;
+    for (int j = lane; j < nk; j += 32) cp_async16(&S.h[warp][sl][j], h16 + k0 + j);
+    const int qa = k0 & ~3, qn = ((k0 + nk + 3) & ~3) - qa;
+    for (int j = lane * 4; j < qn; j += 128) cp_async16(&S.q[warp][sl][j], h16qc + qa + j);
+  };
+#pragma unroll
+  for (int i = 0; i < SLOTS - 1; i++) {
+    if (i < nmine) issue(i);
+    cp_async_commit();
+  }
+  load_tile<float, 3, NT, true>(S.tile, pj.z, N, 0, L0, L1, L2, latnode, x);
+  __syncthreads();
+  // pressure row of m (warp 0, direct loads; B = pv plane by plane)
+  if (warp == 0) {
+    float acc = 0.f;
+    for (int j = lane; j < K; j += 32) {
+      const long k = pi.z + j;
+      const float *xt = S.tile[364 + tcq[k]];
+      acc += pv[k] * xt[0] + pv[nqqL + k] * xt[1] + pv[2 * nqqL + k] * xt[2];
+    }
+    for (int j = lane; j < pj.y; j += 32) acc += pp[pi.w + j] * S.tile[364 + tcl[pi.w + j]][3];
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+    if (lane == 0) S.res[K * 3] = b[4L * m + 3] - acc;
+  }
+  struct RowSmall {
+    float sc0, sc1, sc2, l0, l1, l2;
+    float4 bv;
+    int lcode;
+  };
+  auto small = [&](int i) {
+    RowSmall q;
+    q.sc0 = q.sc1 = q.sc2 = q.l0 = q.l1 = q.l2 = 0.f;
+    q.bv = make_float4(0.f, 0.f, 0.f, 0.f);
+    q.lcode = 0;
+    if (i < nmine) {
+      const int4 ri = S.ri[warp + i * NW];
+      const int node = ri.x, nl = (ri.w >> 8) & 0xff;
+      q.sc0 = vsc[node];
+      q.sc1 = vsc[(long)N + node];
+      q.sc2 = vsc[2L * N + node];
+      if (lane < nl) {
+        q.lcode = tcl[ri.z + lane];
+        q.l0 = vp[ri.z + lane];
+        q.l1 = vp[nql + ri.z + lane];
+        q.l2 = vp[2 * nql + ri.z + lane];
+      }
+      if (lane == 0) q.bv = reinterpret_cast<const float4 *>(b)[node];
+    }
+    return q;
+  };
+  RowSmall nxt = small(0);
+  for (int i = 0; i < nmine; i++) {
+    if (i + SLOTS - 1 < nmine) issue(i + SLOTS - 1);
+    cp_async_commit();
+    const RowSmall cur = nxt;
+    nxt = small(i + 1);
+    const int r = warp + i * NW;
+    const int4 ri = S.ri[r];
+    const int k0 = ri.y, nk = ri.w & 0xff, nl = (ri.w >> 8) & 0xff, tb = ri.w >> 16;
+    cp_async_wait<SLOTS - 1>();
+    __syncwarp();
+    const int sl = i % SLOTS;
+    const int qo = k0 & 3;
+    float a0 = 0.f, a1 = 0.f, a2 = 0.f;
+    for (int j = lane; j < nk; j += 32) {
+      const uint4 h = S.h[warp][sl][j];
+      const uint32_t e = S.q[warp][sl][qo + j];
+      const float *xt = S.tile[tb + (int)(int16_t)(e >> 16)];
+      float2 f;
+      f = h2f(h.x);
+      a0 += f.x * xt[0] + f.y * xt[1];
+      f = h2f(h.y);
+      a0 += f.x * xt[2];
+      a1 += f.y * xt[0];
+      f = h2f(h.z);
+      a1 += f.x * xt[1] + f.y * xt[2];
+      f = h2f(h.w);
+      a2 += f.x * xt[0] + f.y * xt[1];
+      a2 += h2f(e).x * xt[2];
+    }
+    a0 *= cur.sc0;
+    a1 *= cur.sc1;
+    a2 *= cur.sc2;
+    if (lane < nl) {
+      const float pval = S.tile[tb + cur.lcode][3];
+      a0 += cur.l0 * pval;
+      a1 += cur.l1 * pval;
+      a2 += cur.l2 * pval;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      a0 += __shfl_down_sync(0xffffffffu, a0, o);
+      a1 += __shfl_down_sync(0xffffffffu, a1, o);
+      a2 += __shfl_down_sync(0xffffffffu, a2, o);
+    }
+    if (lane == 0) {
+      S.res[r * 3] = cur.bv.x - a0;
+      S.res[r * 3 + 1] = cur.bv.y - a1;
+      S.res[r * 3 + 2] = cur.bv.z - a2;
+    }
+    __syncwarp();  // slot sl is refilled by the copies issued in iteration i + 1
+  }
+  cp_async_wait<0>();
+  __syncthreads();
+  patch_solve<float, 3, NT>(S.res, S.red, K, m, g0, vk, pk, dlt, pres_off, omega);
+}
+
+// TILE phase 2: x += corrections of one colour (each star node and patch vertex once)
+template <class T, int D, bool I4>
+__global__ void k_vanka_apply(const int *__restrict__ vrows, int nr, long gbase, const int *__restrict__ items,
+                              int npatch, int N, const T *__restrict__ dlt, long pres_off, T *__restrict__ x) {
+  EXF_PDL_WAIT();
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < nr) {
+    const int n = vrows[i];
+#pragma unroll
+    for (int a = 0; a < D; a++) x[Lay<I4>::v(a, n, N)] += dlt[(gbase + i) * D + a];
+  } else if (i < (long)nr + npatch) {
+    const int m = items[i - nr];
+    x[Lay<I4>::p(m, N, D)] += dlt[pres_off + m];
+  }
+}
+
+// kernel tuning: levels with many waves of rows stream the matrix (occupancy first),
+// small levels are latency-bound (every block of a row in flight at once)
+#ifndef EXF_UNR_BIG32
+#define EXF_UNR_BIG32 1
+#endif
+#ifndef EXF_MINB_BIG32
+#define EXF_MINB_BIG32 8
+#endif
+#ifndef EXF_UNR_BIG64
+#define EXF_UNR_BIG64 1
+#endif
+#ifndef EXF_MINB_BIG64
+#define EXF_MINB_BIG64 6
+#endif
+#ifndef EXF_ST_SLOTS
+#define EXF_ST_SLOTS 2
+#endif
+
 template <class T, int D>
-static int vanka_sweep(exf_sys *s, int lev, const exf_mg_params *p, T *x, const T *b) {
+static int vanka_sweep_rows(exf_sys *s, int lev, const exf_mg_params *p, T *x, const T *b) {
   SysLevel &L = s->L[lev];
+  constexpr bool I4 = sizeof(T) == 4;
   constexpr int NTS = D == 3 ? 128 : 64;
+  constexpr int SU = D == 3 ? 3 : 1;  // 3D stars: 125 nodes x 3 <= 3 x 128; 2D: 25 x 2 <= 64
   constexpr int LPR = D == 3 ? 32 : 16;
   constexpr int NTR = 256;
+  constexpr int UNR_S = sizeof(T) == 4 ? EXF_UNR_BIG32 : EXF_UNR_BIG64;
+  constexpr int MINB_S = sizeof(T) == 4 ? EXF_MINB_BIG32 : EXF_MINB_BIG64;
+  constexpr int UNR_L = (D == 3 && sizeof(T) == 4) ? 4 : 2;
   T *res = VK<T>::res(L);
   const long pres_off = (long)L.vrow_off[L.ncolour] * D;
   for (int cc = 0; cc < L.ncolour; cc++) {
@@ -486,21 +1124,163 @@ static int vanka_sweep(exf_sys *s, int lev, const exf_mg_params *p, T *x, const 
     const int n = L.col_off[c + 1] - L.col_off[c];
     if (n == 0) continue;
     const int nr = L.vrow_off[c + 1] - L.vrow_off[c];
-    const int *items = L.col_items.p + L.col_off[c];
-    EXF_CUDA(launch_pdl(k_vanka_rows<T, D, LPR, NTR>, dim3(nblk((long)(nr + n) * LPR, NTR)), dim3(NTR), 0, s->stream,
-                        L.vrows.p + L.vrow_off[c], nr, L.vrow_off[c], items, n, L.N, L.qq_ptr.p, L.qq_col.p,
-                        L.ql_ptr.p, L.ql_col.p, L.nqq, L.nql, L.nqqL, VT<T>::vv(L), VT<T>::vp(L), VT<T>::pv(L),
-                        VT<T>::pp(L), x, b, res, pres_off));
-    EXF_CUDA(launch_pdl(k_vanka_solve<T, D, NTS>, dim3(n), dim3(NTS), 0, s->stream, items, L.N, L.qq_ptr.p,
-                        L.vrows.p, L.pstart.p, VK<T>::vk(L), VK<T>::pk(L), res, pres_off, x, (T)p->omega));
+    const int4 *pin = L.pinfo.p + 2L * L.col_off[c];
+    const long nthr = (long)(nr + n) * LPR;
+    const bool big = nthr > 4L * s->nsm * 2048;
+    if constexpr (sizeof(T) == 4) {
+      using VB = Packed16<D>;
+      const VB vb{L.qq_col.p, L.h16.p, L.h16cx.p};
+      auto kern = big ? k_vanka_rows<T, D, LPR, NTR, I4, UNR_S, MINB_S, VB>
+                      : k_vanka_rows<T, D, LPR, NTR, I4, UNR_L, 1, VB>;
+      EXF_CUDA(launch_pdl(kern, dim3(nblk(nthr, NTR)), dim3(NTR), 0, s->stream, L.vrinfo.p + L.vrow_off[c], nr,
+                          L.vrow_off[c], pin, n, L.N, vb, (const T *)L.vsc.p, L.qq_col.p, L.ql_col.p, L.nql, L.nqqL,
+                          VT<T>::vp(L), VT<T>::pv(L), VT<T>::pp(L), x, b, res, pres_off));
+    } else {
+      using VB = PlanarBlocks<T, D * D>;
+      const VB vb{L.qq_col.p, VT<T>::vv(L), L.nqq};
+      auto kern = big ? k_vanka_rows<T, D, LPR, NTR, I4, UNR_S, MINB_S, VB>
+                      : k_vanka_rows<T, D, LPR, NTR, I4, UNR_L, 1, VB>;
+      EXF_CUDA(launch_pdl(kern, dim3(nblk(nthr, NTR)), dim3(NTR), 0, s->stream, L.vrinfo.p + L.vrow_off[c], nr,
+                          L.vrow_off[c], pin, n, L.N, vb, (const T *)nullptr, L.qq_col.p, L.ql_col.p, L.nql, L.nqqL,
+                          VT<T>::vp(L), VT<T>::pv(L), VT<T>::pp(L), x, b, res, pres_off));
+    }
+    EXF_CUDA(launch_pdl(k_vanka_solve<T, D, NTS, I4, SU>, dim3(n), dim3(NTS), 0, s->stream, pin, L.N, L.vrows.p,
+                        VK<T>::vk(L), VK<T>::pk(L), res, pres_off, x, (T)p->omega));
     EXF_COUNT(2);
   }
   return EXF_OK;
 }
 
+template <class T, int D>
+static int vanka_sweep_tile(exf_sys *s, int lev, const exf_mg_params *p, T *x, const T *b) {
+  SysLevel &L = s->L[lev];
+  constexpr bool I4 = sizeof(T) == 4;
+  constexpr int NT = D == 3 ? 256 : 64;
+  constexpr int LPR = D == 3 ? 32 : 8;
+  constexpr int UNR = sizeof(T) == 4 ? 4 : 1;
+  constexpr int SNT = 256, SLOTS = EXF_ST_SLOTS;
+  T *dlt = VK<T>::res(L);
+  const long pres_off = (long)L.vrow_off[L.ncolour] * D;
+  if constexpr (sizeof(T) == 4 && D == 3) {
+    // dynamic shared memory above 48 KB: opt in once per device
+    static bool attr_set[64] = {false};
+    const int dev = s->mesh->device;
+    if (dev < 0 || dev >= 64) {
+      set_error("device ordinal %d out of range", dev);
+      return EXF_ERR_ARG;
+    }
+    if (!attr_set[dev]) {
+      EXF_CUDA(cudaFuncSetAttribute(k_vanka_stream<SNT, SLOTS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)sizeof(StreamSmem<SNT, SLOTS>)));
+      attr_set[dev] = true;
+    }
+  }
+  for (int cc = 0; cc < L.ncolour; cc++) {
+    const int c = p->reverse_colours ? L.ncolour - 1 - cc : cc;
+    const int n = L.col_off[c + 1] - L.col_off[c];
+    if (n == 0) continue;
+    const int nr = L.vrow_off[c + 1] - L.vrow_off[c];
+    const int4 *pin = L.pinfo.p + 2L * L.col_off[c];
+    if constexpr (sizeof(T) == 4 && D == 3) {
+      EXF_CUDA(launch_pdl(k_vanka_stream<SNT, SLOTS>, dim3(n), dim3(SNT), sizeof(StreamSmem<SNT, SLOTS>), s->stream,
+                          pin, (const int4 *)L.vrinfo.p, L.N, L.Ll[0], L.Ll[1], L.Ll[2], (const int *)L.latnode.p,
+                          (const uint4 *)L.h16.p, (const uint32_t *)L.h16qc.p, (const float *)L.vsc.p,
+                          (const int16_t *)L.tcq.p, (const int16_t *)L.tcl.p, L.nql, L.nqqL,
+                          (const float *)VT<T>::vp(L), (const float *)VT<T>::pv(L), (const float *)VT<T>::pp(L),
+                          (const float *)VK<T>::vk(L), (const float *)VK<T>::pk(L), (const float *)x,
+                          (const float *)b, (float *)dlt, pres_off, (float)p->omega));
+    } else if constexpr (sizeof(T) == 4) {
+      using BL = TileBlocks16<D>;
+      const BL bl{L.h16.p, L.h16qc.p, L.tcq.p};
+      EXF_CUDA(launch_pdl(k_vanka_tile<T, D, NT, LPR, UNR, I4, BL>, dim3(n), dim3(NT), 0, s->stream, pin,
+                          (const int4 *)L.vrinfo.p, L.N, L.NL, L.Ll[0], L.Ll[1], L.Ll[2], (const int *)L.latnode.p,
+                          bl, (const T *)L.vsc.p, (const int16_t *)L.tcq.p, (const int16_t *)L.tcl.p, L.nql, L.nqqL,
+                          VT<T>::vp(L), VT<T>::pv(L), VT<T>::pp(L), VK<T>::vk(L), VK<T>::pk(L), x, b, dlt, pres_off,
+                          (T)p->omega));
+    } else {
+      using BL = TileBlocksPlanar<T, D * D>;
+      const BL bl{VT<T>::vv(L), L.nqq, L.tcq.p};
+      EXF_CUDA(launch_pdl(k_vanka_tile<T, D, NT, LPR, UNR, I4, BL>, dim3(n), dim3(NT), 0, s->stream, pin,
+                          (const int4 *)L.vrinfo.p, L.N, L.NL, L.Ll[0], L.Ll[1], L.Ll[2], (const int *)L.latnode.p,
+                          bl, (const T *)nullptr, (const int16_t *)L.tcq.p, (const int16_t *)L.tcl.p, L.nql, L.nqqL,
+                          VT<T>::vp(L), VT<T>::pv(L), VT<T>::pp(L), VK<T>::vk(L), VK<T>::pk(L), x, b, dlt, pres_off,
+                          (T)p->omega));
+    }
+    EXF_CUDA(launch_pdl(k_vanka_apply<T, D, I4>, dim3(nblk((long)nr + n, 256)), dim3(256), 0, s->stream,
+                        L.vrows.p + L.vrow_off[c], nr, (long)L.vrow_off[c], L.col_items.p + L.col_off[c], n, L.N,
+                        (const T *)dlt, pres_off, x));
+    EXF_COUNT(2);
+  }
+  return EXF_OK;
+}
+
+// AUTO runs the ROWS pair: on the channel, cavity and Boussinesq hierarchies it was
+// measured at least as fast as the tile kernels on every level
+template <class T, int D>
+static int vanka_sweep(exf_sys *s, int lev, const exf_mg_params *p, T *x, const T *b) {
+  SysLevel &L = s->L[lev];
+  if (p->vanka_kernel == EXF_VANKA_TILE) {
+    if (!L.tile_ok) {
+      set_error("Vanka tile kernel: a star or row of level %d exceeds the 5^d-node patch", lev);
+      return EXF_ERR_UNSUPPORTED;
+    }
+    return vanka_sweep_tile<T, D>(s, lev, p, x, b);
+  }
+  return vanka_sweep_rows<T, D>(s, lev, p, x, b);
+}
+
+// FP16 copy of the velocity blocks for the FP32 smoother: row (n, a) is scaled by its
+// largest magnitude over every block and column, so each stored entry lies in [-1, 1]
+// (no overflow; entries below 2^-14 of the row maximum lose relative precision, which
+// bounds their absolute error by 2^-25 of the row maximum).  Records as read by
+// Packed16 and TileBlocks16 / k_vanka_stream.  One warp per node.
+template <int D>
+__global__ void k_pack16(int N, const int *__restrict__ qq_ptr, const int *__restrict__ qq_col,
+                         const int16_t *__restrict__ tcq, long nqq, const double *__restrict__ vv,
+                         void *__restrict__ h16, uint2 *__restrict__ cx, uint32_t *__restrict__ qc,
+                         float *__restrict__ vsc) {
+  const int n = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+  if (n >= N) return;  // uniform per warp
+  const int k0 = qq_ptr[n], k1 = qq_ptr[n + 1];
+  double sc[D];
+  for (int a = 0; a < D; a++) {
+    double mx = 0.;
+    for (int k = k0 + lane; k < k1; k += 32)
+      for (int bb = 0; bb < D; bb++) mx = fmax(mx, fabs(vv[(long)(a * D + bb) * nqq + k]));
+    for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    sc[a] = (mx > 0. && mx < 1e300) ? mx : 1.;
+    if (lane == 0) vsc[(long)a * N + n] = (float)sc[a];
+  }
+  for (int k = k0 + lane; k < k1; k += 32) {
+    unsigned short hv[D * D + 1];
+    for (int q = 0; q < D * D; q++) {
+      const __half hq = __float2half_rn((float)(vv[(long)q * nqq + k] / sc[q / D]));
+      memcpy(&hv[q], &hq, 2);
+    }
+    hv[D * D] = 0;
+    unsigned w[(D * D + 1) / 2];
+    for (int i = 0; i < (D * D + 1) / 2; i++) w[i] = (unsigned)hv[2 * i] | ((unsigned)hv[2 * i + 1] << 16);
+    if constexpr (D == 3) {
+      reinterpret_cast<uint4 *>(h16)[k] = make_uint4(w[0], w[1], w[2], w[3]);
+      cx[k] = make_uint2((unsigned)qq_col[k], w[4]);
+      qc[k] = (w[4] & 0xffffu) | ((uint32_t)(uint16_t)tcq[k] << 16);
+    } else {
+      reinterpret_cast<uint2 *>(h16)[k] = make_uint2(w[0], w[1]);
+    }
+  }
+}
+
 int vanka_prep(exf_sys *s, int lev) {
   if (s->kind != EXF_KIND_NS) return EXF_OK;
   SysLevel &L = s->L[lev];
+  if (s->dim == 2)
+    k_pack16<2><<<nblk(L.N, 8), 256, 0, s->stream>>>(L.N, L.qq_ptr.p, L.qq_col.p, L.tcq.p, L.nqq, L.A.vv.p,
+                                                      L.h16.p, nullptr, nullptr, L.vsc.p);
+  else
+    k_pack16<3><<<nblk(L.N, 8), 256, 0, s->stream>>>(L.N, L.qq_ptr.p, L.qq_col.p, L.tcq.p, L.nqq, L.A.vv.p,
+                                                      L.h16.p, L.h16cx.p, L.h16qc.p, L.vsc.p);
+  EXF_LAUNCH_CHECK();
+  EXF_COUNT(1);
   const unsigned grid = nblk(L.NL, 4);
   if (s->dim == 2)
     k_vanka_prep<2><<<grid, 128, 0, s->stream>>>(L.NL, L.pstart.p, L.qq_ptr.p, L.qq_col.p, L.ql_ptr.p,
@@ -717,25 +1497,33 @@ int coarse_factor(exf_sys *s) {
   return EXF_OK;
 }
 
-// x = A0^{-1} (b * gmask), one warp per row, FP64 arithmetic for either vector type
-template <class T>
+// x = A0^{-1} (b * gmask), one warp per row, FP64 arithmetic for either vector type;
+// with I4 vectors DOF j is slot j / N0 of node j % N0 (pressure: slot 3 of node j - d*N0)
+template <bool I4>
+__device__ __forceinline__ long coarse_slot(int j, int N0, int d) {
+  if (!I4) return j;
+  return j < d * N0 ? 4L * (j % N0) + j / N0 : 4L * (j - d * N0) + 3;
+}
+template <class T, bool I4>
 __global__ void k_coarse_gemv(const double *__restrict__ inv, int n, const double *__restrict__ gmask,
-                              const T *__restrict__ b, T *__restrict__ x) {
+                              const T *__restrict__ b, T *__restrict__ x, int N0, int d) {
   EXF_PDL_WAIT();
   const int row = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5), lane = threadIdx.x & 31;
   if (row >= n) return;
   double acc = 0.;
-  for (int j = lane; j < n; j += 32) acc += inv[(long)row * n + j] * (gmask[j] * (double)b[j]);
+  for (int j = lane; j < n; j += 32)
+    acc += inv[(long)row * n + j] * (gmask[j] * (double)b[coarse_slot<I4>(j, N0, d)]);
   for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
-  if (lane == 0) x[row] = (T)acc;
+  if (lane == 0) x[coarse_slot<I4>(row, N0, d)] = (T)acc;
 }
 
 template <class T>
 int coarse_apply(exf_sys *s, const T *b, T *x) {
   if (!s->coarse_ok) EXF_TRY(coarse_factor(s));
   const int n = s->L[0].ndof;
-  EXF_CUDA(launch_pdl(k_coarse_gemv<T>, dim3(nblk(n, 8)), dim3(256), 0, s->stream, s->coarse_inv.p, n, s->gmask0.p,
-                      b, x));
+  auto kern = (s->nv1 && sizeof(T) == 4) ? k_coarse_gemv<T, true> : k_coarse_gemv<T, false>;
+  EXF_CUDA(launch_pdl(kern, dim3(nblk(n, 8)), dim3(256), 0, s->stream, s->coarse_inv.p, n, s->gmask0.p, b, x,
+                      s->L[0].N, s->nv2));
   EXF_COUNT(1);
   return EXF_OK;
 }
@@ -758,23 +1546,28 @@ int zero_vec(cudaStream_t st, T *a, long n) {
 template int zero_vec<double>(cudaStream_t, double *, long);
 template int zero_vec<float>(cudaStream_t, float *, long);
 
-__global__ void k_cast_d2f(const double *a, float *b, long n) {
+// FP64 DOF-order vectors <-> FP32 V-cycle vectors (I4 when i4 != 0: N nodes, d velocity
+// components)
+__device__ __forceinline__ long i4_slot(long i, int N, int d) {
+  return i < (long)d * N ? 4 * (i % N) + i / N : 4 * (i - (long)d * N) + 3;
+}
+__global__ void k_cast_d2f(const double *a, float *b, long n, int i4, int N, int d) {
   EXF_PDL_WAIT();
   long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n) b[i] = (float)a[i];
+  if (i < n) b[i4 ? i4_slot(i, N, d) : i] = (float)a[i];
 }
-__global__ void k_add_f2d(const float *a, double *b, long n) {
+__global__ void k_add_f2d(const float *a, double *b, long n, int i4, int N, int d) {
   EXF_PDL_WAIT();
   long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n) b[i] += (double)a[i];
+  if (i < n) b[i] += (double)a[i4 ? i4_slot(i, N, d) : i];
 }
-int cast_d2f(cudaStream_t st, const double *a, float *b, long n) {
-  EXF_CUDA(launch_pdl(k_cast_d2f, dim3(nblk(n, 256)), dim3(256), 0, st, a, b, n));
+int cast_d2f(cudaStream_t st, const double *a, float *b, long n, int i4, int N, int d) {
+  EXF_CUDA(launch_pdl(k_cast_d2f, dim3(nblk(n, 256)), dim3(256), 0, st, a, b, n, i4, N, d));
   EXF_COUNT(1);
   return EXF_OK;
 }
-int add_f2d(cudaStream_t st, const float *a, double *b, long n) {
-  EXF_CUDA(launch_pdl(k_add_f2d, dim3(nblk(n, 256)), dim3(256), 0, st, a, b, n));
+int add_f2d(cudaStream_t st, const float *a, double *b, long n, int i4, int N, int d) {
+  EXF_CUDA(launch_pdl(k_add_f2d, dim3(nblk(n, 256)), dim3(256), 0, st, a, b, n, i4, N, d));
   EXF_COUNT(1);
   return EXF_OK;
 }

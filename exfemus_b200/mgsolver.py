@@ -37,6 +37,7 @@ def mg_params(**kw):
     p.nu_pre, p.nu_post, p.double_below_top = 2, 2, 1
     p.smoother, p.omega, p.corr_damp = _lib.SMOOTH_GS, 0.4, 0.95
     p.cond_corr, p.reverse_colours, p.precision, p.use_graph = 0, 0, _lib.PREC_FP64, 1
+    p.vanka_kernel = _lib.VANKA_AUTO
     for k, v in kw.items():
         setattr(p, k, v)
     return p

@@ -61,6 +61,12 @@ extern "C" {
 #define EXF_PREC_FP64 0          /* everything FP64                                 */
 #define EXF_PREC_MIXED 1         /* FP32 V-cycle inside FP64 defect correction      */
 
+/* Vanka kernel selection (exf_mg_params.vanka_kernel): both compute the same update and
+ * differ only in the order of floating-point sums.  AUTO uses ROWS. */
+#define EXF_VANKA_AUTO 0
+#define EXF_VANKA_TILE 1         /* one CTA per patch, iterate staged in shared memory */
+#define EXF_VANKA_ROWS 2         /* star-row residual kernel + patch-solve kernel      */
+
 typedef struct {
   int dim;          /* 2 (quad9/quad4) or 3 (hex27/hex8)                          */
   int nlev;         /* geometric levels                                            */
@@ -96,6 +102,7 @@ typedef struct {
   int reverse_colours; /* 1: colours swept in reverse order                        */
   int precision;       /* EXF_PREC_*                                               */
   int use_graph;       /* 1: replay each V-cycle from a captured CUDA graph        */
+  int vanka_kernel;    /* EXF_VANKA_*                                              */
 } exf_mg_params;
 
 typedef struct {

@@ -104,7 +104,13 @@ def test_solver_operations_match_oracle(case):
         assert rel(gs.prolong(lev + 1, xc), P @ xc) < 1e-14
 
 
-def test_smoother_sweep_matches_oracle(case, oracle_mod):
+# Vanka kernels: TILE (one CTA per patch, iterate staged in shared memory) and ROWS (row
+# kernel + patch-solve kernel); the library picks per level, the tests force each
+VK = [_lib.VANKA_TILE, _lib.VANKA_ROWS]
+
+
+@pytest.mark.parametrize("vk", VK)
+def test_smoother_sweep_matches_oracle(case, oracle_mod, vk):
     _assemble_both(case)
     gs, os_ = case["gs"], case["os"]
     rng = np.random.default_rng(5)
@@ -114,7 +120,7 @@ def test_smoother_sweep_matches_oracle(case, oracle_mod):
         for lev in range(1, case["nlev"]):
             x = rng.standard_normal(gs.ndof(lev))
             b = rng.standard_normal(gs.ndof(lev))
-            gp = ex.mg_params(smoother=smoother, omega=0.4, reverse_colours=rev)
+            gp = ex.mg_params(smoother=smoother, omega=0.4, reverse_colours=rev, vanka_kernel=vk)
             op = or_mg(oracle_mod, smoother=1 if ns else 0, omega=0.4, reverse_colours=rev)
             xg = gs.smooth(lev, gp, 2, x, b)
             xo = os_.smooth(lev, op, 2, x, b)
@@ -128,13 +134,14 @@ def test_coarse_direct_solve(case):
     assert rel(gs.coarse_solve(b), os_.coarse_solve(b)) < 1e-10
 
 
-def test_multigrid_fp64_matches_oracle_per_cycle(case, oracle_mod):
+@pytest.mark.parametrize("vk", VK)
+def test_multigrid_fp64_matches_oracle_per_cycle(case, oracle_mod, vk):
     _assemble_both(case)
     gs, os_ = case["gs"], case["os"]
     ns = case["kind"] == 1
     nu = (3, 3) if ns else (2, 2)
     gp = ex.mg_params(eps=1e-11, max_cycles=80, nu_pre=nu[0], nu_post=nu[1],
-                      smoother=_lib.SMOOTH_VANKA if ns else _lib.SMOOTH_GS, omega=0.4)
+                      smoother=_lib.SMOOTH_VANKA if ns else _lib.SMOOTH_GS, omega=0.4, vanka_kernel=vk)
     op = or_mg(oracle_mod, eps=1e-11, max_cycles=80, nu_pre=nu[0], nu_post=nu[1], smoother=1 if ns else 0,
                omega=0.4)
     x0 = case["xold"]
@@ -149,14 +156,15 @@ def test_multigrid_fp64_matches_oracle_per_cycle(case, oracle_mod):
     assert rel(gs.x(), xo) < 1e-9
 
 
-def test_mixed_precision_matches_fp64_oracle(case, oracle_mod):
+@pytest.mark.parametrize("vk", VK)
+def test_mixed_precision_matches_fp64_oracle(case, oracle_mod, vk):
     _assemble_both(case)
     gs, os_ = case["gs"], case["os"]
     ns = case["kind"] == 1
     nu = (3, 3) if ns else (2, 2)
     gp = ex.mg_params(eps=1e-12, max_cycles=120, nu_pre=nu[0], nu_post=nu[1],
                       smoother=_lib.SMOOTH_VANKA if ns else _lib.SMOOTH_GS, omega=0.4,
-                      precision=_lib.PREC_MIXED)
+                      precision=_lib.PREC_MIXED, vanka_kernel=vk)
     op = or_mg(oracle_mod, eps=1e-13, max_cycles=150, nu_pre=nu[0], nu_post=nu[1], smoother=1 if ns else 0,
                omega=0.4)
     x0 = case["xold"]
