@@ -1024,6 +1024,15 @@ int exf_level_bytes(exf_sys *s, int lev, int precision, double *spmv_bytes, doub
   auto vrow = [&](int n) {  // bytes of the d velocity rows of node n
     return (double)(qp[n + 1] - qp[n]) * (d * d * vb + 4.) + (double)(lp[n + 1] - lp[n]) * (d * vb + 4.) + 8.;
   };
+  // a star row as the Vanka row kernel reads it: FP16 records in the FP32 smoother
+  // (3D: 16 + 8 bytes per block; 2D: 8 + 4), FP64 planes + column otherwise; pressure
+  // couplings; its descriptor (16) and, for FP16, its d row scales
+  const bool h16 = precision == EXF_PREC_MIXED;
+  auto srow = [&](int n) {
+    const double blk = h16 ? (d == 3 ? 24. : 12.) : d * d * vb + 4.;
+    return (double)(qp[n + 1] - qp[n]) * blk + (double)(lp[n + 1] - lp[n]) * (d * vb + 4.) + 16. +
+           (h16 ? d * 4. : 0.);
+  };
   auto prow = [&](int m) {
     return (double)(qp[m + 1] - qp[m]) * (d * vb) + (double)(lp[m + 1] - lp[m]) * vb + 4.;
   };
@@ -1039,7 +1048,7 @@ int exf_level_bytes(exf_sys *s, int lev, int precision, double *spmv_bytes, doub
     } else {
       double B = 0.;
       for (int m = 0; m < L.NL; m++) {
-        for (int k = qp[m]; k < qp[m + 1]; k++) B += vrow(qc[k]) + 3. * d * vb;  // rows + b, x read/write
+        for (int k = qp[m]; k < qp[m + 1]; k++) B += srow(qc[k]) + 3. * d * vb;  // rows + b, x read/write
         B += prow(m) + 3. * vb;
       }
       *sweep_bytes = B;

@@ -141,3 +141,28 @@ def make_case(name, device=0, **over):
         ns.set_xold(ns_initial(w, xyz, mesh.ntop, ns.ntop_dof))
         ns.set_x(ns.xold())
     return out
+
+
+def picard(case, steps, precision=None, on_step=None):
+    """Segregated Picard iteration: every step runs MGTimeStep of each equation in map
+    order (NS, then T), as MGEquationsSystem::eqnmap_timestep_loop does
+    (src/MGEquationsSystem.C:422-432); each MGTimeStep assembles every level, solves and
+    updates x_old."""
+    stats = []
+    for it in range(steps):
+        row = {}
+        for key in ("NS", "T"):
+            if key not in case:
+                continue
+            s, p = case[key], case["mg_" + key]
+            if precision is not None:
+                p.precision = precision
+            st = s.MGTimeStep(0.0, p)
+            if not st.converged:
+                raise RuntimeError("%s solve at Picard step %d: rel %.3e after %d cycles"
+                                   % (key, it, st.rel_res, st.cycles))
+            row[key] = (st.cycles, st.seconds, st.rel_res)
+        stats.append(row)
+        if on_step:
+            on_step(it, row)
+    return stats

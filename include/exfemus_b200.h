@@ -204,7 +204,10 @@ EXF_API long long exf_launch_count(void);
  * that overlap on the GPU race.  It has no counterpart in the reference. */
 EXF_API int exf_resid_norm_static(exf_sys *s, int lev, const double *x, const double *b, double *r,
                                   double *norm2);
-/* algorithmic bytes of one residual (spmv) and one smoother sweep on level lev */
+/* algorithmic bytes of one residual (spmv: every matrix row once, FP32 or FP64 values)
+ * and of one smoother sweep on level lev (GS: every row once; Vanka: every star row of
+ * every patch in the value format the sweep reads, since each colour recomputes the
+ * residuals of its stars from the iterate at its start) */
 EXF_API int exf_level_bytes(exf_sys *s, int lev, int precision, double *spmv_bytes, double *sweep_bytes);
 
 #ifdef __cplusplus
