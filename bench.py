@@ -304,6 +304,8 @@ def run_ours(args, ws, rank, local):
     vcycle_ms = tv.value
     _lib.check(L.exf_time_op(ns.h, 2, top, C.byref(mg_mixed), C.byref(ns.phys), 3, C.byref(tv)))
     asm_ms = tv.value
+    _lib.check(L.exf_time_op(ns.h, 4, 0, C.byref(mg_mixed), C.byref(ns.phys), 2, C.byref(tv)))
+    coarse_ms = tv.value
     _lib.check(L.exf_time_op(ns.h, 1, top, C.byref(mg_mixed), C.byref(ns.phys), 5, C.byref(tv)))
     sweep_ms = tv.value
     _lib.check(L.exf_time_op(ns.h, 0, top, C.byref(mg_mixed), C.byref(ns.phys), 20, C.byref(tv)))
@@ -360,6 +362,7 @@ def run_ours(args, ws, rank, local):
             "err_mixed_vs_fp64_1e-13": err_mixed, "err_fp64_1e-10_vs_fp64_1e-13": err_fp64,
             "vcycle_dof_per_s": ndof / (vcycle_ms * 1e-3), "vcycle_ms": vcycle_ms,
             "assembly_melem_per_s": nel / (asm_ms * 1e-3) / 1e6, "assembly_ms": asm_ms,
+            "coarse_factor_ms": coarse_ms,
             "spmv_fp32_gbs": b_spmv32.value / (spmv32_ms * 1e-3) / 1e9,
             "spmv_fp64_gbs": b_spmv64.value / (spmv64_ms * 1e-3) / 1e9,
             "roofline": {"kernel": "k_vanka_rows + k_vanka_solve, one FP32 Vanka sweep of the fine level "

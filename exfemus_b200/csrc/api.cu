@@ -988,6 +988,9 @@ int exf_time_op(exf_sys *s, int what, int lev, const exf_mg_params *p, const exf
         }
         return vcycle_fp64(s, p, s->red.out.p + 1);
       }
+      case 4:
+        s->coarse_ok = 0;
+        return coarse_factor(s);
       default:
         set_error("exf_time_op: unknown operation %d", what);
         return EXF_ERR_ARG;

@@ -1334,8 +1334,9 @@ template int smooth<float>(exf_sys *, int, const exf_mg_params *, int, float *, 
 // step k pivots on the largest |a_ik| among unused rows p_k, which leaves
 // W[p_k][j] = A0^{-1}[k][p_j]; the extraction kernel undoes the permutation.  Each coarse
 // solve is then one dense GEMV in FP64.  Pressure-gauge rows become identity rows in the
-// factored copy (the enclosed-flow pressure level is otherwise free).  Ties in the pivot
-// search go to the smallest row index, so the factorisation is deterministic.
+// factored copy (the enclosed-flow pressure level is otherwise free).  The pivot search
+// merges keys of the magnitude's top 44 bits and the row (smallest row among equal keys)
+// with atomicMax, so the factorisation is deterministic.
 __global__ void k_dense_from_csr(const int *ptr, const int *col, const double *val, int n, double *W) {
   int i = blockIdx.x;
   for (int j = threadIdx.x; j < n; j += blockDim.x) W[(long)i * n + j] = 0.;
@@ -1348,94 +1349,107 @@ __global__ void k_gauge_rows(double *W, int n, const double *gmask) {
   for (int j = threadIdx.x; j < n; j += blockDim.x) W[(long)i * n + j] = (j == i) ? 1. : 0.;
 }
 
-__device__ __forceinline__ void argmax_merge(double &v, int &i, double v2, int i2) {
-  if (v2 > v || (v2 == v && i2 >= 0 && (i < 0 || i2 < i))) {
-    v = v2;
-    i = i2;
-  }
+// Pivot key: the top 44 bits of |a| (non-negative doubles order as unsigned integers)
+// above the inverted row index, so the largest magnitude wins and, among magnitudes equal
+// in those bits, the smallest row; 0 = no candidate.  Rows below 2^20.
+__device__ __forceinline__ unsigned long long piv_key(double a, int i) {
+  const unsigned long long b = (unsigned long long)__double_as_longlong(fabs(a));
+  return ((b >> 20) << 20) | (unsigned long long)(0xFFFFF - i);
 }
 
+// block maximum of the keys, then one atomicMax per block on *dst
 template <int NT>
-__device__ void block_argmax(double v, int i, double *sv, int *si, double *bm, int *bi) {
+__device__ __forceinline__ void block_key_max(unsigned long long v, unsigned long long *sk,
+                                              unsigned long long *dst) {
   for (int o = 16; o > 0; o >>= 1) {
-    double v2 = __shfl_down_sync(0xffffffffu, v, o);
-    int i2 = __shfl_down_sync(0xffffffffu, i, o);
-    argmax_merge(v, i, v2, i2);
+    const unsigned long long v2 = __shfl_down_sync(0xffffffffu, v, o);
+    v = v2 > v ? v2 : v;
   }
-  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-  if (l == 0) {
-    sv[w] = v;
-    si[w] = i;
-  }
+  if ((threadIdx.x & 31) == 0) sk[threadIdx.x >> 5] = v;
   __syncthreads();
   if (threadIdx.x == 0) {
-    double bv = -1.;
-    int bidx = -1;
-    for (int k = 0; k < NT / 32; k++) argmax_merge(bv, bidx, sv[k], si[k]);
-    bm[blockIdx.x] = bv;
-    bi[blockIdx.x] = bidx;
+    unsigned long long m = 0;
+    for (int w = 0; w < NT / 32; w++) m = sk[w] > m ? sk[w] : m;
+    if (m) atomicMax(dst, m);
   }
   __syncthreads();
 }
 
+// Step k reads the iterate from Wc and writes the next one to Wn (the two swap every
+// step), so every block can read pivot row p and column k while others write: one
+// grid-wide barrier per pivot.  The pivot row p of step k comes from key[k], merged by
+// one atomicMax per block during step k-1 over the candidates of column k (unused rows);
+// rows are distributed over blocks, columns over threads.
 template <int NT>
 __global__ void __launch_bounds__(NT)
-    k_gj_coop(double *W, int n, int *pivrow, double *colk, double *rowp, double *bm, int *bi, int *used, int *bad) {
+    k_gj_coop(double *__restrict__ W0, double *__restrict__ W1, int n, int *__restrict__ pivrow,
+              unsigned long long *__restrict__ key, int *__restrict__ used, int *__restrict__ bad) {
   namespace cg = cooperative_groups;
   cg::grid_group grid = cg::this_grid();
-  __shared__ double sv[NT / 32];
-  __shared__ int si[NT / 32];
-  __shared__ int s_p;
+  __shared__ unsigned long long sk[NT / 32];
   const long gt = (long)blockIdx.x * NT + threadIdx.x;
   const long nth = (long)gridDim.x * NT;
-  // candidates for column 0
   {
-    double v = -1.;
-    int idx = -1;
-    for (long i = gt; i < n; i += nth) argmax_merge(v, idx, fabs(W[i * n]), (int)i);
-    block_argmax<NT>(v, idx, sv, si, bm, bi);
+    unsigned long long v = 0;
+    for (long i = gt; i < n; i += nth) {
+      const unsigned long long c = piv_key(W0[i * n], (int)i);
+      v = c > v ? c : v;
+    }
+    block_key_max<NT>(v, sk, &key[0]);
   }
   grid.sync();
   for (int k = 0; k < n; k++) {
-    // phase A: every block selects the same pivot row and stashes row p and column k
-    if (threadIdx.x == 0) {
-      double bv = -1.;
-      int bidx = -1;
-      for (int b = 0; b < (int)gridDim.x; b++) argmax_merge(bv, bidx, bm[b], bi[b]);
-      s_p = bidx;
-    }
-    __syncthreads();
-    const int p = s_p;
-    if (p < 0) {  // every remaining row is zero in this column: singular
+    const double *__restrict__ Wc = (k & 1) ? W1 : W0;
+    double *__restrict__ Wn = (k & 1) ? W0 : W1;
+    const unsigned long long kk = __ldcg(&key[k]);
+    if (kk == 0) {  // no candidate row left: singular (uniform across the grid)
       if (gt == 0) *bad = 1;
-      return;     // uniform across the grid: every block took the same branch
+      return;
     }
+    const int p = 0xFFFFF - (int)(kk & 0xFFFFFull);
+    const double *rowp = Wc + (long)p * n;
+    const double piv = rowp[k];
+    const double inv = piv != 0. ? 1. / piv : 0.;
     if (gt == 0) {
       pivrow[k] = p;
       used[p] = 1;
-      if (W[(long)p * n + k] == 0.) *bad = 1;
+      if (piv == 0.) *bad = 1;
     }
-    for (long t = gt; t < n; t += nth) {
-      rowp[t] = W[(long)p * n + t];
-      colk[t] = W[t * n + k];
+    unsigned long long best = 0;
+    for (int i = blockIdx.x; i < n; i += gridDim.x) {
+      const double *Wi = Wc + (long)i * n;
+      double *Oi = Wn + (long)i * n;
+      const double ci = Wi[k];
+      const bool cand = i != p && !used[i];
+      for (int j0 = threadIdx.x; j0 < n; j0 += 4 * NT) {
+        double w[4], r[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+          const int j = j0 + u * NT;
+          w[u] = r[u] = 0.;
+          if (j < n) {
+            w[u] = Wi[j];
+            r[u] = rowp[j];
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+          const int j = j0 + u * NT;
+          if (j < n) {
+            double a;
+            if (i == p) a = (j == k) ? inv : r[u] * inv;
+            else if (j == k) a = -ci * inv;
+            else a = w[u] - ci * r[u] * inv;
+            Oi[j] = a;
+            if (j == k + 1 && cand) {
+              const unsigned long long c = piv_key(a, i);
+              best = c > best ? c : best;
+            }
+          }
+        }
+      }
     }
-    grid.sync();
-    // phase B: update every entry, collect pivot candidates of column k+1
-    const double piv = rowp[k];
-    const double inv = piv != 0. ? 1. / piv : 0.;
-    double v = -1.;
-    int idx = -1;
-    const long nn = (long)n * n;
-    for (long e = gt; e < nn; e += nth) {
-      const int i = (int)(e / n), j = (int)(e % n);
-      double a;
-      if (i == p) a = (j == k) ? inv : rowp[j] * inv;
-      else if (j == k) a = -colk[i] * inv;
-      else a = W[e] - colk[i] * rowp[j] * inv;
-      W[e] = a;
-      if (j == k + 1 && i != p && !used[i]) argmax_merge(v, idx, fabs(a), i);
-    }
-    block_argmax<NT>(v, idx, sv, si, bm, bi);
+    if (k + 1 < n) block_key_max<NT>(best, sk, &key[k + 1]);
     grid.sync();
   }
 }
@@ -1451,39 +1465,51 @@ int coarse_factor(exf_sys *s) {
   SysLevel &L = s->L[0];
   const int n = L.ndof;
   cudaStream_t st = s->stream;
-  DBuf<double> vals, colk, rowp, bm;
-  DBuf<int> bad, pivrow, used, bi;
+  constexpr int NT = 256;
+  DBuf<double> vals, W1;
+  DBuf<int> bad, pivrow, used;
+  DBuf<unsigned long long> key;
+  if (n >= 0xFFFFF) {
+    set_error("coarsest level of %d DOFs exceeds the direct solver's %d", n, 0xFFFFF - 1);
+    return EXF_ERR_UNSUPPORTED;
+  }
   EXF_TRY(vals.alloc(L.nnz));
   EXF_TRY(csr_values(s, 0, vals.p));
   EXF_TRY(s->coarse_work.alloc((size_t)n * n));
-  EXF_TRY(colk.alloc(n));
-  EXF_TRY(rowp.alloc(n));
+  EXF_TRY(W1.alloc((size_t)n * n));
   EXF_TRY(pivrow.alloc(n));
   EXF_TRY(used.alloc(n));
   EXF_TRY(used.zero(st));
   EXF_TRY(bad.alloc(1));
   EXF_TRY(bad.zero(st));
+  EXF_TRY(key.alloc((size_t)n + 1));
+  EXF_TRY(key.zero(st));
   double *W = s->coarse_work.p;
   k_dense_from_csr<<<n, 128, 0, st>>>(L.csr_ptr.p, L.csr_col.p, vals.p, n, W);
   k_gauge_rows<<<n, 128, 0, st>>>(W, n, s->gmask0.p);
   EXF_LAUNCH_CHECK();
-  constexpr int NT = 256;
   int dev = 0, nsm = 0, per_sm = 0;
   EXF_CUDA(cudaGetDevice(&dev));
   EXF_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
   EXF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_gj_coop<NT>, NT, 0));
-  long want = ((long)n * n + NT - 1) / NT;
-  int grid = (int)std::min<long>(std::max(1, nsm * std::min(per_sm, 2)), std::max<long>(1, want));
-  EXF_TRY(bm.alloc(grid));
-  EXF_TRY(bi.alloc(grid));
-  void *args[] = {&W, (void *)&n, &pivrow.p, &colk.p, &rowp.p, &bm.p, &bi.p, &used.p, &bad.p};
+  if (per_sm < 1) {
+    set_error("cooperative factorisation kernel does not fit on an SM");
+    return EXF_ERR_CUDA;
+  }
+#ifndef EXF_GJ_BLOCKS_PER_SM
+#define EXF_GJ_BLOCKS_PER_SM 2
+#endif
+  const int grid = std::max(1, std::min(n, nsm * std::min(per_sm, EXF_GJ_BLOCKS_PER_SM)));  // rows over blocks
+  double *W1p = W1.p;
+  void *args[] = {&W, &W1p, (void *)&n, &pivrow.p, &key.p, &used.p, &bad.p};
   EXF_CUDA(cudaLaunchCooperativeKernel((void *)k_gj_coop<NT>, grid, NT, args, 0, st));
   EXF_COUNT(3);
+  const double *Wfinal = (n & 1) ? W1.p : W;  // step n-1 wrote buffer (n-1)&1 ? W0 : W1
   if (s->coarse_inv.n != (size_t)n * n) {
     EXF_TRY(s->coarse_inv.alloc((size_t)n * n));
     s->buf_epoch++;
   }
-  k_extract_inv<<<n, 128, 0, st>>>(W, n, pivrow.p, s->coarse_inv.p);
+  k_extract_inv<<<n, 128, 0, st>>>(Wfinal, n, pivrow.p, s->coarse_inv.p);
   EXF_LAUNCH_CHECK();
   int hbad = 0;
   EXF_CUDA(cudaMemcpyAsync(&hbad, bad.p, sizeof(int), cudaMemcpyDeviceToHost, st));

@@ -183,7 +183,8 @@ EXF_API int exf_adjoint_backward(exf_sys *s, const exf_phys *ph, const exf_mg_pa
                          double *djdq, double *djdg, exf_solve_stats *st);
 
 /* --- timing of one kernel class on device-resident data (CUDA events) -----------------
- * what: 0 = SpMV residual, 1 = smoother sweep, 2 = assembly (all levels), 3 = V-cycle;
+ * what: 0 = SpMV residual, 1 = smoother sweep, 2 = assembly (all levels), 3 = V-cycle,
+ * 4 = factorisation of the coarsest level (as each solve after an assembly pays it);
  * avg_ms = average duration per launch group over reps, precision per exf_mg_params */
 EXF_API int exf_time_op(exf_sys *s, int what, int lev, const exf_mg_params *p, const exf_phys *ph, int reps,
                 double *avg_ms);
