@@ -31,7 +31,10 @@ WORKLOAD = "channel3d"
 # V-cycles the FP64 algorithm needs on the first Picard system of channel3d (identical
 # iterates on CPU and GPU, checked per cycle by the parity tests); used to scale the
 # bounded CPU sample to seconds-to-1e-10.
-CPU_CYCLES_TO_TOL = 32
+# V-cycles the FP64 multigrid needs on the first Picard system of channel3d to reach
+# 1e-10 (the oracle and the GPU FP64 path share the algorithm and their per-cycle
+# residual histories; measured on the GPU path: 23)
+CPU_CYCLES_TO_TOL = 23
 
 
 def parse():
@@ -179,10 +182,12 @@ def run_reference(args, rank):
         times.append(time.perf_counter() - t0)
     wall = time.perf_counter() - t_all
     t_cycle = float(np.mean(times))
-    value = t_cycle * CPU_CYCLES_TO_TOL
-    sample = ("one FP64 V-cycle (3/3 Vanka sweeps, doubled below the top, direct coarse solve) of the "
-              "first Picard system per step, x %d cycles to 1e-10; assembly of all levels %.2f s" %
-              (CPU_CYCLES_TO_TOL, ref["t_asm"]))
+    # the first solve after assembly also factorised the coarsest level
+    t_factor = max(ref["t_cycle"] - t_cycle, 0.)
+    value = t_factor + t_cycle * CPU_CYCLES_TO_TOL
+    sample = ("coarse factorisation (%.2f s) + one FP64 V-cycle (3/3 Vanka sweeps, doubled below the top, "
+              "direct coarse solve) of the first Picard system per step, x %d cycles to 1e-10; assembly of "
+              "all levels %.2f s" % (t_factor, CPU_CYCLES_TO_TOL, ref["t_asm"]))
     line = {"metric": METRIC, "value": value, "unit": "s", "impl": "reference", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * wall / args.steps,
             "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
@@ -241,18 +246,29 @@ def run_ours(args, ws, rank, local):
     mg_fp64 = ex.mg_params(**{f[0]: getattr(mg_mixed, f[0]) for f in mg_mixed._fields_})
     mg_fp64.precision = _lib.PREC_FP64
 
+    import ctypes as C
+    tvs = C.c_double()
+    x_start = ns.xold()  # the workload's initial field: x_old of the first Picard system
+
     def picard_step():
+        # every step is the first Picard step of the workload (same system, same work):
+        # x_old = initial field, assembly of every level, coarse factorisation + mixed
+        # solve to 1e-10 (device time between events 4 and 5), x_old update
+        ns.set_xold(x_start)
+        ns.set_x(x_start)
         ns.assemble_all()
+        _lib.check(L.exf_event_record(ns.h, 4))
         st = ns.solve(mg_mixed)
+        _lib.check(L.exf_event_record(ns.h, 5))
         if not st.converged:
             raise RuntimeError("solve did not converge: rel %.3e after %d cycles" % (st.rel_res, st.cycles))
         ns.xold_update()
-        return st
+        _lib.check(L.exf_event_elapsed(ns.h, 4, 5, C.byref(tvs)))
+        return st, tvs.value * 1e-3
 
     for _ in range(args.warmup):
         picard_step()
     ns.sync()
-    x_start = ns.x()  # state entering the timed region (replayed by the end-to-end leg)
     barrier(ws)
     clocks = ClockSampler(local)
     clocks.start()
@@ -260,12 +276,11 @@ def run_ours(args, ws, rank, local):
     _lib.check(L.exf_event_record(ns.h, 0))
     solve_s, cycles = [], []
     for _ in range(args.steps):
-        st = picard_step()
-        solve_s.append(st.seconds)
+        st, secs = picard_step()
+        solve_s.append(secs)
         cycles.append(st.cycles)
     _lib.check(L.exf_event_record(ns.h, 1))
     ns.sync()
-    import ctypes as C
     msv = C.c_double()
     _lib.check(L.exf_event_elapsed(ns.h, 0, 1, C.byref(msv)))
     launches = L.exf_launch_count() - n0
@@ -275,9 +290,10 @@ def run_ours(args, ws, rank, local):
     secs_mixed_max = max_over_ranks(ws, secs_mixed)
     step_ms = max_over_ranks(ws, step_ms)
 
-    # mixed vs FP64 on the next Picard system, same initial guess
+    # mixed vs FP64 on the same (first) Picard system, same initial guess
+    ns.set_xold(x_start)
     ns.assemble_all()
-    x0 = ns.x()
+    x0 = x_start
     res = {}
     sols = {}
     for name, p in (("fp64", mg_fp64), ("mixed", mg_mixed)):
@@ -354,8 +370,9 @@ def run_ours(args, ws, rank, local):
             "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": False, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32 V-cycle / f64 defect correction", "data": "synthetic",
             "config": {"workload": args.workload, "mesh": "64x16x16 hex27/hex8, 4 levels (8x2x2 coarsest)",
-                       "ndof": ndof, "nnz_fine": ns.nnz(top), "picard_step": "assembly all levels + mixed solve "
-                       "to 1e-10 + x_old update", "l2": "inputs larger than L2 (fine matrix %.2f GB FP64)"
+                       "ndof": ndof, "nnz_fine": ns.nnz(top), "picard_step": "first Picard system every step "
+                       "(x_old = initial field): assembly of all levels + coarse factorisation + mixed solve to "
+                       "1e-10 + x_old update; value = factorisation + solve (device events)", "l2": "inputs larger than L2 (fine matrix %.2f GB FP64)"
                        % (b_spmv64.value / 1e9), "parallelism": "replicas" if ws > 1 else "single GPU"},
             "secs_fp64": res["fp64"], "secs_mixed": res["mixed"], "speedup_mixed_vs_fp64": res["fp64"] / res["mixed"],
             "cycles_fp64": res["fp64_cycles"], "cycles_mixed": res["mixed_cycles"],

@@ -111,6 +111,7 @@ struct DBuf {
     p = nullptr;
     n = 0;
   }
+  int ensure(size_t count) { return (p && n == (count ? count : 1)) ? EXF_OK : alloc(count); }
   int alloc(size_t count) {
     release();
     if (count == 0) count = 1;
@@ -234,8 +235,11 @@ struct exf_sys {
   std::vector<exf::SysLevel> L;
   exf::DBuf<double> xold, src_qe, rhs_top;  // top-level fields
   exf::DBuf<double> coarse_inv;             // dense inverse of the (gauged) coarsest matrix
-  exf::DBuf<double> coarse_work;            // Gauss-Jordan work [n x 2n]
-  exf::DBuf<int> coarse_piv;
+  exf::DBuf<double> coarse_work, coarse_work2;  // Gauss-Jordan ping-pong pair [n x n] each
+  exf::DBuf<double> coarse_vals;            // CSR values of the coarsest matrix
+  exf::DBuf<int> coarse_piv, coarse_used, coarse_bad;
+  exf::DBuf<unsigned long long> coarse_key; // pivot keys, one per step
+  // (the factorisation workspace is kept between assemblies: no allocation per solve)
   exf::DBuf<double> gmask0;                 // coarse gauge mask (0 at gauge DOFs)
   int coarse_ok = 0;
   int nsm = 148;                             // SMs of the system's device

@@ -1466,26 +1466,25 @@ int coarse_factor(exf_sys *s) {
   const int n = L.ndof;
   cudaStream_t st = s->stream;
   constexpr int NT = 256;
-  DBuf<double> vals, W1;
-  DBuf<int> bad, pivrow, used;
-  DBuf<unsigned long long> key;
   if (n >= 0xFFFFF) {
     set_error("coarsest level of %d DOFs exceeds the direct solver's %d", n, 0xFFFFF - 1);
     return EXF_ERR_UNSUPPORTED;
   }
-  EXF_TRY(vals.alloc(L.nnz));
-  EXF_TRY(csr_values(s, 0, vals.p));
-  EXF_TRY(s->coarse_work.alloc((size_t)n * n));
-  EXF_TRY(W1.alloc((size_t)n * n));
-  EXF_TRY(pivrow.alloc(n));
-  EXF_TRY(used.alloc(n));
+  EXF_TRY(s->coarse_vals.ensure(L.nnz));
+  EXF_TRY(s->coarse_work.ensure((size_t)n * n));
+  EXF_TRY(s->coarse_work2.ensure((size_t)n * n));
+  EXF_TRY(s->coarse_piv.ensure(n));
+  EXF_TRY(s->coarse_used.ensure(n));
+  EXF_TRY(s->coarse_bad.ensure(1));
+  EXF_TRY(s->coarse_key.ensure((size_t)n + 1));
+  DBuf<int> &pivrow = s->coarse_piv, &used = s->coarse_used, &bad = s->coarse_bad;
+  DBuf<unsigned long long> &key = s->coarse_key;
   EXF_TRY(used.zero(st));
-  EXF_TRY(bad.alloc(1));
   EXF_TRY(bad.zero(st));
-  EXF_TRY(key.alloc((size_t)n + 1));
   EXF_TRY(key.zero(st));
+  EXF_TRY(csr_values(s, 0, s->coarse_vals.p));
   double *W = s->coarse_work.p;
-  k_dense_from_csr<<<n, 128, 0, st>>>(L.csr_ptr.p, L.csr_col.p, vals.p, n, W);
+  k_dense_from_csr<<<n, 128, 0, st>>>(L.csr_ptr.p, L.csr_col.p, s->coarse_vals.p, n, W);
   k_gauge_rows<<<n, 128, 0, st>>>(W, n, s->gmask0.p);
   EXF_LAUNCH_CHECK();
   int dev = 0, nsm = 0, per_sm = 0;
@@ -1500,11 +1499,11 @@ int coarse_factor(exf_sys *s) {
 #define EXF_GJ_BLOCKS_PER_SM 2
 #endif
   const int grid = std::max(1, std::min(n, nsm * std::min(per_sm, EXF_GJ_BLOCKS_PER_SM)));  // rows over blocks
-  double *W1p = W1.p;
+  double *W1p = s->coarse_work2.p;
   void *args[] = {&W, &W1p, (void *)&n, &pivrow.p, &key.p, &used.p, &bad.p};
   EXF_CUDA(cudaLaunchCooperativeKernel((void *)k_gj_coop<NT>, grid, NT, args, 0, st));
   EXF_COUNT(3);
-  const double *Wfinal = (n & 1) ? W1.p : W;  // step n-1 wrote buffer (n-1)&1 ? W0 : W1
+  const double *Wfinal = (n & 1) ? W1p : W;  // step n-1 wrote buffer (n-1)&1 ? W0 : W1
   if (s->coarse_inv.n != (size_t)n * n) {
     EXF_TRY(s->coarse_inv.alloc((size_t)n * n));
     s->buf_epoch++;
@@ -1514,7 +1513,6 @@ int coarse_factor(exf_sys *s) {
   int hbad = 0;
   EXF_CUDA(cudaMemcpyAsync(&hbad, bad.p, sizeof(int), cudaMemcpyDeviceToHost, st));
   EXF_CUDA(cudaStreamSynchronize(st));
-  s->coarse_work.release();
   if (hbad) {
     set_error("coarsest matrix is singular");
     return EXF_ERR_SINGULAR;
