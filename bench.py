@@ -46,9 +46,10 @@ def parse():
     ap.add_argument("--workload", default=WORKLOAD)
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--mode", default="bench", choices=["bench", "vcycle", "step"],
+    ap.add_argument("--mode", default="bench", choices=["bench", "vcycle", "step", "workloads"],
                     help="vcycle: assemble once and run one mixed and one FP64 V-cycle; step: one Picard "
-                         "step (assembly of all levels + mixed solve to 1e-10) -- profiling cases")
+                         "step (assembly of all levels + mixed solve to 1e-10) -- profiling cases; "
+                         "workloads: every workload at full size, one JSON line each")
     return ap.parse_args()
 
 
@@ -227,6 +228,123 @@ def run_step(args, local):
     print("step: %d cycles, rel %.3e, %.3f ms" % (st.cycles, st.rel_res, st.seconds * 1e3), flush=True)
 
 
+def top_wall_weights(xyz):
+    """w_i = integral over the wall y = 1 of phi_i (Simpson weights of each quad9 side)."""
+    x, y = xyz
+    w = np.zeros(x.size)
+    top = np.where(y == 1.0)[0]
+    order = top[np.argsort(x[top])]
+    xs = x[order]
+    for k in range(0, len(order) - 2, 2):
+        h = xs[k + 2] - xs[k]
+        w[order[k]] += h / 6
+        w[order[k + 1]] += 4 * h / 6
+        w[order[k + 2]] += h / 6
+    return w
+
+
+def run_workloads(args, local):
+    """Every workload at its full size (one GPU): Picard steps with per-step cycles and
+    device seconds; the adjoint gradient's cost against the forward solve and its
+    central-difference check along seeded random directions."""
+    import ctypes as C
+    import exfemus_b200 as ex
+    from exfemus_b200 import _lib, workloads
+    L = ex.load()
+
+    def picard_run(name, precision):
+        case = ex.make_case(name, device=local)
+        t0 = time.perf_counter()
+        rows = workloads.picard(case, case["w"]["picard"], precision=precision)
+        wall = time.perf_counter() - t0
+        out = {"workload": name, "precision": "mixed" if precision == _lib.PREC_MIXED else "fp64",
+               "steps": len(rows), "wall_s": wall}
+        for key in ("NS", "T"):
+            if key in case:
+                out[key + "_ndof"] = case[key].ntop_dof
+                out[key + "_cycles"] = [r[key][0] for r in rows]
+                out[key + "_solve_s"] = float(sum(r[key][1] for r in rows))
+        return case, out
+
+    # heat2d: one linear solve (Gauss-Seidel multigrid)
+    case = ex.make_case("heat2d", device=local)
+    t = case["T"]
+    t.assemble_all()
+    st = t.solve(case["mg_T"])
+    print(json.dumps({"workload": "heat2d", "ndof": t.ntop_dof, "cycles": st.cycles, "rel_res": st.rel_res,
+                      "solve_s": st.seconds}), flush=True)
+    for name in ("cavity2d", "channel3d"):
+        for prec in (_lib.PREC_FP64, _lib.PREC_MIXED):
+            _, out = picard_run(name, prec)
+            print(json.dumps(out), flush=True)
+    for prec in (_lib.PREC_FP64, _lib.PREC_MIXED):
+        case, out = picard_run("bouss2d", prec)
+        print(json.dumps(out), flush=True)
+
+    # adjoint2d on the converged Boussinesq velocity (mixed run above): T system with
+    # lognormal per-element sources and 64 Legendre modes of left-wall data
+    w = dict(workloads.WORKLOADS["adjoint2d"])
+    mesh, t = case["mesh"], case["T"]
+    t.phys.inv_dt = 0.0  # the steady heat problem on the converged velocity
+    xyz = mesh.xyz()
+    top = w["nlev"] - 1
+    qe = workloads.lognormal_source(mesh.nel(top), seed=0)
+    g = np.zeros(w["modes"])
+    g[0] = 1.0
+    g[1:] = 0.1 * np.random.default_rng(1).standard_normal(w["modes"] - 1) / np.arange(2, w["modes"] + 1)
+    x0 = workloads.t_initial(w, xyz, t.ntop_dof, g_modes=g)
+    wj = np.ascontiguousarray(top_wall_weights(xyz))
+    p = ex.mg_params(eps=1e-12, max_cycles=400, smoother=_lib.SMOOTH_GS, nu_pre=3, nu_post=3)
+    stf = _lib.ExfSolveStats()
+    t.set_xold(x0)
+    t.set_source(qe)
+    tv = C.c_double()
+    _lib.check(L.exf_event_record(t.h, 6))
+    _lib.check(L.exf_adjoint_forward(t.h, C.byref(t.phys), C.byref(p), C.byref(stf)))
+    _lib.check(L.exf_event_record(t.h, 7))
+    _lib.check(L.exf_event_elapsed(t.h, 6, 7, C.byref(tv)))
+    fwd_ms = tv.value
+    djdq = np.zeros(qe.size)
+    djdg = np.zeros(t.ntop_dof)
+    stb = _lib.ExfSolveStats()
+    _lib.check(L.exf_event_record(t.h, 6))
+    _lib.check(L.exf_adjoint_backward(t.h, C.byref(t.phys), C.byref(p), _lib.dptr(wj), _lib.dptr(djdq),
+                                      _lib.dptr(djdg), C.byref(stb)))
+    _lib.check(L.exf_event_record(t.h, 7))
+    _lib.check(L.exf_event_elapsed(t.h, 6, 7, C.byref(tv)))
+    bwd_ms = tv.value
+    # dJ/dg_k = sum over left-wall Dirichlet DOFs of dJ/dg_i P_k(2 y_i - 1)
+    left = xyz[0] == w["box"][0]
+    s_left = 2.0 * xyz[1][left] - 1.0
+    djdmode = np.array([djdg[left] @ workloads.legendre(k, s_left) for k in range(w["modes"])])
+
+    def J(q, gm):
+        t.set_xold(workloads.t_initial(w, xyz, t.ntop_dof, g_modes=gm))
+        t.set_source(q)
+        t.set_x(np.zeros(t.ntop_dof))
+        pf = ex.mg_params(eps=1e-30, max_cycles=100, smoother=_lib.SMOOTH_GS, nu_pre=3, nu_post=3)
+        stj = _lib.ExfSolveStats()
+        rc = L.exf_adjoint_forward(t.h, C.byref(t.phys), C.byref(pf), C.byref(stj))
+        if rc not in (_lib.EXF_OK, _lib.EXF_ERR_NOT_CONVERGED):
+            _lib.check(rc)
+        return float(wj @ t.x())
+
+    rng = np.random.default_rng(16)
+    errs = []
+    h = 1e-6
+    for _ in range(16):
+        dq = rng.standard_normal(qe.size)
+        dg = rng.standard_normal(w["modes"])
+        fd = (J(qe + h * dq, g + h * dg) - J(qe - h * dq, g - h * dg)) / (2 * h)
+        ad = float(djdq @ dq + djdmode @ dg)
+        errs.append(abs(fd - ad) / abs(fd))
+    print(json.dumps({"workload": "adjoint2d", "T_ndof": t.ntop_dof, "n_sources": int(qe.size),
+                      "modes": w["modes"], "forward_ms": fwd_ms, "forward_cycles": stf.cycles,
+                      "forward_rel_res": stf.rel_res, "backward_ms": bwd_ms, "backward_cycles": stb.cycles,
+                      "backward_rel_res": stb.rel_res, "cost_ratio": bwd_ms / fwd_ms,
+                      "fd_rel_err_max": float(max(errs)), "fd_directions": len(errs), "fd_h": h}), flush=True)
+
+
 def run_ours(args, ws, rank, local):
     import exfemus_b200 as ex
     from exfemus_b200 import _lib
@@ -236,6 +354,8 @@ def run_ours(args, ws, rank, local):
         return run_vcycle(args, local)
     if args.mode == "step":
         return run_step(args, local)
+    if args.mode == "workloads":
+        return run_workloads(args, local)
     case = ex.make_case(args.workload, device=local)
     w = case["w"]
     ns = case["NS"]

@@ -10,8 +10,13 @@ pure diagonal, so the scale does not change the solution.
   heat2d     Q2 heat, unit square 32x32, 4 levels, f = 1 + 0.1 u_e, T = 0 on walls, GS 2/2
   cavity2d   Q2-Q1 lid cavity 128x128, 6 levels, Re = 400, 10 Picard steps, Vanka 3/3
   channel3d  hex27/hex8 channel 4x1x1, 64x16x16, 4 levels, Re = 100, 8 Picard steps
-  bouss2d    Q2-Q1 + Q2 differentially heated cavity 256x256, 7 levels, Ra 1e5, Pr 0.71
-  adjoint2d  bouss2d with per-element sources and 64 Legendre modes of left-wall data
+  bouss2d    Q2-Q1 + Q2 differentially heated cavity 256x256, 7 levels, Ra 1e5, Pr 0.71;
+             every segregated Picard step is an implicit pseudo-time step dt = 1 (the
+             reference's transient mass terms, inv_dt = 1): started from rest, the plain
+             steady Picard iterate is a Stokes flow with |u| ~ 1/nu, and the next
+             linearisation is so convection-dominated that the multigrid diverges
+  adjoint2d  the steady heat problem on the converged bouss2d velocity, with per-element
+             sources and 64 Legendre modes of left-wall data
 """
 import math
 
@@ -27,9 +32,9 @@ WORKLOADS = {
     "channel3d": dict(dim=3, nlev=4, n0=(8, 2, 2), box=(0, 4, 0, 1, 0, 1), kind="NS", bc=_lib.BC_CHANNEL,
                       phys=dict(inv_re=0.01), nu=(3, 3), picard=8),
     "bouss2d": dict(dim=2, nlev=7, n0=(4, 4), box=(0, 1, 0, 1), kind="NS+T", bc=_lib.BC_BOUSS_NS,
-                    bc_t=_lib.BC_BOUSS_T, ra=1e5, pr=0.71, nu=(3, 3), picard=15),
+                    bc_t=_lib.BC_BOUSS_T, ra=1e5, pr=0.71, nu=(3, 3), picard=15, inv_dt=1.0),
     "adjoint2d": dict(dim=2, nlev=7, n0=(4, 4), box=(0, 1, 0, 1), kind="NS+T", bc=_lib.BC_BOUSS_NS,
-                      bc_t=_lib.BC_BOUSS_T, ra=1e5, pr=0.71, nu=(3, 3), picard=15, modes=64),
+                      bc_t=_lib.BC_BOUSS_T, ra=1e5, pr=0.71, nu=(3, 3), picard=15, inv_dt=1.0, modes=64),
 }
 
 VANKA_OMEGA = 0.4
@@ -49,8 +54,9 @@ def bouss_phys(w):
     """Nondimensional Boussinesq scaling: nu = sqrt(Pr/Ra), alpha = 1/sqrt(Ra Pr), f = T e_y."""
     nu = math.sqrt(w["pr"] / w["ra"])
     alpha = 1.0 / math.sqrt(w["ra"] * w["pr"])
-    ns = dict(inv_re=nu, buoy=1.0, dirg=(0.0, 1.0, 0.0))
-    t = dict(inv_re=nu, inv_prdl=alpha / nu)
+    inv_dt = w.get("inv_dt", 0.0)
+    ns = dict(inv_re=nu, buoy=1.0, dirg=(0.0, 1.0, 0.0), inv_dt=inv_dt)
+    t = dict(inv_re=nu, inv_prdl=alpha / nu, inv_dt=inv_dt)
     return ns, t
 
 
