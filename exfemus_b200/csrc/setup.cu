@@ -424,13 +424,26 @@ int build_colours(exf_sys *s) {
       EXF_CUDA(cudaMemcpy(L.tcq.p, tq.data(), L.nqq * sizeof(int16_t), cudaMemcpyHostToDevice));
       EXF_TRY(L.tcl.alloc(L.nql));
       EXF_CUDA(cudaMemcpy(L.tcl.p, tl.data(), L.nql * sizeof(int16_t), cudaMemcpyHostToDevice));
+      // order in which each colour's patches are swept: lattice order (z, y, x) of the
+      // vertex, reversed in every other colour, so that a colour starts where the previous
+      // one ended and finds the star rows both read still in L2 (the order inside a
+      // colour does not change its result: its patches are independent)
+      std::vector<int> sweep(items);
+      auto lkey = [&](int v) {
+        return ((long long)latl(v, 2) * L.Ll[1] + latl(v, 1)) * L.Ll[0] + latl(v, 0);
+      };
+      for (int c = 0; c < L.ncolour; c++) {
+        auto b0 = sweep.begin() + L.col_off[c], b1 = sweep.begin() + L.col_off[c + 1];
+        std::sort(b0, b1, [&](int a, int b) { return lkey(a) < lkey(b); });
+        if (c & 1) std::reverse(b0, b1);
+      }
       std::vector<int> rows;
       std::vector<int> pst(L.NL, 0);
       L.vrow_off.assign(L.ncolour + 1, 0);
       for (int c = 0; c < L.ncolour; c++) {
         L.vrow_off[c] = (int)rows.size();
         for (int t = L.col_off[c]; t < L.col_off[c + 1]; t++) {
-          int mm = items[t];
+          int mm = sweep[t];
           pst[mm] = (int)rows.size();
           for (int k = qp[mm]; k < qp[mm + 1]; k++) rows.push_back(qc[k]);
         }
@@ -445,7 +458,7 @@ int build_colours(exf_sys *s) {
       std::vector<int4> vri(rows.size()), pin(2 * (size_t)nitem);
       int kmax = 0, rmax = 0;
       for (int t = 0; t < nitem; t++) {
-        const int mm = items[t];
+        const int mm = sweep[t];
         const int K = qp[mm + 1] - qp[mm];
         kmax = std::max(kmax, K);
         for (int g = pst[mm]; g < pst[mm] + K; g++) {
