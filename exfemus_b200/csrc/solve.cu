@@ -1116,6 +1116,9 @@ static int vanka_sweep_rows(exf_sys *s, int lev, const exf_mg_params *p, T *x, c
   constexpr int NTR = 256;
   constexpr int UNR_S = sizeof(T) == 4 ? EXF_UNR_BIG32 : EXF_UNR_BIG64;
   constexpr int MINB_S = sizeof(T) == 4 ? EXF_MINB_BIG32 : EXF_MINB_BIG64;
+  // 3D FP32 levels of one to four waves: two blocks per lane, 64 registers
+  constexpr int UNR_M = (D == 3 && sizeof(T) == 4) ? 2 : UNR_S;
+  constexpr int MINB_M = (D == 3 && sizeof(T) == 4) ? 4 : MINB_S;
   constexpr int UNR_L = (D == 3 && sizeof(T) == 4) ? 4 : 2;
   T *res = VK<T>::res(L);
   const long pres_off = (long)L.vrow_off[L.ncolour] * D;
@@ -1126,12 +1129,15 @@ static int vanka_sweep_rows(exf_sys *s, int lev, const exf_mg_params *p, T *x, c
     const int nr = L.vrow_off[c + 1] - L.vrow_off[c];
     const int4 *pin = L.pinfo.p + 2L * L.col_off[c];
     const long nthr = (long)(nr + n) * LPR;
-    const bool big = nthr > 4L * s->nsm * 2048;
+    const long wave = (long)s->nsm * 2048;  // resident threads of the GPU
+    const bool big = nthr > (D == 3 ? 4 : 1) * wave;
+    const bool mid = !big && nthr > wave;
     if constexpr (sizeof(T) == 4) {
       using VB = Packed16<D>;
       const VB vb{L.qq_col.p, L.h16.p, L.h16cx.p};
-      auto kern = big ? k_vanka_rows<T, D, LPR, NTR, I4, UNR_S, MINB_S, VB>
-                      : k_vanka_rows<T, D, LPR, NTR, I4, UNR_L, 1, VB>;
+      auto kern = big   ? k_vanka_rows<T, D, LPR, NTR, I4, UNR_S, MINB_S, VB>
+                  : mid ? k_vanka_rows<T, D, LPR, NTR, I4, UNR_M, MINB_M, VB>
+                        : k_vanka_rows<T, D, LPR, NTR, I4, UNR_L, 1, VB>;
       EXF_CUDA(launch_pdl(kern, dim3(nblk(nthr, NTR)), dim3(NTR), 0, s->stream, L.vrinfo.p + L.vrow_off[c], nr,
                           L.vrow_off[c], pin, n, L.N, vb, (const T *)L.vsc.p, L.qq_col.p, L.ql_col.p, L.nql, L.nqqL,
                           VT<T>::vp(L), VT<T>::pv(L), VT<T>::pp(L), x, b, res, pres_off));
