@@ -146,8 +146,15 @@ __device__ __forceinline__ void node_row_dot(int n, int lane, int N, const int *
 // ------------------------------------------------------------------ SpMV
 // row groups: g < N -> Q2 node g (d outputs), g >= N -> Q1 node g-N (1 output).
 // LPR lanes per row group; the node-block index k is shared by the d*d planes.
+// CTAs per SM the register budget must allow (occupancy over per-thread depth: each
+// configuration measured fastest among its neighbours); 3D FP32 also runs 16 lanes per
+// node row, so each warp has two rows in flight
+template <class T, int D>
+constexpr int spmv_minb() {
+  return D == 3 ? (sizeof(T) == 4 ? 8 : 6) : (D == 2 ? 6 : 8);
+}
 template <class T, int D, int LPR, bool NS, int NT, bool I4>
-__global__ void __launch_bounds__(NT)
+__global__ void __launch_bounds__(NT, spmv_minb<T, D>())
     k_spmv_resid(int N, int NL, const int *__restrict__ qq_ptr, const int *__restrict__ qq_col,
                  const int *__restrict__ ql_ptr, const int *__restrict__ ql_col, long nqq, long nql, long nqqL,
                  const T *__restrict__ vv, const T *__restrict__ vp, const T *__restrict__ pv,
@@ -209,7 +216,7 @@ static int launch_spmv(exf_sys *s, int lev, const T *x, const T *b, T *r, double
   SysLevel &L = s->L[lev];
   constexpr int NT = 256;
   constexpr bool I4 = NS && sizeof(T) == 4;
-  constexpr int LPR = D == 3 ? 32 : (NS ? 16 : 8);
+  constexpr int LPR = D == 3 ? (sizeof(T) == 4 ? 16 : 32) : (NS ? 16 : 8);
   long ngroups = (long)L.N + (NS ? L.NL : 0);
   unsigned grid = nblk(ngroups * LPR, NT);
   if (d_norm2) EXF_TRY(ensure_partials(s, grid));
