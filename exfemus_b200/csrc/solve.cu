@@ -1117,8 +1117,11 @@ template <class T, int D>
 static int vanka_sweep_rows(exf_sys *s, int lev, const exf_mg_params *p, T *x, const T *b) {
   SysLevel &L = s->L[lev];
   constexpr bool I4 = sizeof(T) == 4;
-  constexpr int NTS = D == 3 ? 128 : 64;
-  constexpr int SU = D == 3 ? 3 : 1;  // 3D stars: 125 nodes x 3 <= 3 x 128; 2D: 25 x 2 <= 64
+#ifndef EXF_NTS3
+#define EXF_NTS3 256
+#endif
+  constexpr int NTS = D == 3 ? EXF_NTS3 : 64;
+  constexpr int SU = D == 3 ? (375 + NTS - 1) / NTS : 1;  // 3D stars: 125 nodes x 3; 2D: 25 x 2 <= 64
   constexpr int LPR = D == 3 ? 32 : 16;
   constexpr int NTR = 256;
   constexpr int UNR_S = sizeof(T) == 4 ? EXF_UNR_BIG32 : EXF_UNR_BIG64;
