@@ -35,6 +35,16 @@ WORKLOAD = "channel3d"
 # 1e-10 (the oracle and the GPU FP64 path share the algorithm and their per-cycle
 # residual histories; measured on the GPU path: 23)
 CPU_CYCLES_TO_TOL = 23
+# FP64 flops of one hex27/hex8 Navier-Stokes element in k_assemble, counted from its
+# arithmetic (a multiply-add = 2): 729 node pairs x 27 Gauss points x 47 for the velocity
+# blocks, 216 x 27 x 7 for B / B^T, Jacobians, global derivatives and the rhs
+ASM_FLOPS_HEX27_NS = 729 * 27 * 47 + 216 * 27 * 7 + 27 * 9 * 27 * 2 + 27 * 27 * 9 * 2 + 3 * 27 * 27 * 2
+FMA_CHAINS, FMA_ITERS = 8, 4096  # EXF_FMA_CHAINS, EXF_FMA_ITERS of the probe (exf_time_op 5)
+
+
+def torch_sm_count(dev):
+    import torch
+    return torch.cuda.get_device_properties(dev).multi_processor_count
 
 
 def parse():
@@ -442,6 +452,9 @@ def run_ours(args, ws, rank, local):
     asm_ms = tv.value
     _lib.check(L.exf_time_op(ns.h, 4, 0, C.byref(mg_mixed), C.byref(ns.phys), 2, C.byref(tv)))
     coarse_ms = tv.value
+    _lib.check(L.exf_time_op(ns.h, 5, 0, C.byref(mg_mixed), C.byref(ns.phys), 5, C.byref(tv)))
+    nsm = torch_sm_count(local)
+    fma_tflops = 2.0 * FMA_CHAINS * FMA_ITERS * 4 * nsm * 256 / (tv.value * 1e-3) / 1e12
     _lib.check(L.exf_time_op(ns.h, 1, top, C.byref(mg_mixed), C.byref(ns.phys), 5, C.byref(tv)))
     sweep_ms = tv.value
     _lib.check(L.exf_time_op(ns.h, 0, top, C.byref(mg_mixed), C.byref(ns.phys), 20, C.byref(tv)))
@@ -500,6 +513,9 @@ def run_ours(args, ws, rank, local):
             "vcycle_dof_per_s": ndof / (vcycle_ms * 1e-3), "vcycle_ms": vcycle_ms,
             "assembly_melem_per_s": nel / (asm_ms * 1e-3) / 1e6, "assembly_ms": asm_ms,
             "coarse_factor_ms": coarse_ms,
+            "assembly_fp64_tflops": ASM_FLOPS_HEX27_NS * nel / (asm_ms * 1e-3) / 1e12,
+            "fp64_fma_peak_tflops": fma_tflops,
+            "assembly_frac_of_fp64_peak": ASM_FLOPS_HEX27_NS * nel / (asm_ms * 1e-3) / 1e12 / fma_tflops,
             "spmv_fp32_gbs": b_spmv32.value / (spmv32_ms * 1e-3) / 1e9,
             "spmv_fp64_gbs": b_spmv64.value / (spmv64_ms * 1e-3) / 1e9,
             "roofline": {"kernel": "k_vanka_rows + k_vanka_solve, one FP32 Vanka sweep of the fine level "

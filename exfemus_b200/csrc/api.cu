@@ -959,6 +959,31 @@ int exf_coarse_solve(exf_sys *s, const double *b, double *x) {
   return d2h(s, x, dx.p, L.ndof);
 }
 
+}  // extern "C"
+
+namespace exf {
+// FP64 FMA throughput probe: EXF_FMA_CHAINS independent fma chains of EXF_FMA_ITERS
+// steps per thread, 4 CTAs of 256 threads per SM; the sink is written only if a chain
+// ends in NaN, which keeps the chains live without a store per thread
+__device__ double g_fma_sink;
+__global__ void __launch_bounds__(256) k_fma_probe(double seed) {
+  double a[EXF_FMA_CHAINS];
+#pragma unroll
+  for (int c = 0; c < EXF_FMA_CHAINS; c++) a[c] = seed * (threadIdx.x + c + 1);
+  const double m = 1. - 1e-12, k = 1e-12;
+  for (int it = 0; it < EXF_FMA_ITERS; it++) {
+#pragma unroll
+    for (int c = 0; c < EXF_FMA_CHAINS; c++) a[c] = fma(a[c], m, k);
+  }
+  double sum = 0.;
+#pragma unroll
+  for (int c = 0; c < EXF_FMA_CHAINS; c++) sum += a[c];
+  if (sum != sum) g_fma_sink = sum;
+}
+}  // namespace exf
+
+extern "C" {
+
 // device time of one operation class, averaged over reps launches (CUDA events on the
 // system stream, after one untimed warm-up)
 int exf_time_op(exf_sys *s, int what, int lev, const exf_mg_params *p, const exf_phys *ph, int reps,
@@ -991,6 +1016,10 @@ int exf_time_op(exf_sys *s, int what, int lev, const exf_mg_params *p, const exf
       case 4:
         s->coarse_ok = 0;
         return coarse_factor(s);
+      case 5:
+        k_fma_probe<<<4 * s->nsm, 256, 0, s->stream>>>(1e-3);
+        EXF_LAUNCH_CHECK();
+        return EXF_OK;
       default:
         set_error("exf_time_op: unknown operation %d", what);
         return EXF_ERR_ARG;

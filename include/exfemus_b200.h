@@ -182,9 +182,14 @@ EXF_API int exf_adjoint_forward(exf_sys *s, const exf_phys *ph, const exf_mg_par
 EXF_API int exf_adjoint_backward(exf_sys *s, const exf_phys *ph, const exf_mg_params *p, const double *djdx,
                          double *djdq, double *djdg, exf_solve_stats *st);
 
+#define EXF_FMA_CHAINS 8
+#define EXF_FMA_ITERS 4096
+
 /* --- timing of one kernel class on device-resident data (CUDA events) -----------------
  * what: 0 = SpMV residual, 1 = smoother sweep, 2 = assembly (all levels), 3 = V-cycle,
- * 4 = factorisation of the coarsest level (as each solve after an assembly pays it);
+ * 4 = factorisation of the coarsest level (as each solve after an assembly pays it),
+ * 5 = FP64 FMA throughput probe: 4 CTAs of 256 threads per SM, each thread running
+ *     EXF_FMA_CHAINS independent chains of EXF_FMA_ITERS fma (2 flops each);
  * avg_ms = average duration per launch group over reps, precision per exf_mg_params */
 EXF_API int exf_time_op(exf_sys *s, int what, int lev, const exf_mg_params *p, const exf_phys *ph, int reps,
                 double *avg_ms);
