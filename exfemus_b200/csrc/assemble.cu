@@ -156,28 +156,31 @@ struct AsmArgs {
 };
 
 template <int DIM>
-__device__ double jac_sur(const FETab<DIM> *t, int q, const double (*xb)[9]) {
+__device__ double jac_sur(const FETab<DIM> *t, int q, const double (*xx)[FE<DIM>::NEN], const int *sur) {
+  // side coordinates read from the element's coordinates in shared memory (xx[d][sur[s]])
   if (DIM == 2) {
     double dx = 0, dy = 0;
     for (int s = 0; s < 3; s++) {
-      dx += xb[0][s] * t->sdphi[q][s][0];
-      dy += xb[1][s] * t->sdphi[q][s][0];
+      dx += xx[0][sur[s]] * t->sdphi[q][s][0];
+      dy += xx[1][sur[s]] * t->sdphi[q][s][0];
     }
     return sqrt(dx * dx + dy * dy);
   } else {
     double a[3] = {0, 0, 0}, b[3] = {0, 0, 0};
+#pragma unroll 1
     for (int s = 0; s < 9; s++)
       for (int d = 0; d < 3; d++) {
-        a[d] += xb[d][s] * t->sdphi[q][s][0];
-        b[d] += xb[d][s] * t->sdphi[q][s][DIM - 2];
+        a[d] += xx[d][sur[s]] * t->sdphi[q][s][0];
+        b[d] += xx[d][sur[s]] * t->sdphi[q][s][DIM - 2];
       }
     double c0 = a[1] * b[2] - a[2] * b[1], c1 = a[2] * b[0] - a[0] * b[2], c2 = a[0] * b[1] - a[1] * b[0];
     return sqrt(c0 * c0 + c1 * c1 + c2 * c2);
   }
 }
 
+// 3D: register cap for 3 CTAs per SM (79 registers, no spills; measured fastest)
 template <int DIM, int NT>
-__global__ void __launch_bounds__(NT) k_assemble(AsmArgs<DIM> A, int mode) {
+__global__ void __launch_bounds__(NT, DIM == 3 ? 3 : 1) k_assemble(AsmArgs<DIM> A, int mode) {
   using F = FE<DIM>;
   constexpr int NEN = F::NEN, NVX = F::NVX, NQ = F::NQ;
   const int tid = threadIdx.x;
@@ -248,6 +251,7 @@ __global__ void __launch_bounds__(NT) k_assemble(AsmArgs<DIM> A, int mode) {
     for (int a = 0; a < DIM; a++)
       for (int b = 0; b < DIM; b++) {
         double sum = 0.;
+#pragma unroll 1
         for (int s = 0; s < NEN; s++) sum += s_xx[a][s] * t->dphi[q][s][b];
         J[a][b] = sum;
       }
@@ -281,10 +285,12 @@ __global__ void __launch_bounds__(NT) k_assemble(AsmArgs<DIM> A, int mode) {
     double vg[DIM], mod = 1e-20, tg = 0.;
     for (int d = 0; d < DIM; d++) {
       double sum = 0.;
+#pragma unroll 1
       for (int k = 0; k < NEN; k++) sum += s_phi[q][k] * s_vold[d][k];
       vg[d] = sum;
       mod += sum * sum;
     }
+#pragma unroll 1
     for (int k = 0; k < NEN; k++) tg += s_phi[q][k] * s_told[k];
     mod = sqrt(mod);
     double f[DIM];
@@ -337,7 +343,7 @@ __global__ void __launch_bounds__(NT) k_assemble(AsmArgs<DIM> A, int mode) {
     const long blk = qq_ptr[ni] + A.pos_qq[((long)e * NEN + i) * NEN + j];
     if (!ns) {
       double K = 0.;
-#pragma unroll 3
+#pragma unroll 1
       for (int q = 0; q < NQ; q++) {
         const double pi = s_phi[q][i], pj = s_phi[q][j];
         double adv = 0., lap = 0.;
@@ -352,7 +358,7 @@ __global__ void __launch_bounds__(NT) k_assemble(AsmArgs<DIM> A, int mode) {
     } else {
       double M = 0., T[DIM * DIM];
       for (int k = 0; k < DIM * DIM; k++) T[k] = 0.;
-#pragma unroll 3
+#pragma unroll 1
       for (int q = 0; q < NQ; q++) {
         const double pi = s_phi[q][i], pj = s_phi[q][j];
         double gj[DIM], gi[DIM], adv = 0., lap = 0.;
@@ -413,10 +419,7 @@ __global__ void __launch_bounds__(NT) k_assemble(AsmArgs<DIM> A, int mode) {
     if (A.neigh[(long)e * F::NSIDE + sd] != -1) continue;
     const int *sur = A.side.nodes[sd];
     const int last = sur[F::NSN - 1];
-    double xb[DIM][9];
-    for (int k = 0; k < F::NSN; k++)
-      for (int d = 0; d < DIM; d++) xb[d][k] = s_xx[d][sur[k]];
-    const double det = jac_sur<DIM>(t, F::NSQ - 1, xb);
+    const double det = jac_sur<DIM>(t, F::NSQ - 1, s_xx, sur);
     const double ipen = det * ph.penalty;
     double nrm[3];
     for (int d = 0; d < 3; d++) nrm[d] = (double)A.side.dir[sd][d];
@@ -452,7 +455,7 @@ __global__ void __launch_bounds__(NT) k_assemble(AsmArgs<DIM> A, int mode) {
         const double bv = s_bcv[0][lv];
         for (int j = 0; j < F::NSN; j++) {
           double v = 0.;
-          for (int q = 0; q < F::NSQ; q++) v += jac_sur<DIM>(t, q, xb) * t->sw[q] * t->sphi[q][k] * t->sphi[q][j];
+          for (int q = 0; q < F::NSQ; q++) v += jac_sur<DIM>(t, q, s_xx, sur) * t->sw[q] * t->sphi[q][k] * t->sphi[q][j];
           const long bj = qq_ptr[nlv] + A.pos_qq[((long)e * NEN + lv) * NEN + sur[j]];
           A.vv[bj] += bv * bc_alpha * diff_t * v;
         }
