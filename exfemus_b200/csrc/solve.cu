@@ -1125,6 +1125,10 @@ static int vanka_sweep_rows(exf_sys *s, int lev, const exf_mg_params *p, T *x, c
   constexpr int LPR = D == 3 ? 32 : 16;
   constexpr int NTR = 256;
   constexpr int UNR_S = sizeof(T) == 4 ? EXF_UNR_BIG32 : EXF_UNR_BIG64;
+#ifndef EXF_LPR_BIG32
+#define EXF_LPR_BIG32 16
+#endif
+  constexpr int LPR_S = (D == 3 && sizeof(T) == 4) ? EXF_LPR_BIG32 : LPR;
   constexpr int MINB_S = sizeof(T) == 4 ? EXF_MINB_BIG32 : EXF_MINB_BIG64;
   // 3D FP32 levels of one to four waves: two blocks per lane, 64 registers
   constexpr int UNR_M = (D == 3 && sizeof(T) == 4) ? 2 : UNR_S;
@@ -1142,13 +1146,14 @@ static int vanka_sweep_rows(exf_sys *s, int lev, const exf_mg_params *p, T *x, c
     const long wave = (long)s->nsm * 2048;  // resident threads of the GPU
     const bool big = nthr > (D == 3 ? 4 : 1) * wave;
     const bool mid = !big && nthr > wave;
+    const long nthr_s = (long)(nr + n) * LPR_S;
     if constexpr (sizeof(T) == 4) {
       using VB = Packed16<D>;
       const VB vb{L.qq_col.p, L.h16.p, L.h16cx.p};
-      auto kern = big   ? k_vanka_rows<T, D, LPR, NTR, I4, UNR_S, MINB_S, VB>
+      auto kern = big   ? k_vanka_rows<T, D, LPR_S, NTR, I4, UNR_S, MINB_S, VB>
                   : mid ? k_vanka_rows<T, D, LPR, NTR, I4, UNR_M, MINB_M, VB>
                         : k_vanka_rows<T, D, LPR, NTR, I4, UNR_L, 1, VB>;
-      EXF_CUDA(launch_pdl(kern, dim3(nblk(nthr, NTR)), dim3(NTR), 0, s->stream, L.vrinfo.p + L.vrow_off[c], nr,
+      EXF_CUDA(launch_pdl(kern, dim3(nblk(big ? nthr_s : nthr, NTR)), dim3(NTR), 0, s->stream, L.vrinfo.p + L.vrow_off[c], nr,
                           L.vrow_off[c], pin, n, L.N, vb, (const T *)L.vsc.p, L.qq_col.p, L.ql_col.p, L.nql, L.nqqL,
                           VT<T>::vp(L), VT<T>::pv(L), VT<T>::pp(L), x, b, res, pres_off));
     } else {

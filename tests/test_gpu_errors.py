@@ -85,3 +85,21 @@ def test_graph_and_eager_cycles_agree_bitwise(heat):
         assert st.converged
         xs.append(heat.x())
     assert np.array_equal(xs[0], xs[1])
+
+
+def test_timing_probes_and_refactorisation(heat):
+    """exf_time_op 4 (coarse refactorisation) and 5 (FP64 FMA probe) run on an assembled
+    system; a solve after a refactorisation gives the same bits as before it."""
+    L = _lib.load()
+    heat.assemble_all()
+    p = ex.mg_params(precision=_lib.PREC_MIXED)
+    heat.set_x(np.zeros(heat.ntop_dof))
+    heat.solve(p)
+    x0 = heat.x()
+    tv = C.c_double()
+    for what in (4, 5):
+        _lib.check(L.exf_time_op(heat.h, what, 0, C.byref(p), C.byref(heat.phys), 2, C.byref(tv)))
+        assert tv.value > 0.0
+    heat.set_x(np.zeros(heat.ntop_dof))
+    heat.solve(p)
+    assert np.array_equal(heat.x(), x0)

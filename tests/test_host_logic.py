@@ -45,6 +45,28 @@ def test_workload_sizes_and_sources():
     assert abs(t["inv_re"] * t["inv_prdl"] - 1 / np.sqrt(1e5 * 0.71)) < 1e-15
 
 
+def test_bench_top_wall_weights_and_flop_count():
+    """Simpson weights of the wall y = 1 integrate 1 and x^2 exactly on a quad9 mesh
+    row; the per-element flop count of the assembly is the stated sum of its loops."""
+    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    import bench
+    xs = np.linspace(0.0, 1.0, 9)
+    x = np.concatenate([xs, xs])
+    y = np.concatenate([np.ones(9), np.zeros(9)])
+    w = bench.top_wall_weights((x, y))
+    assert abs(w.sum() - 1.0) < 1e-15
+    assert abs(w @ x ** 2 - 1.0 / 3.0) < 1e-15
+    assert np.all(w[9:] == 0)
+    assert bench.ASM_FLOPS_HEX27_NS == 729 * 27 * 47 + 216 * 27 * 7 + 2 * 27 * 27 * 9 * 2 + 3 * 27 * 27 * 2
+
+
+def test_bouss_pseudo_time_step():
+    ns, t = workloads.bouss_phys(workloads.WORKLOADS["bouss2d"])
+    assert ns["inv_dt"] == 1.0 and t["inv_dt"] == 1.0
+    ns0, _ = workloads.bouss_phys(dict(ra=1e5, pr=0.71))
+    assert ns0["inv_dt"] == 0.0
+
+
 def _replica_worker(rank, world, port, out):
     os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank), WORLD_SIZE=str(world),
                       LOCAL_RANK=str(rank))
