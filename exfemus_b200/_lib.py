@@ -31,6 +31,7 @@ PREC_MIXED = 1
 VANKA_AUTO = 0
 VANKA_TILE = 1
 VANKA_ROWS = 2
+VANKA_STREAM = 3
 
 
 class ExfMeshDesc(C.Structure):

@@ -315,7 +315,7 @@ int build_patterns(exf_sys *s) {
       EXF_TRY(L.A32.pv.alloc((size_t)d * L.nqqL));
       EXF_TRY(L.A32.pp.alloc(L.nllL));
       EXF_TRY(L.h16.alloc(d == 3 ? (size_t)L.nqq : ((size_t)L.nqq + 1) / 2));
-      if (d == 3) EXF_TRY(L.h16cx.alloc((size_t)L.nqq));
+      if (d == 3) EXF_TRY(L.h16cx.alloc((size_t)L.nqq + 2));  // 16-byte chunk reads past the end
       if (d == 3) EXF_TRY(L.h16qc.alloc(((size_t)L.nqq + 7) & ~(size_t)3));  // 16-byte chunk reads past the end
       EXF_TRY(L.vsc.alloc((size_t)d * L.N));
     }

@@ -61,11 +61,13 @@ extern "C" {
 #define EXF_PREC_FP64 0          /* everything FP64                                 */
 #define EXF_PREC_MIXED 1         /* FP32 V-cycle inside FP64 defect correction      */
 
-/* Vanka kernel selection (exf_mg_params.vanka_kernel): both compute the same update and
- * differ only in the order of floating-point sums.  AUTO uses ROWS. */
+/* Vanka kernel selection (exf_mg_params.vanka_kernel): all compute the same update and
+ * differ only in the order of floating-point sums.  AUTO uses ROWS (measured fastest). */
 #define EXF_VANKA_AUTO 0
 #define EXF_VANKA_TILE 1         /* one CTA per patch, iterate staged in shared memory */
 #define EXF_VANKA_ROWS 2         /* star-row residual kernel + patch-solve kernel      */
+#define EXF_VANKA_STREAM 3       /* ROWS with the 3D FP32 star rows copied to shared    */
+                                 /* memory by cp.async (persistent warps)               */
 
 typedef struct {
   int dim;          /* 2 (quad9/quad4) or 3 (hex27/hex8)                          */

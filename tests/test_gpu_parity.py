@@ -104,9 +104,10 @@ def test_solver_operations_match_oracle(case):
         assert rel(gs.prolong(lev + 1, xc), P @ xc) < 1e-14
 
 
-# Vanka kernels: TILE (one CTA per patch, iterate staged in shared memory) and ROWS (row
-# kernel + patch-solve kernel); the library picks per level, the tests force each
-VK = [_lib.VANKA_TILE, _lib.VANKA_ROWS]
+# Vanka kernels: TILE (one CTA per patch, iterate staged in shared memory), ROWS (row
+# kernel + patch-solve kernel) and STREAM (ROWS with the 3D FP32 rows streamed through
+# shared memory); the library picks per level, the tests force each
+VK = [_lib.VANKA_TILE, _lib.VANKA_ROWS, _lib.VANKA_STREAM]
 
 
 @pytest.mark.parametrize("vk", VK)
