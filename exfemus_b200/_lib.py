@@ -118,6 +118,7 @@ SIGNATURES = [
                                   C.POINTER(ExfSolveStats)]),
     ("exf_time_op", _I, [_P, _I, _I, C.POINTER(ExfMgParams), C.POINTER(ExfPhys), _I, _DP]),
     ("exf_sync", _I, [_P]),
+    ("exf_timestep_loop", _I, [C.POINTER(_P), _I, C.POINTER(ExfPhys), C.POINTER(ExfMgParams), _I, _IP, _DP]),
     ("exf_event_record", _I, [_P, _I]),
     ("exf_event_elapsed", _I, [_P, _I, _I, _DP]),
     ("exf_launch_count", C.c_longlong, []),

@@ -1089,6 +1089,31 @@ int exf_level_bytes(exf_sys *s, int lev, int precision, double *spmv_bytes, doub
   return EXF_OK;
 }
 
+int exf_timestep_loop(exf_sys *const *sys, int nsys, const exf_phys *phys, const exf_mg_params *params,
+                      int nsteps, int *cycles, double *seconds) {
+  if (!sys || !phys || !params || nsys < 1 || nsteps < 0) {
+    set_error("exf_timestep_loop: bad argument");
+    return EXF_ERR_ARG;
+  }
+  for (int k = 0; k < nsys; k++)
+    if (!sys[k]) {
+      set_error("exf_timestep_loop: system %d is NULL", k);
+      return EXF_ERR_ARG;
+    }
+  for (int step = 0; step < nsteps; step++) {
+    for (int k = 0; k < nsys; k++) {
+      exf_solve_stats st;
+      EXF_TRY(exf_assemble_all(sys[k], &phys[k]));
+      const int rc = exf_mg_solve(sys[k], &params[k], &st);
+      if (cycles) cycles[(long)step * nsys + k] = st.cycles;
+      if (seconds) seconds[(long)step * nsys + k] = st.seconds;
+      if (rc != EXF_OK) return rc;
+      EXF_TRY(exf_sys_xold_update(sys[k]));
+    }
+  }
+  return EXF_OK;
+}
+
 int exf_sync(exf_sys *s) {
   CHECK_SYS(s);
   EXF_CUDA(cudaStreamSynchronize(s->stream));

@@ -332,3 +332,20 @@ class MGSolT(MGSolBase):
 class MGSolNS(MGSolBase):
     """Coupled Navier-Stokes, Taylor-Hood Q2-Q1 (MGSolNS, NS_EQUATIONS==1)."""
     kind = _lib.KIND_NS
+
+
+def timestep_loop(systems, params, nsteps):
+    """MGEquationsSystem::eqnmap_timestep_loop (src/MGEquationsSystem.C:422-432) in the
+    library: nsteps times the MGTimeStep of every system in order (assembly, solve,
+    x_old update) without returning here between them.  params: one exf_mg_params per
+    system.  Returns (cycles, seconds), arrays [nsteps, len(systems)]."""
+    L = _lib.load()
+    n = len(systems)
+    hs = (C.c_void_p * n)(*[s.h for s in systems])
+    phs = (_lib.ExfPhys * n)(*[s.phys for s in systems])
+    ps = (_lib.ExfMgParams * n)(*params)
+    cyc = np.zeros((nsteps, n), dtype=np.int32)
+    sec = np.zeros((nsteps, n))
+    check(L.exf_timestep_loop(hs, n, phs, ps, nsteps, iptr(cyc), dptr(sec)))
+    return cyc, sec
+

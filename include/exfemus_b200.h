@@ -166,6 +166,15 @@ EXF_API int exf_set_matrix(exf_sys *s, int lev, const double *val);
 
 /* --- solve: MGSolve / MGStep (src/MGSolverBase.C:163-289) on device state ------------- */
 EXF_API int exf_mg_solve(exf_sys *s, const exf_mg_params *p, exf_solve_stats *st);
+/* the time / Picard loop of MGEquationsSystem::eqnmap_timestep_loop
+ * (src/MGEquationsSystem.C:422-432): nsteps times, for each of the nsys systems in order,
+ * its MGTimeStep (MGSolverNS.C:722-750, MGSolverT.C:530-561): assemble every level with
+ * phys[k], solve with params[k], x_old = x.  Coupled systems see each other's x_old as
+ * updated within the step.  Per (step, system) the cycles and device seconds of the solve
+ * go to cycles[step*nsys + k] and seconds[...] when those are not NULL.  Stops at the first
+ * failing solve and returns its status. */
+EXF_API int exf_timestep_loop(exf_sys *const *sys, int nsys, const exf_phys *phys, const exf_mg_params *params,
+                              int nsteps, int *cycles, double *seconds);
 /* unit-level operations on host buffers (NumericVectorM::resid / matrix_mult);
  * exf_resid with b == NULL returns r = A x */
 EXF_API int exf_resid(exf_sys *s, int lev, const double *x, const double *b, double *r);

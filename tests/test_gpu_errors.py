@@ -103,3 +103,22 @@ def test_timing_probes_and_refactorisation(heat):
     heat.set_x(np.zeros(heat.ntop_dof))
     heat.solve(p)
     assert np.array_equal(heat.x(), x0)
+
+
+def test_timestep_loop_matches_host_loop(gpu_lib):
+    """exf_timestep_loop (NS then T, every step) gives the bits of the same MGTimeStep
+    sequence driven from here, with the same cycle counts."""
+    from exfemus_b200 import workloads
+
+    def case():
+        return ex.make_case("bouss2d", nlev=3, n0=(4, 4))
+
+    a, b = case(), case()
+    rows = workloads.picard(a, 3)
+    cyc, sec = ex.timestep_loop([b["NS"], b["T"]], [b["mg_NS"], b["mg_T"]], 3)
+    assert [[r["NS"][0], r["T"][0]] for r in rows] == cyc.tolist()
+    assert np.all(sec > 0)
+    assert np.array_equal(a["NS"].x(), b["NS"].x()) and np.array_equal(a["T"].x(), b["T"].x())
+    with pytest.raises(_lib.ExfError) as e:
+        ex.timestep_loop([], [], 1)
+    assert e.value.code == _lib.EXF_ERR_ARG
