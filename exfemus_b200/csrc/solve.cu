@@ -1693,7 +1693,10 @@ int coarse_factor(exf_sys *s) {
   SysLevel &L = s->L[0];
   const int n = L.ndof;
   cudaStream_t st = s->stream;
-  constexpr int NT = 256;
+  #ifndef EXF_GJ_NT
+#define EXF_GJ_NT 512
+#endif
+  constexpr int NT = EXF_GJ_NT;
   if (n >= 0xFFFFF) {
     set_error("coarsest level of %d DOFs exceeds the direct solver's %d", n, 0xFFFFF - 1);
     return EXF_ERR_UNSUPPORTED;
