@@ -32,6 +32,7 @@ VANKA_AUTO = 0
 VANKA_TILE = 1
 VANKA_ROWS = 2
 VANKA_STREAM = 3
+VANKA_BULK = 4
 
 
 class ExfMeshDesc(C.Structure):

@@ -890,6 +890,7 @@ int exf_mg_solve(exf_sys *s, const exf_mg_params *p, exf_solve_stats *st) {
   float ms = 0.f;
   cudaEventElapsedTime(&ms, s->ev0, s->ev1);
   st->seconds = ms * 1e-3;
+  EXF_TRY(device_wait_status(s));
   st->converged = rc == EXF_OK && rel <= p->eps;
   if (rc == EXF_OK && !st->converged) {
     set_error("not converged: rel %.3e after %d cycles", rel, st->cycles);
@@ -945,6 +946,7 @@ int exf_smooth(exf_sys *s, int lev, const exf_mg_params *p, int nsweeps, double 
   EXF_TRY(h2d(s, dx.p, x, L.ndof));
   EXF_TRY(h2d(s, db.p, b, L.ndof));
   EXF_TRY(smooth<double>(s, lev, p, nsweeps, dx.p, db.p));
+  EXF_TRY(device_wait_status(s));
   return d2h(s, x, dx.p, L.ndof);
 }
 

@@ -208,6 +208,18 @@ struct SysLevel {
   DBuf<uint2> h16cx;
   DBuf<uint32_t> h16qc;
   DBuf<float> vsc;
+  // BULK smoother (3D FP32): the h16 / h16cx records of every star row copied row after
+  // row in sweep order, each row padded to an even count, so that the rows of a colour are
+  // one contiguous stream; allocated on the first BULK sweep, refreshed after assembly
+  DBuf<long long> soff;        // [nvrows + 2] first record of each star row (last repeated)
+  std::vector<long long> soff_h;
+  long long nstar = 0;         // soff[nvrows]
+  DBuf<longlong2> bsched;      // BULK stage schedule for a grid of bsched_G CTAs
+  DBuf<int> bsched_off;
+  std::vector<int> bsched_coff;
+  int bsched_G = 0;
+  DBuf<uint4> sv;
+  DBuf<uint2> scx;
   // transfers: Pq/Pl from level-1 to this level (fine rows), Rq/Rl from this level+1
   Transfer Pq, Pl, Rq, Rl;
   DBuf<double> rmask;    // [ndof] restriction row mask (bc0 % 2 of the top DOF)
@@ -282,6 +294,8 @@ template <class T>
 int prolong_add(exf_sys *s, int lev_f, const T *x_c, T *x_f, double damp);
 template <class T>
 int smooth(exf_sys *s, int lev, const exf_mg_params *p, int nsweeps, T *x, const T *b);
+// EXF_ERR_CUDA (and clears the flag) when a bounded in-kernel wait ran out since the last call
+int device_wait_status(exf_sys *s);
 template <class T>
 int coarse_apply(exf_sys *s, const T *b, T *x);
 int gauge_shift(exf_sys *s, double *x);

@@ -479,6 +479,17 @@ int build_colours(exf_sys *s) {
       L.tile_ok = kmax <= smax && rmax <= smax;
       EXF_TRY(L.vrinfo.alloc(vri.size()));
       EXF_CUDA(cudaMemcpy(L.vrinfo.p, vri.data(), vri.size() * sizeof(int4), cudaMemcpyHostToDevice));
+      if (dim == 3) {  // star-major record offsets of the BULK smoother
+        std::vector<long long> so(vri.size() + 1, 0);
+        for (size_t g = 0; g < vri.size(); g++)  // row scales, blocks, couplings; even count
+          so[g + 1] = so[g] + ((2 + (vri[g].w & 0xff) + ((vri[g].w >> 8) & 0xff)) & ~1);
+        L.nstar = so.back();
+        so.push_back(so.back());  // 16-byte copies of offset pairs may read one entry past the end
+        EXF_TRY(L.soff.alloc(so.size()));
+        EXF_CUDA(cudaMemcpy(L.soff.p, so.data(), so.size() * sizeof(long long), cudaMemcpyHostToDevice));
+        L.soff_h = std::move(so);
+        L.bsched_G = 0;
+      }
       EXF_TRY(L.pinfo.alloc(pin.size()));
       EXF_CUDA(cudaMemcpy(L.pinfo.p, pin.data(), pin.size() * sizeof(int4), cudaMemcpyHostToDevice));
       const size_t ne = rows.size() * (size_t)s->nv2;

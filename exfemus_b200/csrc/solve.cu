@@ -1265,6 +1265,246 @@ __global__ void k_vanka_apply(const int *__restrict__ vrows, int nr, long gbase,
   }
 }
 
+// BULK phase 1 for the 3D FP32 smoother.  Each star row is stored star-major (sv, scx:
+// row after row in sweep order) as one self-contained record run: a header {row scales,
+// node} / {nqq | nql << 8}, the FP16 blocks, and the pressure couplings {vp 0..2, column},
+// so a colour's rows are one contiguous stream.  Persistent CTAs own contiguous row
+// ranges, cut on the host into stages of whole rows (at most 32 rows and CAPB records:
+// the schedule, {first row, first record} per stage).  One producer warp fills stage
+// buffers with three bulk copies (values, columns, the rows' record offsets) completed
+// on the stage's "full" mbarrier, with no global load on its path; NWC consumer warps
+// take the stages' row pairs round-robin (16 lanes per row, every column gather of a
+// row issued at once, x gathers mostly L1 hits) and release a stage on its "empty"
+// mbarrier.  Each lane visits the blocks and couplings of its row in the same order as
+// the ROWS kernel, so both give the same sums.  Every wait is bounded: a wait that runs
+// out sets g_wait_timeout and the kernel leaves once its copies have landed.
+#ifndef EXF_WAIT_TRIES
+#define EXF_WAIT_TRIES (1 << 22)
+#endif
+__device__ int g_wait_timeout;
+
+__device__ __forceinline__ unsigned smem_addr(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(uint64_t *b, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(b)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_tx(uint64_t *b, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(b)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t *b) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(b)) : "memory");
+}
+// true once the phase of parity `par` has completed; false after EXF_WAIT_TRIES tries
+__device__ __forceinline__ bool mbar_wait(uint64_t *b, unsigned par) {
+  for (int t = 0; t < EXF_WAIT_TRIES; t++) {
+    unsigned ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_addr(b)), "r"(par)
+        : "memory");
+    if (ok) return true;
+  }
+  return false;
+}
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, unsigned bytes, uint64_t *bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_addr(dst)),
+               "l"(src), "r"(bytes), "r"(smem_addr(bar))
+               : "memory");
+}
+
+static int star_pack(exf_sys *s, int lev);
+
+template <int STG, int CAPB>
+struct BulkSmem {
+  uint4 val[STG][CAPB];   // row headers, FP16 values 0..7 of each block, couplings
+  uint2 cx[STG][CAPB];    // {nqq | nql << 8, 0}, {column, value 8}, {column, 0}
+  long long so[STG][34];  // record offsets of the stage's rows (from an even row index)
+  int nrow[STG];          // rows in the stage; 0 ends the stream
+  int gfirst[STG];        // colour row index of the stage's first row
+  uint64_t full[STG], empty[STG];
+};
+
+template <int NWC, int STG, int CAPB, int UNR, int LPR>
+__global__ void __launch_bounds__(32 * (NWC + 1), 1)
+    k_vanka_rows_bulk(const longlong2 *__restrict__ sched, const int *__restrict__ sched_off, int gbase,
+                      const int4 *__restrict__ pinfo, int npatch, int N, const long long *__restrict__ soff,
+                      const uint4 *__restrict__ sv, const uint2 *__restrict__ scx,
+                      const int *__restrict__ qq_col, const int *__restrict__ ql_col, long nqqL,
+                      const float *__restrict__ pv, const float *__restrict__ pp, const float *__restrict__ x,
+                      const float *__restrict__ b, float *__restrict__ res, long pres_off) {
+  constexpr int RPW = 32 / LPR;  // rows per warp pass
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  BulkSmem<STG, CAPB> &S = *reinterpret_cast<BulkSmem<STG, CAPB> *>(smem_raw);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < STG; s++) {
+      mbar_init(&S.full[s], 1);
+      mbar_init(&S.empty[s], NWC);
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  EXF_PDL_WAIT();
+  if (warp == NWC) {
+    // producer: stage `it` goes to slot it % STG once its previous use is released
+    const int e0 = sched_off[blockIdx.x], nst = sched_off[blockIdx.x + 1] - e0 - 1;
+    longlong2 win = make_longlong2(0, 0);  // schedule entries e0 + wb + lane
+    int wb = -64;
+    int it = 0;
+    bool ok = true;
+    for (;; it++) {
+      const int s = it % STG;
+      if (it >= STG && !mbar_wait(&S.empty[s], ((it / STG) - 1) & 1)) {
+        ok = false;
+        break;
+      }
+      if (it >= nst) {
+        if (lane == 0) {
+          S.nrow[s] = 0;
+          mbar_arrive(&S.full[s]);
+        }
+        it++;
+        break;
+      }
+      if (it + 1 >= wb + 32) {  // entries it and it + 1 in the window
+        wb = it;
+        if (wb + lane <= nst) win = sched[e0 + wb + lane];
+      }
+      const longlong2 st = make_longlong2(__shfl_sync(0xffffffffu, win.x, it - wb),
+                                          __shfl_sync(0xffffffffu, win.y, it - wb));
+      const longlong2 en = make_longlong2(__shfl_sync(0xffffffffu, win.x, it + 1 - wb),
+                                          __shfl_sync(0xffffffffu, win.y, it + 1 - wb));
+      if (lane == 0) {
+        const int r = (int)st.x, m = (int)(en.x - st.x);
+        const unsigned nb = (unsigned)(en.y - st.y);  // records (even)
+        const long long ga = ((long long)gbase + r) & ~1LL;
+        const unsigned ns = (unsigned)((((long long)gbase + r + m + 1 - ga) + 1) & ~1LL);  // offsets, even
+        S.nrow[s] = m;
+        S.gfirst[s] = r;
+        mbar_arrive_tx(&S.full[s], nb * 24u + ns * 8u);
+        if (nb > 0) {
+          bulk_g2s(&S.val[s][0], sv + st.y, nb * 16u, &S.full[s]);
+          bulk_g2s(&S.cx[s][0], scx + st.y, nb * 8u, &S.full[s]);
+        }
+        bulk_g2s(&S.so[s][0], soff + ga, ns * 8u, &S.full[s]);
+      }
+      __syncwarp();
+    }
+    if (!ok) {
+      if (lane == 0) atomicExch(&g_wait_timeout, 1);
+      // let the copies already issued land before the CTA leaves
+      for (int j = max(0, it - STG); j < it; j++) mbar_wait(&S.full[j % STG], (j / STG) & 1);
+    }
+    return;
+  }
+  // consumers: the row groups (RPW rows) of all stages dealt round-robin over the warps
+  const float4 *x4 = reinterpret_cast<const float4 *>(x);
+  const int half = lane / LPR, hl = lane % LPR;
+  int cum = 0;  // row groups of the earlier stages, modulo NWC
+  for (int it = 0;; it++) {
+    const int s = it % STG;
+    if (!mbar_wait(&S.full[s], (it / STG) & 1)) {
+      if (lane == 0) atomicExch(&g_wait_timeout, 1);
+      break;
+    }
+    const int m = S.nrow[s];
+    if (m == 0) break;
+    const int r = S.gfirst[s];
+    const int d = (int)(((long long)gbase + r) & 1LL);
+    const long long base = S.so[s][d];
+    const int np = (m + RPW - 1) / RPW;
+    for (int q = (warp - cum + NWC) % NWC; q < np; q += NWC) {
+      const int j = RPW * q + half;
+      const bool valid = j < m;
+      float acc[3] = {0.f, 0.f, 0.f};
+      const int of = valid ? (int)(S.so[s][d + j] - base) : 0;
+      const uint4 *vr = &S.val[s][of];  // [0]: header; [1, nk]: blocks; then couplings
+      const uint2 *cr = &S.cx[s][of];
+      const uint4 hs = vr[0];
+      const int rw = valid ? (int)cr[0].x : 0;
+      const int nk = rw & 0xff, nl = (rw >> 8) & 0xff;
+      float4 bv = make_float4(0.f, 0.f, 0.f, 0.f);
+      if (valid && hl == 0) bv = reinterpret_cast<const float4 *>(b)[hs.w];
+      for (int i0 = 0; i0 < nk; i0 += UNR * LPR) {
+        int c[UNR];
+        float4 xb[UNR];
+#pragma unroll
+        for (int u = 0; u < UNR; u++) {
+          const int i = i0 + u * LPR + hl;
+          c[u] = i < nk ? (int)cr[1 + i].x : -1;
+        }
+#pragma unroll
+        for (int u = 0; u < UNR; u++) xb[u] = c[u] >= 0 ? x4[c[u]] : make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+        for (int u = 0; u < UNR; u++) {
+          const int i = i0 + u * LPR + hl;
+          if (c[u] >= 0) {
+            const uint4 h = vr[1 + i];
+            float v[9];
+            float2 f;
+            f = h2f(h.x); v[0] = f.x; v[1] = f.y;
+            f = h2f(h.y); v[2] = f.x; v[3] = f.y;
+            f = h2f(h.z); v[4] = f.x; v[5] = f.y;
+            f = h2f(h.w); v[6] = f.x; v[7] = f.y;
+            v[8] = h2f(cr[1 + i].y).x;
+            const float xx[3] = {xb[u].x, xb[u].y, xb[u].z};
+#pragma unroll
+            for (int a = 0; a < 3; a++)
+#pragma unroll
+              for (int bb = 0; bb < 3; bb++) acc[a] += v[a * 3 + bb] * xx[bb];
+          }
+        }
+      }
+      if (valid) {
+        acc[0] *= __uint_as_float(hs.x);
+        acc[1] *= __uint_as_float(hs.y);
+        acc[2] *= __uint_as_float(hs.z);
+      }
+      for (int i = hl; i < nl; i += LPR) {  // pressure couplings {vp 0..2, column}
+        const uint4 q4 = vr[1 + nk + i];
+        const float pval = x4[(int)q4.w].w;
+        acc[0] += __uint_as_float(q4.x) * pval;
+        acc[1] += __uint_as_float(q4.y) * pval;
+        acc[2] += __uint_as_float(q4.z) * pval;
+      }
+#pragma unroll
+      for (int a = 0; a < 3; a++)
+#pragma unroll
+        for (int o = LPR / 2; o > 0; o >>= 1) acc[a] += __shfl_down_sync(0xffffffffu, acc[a], o, LPR);
+      if (valid && hl == 0) {
+        const long g = (long)gbase + r + j;
+        res[g * 3] = bv.x - acc[0];
+        res[g * 3 + 1] = bv.y - acc[1];
+        res[g * 3 + 2] = bv.z - acc[2];
+      }
+    }
+    cum = (cum + np) % NWC;
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&S.empty[s]);
+  }
+  // the pressure rows of this CTA's share of the patches, RPW per warp
+  const int p0 = (int)((long)blockIdx.x * npatch / gridDim.x);
+  const int p1 = (int)((long)(blockIdx.x + 1) * npatch / gridDim.x);
+  for (int q2 = p0 + RPW * warp; q2 < p1; q2 += RPW * NWC) {
+    const int q = q2 + half;
+    float acc[3] = {0.f, 0.f, 0.f};
+    int node = 0;
+    if (q < p1) {
+      const int4 pi = pinfo[2 * q];
+      const int4 pj = pinfo[2 * q + 1];
+      node = pi.x;
+      const float one[3] = {};
+      const PlanarBlocks<float, 3> pb{qq_col, pv, nqqL};
+      patch_row_dot<float, 3, LPR, 4, true, 1>(hl, N, pi.z, pj.x, pi.w, pj.y, pb, ql_col, 0, pp, x, acc, one);
+    }
+#pragma unroll
+    for (int o = LPR / 2; o > 0; o >>= 1) acc[0] += __shfl_down_sync(0xffffffffu, acc[0], o, LPR);
+    if (q < p1 && hl == 0) res[pres_off + node] = b[4L * node + 3] - acc[0];
+  }
+}
+
 // kernel tuning: levels with many waves of rows stream the matrix (occupancy first),
 // small levels are latency-bound (every block of a row in flight at once)
 #ifndef EXF_UNR_BIG32
@@ -1282,6 +1522,57 @@ __global__ void k_vanka_apply(const int *__restrict__ vrows, int nr, long gbase,
 #ifndef EXF_ST_SLOTS
 #define EXF_ST_SLOTS 2
 #endif
+#ifndef EXF_BK_NWC
+#define EXF_BK_NWC 23
+#endif
+#ifndef EXF_BK_STG
+#define EXF_BK_STG 4
+#endif
+#ifndef EXF_BK_CAPB
+#define EXF_BK_CAPB 2048
+#endif
+#ifndef EXF_BK_UNR
+#define EXF_BK_UNR 8
+#endif
+#ifndef EXF_BK_LPR
+#define EXF_BK_LPR 16
+#endif
+#ifndef EXF_AUTO_BULK
+#define EXF_AUTO_BULK 1
+#endif
+
+// stages of the BULK row kernel: per colour and CTA (grid CTAs, rows split evenly), the
+// rows cut greedily into stages of at most 32 rows and capb records, {first row, first
+// record} per stage and one closing entry per CTA
+static int bulk_schedule(SysLevel &L, int grid, int capb) {
+  const std::vector<long long> &so = L.soff_h;
+  std::vector<longlong2> e;
+  std::vector<int> off;
+  L.bsched_coff.assign(L.ncolour, 0);
+  for (int c = 0; c < L.ncolour; c++) {
+    const int gb = L.vrow_off[c], nr = L.vrow_off[c + 1] - gb;
+    L.bsched_coff[c] = (int)off.size();
+    for (int bk = 0; bk < grid; bk++) {
+      off.push_back((int)e.size());
+      const int r0 = (int)((long)bk * nr / grid), r1 = (int)((long)(bk + 1) * nr / grid);
+      int r = r0;
+      while (r < r1) {
+        e.push_back(make_longlong2(r, so[gb + r]));
+        int m = 1;
+        while (m < 32 && r + m < r1 && so[gb + r + m + 1] - so[gb + r] <= capb) m++;
+        r += m;
+      }
+      e.push_back(make_longlong2(r1, so[gb + r1]));
+    }
+    off.push_back((int)e.size());
+  }
+  EXF_TRY(L.bsched.alloc(e.size()));
+  EXF_TRY(L.bsched_off.alloc(off.size()));
+  EXF_CUDA(cudaMemcpy(L.bsched.p, e.data(), e.size() * sizeof(longlong2), cudaMemcpyHostToDevice));
+  EXF_CUDA(cudaMemcpy(L.bsched_off.p, off.data(), off.size() * sizeof(int), cudaMemcpyHostToDevice));
+  L.bsched_G = grid;
+  return EXF_OK;
+}
 
 template <class T, int D>
 static int vanka_sweep_rows(exf_sys *s, int lev, const exf_mg_params *p, T *x, const T *b) {
@@ -1320,6 +1611,49 @@ static int vanka_sweep_rows(exf_sys *s, int lev, const exf_mg_params *p, T *x, c
     // STREAM (selectable, 3D FP32): measured 1.86 ms per channel3d fine sweep against
     // 1.42 ms for the register-pipelined row kernel, so AUTO does not use it
     if constexpr (sizeof(T) == 4 && D == 3) {
+      // AUTO: the bulk kernel on the streaming levels (above four waves of rows)
+      if (p->vanka_kernel == EXF_VANKA_BULK || (p->vanka_kernel == EXF_VANKA_AUTO && EXF_AUTO_BULK && big)) {
+        constexpr int NWC = EXF_BK_NWC, STG = EXF_BK_STG, CAPB = EXF_BK_CAPB, UNR = EXF_BK_UNR,
+                      BLPR = EXF_BK_LPR;
+        static_assert(CAPB >= 512, "a stage holds the longest row (header, 255 blocks, 255 couplings, pad)");
+        using SM = BulkSmem<STG, CAPB>;
+        auto kern = k_vanka_rows_bulk<NWC, STG, CAPB, UNR, BLPR>;
+        static int per_sm[64] = {0};
+        const int dev = s->mesh->device;
+        if (dev < 0 || dev >= 64) {
+          set_error("device ordinal %d out of range", dev);
+          return EXF_ERR_ARG;
+        }
+        if (per_sm[dev] == 0) {
+          EXF_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(SM)));
+          EXF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[dev], kern, 32 * (NWC + 1), sizeof(SM)));
+          if (per_sm[dev] < 1) {
+            set_error("Vanka bulk row kernel does not fit on an SM");
+            return EXF_ERR_UNSUPPORTED;
+          }
+        }
+        const int grid = s->nsm * per_sm[dev];
+        if (!L.sv.p || L.bsched_G != grid) {  // first BULK sweep of this level (or a new grid)
+          cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+          EXF_CUDA(cudaStreamIsCapturing(s->stream, &cs));
+          if (cs != cudaStreamCaptureStatusNone) {
+            set_error("the first BULK sweep of level %d cannot run inside a graph capture", lev);
+            return EXF_ERR_STATE;
+          }
+          if (!L.sv.p) EXF_TRY(star_pack(s, lev));
+          EXF_TRY(bulk_schedule(L, grid, CAPB));
+        }
+        EXF_CUDA(launch_pdl(kern, dim3(grid), dim3(32 * (NWC + 1)), sizeof(SM), s->stream,
+                            (const longlong2 *)L.bsched.p, (const int *)(L.bsched_off.p + L.bsched_coff[c]),
+                            L.vrow_off[c], pin, n, L.N, (const long long *)L.soff.p, (const uint4 *)L.sv.p,
+                            (const uint2 *)L.scx.p, (const int *)L.qq_col.p, (const int *)L.ql_col.p, L.nqqL,
+                            (const float *)VT<T>::pv(L), (const float *)VT<T>::pp(L), (const float *)x,
+                            (const float *)b, (float *)res, pres_off));
+        EXF_CUDA(launch_pdl(k_vanka_solve<T, D, NTS, I4, SU>, dim3(n), dim3(NTS), 0, s->stream, pin, L.N, L.vrows.p,
+                            VK<T>::vk(L), VK<T>::pk(L), res, pres_off, x, (T)p->omega));
+        EXF_COUNT(2);
+        continue;
+      }
       if (p->vanka_kernel == EXF_VANKA_STREAM) {
         if (!L.tile_ok) {
           set_error("Vanka row streaming: a row of level %d exceeds 125 blocks", lev);
@@ -1498,6 +1832,60 @@ __global__ void k_pack16(int N, const int *__restrict__ qq_ptr, const int *__res
   }
 }
 
+// star-major copy of each 3D star row (one warp per row): record 0 is the header
+// {vsc 0..2, node} / {nqq | nql << 8}, records 1..nqq the FP16 blocks, then one record per
+// pressure coupling {vp 0..2 (FP32), column}; the pad record is zero
+__global__ void k_pack_star(int nrows, const int4 *__restrict__ rinfo, const long long *__restrict__ soff, int N,
+                            const uint4 *__restrict__ h16, const uint2 *__restrict__ cx,
+                            const float *__restrict__ vsc, const int *__restrict__ ql_col,
+                            const float *__restrict__ vp, long nql, uint4 *__restrict__ sv,
+                            uint2 *__restrict__ scx) {
+  const long g = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (g >= nrows) return;
+  const int4 ri = rinfo[g];
+  const int node = ri.x, k0 = ri.y, l0 = ri.z, nk = ri.w & 0xff, nl = (ri.w >> 8) & 0xff;
+  const long long o = soff[g];
+  const int w = (int)(soff[g + 1] - o);
+  for (int i = lane; i < w; i += 32) {
+    uint4 v = make_uint4(0u, 0u, 0u, 0u);
+    uint2 c = make_uint2(0u, 0u);
+    if (i == 0) {
+      v = make_uint4(__float_as_uint(vsc[node]), __float_as_uint(vsc[(long)N + node]),
+                     __float_as_uint(vsc[2L * N + node]), (unsigned)node);
+      c = make_uint2((unsigned)(nk | (nl << 8)), 0u);
+    } else if (i <= nk) {
+      v = h16[k0 + i - 1];
+      c = cx[k0 + i - 1];
+    } else if (i <= nk + nl) {
+      const long q = l0 + i - 1 - nk;
+      const int col = ql_col[q];
+      v = make_uint4(__float_as_uint(vp[q]), __float_as_uint(vp[nql + q]), __float_as_uint(vp[2 * nql + q]),
+                     (unsigned)col);
+      c = make_uint2((unsigned)col, 0u);
+    }
+    sv[o + i] = v;
+    scx[o + i] = c;
+  }
+}
+
+static int star_pack(exf_sys *s, int lev) {
+  SysLevel &L = s->L[lev];
+  if (!L.soff.p || !L.h16.p || !L.A32.vp.p) {
+    set_error("star-major records need the 3D FP16 blocks of level %d", lev);
+    return EXF_ERR_STATE;
+  }
+  EXF_TRY(L.sv.ensure((size_t)L.nstar));
+  EXF_TRY(L.scx.ensure((size_t)L.nstar));
+  const int nrows = L.vrow_off[L.ncolour];
+  if (nrows > 0)
+    k_pack_star<<<nblk((long)nrows * 32, 256), 256, 0, s->stream>>>(
+        nrows, L.vrinfo.p, L.soff.p, L.N, L.h16.p, L.h16cx.p, L.vsc.p, L.ql_col.p, L.A32.vp.p, L.nql, L.sv.p,
+        L.scx.p);
+  EXF_CUDA(cudaGetLastError());
+  return EXF_OK;
+}
+
 int vanka_prep(exf_sys *s, int lev) {
   if (s->kind != EXF_KIND_NS) return EXF_OK;
   SysLevel &L = s->L[lev];
@@ -1509,6 +1897,7 @@ int vanka_prep(exf_sys *s, int lev) {
                                                       L.h16.p, L.h16cx.p, L.h16qc.p, L.vsc.p);
   EXF_LAUNCH_CHECK();
   EXF_COUNT(1);
+  if (L.sv.p) EXF_TRY(star_pack(s, lev));  // the BULK smoother's copy is in use: refresh it
   const unsigned grid = nblk(L.NL, 4);
   if (s->dim == 2)
     k_vanka_prep<2><<<grid, 128, 0, s->stream>>>(L.NL, L.pstart.p, L.qq_ptr.p, L.qq_col.p, L.ql_ptr.p,
@@ -1536,6 +1925,20 @@ static int gs_sweep(exf_sys *s, int lev, const exf_mg_params *p, T *x, const T *
     EXF_CUDA(launch_pdl(k_gs_colour<T, LPR>, dim3(nblk((long)n * LPR, 256)), dim3(256), 0, s->stream,
                         L.col_items.p + L.col_off[c], n, L.qq_ptr.p, L.qq_col.p, L.diag_pos.p, VT<T>::vv(L), b, x));
     EXF_COUNT(1);
+  }
+  return EXF_OK;
+}
+
+int device_wait_status(exf_sys *s) {
+  int flag = 0;
+  EXF_CUDA(cudaMemcpyFromSymbolAsync(&flag, g_wait_timeout, sizeof(int), 0, cudaMemcpyDeviceToHost, s->stream));
+  EXF_CUDA(cudaStreamSynchronize(s->stream));
+  if (flag) {
+    const int zero = 0;
+    EXF_CUDA(cudaMemcpyToSymbolAsync(g_wait_timeout, &zero, sizeof(int), 0, cudaMemcpyHostToDevice, s->stream));
+    EXF_CUDA(cudaStreamSynchronize(s->stream));
+    set_error("a bounded wait of the Vanka bulk row kernel ran out");
+    return EXF_ERR_CUDA;
   }
   return EXF_OK;
 }

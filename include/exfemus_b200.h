@@ -68,6 +68,8 @@ extern "C" {
 #define EXF_VANKA_ROWS 2         /* star-row residual kernel + patch-solve kernel      */
 #define EXF_VANKA_STREAM 3       /* ROWS with the 3D FP32 star rows copied to shared    */
                                  /* memory by cp.async (persistent warps)               */
+#define EXF_VANKA_BULK 4         /* ROWS with the 3D FP32 star rows of each persistent  */
+                                 /* CTA streamed by bulk copies through mbarrier stages */
 
 typedef struct {
   int dim;          /* 2 (quad9/quad4) or 3 (hex27/hex8)                          */

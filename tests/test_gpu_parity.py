@@ -107,7 +107,7 @@ def test_solver_operations_match_oracle(case):
 # Vanka kernels: TILE (one CTA per patch, iterate staged in shared memory), ROWS (row
 # kernel + patch-solve kernel) and STREAM (ROWS with the 3D FP32 rows streamed through
 # shared memory); the library picks per level, the tests force each
-VK = [_lib.VANKA_TILE, _lib.VANKA_ROWS, _lib.VANKA_STREAM]
+VK = [_lib.VANKA_TILE, _lib.VANKA_ROWS, _lib.VANKA_STREAM, _lib.VANKA_BULK]
 
 
 @pytest.mark.parametrize("vk", VK)
