@@ -1027,6 +1027,10 @@ int exf_time_op(exf_sys *s, int what, int lev, const exf_mg_params *p, const exf
         return EXF_ERR_ARG;
     }
   };
+  if (what == 6) {
+    *avg_ms = 0.;
+    return wait_probe(s);
+  }
   EXF_TRY(once());
   EXF_CUDA(cudaEventRecord(s->ev0, s->stream));
   for (int i = 0; i < reps; i++) EXF_TRY(once());

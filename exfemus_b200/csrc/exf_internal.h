@@ -296,6 +296,8 @@ template <class T>
 int smooth(exf_sys *s, int lev, const exf_mg_params *p, int nsweeps, T *x, const T *b);
 // EXF_ERR_CUDA (and clears the flag) when a bounded in-kernel wait ran out since the last call
 int device_wait_status(exf_sys *s);
+// runs a bounded wait that nothing completes; returns the resulting device_wait_status
+int wait_probe(exf_sys *s);
 template <class T>
 int coarse_apply(exf_sys *s, const T *b, T *x);
 int gauge_shift(exf_sys *s, double *x);

@@ -506,17 +506,30 @@ __global__ void __launch_bounds__(NT, MINB)
                  const int *__restrict__ ql_col, long nql, long nqqL, const T *__restrict__ vp,
                  const T *__restrict__ pv, const T *__restrict__ pp, const T *__restrict__ x,
                  const T *__restrict__ b, T *__restrict__ res, long pres_off) {
-  EXF_PDL_WAIT();
   const int lane = threadIdx.x % LPR;
   const long g = ((long)blockIdx.x * NT + threadIdx.x) / LPR;
   const bool vel = g < nrows;
   const bool prs = !vel && g < (long)nrows + npatch;
+  // the row descriptors do not change during a sweep: on the latency-bound levels
+  // (MINB 1) load them before the wait
+  int4 q0 = make_int4(0, 0, 0, 0), q1 = q0;
+  auto desc = [&]() {
+    if (vel) {
+      q0 = rinfo[g];
+    } else if (prs) {
+      q0 = pinfo[2 * (g - nrows)];
+      q1 = pinfo[2 * (g - nrows) + 1];
+    }
+  };
+  if constexpr (MINB == 1) desc();
+  EXF_PDL_WAIT();
+  if constexpr (MINB != 1) desc();
   T acc[D], bv[D];
 #pragma unroll
   for (int a = 0; a < D; a++) acc[a] = bv[a] = T(0);
   int node = 0;
   if (vel) {
-    const int4 ri = rinfo[g];
+    const int4 ri = q0;
     node = ri.x;
     if (lane == 0) {
 #pragma unroll
@@ -528,8 +541,7 @@ __global__ void __launch_bounds__(NT, MINB)
     patch_row_dot<T, D, LPR, UNR, I4, D>(lane, N, ri.y, ri.w & 0xff, ri.z, (ri.w >> 8) & 0xff, vb, ql_col, nql, vp,
                                          x, acc, sc);
   } else if (prs) {
-    const int4 pi = pinfo[2 * (g - nrows)];
-    const int4 pj = pinfo[2 * (g - nrows) + 1];
+    const int4 pi = q0, pj = q1;
     node = pi.x;
     if (lane == 0) bv[0] = b[Lay<I4>::p(node, N, D)];
     const T one[D] = {};
@@ -601,8 +613,9 @@ template <class T, int D, int NT, bool I4, int SU>
 __global__ void __launch_bounds__(NT)
     k_vanka_solve(const int4 *__restrict__ pinfo, int N, const int *__restrict__ vrows, const T *__restrict__ vk,
                   const T *__restrict__ pk, const T *__restrict__ res, long pres_off, T *__restrict__ x, T omega) {
-  EXF_PDL_WAIT();
   __shared__ double s_red[NT / 32], s_bc[2];
+  // the patch's coefficients and star rows do not change during a sweep: load them
+  // before waiting for the row kernel
   const int4 pi = pinfo[2 * blockIdx.x];
   const int m = pi.x, KD = pinfo[2 * blockIdx.x + 1].x * D;
   const long g0 = pi.y;
@@ -616,21 +629,24 @@ __global__ void __launch_bounds__(NT)
     ix[u] = -1;
     r_[u] = w0[u] = w1[u] = w2[u] = xv[u] = T(0);
     if (t < KD) {
-      r_[u] = rr[t];
       w0[u] = w[3 * t];
       w1[u] = w[3 * t + 1];
       w2[u] = w[3 * t + 2];
       ix[u] = Lay<I4>::v(t % D, vrows[g0 + t / D], N);
     }
   }
+  double Sd = 0.;
+  if (threadIdx.x == 0) Sd = (double)pk[2 * m];
+  EXF_PDL_WAIT();  // residuals and iterate come from the previous kernels
 #pragma unroll
   for (int u = 0; u < SU; u++)
-    if (ix[u] >= 0) xv[u] = x[ix[u]];
+    if (ix[u] >= 0) {
+      r_[u] = rr[threadIdx.x + u * NT];
+      xv[u] = x[ix[u]];
+    }
   T rp = T(0), xp = T(0);
-  double Sd = 0.;
   if (threadIdx.x == 0) {
     rp = res[pres_off + m];
-    Sd = (double)pk[2 * m];
     xp = x[Lay<I4>::p(m, N, D)];
   }
   double tsum = 0.;
@@ -1294,9 +1310,9 @@ __device__ __forceinline__ void mbar_arrive_tx(uint64_t *b, unsigned bytes) {
 __device__ __forceinline__ void mbar_arrive(uint64_t *b) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(b)) : "memory");
 }
-// true once the phase of parity `par` has completed; false after EXF_WAIT_TRIES tries
-__device__ __forceinline__ bool mbar_wait(uint64_t *b, unsigned par) {
-  for (int t = 0; t < EXF_WAIT_TRIES; t++) {
+// true once the phase of parity `par` has completed; false after `tries` tries
+__device__ __forceinline__ bool mbar_wait(uint64_t *b, unsigned par, int tries = EXF_WAIT_TRIES) {
+  for (int t = 0; t < tries; t++) {
     unsigned ok;
     asm volatile(
         "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
@@ -1346,9 +1362,11 @@ __global__ void __launch_bounds__(32 * (NWC + 1), 1)
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncthreads();
-  EXF_PDL_WAIT();
   if (warp == NWC) {
-    // producer: stage `it` goes to slot it % STG once its previous use is released
+    // producer: stage `it` goes to slot it % STG once its previous use is released.  It
+    // reads only the star-major records, offsets and schedule, which no kernel of the
+    // sweep writes, so it starts streaming without waiting for the previous kernel
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
     const int e0 = sched_off[blockIdx.x], nst = sched_off[blockIdx.x + 1] - e0 - 1;
     longlong2 win = make_longlong2(0, 0);  // schedule entries e0 + wb + lane
     int wb = -64;
@@ -1399,9 +1417,30 @@ __global__ void __launch_bounds__(32 * (NWC + 1), 1)
     }
     return;
   }
-  // consumers: the row groups (RPW rows) of all stages dealt round-robin over the warps
+  EXF_PDL_WAIT();  // x and b come from the previous kernels
   const float4 *x4 = reinterpret_cast<const float4 *>(x);
   const int half = lane / LPR, hl = lane % LPR;
+  // the pressure rows of this CTA's share of the patches, RPW per warp, while the first
+  // stages stream in
+  const int p0 = (int)((long)blockIdx.x * npatch / gridDim.x);
+  const int p1 = (int)((long)(blockIdx.x + 1) * npatch / gridDim.x);
+  for (int q2 = p0 + RPW * warp; q2 < p1; q2 += RPW * NWC) {
+    const int q = q2 + half;
+    float acc[3] = {0.f, 0.f, 0.f};
+    int node = 0;
+    if (q < p1) {
+      const int4 pi = pinfo[2 * q];
+      const int4 pj = pinfo[2 * q + 1];
+      node = pi.x;
+      const float one[3] = {};
+      const PlanarBlocks<float, 3> pb{qq_col, pv, nqqL};
+      patch_row_dot<float, 3, LPR, 4, true, 1>(hl, N, pi.z, pj.x, pi.w, pj.y, pb, ql_col, 0, pp, x, acc, one);
+    }
+#pragma unroll
+    for (int o = LPR / 2; o > 0; o >>= 1) acc[0] += __shfl_down_sync(0xffffffffu, acc[0], o, LPR);
+    if (q < p1 && hl == 0) res[pres_off + node] = b[4L * node + 3] - acc[0];
+  }
+  // consumers: the row groups (RPW rows) of all stages dealt round-robin over the warps
   int cum = 0;  // row groups of the earlier stages, modulo NWC
   for (int it = 0;; it++) {
     const int s = it % STG;
@@ -1484,25 +1523,7 @@ __global__ void __launch_bounds__(32 * (NWC + 1), 1)
     __syncwarp();
     if (lane == 0) mbar_arrive(&S.empty[s]);
   }
-  // the pressure rows of this CTA's share of the patches, RPW per warp
-  const int p0 = (int)((long)blockIdx.x * npatch / gridDim.x);
-  const int p1 = (int)((long)(blockIdx.x + 1) * npatch / gridDim.x);
-  for (int q2 = p0 + RPW * warp; q2 < p1; q2 += RPW * NWC) {
-    const int q = q2 + half;
-    float acc[3] = {0.f, 0.f, 0.f};
-    int node = 0;
-    if (q < p1) {
-      const int4 pi = pinfo[2 * q];
-      const int4 pj = pinfo[2 * q + 1];
-      node = pi.x;
-      const float one[3] = {};
-      const PlanarBlocks<float, 3> pb{qq_col, pv, nqqL};
-      patch_row_dot<float, 3, LPR, 4, true, 1>(hl, N, pi.z, pj.x, pi.w, pj.y, pb, ql_col, 0, pp, x, acc, one);
-    }
-#pragma unroll
-    for (int o = LPR / 2; o > 0; o >>= 1) acc[0] += __shfl_down_sync(0xffffffffu, acc[0], o, LPR);
-    if (q < p1 && hl == 0) res[pres_off + node] = b[4L * node + 3] - acc[0];
-  }
+
 }
 
 // kernel tuning: levels with many waves of rows stream the matrix (occupancy first),
@@ -1927,6 +1948,26 @@ static int gs_sweep(exf_sys *s, int lev, const exf_mg_params *p, T *x, const T *
     EXF_COUNT(1);
   }
   return EXF_OK;
+}
+
+// one CTA waits, bounded, on an mbarrier phase that nothing completes: the wait runs out,
+// sets g_wait_timeout and the kernel returns (exercises the status path of every bounded
+// wait without a fault)
+__global__ void k_wait_probe(int tries) {
+  __shared__ uint64_t bar;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  if (threadIdx.x == 0 && !mbar_wait(&bar, 0u, tries)) atomicExch(&g_wait_timeout, 1);
+}
+
+int wait_probe(exf_sys *s) {
+  k_wait_probe<<<1, 32, 0, s->stream>>>(1 << 14);
+  EXF_LAUNCH_CHECK();
+  EXF_COUNT(1);
+  return device_wait_status(s);
 }
 
 int device_wait_status(exf_sys *s) {

@@ -203,6 +203,10 @@ EXF_API int exf_adjoint_backward(exf_sys *s, const exf_phys *ph, const exf_mg_pa
  * 4 = factorisation of the coarsest level (as each solve after an assembly pays it),
  * 5 = FP64 FMA throughput probe: 4 CTAs of 256 threads per SM, each thread running
  *     EXF_FMA_CHAINS independent chains of EXF_FMA_ITERS fma (2 flops each);
+ * 6 = bounded-wait probe: one kernel waits, with a short limit, on a barrier phase that
+ *     nothing completes; returns EXF_ERR_CUDA with the run-out message, the status every
+ *     bounded in-kernel wait (the BULK smoother's stage barriers) reports, and leaves the
+ *     context usable;
  * avg_ms = average duration per launch group over reps, precision per exf_mg_params */
 EXF_API int exf_time_op(exf_sys *s, int what, int lev, const exf_mg_params *p, const exf_phys *ph, int reps,
                 double *avg_ms);

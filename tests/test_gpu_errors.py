@@ -105,6 +105,25 @@ def test_timing_probes_and_refactorisation(heat):
     assert np.array_equal(heat.x(), x0)
 
 
+def test_bounded_wait_reports_run_out(heat):
+    """exf_time_op 6 runs a bounded in-kernel wait on a barrier phase that nothing
+    completes: the call returns EXF_ERR_CUDA with the run-out message, the flag is cleared,
+    and the context stays usable (a solve afterwards gives the bits of one before)."""
+    L = _lib.load()
+    heat.assemble_all()
+    p = ex.mg_params(precision=_lib.PREC_MIXED)
+    heat.set_x(np.zeros(heat.ntop_dof))
+    heat.solve(p)
+    x0 = heat.x()
+    tv = C.c_double()
+    rc = L.exf_time_op(heat.h, 6, 0, C.byref(p), C.byref(heat.phys), 1, C.byref(tv))
+    assert rc == _lib.EXF_ERR_CUDA
+    assert b"ran out" in L.exf_last_error()
+    heat.set_x(np.zeros(heat.ntop_dof))
+    heat.solve(p)
+    assert np.array_equal(heat.x(), x0)
+
+
 def test_timestep_loop_matches_host_loop(gpu_lib):
     """exf_timestep_loop (NS then T, every step) gives the bits of the same MGTimeStep
     sequence driven from here, with the same cycle counts."""
