@@ -518,7 +518,7 @@ def run_ours(args, ws, rank, local):
             "assembly_frac_of_fp64_peak": ASM_FLOPS_HEX27_NS * nel / (asm_ms * 1e-3) / 1e12 / fma_tflops,
             "spmv_fp32_gbs": b_spmv32.value / (spmv32_ms * 1e-3) / 1e9,
             "spmv_fp64_gbs": b_spmv64.value / (spmv64_ms * 1e-3) / 1e9,
-            "roofline": {"kernel": "k_vanka_rows + k_vanka_solve, one FP32 Vanka sweep of the fine level "
+            "roofline": {"kernel": "k_vanka_rows_bulk + k_vanka_solve, one FP32 Vanka sweep of the fine level "
                                    "(27 colours x 2 launches)", "bound": "hbm",
                          "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "peak_kind": peak_kind, "algorithmic_bytes": b_sweep32.value, "sweep_ms": sweep_ms,

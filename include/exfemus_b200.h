@@ -62,7 +62,9 @@ extern "C" {
 #define EXF_PREC_MIXED 1         /* FP32 V-cycle inside FP64 defect correction      */
 
 /* Vanka kernel selection (exf_mg_params.vanka_kernel): all compute the same update and
- * differ only in the order of floating-point sums.  AUTO uses ROWS (measured fastest). */
+ * differ only in the order of floating-point sums.  AUTO uses BULK on 3D FP32 levels
+ * with more than four waves of rows and ROWS elsewhere (each measured fastest there); BULK
+ * and ROWS give the same bits. */
 #define EXF_VANKA_AUTO 0
 #define EXF_VANKA_TILE 1         /* one CTA per patch, iterate staged in shared memory */
 #define EXF_VANKA_ROWS 2         /* star-row residual kernel + patch-solve kernel      */
