@@ -188,3 +188,28 @@ def test_solve_is_deterministic(case):
                               precision=_lib.PREC_MIXED))
         outs.append(gs.x())
     assert np.array_equal(outs[0], outs[1])
+
+
+def test_bulk_streaming_level_matches_row_kernel_bits():
+    """On a level large enough for AUTO to stream it with the bulk row kernel (the channel3d
+    fine level, 140,481 velocity nodes), the mixed-precision cycles give the same bits as
+    the row kernel everywhere: both kernels sum each star row in the same order."""
+    from exfemus_b200 import workloads
+
+    outs = []
+    for vk in (_lib.VANKA_AUTO, _lib.VANKA_ROWS):
+        case = workloads.make_case("channel3d")
+        ns = case["NS"]
+        ns.assemble_all()
+        p = case["mg_NS"]
+        p.precision = _lib.PREC_MIXED
+        p.vanka_kernel = vk
+        p.max_cycles = 3
+        p.eps = 1e-14
+        ns.set_x(np.zeros(ns.ntop_dof))
+        st = ns.solve(p)
+        outs.append((ns.x(), list(st.hist[: st.cycles])))
+        ns.close()
+        case["mesh"].close()
+    assert np.array_equal(outs[0][0], outs[1][0])
+    assert outs[0][1] == outs[1][1]
