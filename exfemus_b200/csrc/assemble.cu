@@ -206,6 +206,8 @@ __global__ void __launch_bounds__(NT, DIM == 3 ? 3 : 1) k_assemble(AsmArgs<DIM> 
   __shared__ double s_cT[NQ][DIM * DIM];  // JxW*rho*(nu + f_a v_a v_b)
   __shared__ double s_cR[NQ][DIM];     // rhs coefficient per component
   __shared__ double s_h[DIM];
+  __shared__ double s_J[NQ][DIM * DIM];  // Jacobian entries per Gauss point
+  __shared__ double s_vg[NQ][DIM + 1];   // velocity (and temperature) at each Gauss point
 
   const FETab<DIM> *t = A.tab;
   // ---- element data (get_el_dof_bc, get_el_sol)
@@ -246,15 +248,36 @@ __global__ void __launch_bounds__(NT, DIM == 3 ? 3 : 1) k_assemble(AsmArgs<DIM> 
   const exf_phys &ph = A.ph;
   const double diff_t = ph.inv_prdl * ph.inv_re;
   const double q_e = (!ns && A.qe) ? A.qe[e] : 0.;
-  for (int q = tid; q < NQ; q += NT) {
+  // the 27-term sums of every Gauss point first, one per thread (Jacobian entries, then
+  // the interpolated velocity and temperature), each in node order
+  constexpr int NSUM = DIM * DIM + DIM + 1;
+  for (int p = tid; p < NQ * NSUM; p += NT) {
+    const int q = p / NSUM, c = p % NSUM;
+    double sum = 0.;
+    if (c < DIM * DIM) {
+      const int a = c / DIM, b = c % DIM;
+#pragma unroll 1
+      for (int s = 0; s < NEN; s++) sum += s_xx[a][s] * t->dphi[q][s][b];
+      s_J[q][c] = sum;
+    } else if (c < DIM * DIM + DIM) {
+      const int d = c - DIM * DIM;
+#pragma unroll 1
+      for (int k = 0; k < NEN; k++) sum += s_phi[q][k] * s_vold[d][k];
+      s_vg[q][d] = sum;
+    } else {
+#pragma unroll 1
+      for (int k = 0; k < NEN; k++) sum += s_phi[q][k] * s_told[k];
+      s_vg[q][DIM] = sum;
+    }
+  }
+  __syncthreads();
+  // then per (Gauss point, component d): the inverse Jacobian (each of the DIM threads of a
+  // point computes it, the d = 0 one stores it) and row d of the coefficients
+  for (int pq = tid; pq < NQ * DIM; pq += NT) {
+    const int q = pq / DIM, dd = pq % DIM;
     double J[DIM][DIM];
     for (int a = 0; a < DIM; a++)
-      for (int b = 0; b < DIM; b++) {
-        double sum = 0.;
-#pragma unroll 1
-        for (int s = 0; s < NEN; s++) sum += s_xx[a][s] * t->dphi[q][s][b];
-        J[a][b] = sum;
-      }
+      for (int b = 0; b < DIM; b++) J[a][b] = s_J[q][a * DIM + b];
     double det, inv[DIM][DIM];  // inv[b][a] = dxi_b/dx_a
     if (DIM == 2) {
       det = J[0][0] * J[1][1] - J[1][0] * J[0][1];
@@ -278,49 +301,37 @@ __global__ void __launch_bounds__(NT, DIM == 3 ? 3 : 1) k_assemble(AsmArgs<DIM> 
       inv[o][1] = (J[0][1] * J[o][0] - J[0][0] * J[o][1]) * id;
       inv[o][o] = (J[0][0] * J[1][1] - J[0][1] * J[1][0]) * id;
     }
-    for (int i = 0; i < DIM; i++)
-      for (int j = 0; j < DIM; j++) s_ij[q][j + i * DIM] = inv[j][i];
-    double JxW = det * t->w[q];
-    s_JxW[q] = JxW;
-    double vg[DIM], mod = 1e-20, tg = 0.;
+    const double JxW = det * t->w[q];
+    double vg[DIM], mod = 1e-20;
     for (int d = 0; d < DIM; d++) {
-      double sum = 0.;
-#pragma unroll 1
-      for (int k = 0; k < NEN; k++) sum += s_phi[q][k] * s_vold[d][k];
-      vg[d] = sum;
-      mod += sum * sum;
+      vg[d] = s_vg[q][d];
+      mod += vg[d] * vg[d];
     }
-#pragma unroll 1
-    for (int k = 0; k < NEN; k++) tg += s_phi[q][k] * s_told[k];
+    const double tg = s_vg[q][DIM];
     mod = sqrt(mod);
-    double f[DIM];
+    if (dd == 0) {
+      for (int i = 0; i < DIM; i++)
+        for (int j = 0; j < DIM; j++) s_ij[q][j + i * DIM] = inv[j][i];
+      s_JxW[q] = JxW;
+      s_cM[q] = JxW * (ns ? ph.rho : ph.rhocp) * ph.inv_dt;
+    }
+    const int a = dd;
     if (ns) {
-      for (int d = 0; d < DIM; d++) {
-        double pe = 0.5 * mod * s_h[d] / ph.inv_re;
-        f[d] = ph.upwind_ns * ph.rho * 0.5 * (1. / tanh(pe) - 1. / pe) * s_h[d] / mod;
-      }
-      s_cM[q] = JxW * ph.rho * ph.inv_dt;
-      for (int a = 0; a < DIM; a++) {
-        s_cA[q][a] = JxW * ph.rho * vg[a];
-        s_cL[q][a] = JxW * ph.rho * (ph.inv_re + f[a] * vg[a] * vg[a]);
-        for (int b = 0; b < DIM; b++) s_cT[q][a * DIM + b] = JxW * ph.rho * (ph.inv_re + f[a] * vg[a] * vg[b]);
-        s_cR[q][a] = JxW * (ph.rho * vg[a] * ph.inv_dt + ph.rho * ph.ifr * ph.dirg[a] + ph.buoy * tg * ph.dirg[a]);
-      }
+      const double pe = 0.5 * mod * s_h[a] / ph.inv_re;
+      const double fa = ph.upwind_ns * ph.rho * 0.5 * (1. / tanh(pe) - 1. / pe) * s_h[a] / mod;
+      s_cA[q][a] = JxW * ph.rho * vg[a];
+      s_cL[q][a] = JxW * ph.rho * (ph.inv_re + fa * vg[a] * vg[a]);
+      for (int b = 0; b < DIM; b++) s_cT[q][a * DIM + b] = JxW * ph.rho * (ph.inv_re + fa * vg[a] * vg[b]);
+      s_cR[q][a] = JxW * (ph.rho * vg[a] * ph.inv_dt + ph.rho * ph.ifr * ph.dirg[a] + ph.buoy * tg * ph.dirg[a]);
     } else {
-      for (int d = 0; d < DIM; d++) {
-        if (A.vel) {
-          double pe = 0.5 * mod * s_h[d] / diff_t;
-          f[d] = ph.upwind_t * ph.rhocp * 0.5 * (1. / tanh(pe) - 1. / pe) * s_h[d] / mod;
-        } else {
-          f[d] = 0.;
-        }
+      double fa = 0.;
+      if (A.vel) {
+        const double pe = 0.5 * mod * s_h[a] / diff_t;
+        fa = ph.upwind_t * ph.rhocp * 0.5 * (1. / tanh(pe) - 1. / pe) * s_h[a] / mod;
       }
-      s_cM[q] = JxW * ph.rhocp * ph.inv_dt;
-      for (int a = 0; a < DIM; a++) {
-        s_cA[q][a] = JxW * ph.rhocp * vg[a];
-        s_cL[q][a] = JxW * (diff_t + f[a] * vg[a] * vg[a]);
-      }
-      s_cR[q][0] = JxW * (ph.rhocp * tg * ph.inv_dt + q_e);
+      s_cA[q][a] = JxW * ph.rhocp * vg[a];
+      s_cL[q][a] = JxW * (diff_t + fa * vg[a] * vg[a]);
+      if (a == 0) s_cR[q][0] = JxW * (ph.rhocp * tg * ph.inv_dt + q_e);
     }
   }
   __syncthreads();
