@@ -178,9 +178,15 @@ __device__ double jac_sur(const FETab<DIM> *t, int q, const double (*xx)[FE<DIM>
   }
 }
 
-// 3D: register cap for 3 CTAs per SM (79 registers, no spills; measured fastest)
+// 3D: register cap for 4 CTAs per SM (64 registers, no spills; measured fastest)
+#ifndef EXF_ASM_MINB3
+#define EXF_ASM_MINB3 4
+#endif
+#ifndef EXF_ASM_MINB2
+#define EXF_ASM_MINB2 1
+#endif
 template <int DIM, int NT>
-__global__ void __launch_bounds__(NT, DIM == 3 ? 3 : 1) k_assemble(AsmArgs<DIM> A, int mode) {
+__global__ void __launch_bounds__(NT, DIM == 3 ? EXF_ASM_MINB3 : EXF_ASM_MINB2) k_assemble(AsmArgs<DIM> A, int mode) {
   using F = FE<DIM>;
   constexpr int NEN = F::NEN, NVX = F::NVX, NQ = F::NQ;
   const int tid = threadIdx.x;

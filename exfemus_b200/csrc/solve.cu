@@ -1600,7 +1600,7 @@ static int vanka_sweep_rows(exf_sys *s, int lev, const exf_mg_params *p, T *x, c
   SysLevel &L = s->L[lev];
   constexpr bool I4 = sizeof(T) == 4;
 #ifndef EXF_NTS3
-#define EXF_NTS3 256
+#define EXF_NTS3 128
 #endif
   constexpr int NTS = D == 3 ? EXF_NTS3 : 64;
   constexpr int SU = D == 3 ? (375 + NTS - 1) / NTS : 1;  // 3D stars: 125 nodes x 3; 2D: 25 x 2 <= 64
