@@ -1466,6 +1466,18 @@ __global__ void __launch_bounds__(32 * (NWC + 1), 1)
       const int nk = rw & 0xff, nl = (rw >> 8) & 0xff;
       float4 bv = make_float4(0.f, 0.f, 0.f, 0.f);
       if (valid && hl == 0) bv = reinterpret_cast<const float4 *>(b)[hs.w];
+      // the first two pressure couplings of the lane, gathered before the blocks (added
+      // after them, in the same order)
+      uint4 cq0 = make_uint4(0u, 0u, 0u, 0u), cq1 = cq0;
+      float pq0 = 0.f, pq1 = 0.f;
+      if (hl < nl) {
+        cq0 = vr[1 + nk + hl];
+        pq0 = x4[(int)cq0.w].w;
+      }
+      if (hl + LPR < nl) {
+        cq1 = vr[1 + nk + hl + LPR];
+        pq1 = x4[(int)cq1.w].w;
+      }
       for (int i0 = 0; i0 < nk; i0 += UNR * LPR) {
         int c[UNR];
         float4 xb[UNR];
@@ -1501,7 +1513,17 @@ __global__ void __launch_bounds__(32 * (NWC + 1), 1)
         acc[1] *= __uint_as_float(hs.y);
         acc[2] *= __uint_as_float(hs.z);
       }
-      for (int i = hl; i < nl; i += LPR) {  // pressure couplings {vp 0..2, column}
+      if (hl < nl) {  // pressure couplings {vp 0..2, column}
+        acc[0] += __uint_as_float(cq0.x) * pq0;
+        acc[1] += __uint_as_float(cq0.y) * pq0;
+        acc[2] += __uint_as_float(cq0.z) * pq0;
+      }
+      if (hl + LPR < nl) {
+        acc[0] += __uint_as_float(cq1.x) * pq1;
+        acc[1] += __uint_as_float(cq1.y) * pq1;
+        acc[2] += __uint_as_float(cq1.z) * pq1;
+      }
+      for (int i = hl + 2 * LPR; i < nl; i += LPR) {  // further couplings
         const uint4 q4 = vr[1 + nk + i];
         const float pval = x4[(int)q4.w].w;
         acc[0] += __uint_as_float(q4.x) * pval;
@@ -1544,7 +1566,7 @@ __global__ void __launch_bounds__(32 * (NWC + 1), 1)
 #define EXF_ST_SLOTS 2
 #endif
 #ifndef EXF_BK_NWC
-#define EXF_BK_NWC 23
+#define EXF_BK_NWC 19
 #endif
 #ifndef EXF_BK_STG
 #define EXF_BK_STG 4
