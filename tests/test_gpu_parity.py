@@ -190,10 +190,12 @@ def test_solve_is_deterministic(case):
     assert np.array_equal(outs[0], outs[1])
 
 
-def test_bulk_streaming_level_matches_row_kernel_bits():
+@pytest.mark.parametrize("reverse", [0, 1])
+def test_bulk_streaming_level_matches_row_kernel_bits(reverse):
     """On a level large enough for AUTO to stream it with the bulk row kernel (the channel3d
     fine level, 140,481 velocity nodes), the mixed-precision cycles give the same bits as
-    the row kernel everywhere: both kernels sum each star row in the same order."""
+    the row kernel everywhere, in both colour orders: both kernels sum each star row in
+    the same order."""
     from exfemus_b200 import workloads
 
     outs = []
@@ -204,6 +206,7 @@ def test_bulk_streaming_level_matches_row_kernel_bits():
         p = case["mg_NS"]
         p.precision = _lib.PREC_MIXED
         p.vanka_kernel = vk
+        p.reverse_colours = reverse
         p.max_cycles = 3
         p.eps = 1e-14
         ns.set_x(np.zeros(ns.ntop_dof))
