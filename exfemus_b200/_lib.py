@@ -33,6 +33,8 @@ VANKA_TILE = 1
 VANKA_ROWS = 2
 VANKA_STREAM = 3
 VANKA_BULK = 4
+STOP_RELRES = 0
+STOP_REFERENCE = 1
 
 
 class ExfMeshDesc(C.Structure):
@@ -52,12 +54,13 @@ class ExfMgParams(C.Structure):
                 ("nu_pre", C.c_int), ("nu_post", C.c_int), ("double_below_top", C.c_int),
                 ("smoother", C.c_int), ("omega", C.c_double), ("corr_damp", C.c_double),
                 ("cond_corr", C.c_int), ("reverse_colours", C.c_int), ("precision", C.c_int),
-                ("use_graph", C.c_int), ("vanka_kernel", C.c_int)]
+                ("use_graph", C.c_int), ("vanka_kernel", C.c_int), ("stop_test", C.c_int)]
 
 
 class ExfSolveStats(C.Structure):
     _fields_ = [("cycles", C.c_int), ("converged", C.c_int), ("rel_res", C.c_double),
-                ("bnorm", C.c_double), ("seconds", C.c_double), ("hist", C.c_double * 256)]
+                ("bnorm", C.c_double), ("seconds", C.c_double), ("hist", C.c_double * 256),
+                ("last_acc", C.c_double)]
 
 
 class ExfError(RuntimeError):

@@ -116,7 +116,8 @@ using namespace exf;
 extern "C" {
 
 int exf_adjoint_forward(exf_sys *s, const exf_phys *ph, const exf_mg_params *p, exf_solve_stats *st) {
-  if (!s || !ph || !p || !st) return EXF_ERR_ARG;
+  CHECK_SYS(s);
+  if (!ph || !p || !st) return EXF_ERR_ARG;
   if (s->kind != EXF_KIND_T) {
     set_error("the adjoint entry points take the temperature system");
     return EXF_ERR_ARG;
@@ -128,7 +129,8 @@ int exf_adjoint_forward(exf_sys *s, const exf_phys *ph, const exf_mg_params *p, 
 
 int exf_adjoint_backward(exf_sys *s, const exf_phys *ph, const exf_mg_params *p, const double *djdx, double *djdq,
                          double *djdg, exf_solve_stats *st) {
-  if (!s || !ph || !p || !djdx || !st) return EXF_ERR_ARG;
+  CHECK_SYS(s);
+  if (!ph || !p || !djdx || !st) return EXF_ERR_ARG;
   if (s->kind != EXF_KIND_T || !s->assembled) {
     set_error("exf_adjoint_backward needs an assembled temperature system (call exf_adjoint_forward)");
     return EXF_ERR_STATE;

@@ -205,25 +205,48 @@ double *lvr<double>(SysLevel &L) { return L.r.p; }
 template <>
 float *lvr<float>(SysLevel &L) { return L.r32.p; }
 
+// the level's accuracies in the reference's sense are needed for the conditional
+// correction and for the reference stop test
+static bool needs_acc(const exf_mg_params *p) { return p->cond_corr || p->stop_test == EXF_STOP_REFERENCE; }
+
+// One smoothing call of nsw sweeps.  With acc, it also leaves in *slot the squared
+// residual that the reference's level solver reports as its accuracy: LASPACK's
+// stationary iterations evaluate ||r||/||b|| on a residual refreshed only while
+// Iter < MaxIter (SORForwIter, contrib/laspack/itersolv.c:850-894; LastAcc,
+// contrib/laspack/rtc.c:48-70), i.e. the residual of the iterate before the last sweep.
+template <class T>
+static int smooth_acc(exf_sys *s, int lev, const exf_mg_params *p, int nsw, T *x, const T *b, T *r, double *slot) {
+  if (!slot) return smooth<T>(s, lev, p, nsw, x, b);
+  if (nsw > 0) EXF_TRY(smooth<T>(s, lev, p, nsw - 1, x, b));
+  EXF_TRY(spmv_resid<T>(s, lev, x, b, r, slot));
+  if (nsw > 0) EXF_TRY(smooth<T>(s, lev, p, 1, x, b));
+  return EXF_OK;
+}
+
 template <class T>
 static int mg_step(exf_sys *s, int lev, const exf_mg_params *p, bool final_resid, double *d_norm_out) {
   SysLevel &L = s->L[lev];
   T *x = lvx<T>(L), *b = lvb<T>(L), *r = lvr<T>(L);
   const int top = s->nlev - 1;
+  const long len = sizeof(T) == 4 ? L.len32 : (long)L.ndof;
+  double *acc = needs_acc(p) ? s->mg_acc.p + 4 * lev : nullptr;
+  if (acc) EXF_TRY(norm2<T>(s, b, len, acc));
   if (lev == 0) {
     EXF_TRY(coarse_apply<T>(s, b, x));
+    if (acc) EXF_TRY(spmv_resid<T>(s, 0, x, b, r, acc + 2));
     if (final_resid) EXF_TRY(spmv_resid<T>(s, 0, x, b, r, d_norm_out));
     return EXF_OK;
   }
   const int mul = (p->double_below_top && lev < top) ? 2 : 1;
-  EXF_TRY(smooth<T>(s, lev, p, p->nu_pre * mul, x, b));
+  EXF_TRY(smooth_acc<T>(s, lev, p, p->nu_pre * mul, x, b, r, acc ? acc + 1 : nullptr));
   EXF_TRY(spmv_resid<T>(s, lev, x, b, r, nullptr));
   SysLevel &C = s->L[lev - 1];
   EXF_TRY(restrict_op<T>(s, lev - 1, r, lvb<T>(C)));
   EXF_TRY(zero_vec<T>(s->stream, lvx<T>(C), sizeof(T) == 4 ? C.len32 : (long)C.ndof));
   for (int g = 0; g < p->gamma; g++) EXF_TRY(mg_step<T>(s, lev - 1, p, false, nullptr));
-  EXF_TRY(prolong_add<T>(s, lev, lvx<T>(C), x, p->corr_damp));
-  EXF_TRY(smooth<T>(s, lev, p, p->nu_post * mul, x, b));
+  if (p->cond_corr) EXF_TRY(prolong_cond<T>(s, lev, lvx<T>(C), x, p->corr_damp, s->mg_acc.p));
+  else EXF_TRY(prolong_add<T>(s, lev, lvx<T>(C), x, p->corr_damp));
+  EXF_TRY(smooth_acc<T>(s, lev, p, p->nu_post * mul, x, b, r, acc ? acc + 2 : nullptr));
   if (final_resid) EXF_TRY(spmv_resid<T>(s, lev, x, b, r, d_norm_out));
   return EXF_OK;
 }
@@ -256,14 +279,16 @@ const char *exf_last_error(void) { return g_err; }
 long long exf_launch_count(void) { return (long long)__atomic_load_n(&g_launches, __ATOMIC_RELAXED); }
 
 int exf_event_record(exf_sys *s, int slot) {
-  if (!s || slot < 0 || slot >= 8) return EXF_ERR_ARG;
+  CHECK_SYS(s);
+  if (slot < 0 || slot >= 8) return EXF_ERR_ARG;
   if (!s->user_ev[slot]) EXF_CUDA(cudaEventCreate(&s->user_ev[slot]));
   EXF_CUDA(cudaEventRecord(s->user_ev[slot], s->stream));
   return EXF_OK;
 }
 
 int exf_event_elapsed(exf_sys *s, int a, int b, double *ms) {
-  if (!s || !ms || a < 0 || a >= 8 || b < 0 || b >= 8 || !s->user_ev[a] || !s->user_ev[b]) return EXF_ERR_ARG;
+  CHECK_SYS(s);
+  if (!ms || a < 0 || a >= 8 || b < 0 || b >= 8 || !s->user_ev[a] || !s->user_ev[b]) return EXF_ERR_ARG;
   EXF_CUDA(cudaEventSynchronize(s->user_ev[b]));
   float f = 0.f;
   EXF_CUDA(cudaEventElapsedTime(&f, s->user_ev[a], s->user_ev[b]));
@@ -290,6 +315,7 @@ int exf_mesh_create(const exf_mesh_desc *desc, exf_mesh **out) {
   for (int d = 0; d < 3; d++) m->n0[d] = desc->n0[d];
   for (int d = 0; d < 6; d++) m->box[d] = desc->box[d];
   int rc = build_mesh_host(m);
+  if (rc == EXF_OK) rc = upload_fe_table(m);
   if (rc != EXF_OK) {
     delete m;
     return rc;
@@ -299,6 +325,7 @@ int exf_mesh_create(const exf_mesh_desc *desc, exf_mesh **out) {
 }
 
 int exf_mesh_destroy(exf_mesh *m) {
+  if (m) cudaSetDevice(m->device);
   delete m;
   return EXF_OK;
 }
@@ -402,6 +429,8 @@ int exf_sys_create(exf_mesh *m, int kind, exf_sys **out) {
     if (rc == EXF_OK) rc = s->src_qe.alloc(m->lev[s->nlev - 1].nel);
     if (rc == EXF_OK) rc = s->src_qe.zero(s->stream);
     if (rc == EXF_OK) rc = s->red.out.alloc(16);
+    if (rc == EXF_OK) rc = s->wait_flag.alloc(1);
+    if (rc == EXF_OK) rc = s->wait_flag.zero(s->stream);
     if (rc == EXF_OK) rc = sys_upload_bc(s);
   }
   if (rc != EXF_OK) {
@@ -414,6 +443,7 @@ int exf_sys_create(exf_mesh *m, int kind, exf_sys **out) {
 
 int exf_sys_destroy(exf_sys *s) {
   if (!s) return EXF_OK;
+  cudaSetDevice(s->mesh->device);
   for (int k = 0; k < 2; k++)
     if (s->graph[k]) cudaGraphExecDestroy(s->graph[k]);
   if (s->stream) cudaStreamSynchronize(s->stream);
@@ -426,22 +456,6 @@ int exf_sys_destroy(exf_sys *s) {
   delete s;
   return EXF_OK;
 }
-
-#define CHECK_SYS(s)                      \
-  do {                                    \
-    if (!(s)) {                           \
-      set_error("null system handle");    \
-      return EXF_ERR_ARG;                 \
-    }                                     \
-  } while (0)
-#define CHECK_LEV(s, lev)                                 \
-  do {                                                    \
-    CHECK_SYS(s);                                         \
-    if ((lev) < 0 || (lev) >= (s)->nlev) {                \
-      set_error("level %d out of range", (int)(lev));     \
-      return EXF_ERR_ARG;                                 \
-    }                                                     \
-  } while (0)
 
 int exf_sys_ndof(const exf_sys *s, int lev, int *ndof) {
   CHECK_LEV(s, lev);
@@ -784,6 +798,8 @@ static unsigned long long params_key(const exf_mg_params *p) {
   mix((unsigned long long)p->reverse_colours);
   mix((unsigned long long)p->precision);
   mix((unsigned long long)p->vanka_kernel);
+  mix((unsigned long long)p->cond_corr);
+  mix((unsigned long long)p->stop_test);
   return h | 1ull;
 }
 
@@ -838,10 +854,13 @@ int exf_mg_solve(exf_sys *s, const exf_mg_params *p, exf_solve_stats *st) {
     set_error("exf_mg_solve before assembly");
     return EXF_ERR_STATE;
   }
-  if (p->gamma < 1 || p->nu_pre < 0 || p->nu_post < 0 || p->max_cycles < 0) return EXF_ERR_ARG;
-  if (p->cond_corr) {
-    set_error("conditional coarse correction is not implemented on the device");
-    return EXF_ERR_UNSUPPORTED;
+  if (p->gamma < 1 || p->nu_pre < 0 || p->nu_post < 0 || p->max_cycles < 0 ||
+      (p->stop_test != EXF_STOP_RELRES && p->stop_test != EXF_STOP_REFERENCE))
+    return EXF_ERR_ARG;
+  if (needs_acc(p) && s->mg_acc.n != (size_t)4 * s->nlev) {
+    EXF_TRY(s->mg_acc.alloc(4 * (size_t)s->nlev));
+    EXF_TRY(s->mg_acc.zero(s->stream));
+    s->buf_epoch++;
   }
   memset(st, 0, sizeof(*st));
   SysLevel &T = s->L[s->nlev - 1];
@@ -861,12 +880,19 @@ int exf_mg_solve(exf_sys *s, const exf_mg_params *p, exf_solve_stats *st) {
   double rel = sqrt(r2) / den;
   st->rel_res = rel;
   int rc = EXF_OK;
+  // stop tests: ||b-Ax||/||b|| <= eps, or the reference's exit test rest < eps*(1+||b||)
+  // (src/MGSolverBase.C:201) with rest the top level's accuracy of the last cycle (FP64; in
+  // mixed precision the top level of the FP32 cycle solves for the correction, so rest is
+  // the FP64 outer relative residual there)
+  const bool ref_stop = p->stop_test == EXF_STOP_REFERENCE;
+  const double lim = ref_stop ? p->eps * (1. + bn) : p->eps;
+  bool done = !ref_stop && rel <= p->eps;
   if (!std::isfinite(rel) || !std::isfinite(bn)) {
     set_error("multigrid diverged: non-finite initial residual or rhs");
     rc = EXF_ERR_DIVERGED;
-    rel = p->eps;  // skip the cycle loop
+    done = true;  // skip the cycle loop
   }
-  while (rel > p->eps && st->cycles < p->max_cycles) {
+  while (!done && st->cycles < p->max_cycles) {
     // the first cycle runs eagerly (it sizes every scratch buffer); later cycles replay a
     // captured CUDA graph of the whole cycle when use_graph is set
     if (p->use_graph && st->cycles > 0) {
@@ -879,11 +905,18 @@ int exf_mg_solve(exf_sys *s, const exf_mg_params *p, exf_solve_stats *st) {
     if (st->cycles < 256) st->hist[st->cycles] = rel;
     st->cycles++;
     st->rel_res = rel;
+    st->last_acc = rel;
+    if (needs_acc(p) && p->precision != EXF_PREC_MIXED) {
+      double a2 = 0.;
+      EXF_TRY(read_scalar(s, s->mg_acc.p + 4 * (s->nlev - 1) + 2, &a2));
+      st->last_acc = sqrt(a2) / den;
+    }
     if (!std::isfinite(rel)) {
       rc = EXF_ERR_DIVERGED;
       set_error("multigrid diverged at cycle %d", st->cycles);
       break;
     }
+    done = ref_stop ? st->last_acc < lim : rel <= p->eps;
   }
   EXF_CUDA(cudaEventRecord(s->ev1, s->stream));
   EXF_CUDA(cudaEventSynchronize(s->ev1));
@@ -891,7 +924,7 @@ int exf_mg_solve(exf_sys *s, const exf_mg_params *p, exf_solve_stats *st) {
   cudaEventElapsedTime(&ms, s->ev0, s->ev1);
   st->seconds = ms * 1e-3;
   EXF_TRY(device_wait_status(s));
-  st->converged = rc == EXF_OK && rel <= p->eps;
+  st->converged = rc == EXF_OK && (ref_stop ? (st->cycles > 0 && st->last_acc < lim) : rel <= p->eps);
   if (rc == EXF_OK && !st->converged) {
     set_error("not converged: rel %.3e after %d cycles", rel, st->cycles);
     rc = EXF_ERR_NOT_CONVERGED;

@@ -483,19 +483,26 @@ __global__ void __launch_bounds__(NT, DIM == 3 ? EXF_ASM_MINB3 : EXF_ASM_MINB2) 
 }
 
 template <int DIM>
+static int upload_tab(exf_mesh *m) {
+  FETab<DIM> h;
+  fill_tab<DIM>(h);
+  EXF_TRY(m->d_fetab.alloc(sizeof(FETab<DIM>)));
+  EXF_CUDA(cudaMemcpy(m->d_fetab.p, &h, sizeof(FETab<DIM>), cudaMemcpyHostToDevice));
+  return EXF_OK;
+}
+
+// the mesh owns its element type's FE tables on its own device, so systems on different
+// devices (driven from different threads) never share or replace them
+int upload_fe_table(exf_mesh *m) { return m->dim == 2 ? upload_tab<2>(m) : upload_tab<3>(m); }
+
+template <int DIM>
 static int assemble_dim(exf_sys *s, const exf_phys *ph, int lev, int mode) {
-  static FETab<DIM> *d_tab = nullptr;
-  static int tab_dev = -1;
-  int dev = 0;
-  cudaGetDevice(&dev);
-  if (!d_tab || tab_dev != dev) {
-    FETab<DIM> h;
-    fill_tab<DIM>(h);
-    EXF_CUDA(cudaMalloc(&d_tab, sizeof(FETab<DIM>)));
-    EXF_CUDA(cudaMemcpy(d_tab, &h, sizeof(FETab<DIM>), cudaMemcpyHostToDevice));
-    tab_dev = dev;
-  }
   exf_mesh *m = s->mesh;
+  if (!m->d_fetab.p || m->d_fetab.n != sizeof(FETab<DIM>)) {
+    set_error("assembly: the mesh has no FE tables of dimension %d", DIM);
+    return EXF_ERR_STATE;
+  }
+  const FETab<DIM> *d_tab = reinterpret_cast<const FETab<DIM> *>(m->d_fetab.p);
   SysLevel &L = s->L[lev];
   const MeshLevel &ml = m->lev[lev];
   const int top = s->nlev - 1;

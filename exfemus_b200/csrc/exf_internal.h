@@ -147,6 +147,9 @@ struct exf_mesh {
   std::vector<exf::MeshLevel> lev;
   exf::DBuf<double> d_xyz;
   exf::DBuf<int> d_lat;
+  // FE tables of the assembly (Gauss points, shape values and derivatives, surface
+  // rules) on the mesh's device: written once in exf_mesh_create, read-only after
+  exf::DBuf<unsigned char> d_fetab;
 };
 
 namespace exf {
@@ -260,6 +263,11 @@ struct exf_sys {
   int transposed = 0;
   exf_sys *other = nullptr;                 // coupled system (T <- NS velocity, NS <- T)
   exf::Partials red;
+  exf::DBuf<int> wait_flag;                 // set by a bounded in-kernel wait that ran out
+  // per level {||b_L||^2, r^2 before the last pre-smoothing sweep, r^2 before the last
+  // post-smoothing sweep (coarsest: after the solve), -}: the accuracies the reference's
+  // level solver reports, for the conditional correction and the reference stop test
+  exf::DBuf<double> mg_acc;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   cudaEvent_t user_ev[8] = {nullptr};
   // captured V-cycle graphs (per precision)
@@ -270,9 +278,37 @@ struct exf_sys {
   unsigned graph_epoch[2] = {0, 0};
 };
 
+// Entry-point guards: a null handle is an argument error; otherwise the system's device
+// becomes current for the calling thread, so one thread may drive systems on several
+// devices and threads with different current devices may each drive their own systems.
+#define CHECK_SYS(s)                                                            \
+  do {                                                                          \
+    if (!(s)) {                                                                 \
+      exf::set_error("null system handle");                                     \
+      return EXF_ERR_ARG;                                                       \
+    }                                                                           \
+    EXF_CUDA(cudaSetDevice((s)->mesh->device));                                 \
+  } while (0)
+#define CHECK_LEV(s, lev)                                                       \
+  do {                                                                          \
+    CHECK_SYS(s);                                                               \
+    if ((lev) < 0 || (lev) >= (s)->nlev) {                                      \
+      exf::set_error("level %d out of range", (int)(lev));                      \
+      return EXF_ERR_ARG;                                                       \
+    }                                                                           \
+  } while (0)
+
 namespace exf {
+// lanes per node row of the residual kernel k_spmv_resid<T, D, LPR, NS, ...>: one choice
+// shared by every launcher of the kernel (3D FP32 runs two rows per warp)
+template <class T, int D, bool NS>
+constexpr int spmv_lpr() {
+  return D == 3 ? (sizeof(T) == 4 ? 16 : 32) : (NS ? 16 : 8);
+}
+
 // kernels / launchers implemented in the .cu files
 int build_mesh_host(exf_mesh *m);
+int upload_fe_table(exf_mesh *m);  // FE tables of the mesh's element type, on its device
 int build_patterns(exf_sys *s);
 int build_transfers(exf_sys *s);
 int update_rmask(exf_sys *s);
@@ -305,7 +341,12 @@ int cast_d2f(cudaStream_t st, const double *a, float *b, long n, int i4, int N, 
 template <class T>
 int zero_vec(cudaStream_t st, T *a, long n);
 int add_f2d(cudaStream_t st, const float *a, double *b, long n, int i4, int N, int d);
-int norm2(exf_sys *s, const double *v, long n, double *d_out);
+template <class T>
+int norm2(exf_sys *s, const T *v, long n, double *d_out);
+// x_f += damp * P x_c only where the reference's conditional correction applies (acc:
+// per level {||b||^2, pre-smoothing r^2, post-smoothing r^2, -}, see mg_step)
+template <class T>
+int prolong_cond(exf_sys *s, int lev_f, const T *x_c, T *x_f, double damp, const double *acc);
 int vcycle_fp64(exf_sys *s, const exf_mg_params *p, double *d_relres);
 int vcycle_mixed(exf_sys *s, const exf_mg_params *p);
 }  // namespace exf

@@ -10,11 +10,14 @@
 // routine.
 //
 // The array holds at most EXF_STATIC_PARTIALS partial sums (one per block of the
-// residual kernel, 256 KB); larger levels are rejected with EXF_ERR_ARG.  Every GPU that
+// residual kernel, 256 KB); larger levels are rejected with EXF_ERR_ARG.  The call
+// returns once the system stream has finished it (it synchronizes that stream).  Every GPU that
 // loads the library holds the array until the process exits.  Every call on a device
 // shares the one array and leaves its last contents there; each call overwrites exactly
 // the partial sums it reads, so nothing has to start at zero, but two calls whose work
 // overlaps on the GPU (different streams or systems at the same time) race on it.
+#include <mutex>
+
 #include "exf_internal.h"
 
 namespace exf {
@@ -27,13 +30,13 @@ __global__ void k_spmv_resid(int N, int NL, const int *__restrict__ qq_ptr, cons
 __global__ void k_reduce_partials(const double *part, int n, double *out);
 }  // namespace exf
 
-#define EXF_STATIC_PARTIALS 32768
-
 static __device__ __align__(256) double g_static_partials[EXF_STATIC_PARTIALS];
 
 // device address of g_static_partials per device, resolved on the first call with that
-// device current (the host name of the array is not a device address)
+// device current (the host name of the array is not a device address); the lock makes
+// the first calls of threads on one device resolve it once
 static double *g_partials_addr[64] = {nullptr};
+static std::mutex g_partials_lock;
 
 using namespace exf;
 
@@ -41,7 +44,7 @@ template <int D, bool NS>
 static int resid_norm_static(exf_sys *s, int lev, const double *x, const double *b, double *r, double *norm2) {
   SysLevel &L = s->L[lev];
   constexpr int NT = 256;
-  constexpr int LPR = D == 3 ? 32 : (NS ? 16 : 8);
+  constexpr int LPR = spmv_lpr<double, D, NS>();  // the launch shape of the allocating residual
   const long ngroups = (long)L.N + (NS ? L.NL : 0);
   const long grid = (ngroups * LPR + NT - 1) / NT;
   if (grid > EXF_STATIC_PARTIALS) {
@@ -55,12 +58,16 @@ static int resid_norm_static(exf_sys *s, int lev, const double *x, const double 
     set_error("exf_resid_norm_static: device ordinal %d out of range", dev);
     return EXF_ERR_ARG;
   }
-  if (!g_partials_addr[dev]) {
-    void *ptr = nullptr;
-    EXF_CUDA(cudaGetSymbolAddress(&ptr, g_static_partials));
-    g_partials_addr[dev] = static_cast<double *>(ptr);
+  double *part = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(g_partials_lock);
+    if (!g_partials_addr[dev]) {
+      void *ptr = nullptr;
+      EXF_CUDA(cudaGetSymbolAddress(&ptr, g_static_partials));
+      g_partials_addr[dev] = static_cast<double *>(ptr);
+    }
+    part = g_partials_addr[dev];
   }
-  double *part = g_partials_addr[dev];
   k_spmv_resid<double, D, LPR, NS, NT, false><<<(unsigned)grid, NT, 0, s->stream>>>(
       L.N, L.NL, L.qq_ptr.p, L.qq_col.p, L.ql_ptr.p, L.ql_col.p, L.nqq, L.nql, L.nqqL, L.A.vv.p, L.A.vp.p, L.A.pv.p,
       L.A.pp.p, x, b, r, part);
@@ -82,6 +89,14 @@ extern "C" int exf_resid_norm_static(exf_sys *s, int lev, const double *x, const
     return EXF_ERR_STATE;
   }
   EXF_CUDA(cudaSetDevice(s->mesh->device));
+  // the call waits for its result on the system stream; a stream that is being captured
+  // cannot be waited on, so the call is refused there and leaves the capture intact
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  EXF_CUDA(cudaStreamIsCapturing(s->stream, &cs));
+  if (cs != cudaStreamCaptureStatusNone) {
+    set_error("exf_resid_norm_static synchronizes the system stream, which is being captured");
+    return EXF_ERR_STATE;
+  }
   const bool ns = s->kind == EXF_KIND_NS;
   int rc;
   if (s->dim == 2) rc = ns ? resid_norm_static<2, true>(s, lev, x, b, r, norm2)

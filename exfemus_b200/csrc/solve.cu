@@ -11,6 +11,7 @@
 #include <cooperative_groups.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <type_traits>
@@ -216,7 +217,7 @@ static int launch_spmv(exf_sys *s, int lev, const T *x, const T *b, T *r, double
   SysLevel &L = s->L[lev];
   constexpr int NT = 256;
   constexpr bool I4 = NS && sizeof(T) == 4;
-  constexpr int LPR = D == 3 ? (sizeof(T) == 4 ? 16 : 32) : (NS ? 16 : 8);
+  constexpr int LPR = spmv_lpr<T, D, NS>();
   long ngroups = (long)L.N + (NS ? L.NL : 0);
   unsigned grid = nblk(ngroups * LPR, NT);
   if (d_norm2) EXF_TRY(ensure_partials(s, grid));
@@ -240,6 +241,16 @@ int spmv_resid(exf_sys *s, int lev, const T *x, const T *b, T *r, double *d_norm
 }
 template int spmv_resid<double>(exf_sys *, int, const double *, const double *, double *, double *);
 template int spmv_resid<float>(exf_sys *, int, const float *, const float *, float *, double *);
+// the FP64 residual kernels that the allocation-free residual (noalloc.cu) launches with
+// the same lanes per row
+#define EXF_SPMV64_INST(D, NS)                                                                                  \
+  template __global__ void k_spmv_resid<double, D, spmv_lpr<double, D, NS>(), NS, 256, false>(                 \
+      int, int, const int *, const int *, const int *, const int *, long, long, long, const double *,            \
+      const double *, const double *, const double *, const double *, const double *, double *, double *);
+EXF_SPMV64_INST(1, false)
+EXF_SPMV64_INST(2, true)
+EXF_SPMV64_INST(3, true)
+#undef EXF_SPMV64_INST
 
 // ------------------------------------------------------------ transfers
 // b_c[(a,c)] = mask[(a,c)] * sum_f R[c,f] r_f[(a,f)]   (restriction, rows = coarse DOFs)
@@ -288,9 +299,16 @@ __global__ void k_prolong(int nv2, int nv1, int Nf, int NLf, int Nc, const int *
                           const int *__restrict__ pq_col, const T *__restrict__ pq_val,
                           const int *__restrict__ pl_ptr, const int *__restrict__ pl_col,
                           const T *__restrict__ pl_val, const T *__restrict__ xc, T *__restrict__ xf, T damp,
-                          int overwrite, const double *cond_rest) {
+                          int overwrite, const double *lacc, int lf) {
   EXF_PDL_WAIT();
-  if (cond_rest && !(cond_rest[1] < cond_rest[0])) return;
+  // the reference's conditional correction (src/MGSolverBase.C:262-263): added only when
+  // the coarse level's accuracy is below this level's pre-smoothing accuracy; lacc holds
+  // per level {||b||^2, pre-smoothing r^2, post-smoothing (coarsest: solve) r^2, -}
+  if (lacc) {
+    const double bf = lacc[4 * lf] > 0. ? sqrt(lacc[4 * lf]) : 1.;
+    const double bc = lacc[4 * (lf - 1)] > 0. ? sqrt(lacc[4 * (lf - 1)]) : 1.;
+    if (!(sqrt(lacc[4 * (lf - 1) + 2]) / bc < sqrt(lacc[4 * lf + 1]) / bf)) return;
+  }
   long row = (long)blockIdx.x * blockDim.x + threadIdx.x;
   long nq = (long)nv2 * Nf;
   if (row >= nq + (long)nv1 * NLf) return;
@@ -311,7 +329,7 @@ __global__ void k_prolong(int nv2, int nv1, int Nf, int NLf, int Nc, const int *
 
 template <class T>
 static int prolong_impl(exf_sys *s, int lev_f, const T *x_c, T *x_f, double damp, int overwrite,
-                        const double *cond) {
+                        const double *acc) {
   SysLevel &F = s->L[lev_f];
   SysLevel &C = s->L[lev_f - 1];
   long nrow = F.ndof;
@@ -319,7 +337,7 @@ static int prolong_impl(exf_sys *s, int lev_f, const T *x_c, T *x_f, double damp
   EXF_CUDA(launch_pdl(kern, dim3(nblk(nrow, 256)), dim3(256), 0, s->stream, s->nv2, s->nv1, F.N, F.NL, C.N,
                       F.Pq.ptr.p, F.Pq.col.p, VT<T>::pq(F.Pq), s->nv1 ? F.Pl.ptr.p : nullptr,
                       s->nv1 ? F.Pl.col.p : nullptr, s->nv1 ? VT<T>::pq(F.Pl) : nullptr, x_c, x_f, (T)damp, overwrite,
-                      cond));
+                      acc, lev_f));
   EXF_COUNT(1);
   return EXF_OK;
 }
@@ -331,8 +349,8 @@ int prolong_add(exf_sys *s, int lev_f, const T *x_c, T *x_f, double damp) {
 template int prolong_add<double>(exf_sys *, int, const double *, double *, double);
 template int prolong_add<float>(exf_sys *, int, const float *, float *, double);
 template <class T>
-int prolong_cond(exf_sys *s, int lev_f, const T *x_c, T *x_f, double damp, const double *cond) {
-  return prolong_impl<T>(s, lev_f, x_c, x_f, damp, 0, cond);
+int prolong_cond(exf_sys *s, int lev_f, const T *x_c, T *x_f, double damp, const double *acc) {
+  return prolong_impl<T>(s, lev_f, x_c, x_f, damp, 0, acc);
 }
 template int prolong_cond<double>(exf_sys *, int, const double *, double *, double, const double *);
 template int prolong_cond<float>(exf_sys *, int, const float *, float *, double, const double *);
@@ -1293,11 +1311,10 @@ __global__ void k_vanka_apply(const int *__restrict__ vrows, int nr, long gbase,
 // row issued at once, x gathers mostly L1 hits) and release a stage on its "empty"
 // mbarrier.  Each lane visits the blocks and couplings of its row in the same order as
 // the ROWS kernel, so both give the same sums.  Every wait is bounded: a wait that runs
-// out sets g_wait_timeout and the kernel leaves once its copies have landed.
+// out sets the system's wait flag and the kernel leaves once its copies have landed.
 #ifndef EXF_WAIT_TRIES
 #define EXF_WAIT_TRIES (1 << 22)
 #endif
-__device__ int g_wait_timeout;
 
 __device__ __forceinline__ unsigned smem_addr(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
 __device__ __forceinline__ void mbar_init(uint64_t *b, unsigned count) {
@@ -1349,7 +1366,8 @@ __global__ void __launch_bounds__(32 * (NWC + 1), 1)
                       const uint4 *__restrict__ sv, const uint2 *__restrict__ scx,
                       const int *__restrict__ qq_col, const int *__restrict__ ql_col, long nqqL,
                       const float *__restrict__ pv, const float *__restrict__ pp, const float *__restrict__ x,
-                      const float *__restrict__ b, float *__restrict__ res, long pres_off) {
+                      const float *__restrict__ b, float *__restrict__ res, long pres_off,
+                      int *__restrict__ wait_flag) {
   constexpr int RPW = 32 / LPR;  // rows per warp pass
   extern __shared__ __align__(16) unsigned char smem_raw[];
   BulkSmem<STG, CAPB> &S = *reinterpret_cast<BulkSmem<STG, CAPB> *>(smem_raw);
@@ -1411,7 +1429,7 @@ __global__ void __launch_bounds__(32 * (NWC + 1), 1)
       __syncwarp();
     }
     if (!ok) {
-      if (lane == 0) atomicExch(&g_wait_timeout, 1);
+      if (lane == 0) atomicExch(wait_flag, 1);
       // let the copies already issued land before the CTA leaves
       for (int j = max(0, it - STG); j < it; j++) mbar_wait(&S.full[j % STG], (j / STG) & 1);
     }
@@ -1445,7 +1463,7 @@ __global__ void __launch_bounds__(32 * (NWC + 1), 1)
   for (int it = 0;; it++) {
     const int s = it % STG;
     if (!mbar_wait(&S.full[s], (it / STG) & 1)) {
-      if (lane == 0) atomicExch(&g_wait_timeout, 1);
+      if (lane == 0) atomicExch(wait_flag, 1);
       break;
     }
     const int m = S.nrow[s];
@@ -1661,21 +1679,25 @@ static int vanka_sweep_rows(exf_sys *s, int lev, const exf_mg_params *p, T *x, c
         static_assert(CAPB >= 512, "a stage holds the longest row (header, 255 blocks, 255 couplings, pad)");
         using SM = BulkSmem<STG, CAPB>;
         auto kern = k_vanka_rows_bulk<NWC, STG, CAPB, UNR, BLPR>;
-        static int per_sm[64] = {0};
+        // CTAs per SM, per device (threads driving systems on one device may both resolve
+        // it; they store the same value)
+        static std::atomic<int> per_sm[64];
         const int dev = s->mesh->device;
         if (dev < 0 || dev >= 64) {
           set_error("device ordinal %d out of range", dev);
           return EXF_ERR_ARG;
         }
-        if (per_sm[dev] == 0) {
+        int nper = per_sm[dev].load(std::memory_order_acquire);
+        if (nper == 0) {
           EXF_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(SM)));
-          EXF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[dev], kern, 32 * (NWC + 1), sizeof(SM)));
-          if (per_sm[dev] < 1) {
+          EXF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nper, kern, 32 * (NWC + 1), sizeof(SM)));
+          if (nper < 1) {
             set_error("Vanka bulk row kernel does not fit on an SM");
             return EXF_ERR_UNSUPPORTED;
           }
+          per_sm[dev].store(nper, std::memory_order_release);
         }
-        const int grid = s->nsm * per_sm[dev];
+        const int grid = s->nsm * nper;
         if (!L.sv.p || L.bsched_G != grid) {  // first BULK sweep of this level (or a new grid)
           cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
           EXF_CUDA(cudaStreamIsCapturing(s->stream, &cs));
@@ -1691,7 +1713,7 @@ static int vanka_sweep_rows(exf_sys *s, int lev, const exf_mg_params *p, T *x, c
                             L.vrow_off[c], pin, n, L.N, (const long long *)L.soff.p, (const uint4 *)L.sv.p,
                             (const uint2 *)L.scx.p, (const int *)L.qq_col.p, (const int *)L.ql_col.p, L.nqqL,
                             (const float *)VT<T>::pv(L), (const float *)VT<T>::pp(L), (const float *)x,
-                            (const float *)b, (float *)res, pres_off));
+                            (const float *)b, (float *)res, pres_off, s->wait_flag.p));
         EXF_CUDA(launch_pdl(k_vanka_solve<T, D, NTS, I4, SU>, dim3(n), dim3(NTS), 0, s->stream, pin, L.N, L.vrows.p,
                             VK<T>::vk(L), VK<T>::pk(L), res, pres_off, x, (T)p->omega));
         EXF_COUNT(2);
@@ -1973,20 +1995,20 @@ static int gs_sweep(exf_sys *s, int lev, const exf_mg_params *p, T *x, const T *
 }
 
 // one CTA waits, bounded, on an mbarrier phase that nothing completes: the wait runs out,
-// sets g_wait_timeout and the kernel returns (exercises the status path of every bounded
-// wait without a fault)
-__global__ void k_wait_probe(int tries) {
+// sets the system's wait flag and the kernel returns (exercises the status path of every
+// bounded wait without a fault)
+__global__ void k_wait_probe(int tries, int *wait_flag) {
   __shared__ uint64_t bar;
   if (threadIdx.x == 0) {
     mbar_init(&bar, 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncthreads();
-  if (threadIdx.x == 0 && !mbar_wait(&bar, 0u, tries)) atomicExch(&g_wait_timeout, 1);
+  if (threadIdx.x == 0 && !mbar_wait(&bar, 0u, tries)) atomicExch(wait_flag, 1);
 }
 
 int wait_probe(exf_sys *s) {
-  k_wait_probe<<<1, 32, 0, s->stream>>>(1 << 14);
+  k_wait_probe<<<1, 32, 0, s->stream>>>(1 << 14, s->wait_flag.p);
   EXF_LAUNCH_CHECK();
   EXF_COUNT(1);
   return device_wait_status(s);
@@ -1994,11 +2016,10 @@ int wait_probe(exf_sys *s) {
 
 int device_wait_status(exf_sys *s) {
   int flag = 0;
-  EXF_CUDA(cudaMemcpyFromSymbolAsync(&flag, g_wait_timeout, sizeof(int), 0, cudaMemcpyDeviceToHost, s->stream));
+  EXF_CUDA(cudaMemcpyAsync(&flag, s->wait_flag.p, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
   EXF_CUDA(cudaStreamSynchronize(s->stream));
   if (flag) {
-    const int zero = 0;
-    EXF_CUDA(cudaMemcpyToSymbolAsync(g_wait_timeout, &zero, sizeof(int), 0, cudaMemcpyHostToDevice, s->stream));
+    EXF_CUDA(cudaMemsetAsync(s->wait_flag.p, 0, sizeof(int), s->stream));
     EXF_CUDA(cudaStreamSynchronize(s->stream));
     set_error("a bounded wait of the Vanka bulk row kernel ran out");
     return EXF_ERR_CUDA;
@@ -2293,24 +2314,30 @@ int add_f2d(cudaStream_t st, const float *a, double *b, long n, int i4, int N, i
   return EXF_OK;
 }
 
-template <int NT>
-__global__ void k_norm2_part(const double *v, long n, double *part) {
+template <int NT, class T>
+__global__ void k_norm2_part(const T *v, long n, double *part) {
   EXF_PDL_WAIT();
   __shared__ double sh[32];
   double acc = 0.;
-  for (long i = (long)blockIdx.x * NT + threadIdx.x; i < n; i += (long)gridDim.x * NT) acc += v[i] * v[i];
+  for (long i = (long)blockIdx.x * NT + threadIdx.x; i < n; i += (long)gridDim.x * NT)
+    acc += (double)v[i] * (double)v[i];
   acc = block_sum<NT>(acc, sh);
   if (threadIdx.x == 0) part[blockIdx.x] = acc;
 }
-int norm2(exf_sys *s, const double *v, long n, double *d_out) {
+// ||v||^2 into *d_out (FP64 sums in a fixed order; FP32 vectors are node-interleaved with
+// zero padding slots, which add nothing)
+template <class T>
+int norm2(exf_sys *s, const T *v, long n, double *d_out) {
   const int grid = 296;
   EXF_TRY(ensure_partials(s, grid));
-  k_norm2_part<256><<<grid, 256, 0, s->stream>>>(v, n, s->red.part.p);
-  k_reduce_partials<<<1, 1024, 0, s->stream>>>(s->red.part.p, grid, d_out);
-  EXF_LAUNCH_CHECK();
+  EXF_CUDA(launch_pdl(k_norm2_part<256, T>, dim3(grid), dim3(256), 0, s->stream, v, n, s->red.part.p));
+  EXF_CUDA(launch_pdl(k_reduce_partials, dim3(1), dim3(1024), 0, s->stream, (const double *)s->red.part.p, grid,
+                      d_out));
   EXF_COUNT(2);
   return EXF_OK;
 }
+template int norm2<double>(exf_sys *, const double *, long, double *);
+template int norm2<float>(exf_sys *, const float *, long, double *);
 
 // pressure gauge: p -= p[gauge] on the top level
 __global__ void k_gauge_read(const double *x, long idx, double *out) {

@@ -104,12 +104,23 @@ typedef struct {
   int smoother;        /* EXF_SMOOTH_*                                             */
   double omega;        /* Vanka damping                                            */
   double corr_damp;    /* coarse-correction factor (reference 0.95)                */
-  int cond_corr;       /* 1: reference's conditional coarse correction             */
+  int cond_corr;       /* 1: reference's conditional coarse correction: x += 0.95 P x_c */
+                       /* only when the coarse accuracy is below the pre-smoothing one */
+                       /* (src/MGSolverBase.C:262-263)                                 */
   int reverse_colours; /* 1: colours swept in reverse order                        */
   int precision;       /* EXF_PREC_*                                               */
   int use_graph;       /* 1: replay each V-cycle from a captured CUDA graph        */
   int vanka_kernel;    /* EXF_VANKA_*                                              */
+  int stop_test;       /* EXF_STOP_*                                               */
 } exf_mg_params;
+
+/* stop tests of exf_mg_solve.  A level's accuracy is what the reference's level solver
+ * reports (LASPACK's LastAcc): ||b - A x|| / ||b|| of the iterate before the last sweep of
+ * a smoothing call (of the coarsest level: after its solve). */
+#define EXF_STOP_RELRES 0     /* ||b - A x|| / ||b|| <= eps after a cycle                  */
+#define EXF_STOP_REFERENCE 1  /* rest < eps*(1 + ||b||), rest = the top level's accuracy of */
+                              /* the cycle's post-smoothing (src/MGSolverBase.C:201); in    */
+                              /* mixed precision rest is the FP64 relative residual        */
 
 typedef struct {
   int cycles;
@@ -118,6 +129,7 @@ typedef struct {
   double bnorm;
   double seconds;      /* device time of the solve (CUDA events on the system stream) */
   double hist[256];    /* relative residual after each cycle                       */
+  double last_acc;     /* the top level's accuracy of the last cycle (EXF_STOP_*)  */
 } exf_solve_stats;
 
 typedef struct exf_mesh exf_mesh;
@@ -222,11 +234,14 @@ EXF_API long long exf_launch_count(void);
  * allocate device memory while they run (the host application owns every allocation,
  * or memory is reserved before a run).  x, b, r and norm2 are DEVICE buffers owned by the
  * caller (ndof doubles; norm2 one double).  The norm's per-block partial sums live in a
- * fixed file-scope device array of 32768 doubles held by every GPU that loads the
- * library; levels needing more partial sums are rejected with EXF_ERR_ARG.  Nothing is
- * allocated or freed.  The first call on a device resolves the array's device address,
- * so make that first call before any stream capture.  All calls share the array: calls
- * that overlap on the GPU race.  It has no counterpart in the reference. */
+ * fixed file-scope device array of EXF_STATIC_PARTIALS doubles held by every GPU that
+ * loads the library; levels needing more partial sums are rejected with EXF_ERR_ARG.
+ * Nothing is allocated or freed.  The first call on a device resolves the array's device
+ * address, so make that first call before any stream capture.  The call returns once the
+ * system stream has finished it (it synchronizes that stream); while that stream is being
+ * captured it returns EXF_ERR_STATE and leaves the capture alone.  All calls share the
+ * array: calls that overlap on the GPU race.  It has no counterpart in the reference. */
+#define EXF_STATIC_PARTIALS 32768
 EXF_API int exf_resid_norm_static(exf_sys *s, int lev, const double *x, const double *b, double *r,
                                   double *norm2);
 /* algorithmic bytes of one residual (spmv: every matrix row once, FP32 or FP64 values)

@@ -9,4 +9,4 @@ LASPACK C library compiled from its own sources (absent when the reference tree 
 not available at build time).
 """
 from .pyoracle import (OrMesh, OrSys, OrPhys, OrMgParams, OrMgStats, Laspack, build,  # noqa: F401
-                       laspack_available, oracle_lib)
+                       laspack_available, oracle_lib, set_threads, get_threads)

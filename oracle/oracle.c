@@ -22,6 +22,9 @@
 #include "oracle.h"
 
 #include <math.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
 #include <stdlib.h>
 #include <string.h>
 
@@ -423,6 +426,8 @@ struct or_sys {
   int lu_ok;
   int **colour;     /* per level item colour */
   int *ncolour;
+  int **col_items;  /* per level: items grouped by colour, ascending within a colour */
+  int **col_off;    /* per level: [ncolour+1] offsets into col_items */
 };
 
 static void csr_alloc(csr *c, int n, long nnz) {
@@ -666,6 +671,15 @@ static void build_colours(or_sys *s, int l) {
     s->colour[l][i] = c;
   }
   s->ncolour[l] = m->dim == 2 ? 9 : 27;
+  int nc = s->ncolour[l];
+  s->col_off[l] = (int *)calloc(nc + 1, sizeof(int));
+  s->col_items[l] = (int *)malloc((nitem > 0 ? nitem : 1) * sizeof(int));
+  for (int i = 0; i < nitem; i++) s->col_off[l][s->colour[l][i] + 1]++;
+  for (int c = 0; c < nc; c++) s->col_off[l][c + 1] += s->col_off[l][c];
+  int *fill = (int *)malloc((nc + 1) * sizeof(int));
+  memcpy(fill, s->col_off[l], (nc + 1) * sizeof(int));
+  for (int i = 0; i < nitem; i++) s->col_items[l][fill[s->colour[l][i]]++] = i;
+  free(fill);
 }
 
 or_sys *or_sys_new(const or_mesh *m, int kind) {
@@ -711,6 +725,8 @@ or_sys *or_sys_new(const or_mesh *m, int kind) {
   s->r = (double **)calloc(L, sizeof(double *));
   s->colour = (int **)calloc(L, sizeof(int *));
   s->ncolour = (int *)calloc(L, sizeof(int));
+  s->col_items = (int **)calloc(L, sizeof(int *));
+  s->col_off = (int **)calloc(L, sizeof(int *));
   for (int l = 0; l < L; l++) {
     build_node_pattern(s, l);
     build_matrix_pattern(s, l);
@@ -741,7 +757,11 @@ void or_sys_free(or_sys *s) {
     free(s->b[l]);
     free(s->r[l]);
     free(s->colour[l]);
+    free(s->col_items[l]);
+    free(s->col_off[l]);
   }
+  free(s->col_items);
+  free(s->col_off);
   free(s->node_dof);
   free(s->qq_ptr);
   free(s->qq_idx);
@@ -908,13 +928,209 @@ static void side_normal(int dim, int sd, double *nrm) {
   for (int d = 0; d < 3; d++) nrm[d] = (double)dir[d];
 }
 
+/* One element of MGSolT::GenMatRhs (template_appl/nse/SRC/MGSolverT.C:93-525) or
+ * MGSolNS::GenMatRhs (template_appl/nse/SRC/MGSolverNS.C:108-717): local matrix and rhs,
+ * boundary sides, scatter into the level matrix (A[Level]->add_matrix) and rhs. */
+static void asm_element(or_sys *s, int lev, int mode, const or_phys *ph, const double *xold, const double *vel,
+                        const double *temp, const double *qe, const fe_tab *t, int e, double *Ke, double *Fe,
+                        double *rhs) {
+  const or_mesh *m = s->m;
+  int dim = m->dim, nen = m->nen, nvx = m->nvx, top = s->nlev - 1, off = m->ntop;
+  csr *A = &s->A[lev];
+  int nv2 = s->nv2, nvars = s->nvars;
+  int nloc = nv2 * nen + s->nv1 * nvx;
+  int dofs[MAXEN * 4];
+  int bcv[4][MAXEN], bcb[4][MAXEN];
+  double xx[3 * MAXEN];
+  double uold[4][MAXEN], vold[3][MAXEN], told[MAXEN];
+  double diff_t = ph->inv_prdl * ph->inv_re;
+  const int *c = m->conn[lev] + (long)e * nen;
+  memset(Ke, 0, (size_t)nloc * nloc * sizeof(double));
+  memset(Fe, 0, nloc * sizeof(double));
+  /* get_el_dof_bc (src/MGSolverDA.C:987-1041) and get_el_sol (src/MGSolverBase.C:336-354) */
+  for (int k = 0; k < nen; k++) {
+    for (int d = 0; d < dim; d++) xx[d * nen + k] = m->xyz[c[k] + (long)d * off];
+    for (int v = 0; v < nvars; v++) {
+      int quad = v < nv2;
+      if (!quad && k >= nvx) continue;
+      int loc = quad ? v * nen + k : nv2 * nen + k;
+      dofs[loc] = s->node_dof[lev][c[k] + v * off];
+      int td = s->node_dof[top][c[k] + v * off];
+      bcv[v][k] = s->bc0[td];
+      bcb[v][k] = s->bc1[td];
+      uold[v][k] = xold ? xold[td] : 0.;
+    }
+    for (int d = 0; d < dim; d++) vold[d][k] = 0.;
+    if (s->kind == 0 && vel) {
+      /* NS field coupled into T: velocity components are the first dim vars of
+       * the NS system on the top level (same node numbering). */
+      int Ntop = m->nnodes[top];
+      for (int d = 0; d < dim; d++) vold[d][k] = vel[c[k] + d * Ntop];
+    }
+    if (s->kind == 1)
+      for (int d = 0; d < dim; d++) vold[d][k] = uold[d][k];
+    told[k] = 0.;
+    if (s->kind == 1 && temp) told[k] = temp[c[k]];
+    if (s->kind == 0) told[k] = uold[0][k];
+  }
+  double h[3];
+  {
+    int v2 = dim == 2 ? 2 : 6, v3 = dim == 2 ? 3 : 7;
+    for (int d = 0; d < dim; d++) {
+      h[d] = fabs(xx[d * nen + v2] - xx[d * nen + 0]);
+      double h1 = fabs(xx[d * nen + v3] - xx[d * nen + 1]);
+      if (h[d] < h1) h[d] = h1;
+    }
+  }
+  double q_e = (s->kind == 0 && qe && lev == top) ? qe[e] : 0.;
+  for (int q = 0; q < t->ng; q++) {
+    double ij[9];
+    double det = jac(t, q, xx, nen, ij);
+    double JxW = det * t->w[q];
+    double dphi[MAXEN][3];
+    for (int sh = 0; sh < nen; sh++)
+      for (int i = 0; i < dim; i++) {
+        double sum = 0.;
+        for (int j = 0; j < dim; j++) sum += ij[j + i * dim] * t->dphi[q][sh][j];
+        dphi[sh][i] = sum;
+      }
+    const double *phi = t->phi[q];
+    double vg[3] = {0, 0, 0}, mod = 1e-20;
+    for (int d = 0; d < dim; d++) {
+      for (int k = 0; k < nen; k++) vg[d] += phi[k] * vold[d][k];
+      mod += vg[d] * vg[d];
+    }
+    mod = sqrt(mod);
+    if (s->kind == 0) {
+      double f[3], tg = 0.;
+      for (int d = 0; d < dim; d++) f[d] = (vel ? upwind_f(ph->upwind_t, ph->rhocp, mod, h[d], diff_t) : 0.);
+      for (int k = 0; k < nen; k++) tg += phi[k] * told[k];
+      for (int i = 0; i < nen; i++) {
+        double dt = JxW * bcv[0][i];
+        if (mode == 1) Fe[i] += dt * (ph->rhocp * tg * phi[i] * ph->inv_dt + q_e * phi[i]);
+        for (int j = 0; j < nen; j++) {
+          double adv = 0., lap = 0.;
+          for (int d = 0; d < dim; d++) {
+            adv += vg[d] * dphi[j][d];
+            lap += (diff_t + f[d] * vg[d] * vg[d]) * dphi[j][d] * dphi[i][d];
+          }
+          Ke[i * nloc + j] += dt * (ph->rhocp * phi[i] * phi[j] * ph->inv_dt + ph->rhocp * adv * phi[i] + lap);
+        }
+      }
+    } else {
+      double f[3], tg = 0.;
+      for (int d = 0; d < dim; d++) f[d] = upwind_f(ph->upwind_ns, ph->rho, mod, h[d], ph->inv_re);
+      for (int k = 0; k < nen; k++) tg += phi[k] * told[k];
+      const double *psi = t->psi[q];
+      double nu = ph->inv_re, rho = ph->rho;
+      for (int i = 0; i < nen; i++) {
+        for (int a = 0; a < dim; a++) {
+          int row = a * nen + i;
+          double dt = JxW * bcv[a][i];
+          if (mode == 1)
+            Fe[row] += dt * (rho * vg[a] * phi[i] * ph->inv_dt + rho * ph->ifr * ph->dirg[a] * phi[i] +
+                             ph->buoy * tg * ph->dirg[a] * phi[i]);
+          for (int j = 0; j < nen; j++) {
+            double adv = 0., lap = 0.;
+            for (int d = 0; d < dim; d++) {
+              adv += vg[d] * dphi[j][d] * phi[i];
+              lap += (nu + f[d] * vg[d] * vg[d]) * dphi[j][d] * dphi[i][d];
+            }
+            Ke[row * nloc + a * nen + j] +=
+                dt * rho *
+                (phi[j] * phi[i] * ph->inv_dt + adv + lap + (nu + f[a] * vg[a] * vg[a]) * dphi[j][a] * dphi[i][a]);
+            for (int bb = 1; bb < dim; bb++) {
+              int b = (a + bb) % dim;
+              Ke[row * nloc + b * nen + j] += dt * rho * (nu + f[a] * vg[a] * vg[b]) * dphi[j][a] * dphi[i][b];
+            }
+          }
+          for (int j = 0; j < nvx; j++) Ke[row * nloc + nv2 * nen + j] += dt * (-psi[j] * dphi[i][a]);
+        }
+      }
+      for (int i = 0; i < nvx; i++) {
+        int row = nv2 * nen + i;
+        for (int j = 0; j < nen; j++)
+          for (int b = 0; b < dim; b++) Ke[row * nloc + b * nen + j] += JxW * rho * psi[i] * dphi[j][b];
+      }
+    }
+  }
+  /* boundary sides (MGSolverT.C boundary block; MGSolverNS.C:495-687) */
+  for (int sd = 0; sd < m->nsides; sd++) {
+    if (m->neigh[lev][(long)e * m->nsides + sd] != -1) continue;
+    const int *sur = dim == 2 ? Q9_SIDE[sd] : H27_FACE[sd];
+    int nsn = m->nsn;
+    double xb[3 * 9];
+    for (int k = 0; k < nsn; k++)
+      for (int d = 0; d < dim; d++) xb[d * nsn + k] = xx[d * nen + sur[k]];
+    double nrm[3];
+    side_normal(dim, sd, nrm);
+    int last = sur[nsn - 1];
+    for (int a = 0; a < nv2; a++) {
+      if (bcv[a][last] == 0) {
+        double det = jac_sur(t, t->sng - 1, xb, nsn);
+        double ipen = det * ph->penalty;
+        if (s->kind == 0) {
+          int bc_beta = bcb[0][last] % 2;
+          for (int k = 0; k < nsn; k++) {
+            int lv = sur[k];
+            if (mode == 1) Fe[lv] += bc_beta * ipen * uold[0][lv];
+            Ke[lv * nloc + lv] += ipen;
+          }
+        } else {
+          for (int k = 0; k < nsn; k++) {
+            int lv = sur[k];
+            int row = a * nen + lv;
+            int bs = bcb[a][lv];
+            int bc_rhs = (bs & 4) >> 2, bc_tg = (bs & 2) >> 1, bc_n = bs % 2;
+            double vdn = 0.;
+            for (int d = 0; d < dim; d++) vdn += nrm[d] * uold[d][lv];
+            if (mode == 1)
+              Fe[row] += bc_rhs * ipen *
+                         ((1 - bc_n) * (1 - bc_tg) * uold[a][lv] + bc_n * vdn * nrm[a] +
+                          bc_tg * (uold[a][lv] - vdn * nrm[a]));
+            Ke[row * nloc + row] +=
+                ((1 - bc_n) * (1 - bc_tg) + bc_tg) * ipen + ipen * nrm[a] * nrm[a] * (bc_n - bc_tg);
+            for (int b = a + 1; b < dim; b++)
+              Ke[row * nloc + b * nen + lv] += ipen * nrm[b] * nrm[a] * (bc_n - bc_tg);
+          }
+        }
+      } else if (s->kind == 0 && bcb[0][last] != 0) {
+        /* Robin: k dT/dn = -h T (MGSolverT.C Neumann block); constant terms are 0 there */
+        for (int q = 0; q < t->sng; q++) {
+          double JxW = jac_sur(t, q, xb, nsn) * t->sw[q];
+          for (int i = 0; i < nsn; i++) {
+            int lei = sur[i];
+            int bs = bcb[0][lei];
+            double dt = JxW * bcv[0][lei];
+            int bc_alpha = (bs & 2) >> 1;
+            for (int j = 0; j < nsn; j++)
+              Ke[lei * nloc + sur[j]] += dt * bc_alpha * diff_t * t->sphi[q][i] * t->sphi[q][j];
+          }
+        }
+      }
+    }
+  }
+  /* scatter (A[Level]->add_matrix, b[Level]->add_vector) */
+  for (int i = 0; i < nloc; i++) {
+    int gi = dofs[i];
+    if (mode == 1) rhs[gi] += Fe[i];
+    for (int j = 0; j < nloc; j++) {
+      double v = Ke[i * nloc + j];
+      int pos = find_col(A, gi, dofs[j]);
+      A->val[pos] += v;
+    }
+  }
+}
+
 /* MGSolT::GenMatRhs (template_appl/nse/SRC/MGSolverT.C:93-525) and
- * MGSolNS::GenMatRhs (template_appl/nse/SRC/MGSolverNS.C:108-717). */
+ * MGSolNS::GenMatRhs (template_appl/nse/SRC/MGSolverNS.C:108-717).  Elements are taken
+ * colour after colour ((ex&1)|(ey&1)<<1|(ez&1)<<2); elements of one colour share no node,
+ * so they scatter into disjoint rows and run in parallel, and every matrix entry receives
+ * its element contributions in colour order whatever the thread count. */
 void or_sys_assemble(or_sys *s, int lev, int mode, const or_phys *ph, const double *xold, const double *vel,
                      const double *temp, const double *qe) {
   const or_mesh *m = s->m;
-  int dim = m->dim, nen = m->nen, nvx = m->nvx, top = s->nlev - 1, off = m->ntop;
-  int N = m->nnodes[lev];
+  int dim = m->dim, nen = m->nen, nvx = m->nvx, top = s->nlev - 1;
   fe_tab t;
   fe_init(&t, dim);
   csr *A = &s->A[lev];
@@ -924,197 +1140,22 @@ void or_sys_assemble(or_sys *s, int lev, int mode, const or_phys *ph, const doub
     rhs = s->b[lev];
     memset(rhs, 0, s->ndof[lev] * sizeof(double));
   }
-  int nv2 = s->nv2, nvars = s->nvars;
-  int nloc = nv2 * nen + s->nv1 * nvx;
-  double *Ke = (double *)malloc((size_t)nloc * nloc * sizeof(double));
-  double *Fe = (double *)malloc(nloc * sizeof(double));
-  int dofs[MAXEN * 4];
-  int bcv[4][MAXEN], bcb[4][MAXEN];
-  double xx[3 * MAXEN];
-  double uold[4][MAXEN], vold[3][MAXEN], told[MAXEN];
-  double diff_t = ph->inv_prdl * ph->inv_re;
-  for (int e = 0; e < m->nel[lev]; e++) {
-    const int *c = m->conn[lev] + (long)e * nen;
-    memset(Ke, 0, (size_t)nloc * nloc * sizeof(double));
-    memset(Fe, 0, nloc * sizeof(double));
-    /* get_el_dof_bc (src/MGSolverDA.C:987-1041) and get_el_sol (src/MGSolverBase.C:336-354) */
-    for (int k = 0; k < nen; k++) {
-      for (int d = 0; d < dim; d++) xx[d * nen + k] = m->xyz[c[k] + (long)d * off];
-      for (int v = 0; v < nvars; v++) {
-        int quad = v < nv2;
-        if (!quad && k >= nvx) continue;
-        int loc = quad ? v * nen + k : nv2 * nen + k;
-        dofs[loc] = s->node_dof[lev][c[k] + v * off];
-        int td = s->node_dof[top][c[k] + v * off];
-        bcv[v][k] = s->bc0[td];
-        bcb[v][k] = s->bc1[td];
-        uold[v][k] = xold ? xold[td] : 0.;
-      }
-      for (int d = 0; d < dim; d++) vold[d][k] = 0.;
-      if (s->kind == 0 && vel) {
-        /* NS field coupled into T: velocity components are the first dim vars of
-         * the NS system on the top level (same node numbering). */
-        int Ntop = m->nnodes[top];
-        for (int d = 0; d < dim; d++) vold[d][k] = vel[c[k] + d * Ntop];
-      }
-      if (s->kind == 1)
-        for (int d = 0; d < dim; d++) vold[d][k] = uold[d][k];
-      told[k] = 0.;
-      if (s->kind == 1 && temp) told[k] = temp[c[k]];
-      if (s->kind == 0) told[k] = uold[0][k];
-    }
-    double h[3];
+  int nloc = s->nv2 * nen + s->nv1 * nvx;
+  const int nel = m->nel[lev], ncol = 1 << dim;
+  for (int c = 0; c < ncol; c++) {
+#pragma omp parallel
     {
-      int v2 = dim == 2 ? 2 : 6, v3 = dim == 2 ? 3 : 7;
-      for (int d = 0; d < dim; d++) {
-        h[d] = fabs(xx[d * nen + v2] - xx[d * nen + 0]);
-        double h1 = fabs(xx[d * nen + v3] - xx[d * nen + 1]);
-        if (h[d] < h1) h[d] = h1;
-      }
-    }
-    double q_e = (s->kind == 0 && qe && lev == top) ? qe[e] : 0.;
-    for (int q = 0; q < t.ng; q++) {
-      double ij[9];
-      double det = jac(&t, q, xx, nen, ij);
-      double JxW = det * t.w[q];
-      double dphi[MAXEN][3];
-      for (int sh = 0; sh < nen; sh++)
-        for (int i = 0; i < dim; i++) {
-          double sum = 0.;
-          for (int j = 0; j < dim; j++) sum += ij[j + i * dim] * t.dphi[q][sh][j];
-          dphi[sh][i] = sum;
-        }
-      const double *phi = t.phi[q];
-      double vg[3] = {0, 0, 0}, mod = 1e-20;
-      for (int d = 0; d < dim; d++) {
-        for (int k = 0; k < nen; k++) vg[d] += phi[k] * vold[d][k];
-        mod += vg[d] * vg[d];
-      }
-      mod = sqrt(mod);
-      if (s->kind == 0) {
-        double f[3], tg = 0.;
-        for (int d = 0; d < dim; d++) f[d] = (vel ? upwind_f(ph->upwind_t, ph->rhocp, mod, h[d], diff_t) : 0.);
-        for (int k = 0; k < nen; k++) tg += phi[k] * told[k];
-        for (int i = 0; i < nen; i++) {
-          double dt = JxW * bcv[0][i];
-          if (mode == 1) Fe[i] += dt * (ph->rhocp * tg * phi[i] * ph->inv_dt + q_e * phi[i]);
-          for (int j = 0; j < nen; j++) {
-            double adv = 0., lap = 0.;
-            for (int d = 0; d < dim; d++) {
-              adv += vg[d] * dphi[j][d];
-              lap += (diff_t + f[d] * vg[d] * vg[d]) * dphi[j][d] * dphi[i][d];
-            }
-            Ke[i * nloc + j] += dt * (ph->rhocp * phi[i] * phi[j] * ph->inv_dt + ph->rhocp * adv * phi[i] + lap);
-          }
-        }
-      } else {
-        double f[3], tg = 0.;
-        for (int d = 0; d < dim; d++) f[d] = upwind_f(ph->upwind_ns, ph->rho, mod, h[d], ph->inv_re);
-        for (int k = 0; k < nen; k++) tg += phi[k] * told[k];
-        const double *psi = t.psi[q];
-        double nu = ph->inv_re, rho = ph->rho;
-        for (int i = 0; i < nen; i++) {
-          for (int a = 0; a < dim; a++) {
-            int row = a * nen + i;
-            double dt = JxW * bcv[a][i];
-            if (mode == 1)
-              Fe[row] += dt * (rho * vg[a] * phi[i] * ph->inv_dt + rho * ph->ifr * ph->dirg[a] * phi[i] +
-                               ph->buoy * tg * ph->dirg[a] * phi[i]);
-            for (int j = 0; j < nen; j++) {
-              double adv = 0., lap = 0.;
-              for (int d = 0; d < dim; d++) {
-                adv += vg[d] * dphi[j][d] * phi[i];
-                lap += (nu + f[d] * vg[d] * vg[d]) * dphi[j][d] * dphi[i][d];
-              }
-              Ke[row * nloc + a * nen + j] +=
-                  dt * rho *
-                  (phi[j] * phi[i] * ph->inv_dt + adv + lap + (nu + f[a] * vg[a] * vg[a]) * dphi[j][a] * dphi[i][a]);
-              for (int bb = 1; bb < dim; bb++) {
-                int b = (a + bb) % dim;
-                Ke[row * nloc + b * nen + j] += dt * rho * (nu + f[a] * vg[a] * vg[b]) * dphi[j][a] * dphi[i][b];
-              }
-            }
-            for (int j = 0; j < nvx; j++) Ke[row * nloc + nv2 * nen + j] += dt * (-psi[j] * dphi[i][a]);
-          }
-        }
-        for (int i = 0; i < nvx; i++) {
-          int row = nv2 * nen + i;
-          for (int j = 0; j < nen; j++)
-            for (int b = 0; b < dim; b++) Ke[row * nloc + b * nen + j] += JxW * rho * psi[i] * dphi[j][b];
-        }
-      }
-    }
-    /* boundary sides (MGSolverT.C boundary block; MGSolverNS.C:495-687) */
-    for (int sd = 0; sd < m->nsides; sd++) {
-      if (m->neigh[lev][(long)e * m->nsides + sd] != -1) continue;
-      const int *sur = dim == 2 ? Q9_SIDE[sd] : H27_FACE[sd];
-      int nsn = m->nsn;
-      double xb[3 * 9];
-      for (int k = 0; k < nsn; k++)
-        for (int d = 0; d < dim; d++) xb[d * nsn + k] = xx[d * nen + sur[k]];
-      double nrm[3];
-      side_normal(dim, sd, nrm);
-      int last = sur[nsn - 1];
-      for (int a = 0; a < nv2; a++) {
-        if (bcv[a][last] == 0) {
-          double det = jac_sur(&t, t.sng - 1, xb, nsn);
-          double ipen = det * ph->penalty;
-          if (s->kind == 0) {
-            int bc_beta = bcb[0][last] % 2;
-            for (int k = 0; k < nsn; k++) {
-              int lv = sur[k];
-              if (mode == 1) Fe[lv] += bc_beta * ipen * uold[0][lv];
-              Ke[lv * nloc + lv] += ipen;
-            }
-          } else {
-            for (int k = 0; k < nsn; k++) {
-              int lv = sur[k];
-              int row = a * nen + lv;
-              int bs = bcb[a][lv];
-              int bc_rhs = (bs & 4) >> 2, bc_tg = (bs & 2) >> 1, bc_n = bs % 2;
-              double vdn = 0.;
-              for (int d = 0; d < dim; d++) vdn += nrm[d] * uold[d][lv];
-              if (mode == 1)
-                Fe[row] += bc_rhs * ipen *
-                           ((1 - bc_n) * (1 - bc_tg) * uold[a][lv] + bc_n * vdn * nrm[a] +
-                            bc_tg * (uold[a][lv] - vdn * nrm[a]));
-              Ke[row * nloc + row] +=
-                  ((1 - bc_n) * (1 - bc_tg) + bc_tg) * ipen + ipen * nrm[a] * nrm[a] * (bc_n - bc_tg);
-              for (int b = a + 1; b < dim; b++)
-                Ke[row * nloc + b * nen + lv] += ipen * nrm[b] * nrm[a] * (bc_n - bc_tg);
-            }
-          }
-        } else if (s->kind == 0 && bcb[0][last] != 0) {
-          /* Robin: k dT/dn = -h T (MGSolverT.C Neumann block); constant terms are 0 there */
-          for (int q = 0; q < t.sng; q++) {
-            double JxW = jac_sur(&t, q, xb, nsn) * t.sw[q];
-            for (int i = 0; i < nsn; i++) {
-              int lei = sur[i];
-              int bs = bcb[0][lei];
-              double dt = JxW * bcv[0][lei];
-              int bc_alpha = (bs & 2) >> 1;
-              for (int j = 0; j < nsn; j++)
-                Ke[lei * nloc + sur[j]] += dt * bc_alpha * diff_t * t.sphi[q][i] * t.sphi[q][j];
-            }
-          }
-        }
-      }
-    }
-    /* scatter (A[Level]->add_matrix, b[Level]->add_vector) */
-    for (int i = 0; i < nloc; i++) {
-      int gi = dofs[i];
-      if (mode == 1) rhs[gi] += Fe[i];
-      for (int j = 0; j < nloc; j++) {
-        double v = Ke[i * nloc + j];
-        int pos = find_col(A, gi, dofs[j]);
-        A->val[pos] += v;
-      }
+      double *Ke = (double *)malloc((size_t)nloc * nloc * sizeof(double));
+      double *Fe = (double *)malloc(nloc * sizeof(double));
+#pragma omp for schedule(dynamic, 4)
+      for (int e = 0; e < nel; e++)
+        if (m->ecol[lev][e] == c) asm_element(s, lev, mode, ph, xold, vel, temp, qe, &t, e, Ke, Fe, rhs);
+      free(Ke);
+      free(Fe);
     }
   }
   if (mode == 1 && lev == top) memcpy(s->rhs, rhs, s->ndof[lev] * sizeof(double));
   if (lev == 0) s->lu_ok = 0;
-  free(Ke);
-  free(Fe);
 }
 
 void or_sys_get_matrix(const or_sys *s, int lev, double *val) {
@@ -1143,9 +1184,26 @@ void or_sys_transpose_all(or_sys *s) {
   s->lu_ok = 0;
 }
 
+/* ============================================================== threads */
+void or_set_threads(int n) {
+#ifdef _OPENMP
+  if (n > 0) omp_set_num_threads(n);
+#else
+  (void)n;
+#endif
+}
+int or_get_threads(void) {
+#ifdef _OPENMP
+  return omp_get_max_threads();
+#else
+  return 1;
+#endif
+}
+
 /* ============================================================== solvers */
 void or_spmv(const or_sys *s, int lev, const double *x, double *y) {
   const csr *A = &s->A[lev];
+#pragma omp parallel for schedule(static)
   for (int i = 0; i < A->n; i++) {
     double sum = 0.;
     for (int q = A->ptr[i]; q < A->ptr[i + 1]; q++) sum += A->val[q] * x[A->col[q]];
@@ -1156,13 +1214,14 @@ void or_spmv(const or_sys *s, int lev, const double *x, double *y) {
 /* LaspackVectorM::resid (contrib/matrix/laspack_vectorM.C:147-168) */
 static double resid(const or_sys *s, int lev, const double *x, const double *b, double *r) {
   const csr *A = &s->A[lev];
-  double nr = 0.;
+#pragma omp parallel for schedule(static)
   for (int i = 0; i < A->n; i++) {
     double sum = 0.;
     for (int q = A->ptr[i]; q < A->ptr[i + 1]; q++) sum += A->val[q] * x[A->col[q]];
     r[i] = b[i] - sum;
-    nr += r[i] * r[i];
   }
+  double nr = 0.; /* in row order, whatever the thread count */
+  for (int i = 0; i < A->n; i++) nr += r[i] * r[i];
   return sqrt(nr);
 }
 static double norm2(const double *v, int n) {
@@ -1172,6 +1231,7 @@ static double norm2(const double *v, int n) {
 }
 /* LaspackVectorM::matrix_mult (laspack_vectorM.C:170-189) */
 static void matmul(const csr *M, const double *x, double *y) {
+#pragma omp parallel for schedule(static)
   for (int i = 0; i < M->n; i++) {
     double sum = 0.;
     for (int q = M->ptr[i]; q < M->ptr[i + 1]; q++) sum += M->val[q] * x[M->col[q]];
@@ -1180,14 +1240,17 @@ static void matmul(const csr *M, const double *x, double *y) {
 }
 
 /* multi-colour Gauss-Seidel (the parallel ordering of SORForwIter at omega=1,
- * contrib/laspack/itersolv.c:850-894) */
+ * contrib/laspack/itersolv.c:850-894); rows of one colour are not coupled, so each
+ * colour's rows are updated in parallel exactly as in sequence */
 static void gs_sweep(or_sys *s, int lev, double *x, const double *b, int reverse) {
   const csr *A = &s->A[lev];
   int nc = s->ncolour[lev];
   for (int cc = 0; cc < nc; cc++) {
     int c = reverse ? nc - 1 - cc : cc;
-    for (int i = 0; i < A->n; i++) {
-      if (s->colour[lev][i] != c) continue;
+    const int t0 = s->col_off[lev][c], t1 = s->col_off[lev][c + 1];
+#pragma omp parallel for schedule(static)
+    for (int t = t0; t < t1; t++) {
+      const int i = s->col_items[lev][t];
       double sum = b[i], d = 0.;
       for (int q = A->ptr[i]; q < A->ptr[i + 1]; q++) {
         if (A->col[q] == i) d = A->val[q];
@@ -1203,10 +1266,12 @@ static void gs_sweep(or_sys *s, int lev, double *x, const double *b, int reverse
  * the pressure-pressure entry and a damping omega.  Within one colour every patch's
  * correction is computed from the iterate at the start of the colour and then all
  * corrections are applied (patches of one colour are disjoint), so the result does not
- * depend on the order of patches inside a colour; colours run in sequence. */
+ * depend on the order of patches inside a colour, and a colour's patches run in
+ * parallel; colours run in sequence. */
+#define OR_MAXSTAR (3 * 125 + 8)
 static void vanka_sweep(or_sys *s, int lev, double *x, const double *b, double omega, int reverse, int l1) {
   const csr *A = &s->A[lev];
-  int N = s->m->nnodes[lev], nv2 = s->nv2, NL = s->nl[lev];
+  int N = s->m->nnodes[lev], nv2 = s->nv2;
   int nc = s->ncolour[lev];
   int pbase = nv2 * N;
   int n = s->ndof[lev];
@@ -1214,54 +1279,60 @@ static void vanka_sweep(or_sys *s, int lev, double *x, const double *b, double o
   char *touched = (char *)calloc(n, 1);
   for (int cc = 0; cc < nc; cc++) {
     int c = reverse ? nc - 1 - cc : cc;
-    for (int mnode = 0; mnode < NL; mnode++) {
-      if (s->colour[lev][mnode] != c) continue;
-      int pi = pbase + mnode;
-      double rp = b[pi], cpp = 0.;
-      double S = 0., T = 0.;
-      for (int q = A->ptr[pi]; q < A->ptr[pi + 1]; q++) {
-        int j = A->col[q];
-        rp -= A->val[q] * x[j];
-        if (j == pi) cpp = A->val[q];
-      }
-      /* pass 1: Schur sums */
-      for (int q = A->ptr[pi]; q < A->ptr[pi + 1]; q++) {
-        int j = A->col[q];
-        if (j >= pbase) continue;
-        double r = b[j], a = 0., g = 0., al1 = 0.;
-        for (int qq = A->ptr[j]; qq < A->ptr[j + 1]; qq++) {
-          int cj = A->col[qq];
-          r -= A->val[qq] * x[cj];
-          if (cj == j) a = A->val[qq];
-          if (cj == pi) g = A->val[qq];
-          if (cj < pbase && cj != j) al1 += fabs(A->val[qq]);
+    const int t0 = s->col_off[lev][c], t1 = s->col_off[lev][c + 1];
+#pragma omp parallel
+    {
+      /* per star DOF of the patch: its diagonal (l1-modified) and its B^T coupling */
+      double sa[OR_MAXSTAR], sg[OR_MAXSTAR];
+#pragma omp for schedule(dynamic, 8)
+      for (int t = t0; t < t1; t++) {
+        const int mnode = s->col_items[lev][t];
+        int pi = pbase + mnode;
+        double rp = b[pi], cpp = 0.;
+        double S = 0., T = 0.;
+        for (int q = A->ptr[pi]; q < A->ptr[pi + 1]; q++) {
+          int j = A->col[q];
+          rp -= A->val[q] * x[j];
+          if (j == pi) cpp = A->val[q];
         }
-        if (l1) a = (a >= 0 ? a + 0.5 * al1 : a - 0.5 * al1);
-        S += A->val[q] * g / a;
-        T += A->val[q] * r / a;
-        dx[j] = r; /* keep the residual for pass 2 */
-        touched[j] = 1;
-      }
-      S -= cpp;
-      T -= rp;
-      double dp = (fabs(S) > 1e-300) ? T / S : 0.;
-      /* pass 2: velocity corrections */
-      for (int q = A->ptr[pi]; q < A->ptr[pi + 1]; q++) {
-        int j = A->col[q];
-        if (j >= pbase) continue;
-        double a = 0., g = 0., al1 = 0.;
-        for (int qq = A->ptr[j]; qq < A->ptr[j + 1]; qq++) {
-          int cj = A->col[qq];
-          if (cj == j) a = A->val[qq];
-          if (cj == pi) g = A->val[qq];
-          if (cj < pbase && cj != j) al1 += fabs(A->val[qq]);
+        /* pass 1: Schur sums */
+        int ns = 0;
+        for (int q = A->ptr[pi]; q < A->ptr[pi + 1]; q++) {
+          int j = A->col[q];
+          if (j >= pbase) continue;
+          double r = b[j], a = 0., g = 0., al1 = 0.;
+          for (int qq = A->ptr[j]; qq < A->ptr[j + 1]; qq++) {
+            int cj = A->col[qq];
+            r -= A->val[qq] * x[cj];
+            if (cj == j) a = A->val[qq];
+            if (cj == pi) g = A->val[qq];
+            if (cj < pbase && cj != j) al1 += fabs(A->val[qq]);
+          }
+          if (l1) a = (a >= 0 ? a + 0.5 * al1 : a - 0.5 * al1);
+          S += A->val[q] * g / a;
+          T += A->val[q] * r / a;
+          dx[j] = r; /* keep the residual for pass 2 */
+          touched[j] = 1;
+          sa[ns] = a;
+          sg[ns] = g;
+          ns++;
         }
-        if (l1) a = (a >= 0 ? a + 0.5 * al1 : a - 0.5 * al1);
-        dx[j] = omega * (dx[j] - g * dp) / a;
+        S -= cpp;
+        T -= rp;
+        double dp = (fabs(S) > 1e-300) ? T / S : 0.;
+        /* pass 2: velocity corrections */
+        ns = 0;
+        for (int q = A->ptr[pi]; q < A->ptr[pi + 1]; q++) {
+          int j = A->col[q];
+          if (j >= pbase) continue;
+          dx[j] = omega * (dx[j] - sg[ns] * dp) / sa[ns];
+          ns++;
+        }
+        dx[pi] = omega * dp;
+        touched[pi] = 1;
       }
-      dx[pi] = omega * dp;
-      touched[pi] = 1;
     }
+#pragma omp parallel for schedule(static)
     for (int i = 0; i < n; i++)
       if (touched[i]) {
         x[i] += dx[i];
@@ -1415,6 +1486,7 @@ static int coarse_factor(or_sys *s) {
         a[(size_t)p * n + j] = t;
       }
     double inv = 1. / a[(size_t)k * n + k];
+#pragma omp parallel for schedule(static) if (n - k > 64)
     for (int i = k + 1; i < n; i++) {
       double l = a[(size_t)i * n + k] * inv;
       a[(size_t)i * n + k] = l;
@@ -1452,7 +1524,24 @@ int or_coarse_solve(or_sys *s, const double *b, double *x) {
   return 0;
 }
 
-/* MGSolBase::MGStep (src/MGSolverBase.C:212-289) */
+/* One smoothing call of nsweeps sweeps that also returns the accuracy the reference's
+ * level solver reports (LaspackLinearSolverM::solve returns GetLastAccuracy(),
+ * contrib/matrix/laspack_linear_solverM.C:123-125): RTCResult stores ||r||/||b||
+ * (contrib/laspack/rtc.c:48-70), and the stationary iterations evaluate it on a residual
+ * they refresh only while Iter < MaxIter (SORForwIter, contrib/laspack/itersolv.c:850-894),
+ * so after nsweeps >= 1 sweeps it is the relative residual of the iterate before the last
+ * sweep; with no sweep, that of the iterate as given. */
+static double smooth_acc(or_sys *s, int L, const or_mg_params *p, int nsweeps, double *x, const double *b,
+                         double bn) {
+  if (nsweeps > 0) or_smooth(s, L, p, nsweeps - 1, x, b);
+  double acc = resid(s, L, x, b, s->r[L]) / bn;
+  if (nsweeps > 0) or_smooth(s, L, p, 1, x, b);
+  return acc;
+}
+
+/* MGSolBase::MGStep (src/MGSolverBase.C:212-289).  Returns the level's accuracy in the
+ * reference's sense (smooth_acc of the post-smoothing call; after the coarse solve, its
+ * relative residual), leaves r[L] = b - A x of the final iterate. */
 static double mg_step(or_sys *s, int L, const or_mg_params *p) {
   int top = s->nlev - 1;
   double *x = s->x[L], *b = s->b[L], *r = s->r[L];
@@ -1463,21 +1552,24 @@ static double mg_step(or_sys *s, int L, const or_mg_params *p) {
     return resid(s, 0, x, b, r) / bn;
   }
   int mul = (p->double_below_top && L < top) ? 2 : 1;
-  or_smooth(s, L, p, p->nu_pre * mul, x, b);
-  double rest = resid(s, L, x, b, r) / bn;
+  double rest = smooth_acc(s, L, p, p->nu_pre * mul, x, b, bn);
+  resid(s, L, x, b, r);
   matmul(&s->R[L - 1], r, s->b[L - 1]);
   memset(s->x[L - 1], 0, s->ndof[L - 1] * sizeof(double));
   double crest = 0.;
   for (int g = 0; g < p->gamma; g++) crest = mg_step(s, L - 1, p);
   matmul(&s->P[L], s->x[L - 1], r);
-  if (!p->cond_corr || crest < rest)
+  if (!p->cond_corr || crest < rest) /* the conditional correction of :262-263 */
     for (int i = 0; i < s->ndof[L]; i++) x[i] += p->corr_damp * r[i];
-  or_smooth(s, L, p, p->nu_post * mul, x, b);
-  return resid(s, L, x, b, r) / bn;
+  rest = smooth_acc(s, L, p, p->nu_post * mul, x, b, bn);
+  resid(s, L, x, b, r);
+  return rest;
 }
 
 /* MGSolBase::MGSolve (src/MGSolverBase.C:163-208): V-cycles until the relative
- * residual ||b-Ax||/||b|| reaches eps (stated stop test of the workloads). */
+ * residual ||b-Ax||/||b|| reaches eps (stop_test 0, the workloads' stated test), or
+ * until the top level's accuracy in the reference's sense falls below eps*(1+||b||)
+ * (stop_test 1, the exit test of :201).  hist holds the relative residual. */
 int or_mg_solve(or_sys *s, const or_mg_params *p, double *x, or_mg_stats *st) {
   int top = s->nlev - 1, n = s->ndof[top];
   memcpy(s->b[top], s->rhs, n * sizeof(double));
@@ -1486,17 +1578,20 @@ int or_mg_solve(or_sys *s, const or_mg_params *p, double *x, or_mg_stats *st) {
   st->bnorm = bn;
   st->converged = 0;
   st->cycles = 0;
+  st->last_acc = 0.;
   double rel = resid(s, top, s->x[top], s->b[top], s->r[top]) / (bn > 0 ? bn : 1.);
   st->rel_res = rel;
-  if (rel <= p->eps) st->converged = 1;
+  if (p->stop_test == 0 && rel <= p->eps) st->converged = 1;
   while (!st->converged && st->cycles < p->max_cycles) {
-    rel = mg_step(s, top, p);
+    double acc = mg_step(s, top, p);
+    rel = norm2(s->r[top], n) / (bn > 0 ? bn : 1.);
     gauge_shift(s, s->x[top]);
     if (st->cycles < 256) st->hist[st->cycles] = rel;
     st->cycles++;
     st->rel_res = rel;
+    st->last_acc = acc;
     if (!(rel == rel)) break;
-    if (rel <= p->eps) st->converged = 1;
+    if (p->stop_test == 1 ? acc < p->eps * (1. + bn) : rel <= p->eps) st->converged = 1;
   }
   memcpy(x, s->x[top], n * sizeof(double));
   return st->converged ? 0 : 1;

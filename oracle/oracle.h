@@ -3,8 +3,9 @@
  *
  * TEST INFRASTRUCTURE ONLY.  Nothing in the product library links or calls this
  * code; it is the checker used by tests/, by __graft_entry__.smoke() and by the
- * cpu_baseline leg of bench.py.  All arithmetic is FP64 and single-threaded, as the
- * reference's LASPACK path is (src/MGSolverBase.C:51-55).
+ * cpu_baseline leg of bench.py.  All arithmetic is FP64.  The reference's LASPACK path
+ * is single-process (src/MGSolverBase.C:51-55); here the independent items of one colour
+ * may run on several threads (or_set_threads) without changing any result.
  *
  * Parity anchors: the reference ships no golden vectors or asserting tests.  The
  * restatement is pinned (a) against the reference's own embedding tables and
@@ -47,6 +48,7 @@ typedef struct {
   double corr_damp;  /* coarse-correction factor (0.95 in the reference)          */
   int cond_corr;     /* 1 = reference's conditional correction                    */
   int reverse_colours; /* 1 = sweep colours in reverse order (adjoint)            */
+  int stop_test;     /* 0: ||b-Ax||/||b|| <= eps; 1: reference accuracy < eps(1+||b||) */
 } or_mg_params;
 
 typedef struct {
@@ -55,6 +57,7 @@ typedef struct {
   double rel_res;
   double bnorm;
   double hist[256];
+  double last_acc;   /* top-level accuracy of the last cycle in the reference's sense */
 } or_mg_stats;
 
 /* ------------------------------------------------------------------ mesh */
@@ -100,6 +103,14 @@ void or_sys_set_matrix(or_sys *s, int lev, const double *val);
 void or_sys_get_rhs(const or_sys *s, double *rhs);
 void or_sys_set_rhs(or_sys *s, const double *rhs);
 void or_sys_transpose_all(or_sys *s);
+
+/* -------------------------------------------------------------- threads */
+/* Loops over independent items of one colour (Vanka patches, Gauss-Seidel rows, assembly
+ * elements) and over matrix rows run on this many threads (OpenMP builds; 1 otherwise).
+ * Every item is computed by one thread in a fixed order and every reduction runs in row
+ * order, so results do not depend on the thread count. */
+void or_set_threads(int n);
+int or_get_threads(void);
 
 /* -------------------------------------------------------------- solvers */
 void or_spmv(const or_sys *s, int lev, const double *x, double *y);

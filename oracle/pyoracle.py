@@ -30,12 +30,12 @@ class OrMgParams(C.Structure):
     _fields_ = [("eps", C.c_double), ("max_cycles", C.c_int), ("gamma", C.c_int),
                 ("nu_pre", C.c_int), ("nu_post", C.c_int), ("double_below_top", C.c_int),
                 ("smoother", C.c_int), ("omega", C.c_double), ("corr_damp", C.c_double),
-                ("cond_corr", C.c_int), ("reverse_colours", C.c_int)]
+                ("cond_corr", C.c_int), ("reverse_colours", C.c_int), ("stop_test", C.c_int)]
 
 
 class OrMgStats(C.Structure):
     _fields_ = [("cycles", C.c_int), ("converged", C.c_int), ("rel_res", C.c_double),
-                ("bnorm", C.c_double), ("hist", C.c_double * 256)]
+                ("bnorm", C.c_double), ("hist", C.c_double * 256), ("last_acc", C.c_double)]
 
 
 def oracle_lib():
@@ -86,6 +86,8 @@ def oracle_lib():
         L.or_mg_solve.restype = I
         L.or_coarse_solve.argtypes = [P, dp, dp]
         L.or_smooth.argtypes = [P, I, C.POINTER(OrMgParams), I, dp, dp]
+        L.or_set_threads.argtypes = [I]
+        L.or_get_threads.restype = I
         L.or_fe_tables.argtypes = [I, dp, dp, dp, dp]
         L.or_side_table.argtypes = [I, ip]
         _LIB = L
@@ -321,3 +323,12 @@ class Laspack:
         self.L.lpb_sorforw(len(rp) - 1, rp, col, val, np.ascontiguousarray(b, np.float64), x, nsweeps, omega,
                            C.byref(acc))
         return x, acc.value
+
+
+def set_threads(n):
+    """Threads of the oracle's parallel loops (results do not depend on the count)."""
+    oracle_lib().or_set_threads(int(n))
+
+
+def get_threads():
+    return int(oracle_lib().or_get_threads())

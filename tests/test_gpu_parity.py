@@ -157,6 +157,40 @@ def test_multigrid_fp64_matches_oracle_per_cycle(case, oracle_mod, vk):
     assert rel(gs.x(), xo) < 1e-9
 
 
+@pytest.mark.parametrize("cond,stop", [(1, 0), (0, 1), (1, 1)])
+def test_reference_correction_and_stop_test_match_oracle(case, oracle_mod, cond, stop):
+    """The reference's conditional coarse correction (src/MGSolverBase.C:262-263) and its
+    exit test rest < Eps(1 + ||b||) (:201), with every level's accuracy taken as LASPACK
+    reports it (the relative residual before the last sweep of a smoothing call): the
+    same cycle count, per-cycle relative residuals and top-level accuracies within 1e-6,
+    and the same solution as the oracle.  Near convergence the conditional correction
+    stops adding the coarse correction, so the cycle count is capped."""
+    _assemble_both(case)
+    gs, os_ = case["gs"], case["os"]
+    ns = case["kind"] == 1
+    nu = (3, 3) if ns else (2, 2)
+    kw = dict(eps=1e-11, max_cycles=30, nu_pre=nu[0], nu_post=nu[1], omega=0.4, cond_corr=cond)
+    gp = ex.mg_params(smoother=_lib.SMOOTH_VANKA if ns else _lib.SMOOTH_GS, stop_test=stop, **kw)
+    op = or_mg(oracle_mod, smoother=1 if ns else 0, stop_test=stop, **kw)
+    x0 = case["xold"]
+    gs.set_x(x0)
+    st = gs.solve(gp)
+    xo, sto = os_.mg_solve(op, x0=x0)
+    assert st.cycles == sto.cycles and bool(st.converged) == bool(sto.converged)
+    hist_g = np.array(st.hist[:st.cycles])
+    hist_o = np.array(sto.hist[:sto.cycles])
+    assert np.all(np.abs(hist_g - hist_o) <= 1e-6 * hist_o + 1e-14), (hist_g, hist_o)
+    assert abs(st.last_acc - sto.last_acc) <= 1e-6 * sto.last_acc + 1e-14
+    assert rel(gs.x(), xo) < 1e-9
+    # the same options in mixed precision run; without the conditional correction they
+    # converge, with it they stall as the FP64 cycles do
+    gs.set_x(x0)
+    st32 = gs.solve(ex.mg_params(smoother=_lib.SMOOTH_VANKA if ns else _lib.SMOOTH_GS, stop_test=stop,
+                                 precision=_lib.PREC_MIXED, **kw))
+    assert st32.cycles >= 1 and np.isfinite(st32.rel_res)
+    assert st32.rel_res < (1e-9 if not cond else 1.01 * st32.hist[0])
+
+
 @pytest.mark.parametrize("vk", VK)
 def test_mixed_precision_matches_fp64_oracle(case, oracle_mod, vk):
     _assemble_both(case)

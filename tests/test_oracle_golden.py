@@ -231,3 +231,66 @@ def test_oracle_vanka_mg_cavity_small(oracle_mod):
     s.assemble_all(or_phys(oracle_mod, inv_re=1 / 400.), xold=xold)
     xs, st = s.mg_solve(or_mg(oracle_mod, smoother=1, nu_pre=3, nu_post=3, max_cycles=60), x0=xold)
     assert st.converged
+
+
+def _upwind_f(up, rho, mod, h, diff):
+    """f_upwind of the NS volume terms (template_appl/nse/SRC/MGSolverNS.C:336-339)."""
+    pe = 0.5 * mod * h / diff
+    return up * rho * 0.5 * (1.0 / np.tanh(pe) - 1.0 / pe) * h / mod
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+def test_ns_operator_reproduces_quadratic_flow(oracle_mod, dim):
+    """Manufactured solution for the Navier-Stokes volume terms (MGSolverNS.C:401-489).
+
+    Velocity u = (y^2, x^2) in 2D, (y^2, z^2, x^2) in 3D (divergence-free, exactly in the
+    Q2 space), pressure p = x + 2y (+ 3z) (exactly in the Q1 space), advecting field
+    v = x_old = (1, 0, 0), natural flags everywhere (no boundary terms).  For a row whose
+    test function vanishes on the boundary, the weak form integrates by parts to
+    int phi_i [ v.grad u_a - sum_k (nu + f_k v_k^2) d_kk u_a - (nu + f_a v_a^2) d_aa u_a
+               - sum_{b != a} (nu + f_a v_a v_b) d_ab u_b + d_a p ]
+    and every bracket is affine in x, so on a uniform mesh the row equals the bracket at
+    the node times int phi_i (1D weights h/3 at vertices, 2h/3 at midpoints).  Every
+    pressure row is int psi_m div u = 0."""
+    nu = 0.01
+    if dim == 2:
+        n0, box, nlev = (4, 4), (0, 1, 0, 1), 2
+    else:
+        n0, box, nlev = (3, 2, 2), (0, 1.5, 0, 1, 0, 1), 2
+    m = oracle_mod.OrMesh(dim, nlev, n0, box)
+    s = oracle_mod.OrSys(m, 1)
+    top = nlev - 1
+    n, N, NL = s.ndof(top), m.nnodes(top), m.nnodes(top - 1)
+    X = m.xyz()
+    h = [(box[2 * d + 1] - box[2 * d]) / (n0[d] << top) for d in range(dim)]
+    xold = np.zeros(n)
+    xold[:N] = 1.0  # v = (1, 0, 0)
+    s.assemble(top, 1, or_phys(oracle_mod, inv_re=nu), xold=xold)
+    A = sp.csr_matrix((s.matrix(top), s.pattern(top)[1], s.pattern(top)[0]), shape=(n, n))
+    x = np.zeros(n)
+    if dim == 2:
+        x[:N], x[N:2 * N] = X[1] ** 2, X[0] ** 2
+        x[2 * N:] = X[0][:NL] + 2 * X[1][:NL]
+    else:
+        x[:N], x[N:2 * N], x[2 * N:3 * N] = X[1] ** 2, X[2] ** 2, X[0] ** 2
+        x[3 * N:] = X[0][:NL] + 2 * X[1][:NL] + 3 * X[2][:NL]
+    y = A @ x
+    fx = _upwind_f(0.1, 1.0, 1.0, h[0], nu)
+    lat = m.lattice()[:N]
+    interior = np.ones(N, bool)
+    W = np.ones(N)
+    for d in range(dim):
+        k = np.rint((X[d] - box[2 * d]) / (h[d] / 2)).astype(int)
+        interior &= (k > 0) & (k < 2 * (n0[d] << top))
+        W *= np.where(k % 2 == 0, h[d] / 3, 2 * h[d] / 3)
+    assert lat.shape[0] == N
+    xi = X[0]
+    if dim == 2:
+        expect = [W * (-2 * nu + 1.0), W * (2 * xi - 2 * (nu + fx) + 2.0)]
+    else:
+        expect = [W * (-2 * nu + 1.0), W * (-2 * nu + 2.0), W * (2 * xi - 2 * (nu + fx) + 3.0)]
+    for a in range(dim):
+        got = y[a * N:(a + 1) * N][interior]
+        ref = expect[a][interior]
+        assert np.abs(got - ref).max() <= 1e-12 * np.abs(ref).max(), (a, np.abs(got - ref).max())
+    assert np.abs(y[dim * N:]).max() <= 1e-13 * np.abs(y[:dim * N]).max()

@@ -26,7 +26,7 @@ def _static_resid(L, sys, lev, x, b):
     return rc, tr.cpu().numpy(), float(tn.cpu().item())
 
 
-@pytest.mark.parametrize("kind", ["heat", "ns2d", "ns3d"])
+@pytest.mark.parametrize("kind", ["heat", "heat3d", "ns2d", "ns3d"])
 def test_static_resid_matches_allocating_entry_point(kind):
     import exfemus_b200 as ex
     from exfemus_b200 import _lib
@@ -36,6 +36,11 @@ def test_static_resid_matches_allocating_entry_point(kind):
         s = ex.MGSolT(m)
         s.GenBc(_lib.BC_HEAT_DIRICHLET)
         s.set_source(np.ones(m.nel(2)))
+    elif kind == "heat3d":
+        m = ex.Mesh(3, 2, (2, 2, 2), (0, 1, 0, 1, 0, 1))
+        s = ex.MGSolT(m)
+        s.GenBc(_lib.BC_HEAT_DIRICHLET)
+        s.set_source(np.ones(m.nel(1)))
     elif kind == "ns2d":
         m = ex.Mesh(2, 3, (4, 4), (0, 1, 0, 1))
         s = ex.MGSolNS(m)
@@ -72,3 +77,22 @@ def test_static_resid_rejects_bad_calls():
     x = np.zeros(s.ndof(0))
     rc, _, _ = _static_resid(L, s, 0, x, x)
     assert rc == _lib.EXF_ERR_STATE  # not assembled yet
+
+
+def test_static_resid_rejects_levels_above_the_array():
+    """A level needing more partial sums than the fixed array holds is refused with
+    EXF_ERR_ARG before any launch: 1025 x 1025 Q2 nodes at 8 lanes per row need 32,833
+    blocks of 256 threads, one more than 32,768 would allow."""
+    import exfemus_b200 as ex
+    from exfemus_b200 import _lib
+    L = _lib.load()
+    m = ex.Mesh(2, 1, (512, 512), (0, 1, 0, 1))
+    s = ex.MGSolT(m)
+    s.GenBc(_lib.BC_HEAT_DIRICHLET)
+    s.assemble_all()
+    n = s.ndof(0)
+    assert n == 1025 * 1025 and (n * 8 + 255) // 256 > 32768
+    x = np.zeros(n)
+    rc, _, _ = _static_resid(L, s, 0, x, x)
+    assert rc == _lib.EXF_ERR_ARG
+    assert b"static array holds 32768" in L.exf_last_error()
