@@ -42,11 +42,17 @@ class ExfMeshDesc(C.Structure):
                 ("device", C.c_int)]
 
 
+class ExfMeshData(C.Structure):
+    _fields_ = [("dim", C.c_int), ("nlev", C.c_int), ("device", C.c_int), ("nnodes", C.c_void_p),
+                ("nvert0", C.c_int), ("xyz", C.c_void_p), ("nel", C.c_void_p), ("conn", C.c_void_p),
+                ("neigh", C.c_void_p), ("parent", C.c_void_p)]
+
+
 class ExfPhys(C.Structure):
     _fields_ = [("inv_re", C.c_double), ("inv_prdl", C.c_double), ("rho", C.c_double),
                 ("rhocp", C.c_double), ("inv_dt", C.c_double), ("penalty", C.c_double),
                 ("upwind_ns", C.c_double), ("upwind_t", C.c_double), ("ifr", C.c_double),
-                ("dirg", C.c_double * 3), ("buoy", C.c_double)]
+                ("dirg", C.c_double * 3), ("buoy", C.c_double), ("traction", C.c_double)]
 
 
 class ExfMgParams(C.Structure):
@@ -54,7 +60,8 @@ class ExfMgParams(C.Structure):
                 ("nu_pre", C.c_int), ("nu_post", C.c_int), ("double_below_top", C.c_int),
                 ("smoother", C.c_int), ("omega", C.c_double), ("corr_damp", C.c_double),
                 ("cond_corr", C.c_int), ("reverse_colours", C.c_int), ("precision", C.c_int),
-                ("use_graph", C.c_int), ("vanka_kernel", C.c_int), ("stop_test", C.c_int)]
+                ("use_graph", C.c_int), ("vanka_kernel", C.c_int), ("stop_test", C.c_int),
+                ("fp32_blocks", C.c_int)]
 
 
 class ExfSolveStats(C.Structure):
@@ -128,6 +135,9 @@ SIGNATURES = [
     ("exf_launch_count", C.c_longlong, []),
     ("exf_level_bytes", _I, [_P, _I, _I, _DP, _DP]),
     ("exf_resid_norm_static", _I, [_P, _I, _P, _P, _P, _P]),
+    ("exf_mesh_upload", _I, [C.POINTER(ExfMeshData), C.POINTER(_P)]),
+    ("exf_sys_set_transfer", _I, [_P, _I, _I, _I, _IP, _IP, _IP, _DP]),
+    ("exf_sys_check_pattern", _I, [_P, _I, _I, _IP, _IP, _IP]),
 ]
 
 

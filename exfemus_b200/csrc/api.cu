@@ -7,8 +7,11 @@
 // relative residual ||b-Ax||/||b|| of the top level.  Mixed precision: the residual,
 // solution update and coarse solve are FP64; the V-cycle (smoother, residuals, transfers)
 // runs on FP32 copies of the level matrices (defect correction).
+#include <algorithm>
+#include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstddef>
 #include <cstring>
 #include <vector>
 
@@ -444,8 +447,10 @@ int exf_sys_create(exf_mesh *m, int kind, exf_sys **out) {
 int exf_sys_destroy(exf_sys *s) {
   if (!s) return EXF_OK;
   cudaSetDevice(s->mesh->device);
-  for (int k = 0; k < 2; k++)
+  for (int k = 0; k < 2; k++) {
     if (s->graph[k]) cudaGraphExecDestroy(s->graph[k]);
+    if (s->loop_graph[k]) cudaGraphExecDestroy(s->loop_graph[k]);
+  }
   if (s->stream) cudaStreamSynchronize(s->stream);
   s->L.clear();
   for (int k = 0; k < 8; k++)
@@ -482,12 +487,26 @@ int exf_sys_bc_preset(exf_sys *s, int preset) {
     set_error("unknown bc preset %d", preset);
     return EXF_ERR_ARG;
   }
+  // pressure gauge node of the enclosed-flow presets: node 0 of a generated box (its
+  // corner (x0, y0, z0)); on an uploaded mesh the pressure node first in (z, y, x) order
+  // of the coordinates, the same physical node whatever the numbering
+  int gauge = 0;
+  if (!m->lattice && s->nv1) gauge = node_zyx_order(m, T.NL)[0];
+  // walls: lattice planes of a generated box; for uploaded meshes the faces of the
+  // coordinate bounding box (within 1e-10 of its extent)
   for (int n = 0; n < m->ntop; n++) {
-    const int *p = &m->lat[3 * n];
     int lo[3], hi[3], onb = 0;
     for (int d = 0; d < 3; d++) {
-      lo[d] = d < dim && p[d] == 0;
-      hi[d] = d < dim && p[d] == m->L[d] - 1;
+      if (m->lattice) {
+        const int *p = &m->lat[3 * n];
+        lo[d] = d < dim && p[d] == 0;
+        hi[d] = d < dim && p[d] == m->L[d] - 1;
+      } else {
+        const double x = d < dim ? m->xyz[(size_t)n + (size_t)d * m->ntop] : 0.;
+        const double tol = 1e-10 * std::max(m->box[2 * d + 1] - m->box[2 * d], 1e-300);
+        lo[d] = d < dim && fabs(x - m->box[2 * d]) <= tol;
+        hi[d] = d < dim && fabs(x - m->box[2 * d + 1]) <= tol;
+      }
       onb |= lo[d] | hi[d];
     }
     if (!onb) continue;  // interior nodes keep (1,1) (bc_intern_read)
@@ -505,7 +524,7 @@ int exf_sys_bc_preset(exf_sys *s, int preset) {
           if (quad) {
             b0 = 0;
             b1 = (v == 0 && hi[1] && !lo[0] && !hi[0]) ? 4 : 0;
-          } else if (n == 0) {
+          } else if (n == gauge) {
             b0 = 0;  // pressure gauge node
           }
           break;
@@ -522,7 +541,7 @@ int exf_sys_bc_preset(exf_sys *s, int preset) {
           if (quad) {
             b0 = 0;
             b1 = 0;
-          } else if (n == 0) {
+          } else if (n == gauge) {
             b0 = 0;
           }
           break;
@@ -600,12 +619,59 @@ static void expand_transfer(const exf_sys *s, const Transfer &Tq, const Transfer
     }
 }
 
+int exf_sys_set_transfer(exf_sys *s, int lev, int kind, int block, const int dim[2], const int *len, const int *pos,
+                         const double *val) {
+  CHECK_LEV(s, lev);
+  return set_transfer(s, lev, kind, block, dim, len, pos, val);
+}
+
+int exf_sys_check_pattern(exf_sys *s, int lev, int block, const int dim[2], const int *len, const int *pos) {
+  CHECK_LEV(s, lev);
+  SysLevel &L = s->L[lev];
+  if (!dim || !len || !pos || (block != 22 && block != 21 && block != 12 && block != 11) ||
+      (block != 22 && !s->nv1)) {
+    set_error("exf_sys_check_pattern: bad argument");
+    return EXF_ERR_ARG;
+  }
+  const bool qrow = block / 10 == 2, qcol = block % 10 == 2;
+  const int nrow = qrow ? L.N : L.NL, ncol = qcol ? L.N : L.NL;
+  if (dim[0] != nrow || dim[1] != ncol) {
+    set_error("exf_sys_check_pattern: block %d is %dx%d, level %d has %dx%d", block, dim[0], dim[1], lev, nrow, ncol);
+    return EXF_ERR_ARG;
+  }
+  std::vector<int> p(L.N + 1), c(qcol ? L.nqq : L.nql);
+  EXF_CUDA(cudaMemcpy(p.data(), qcol ? L.qq_ptr.p : L.ql_ptr.p, (L.N + 1) * sizeof(int), cudaMemcpyDeviceToHost));
+  EXF_CUDA(cudaMemcpy(c.data(), qcol ? L.qq_col.p : L.ql_col.p, c.size() * sizeof(int), cudaMemcpyDeviceToHost));
+  std::vector<int> row;
+  for (int i = 0; i < nrow; i++) {  // the pressure rows of node m use the node's lists
+    if (len[i + 1] < len[i]) {
+      set_error("exf_sys_check_pattern: row offsets decrease at row %d", i);
+      return EXF_ERR_ARG;
+    }
+    row.assign(pos + len[i], pos + len[i + 1]);
+    std::sort(row.begin(), row.end());
+    if (row.size() != (size_t)(p[i + 1] - p[i]) || !std::equal(row.begin(), row.end(), c.begin() + p[i])) {
+      set_error("exf_sys_check_pattern: block %d row %d differs from the element couplings (%zu entries, %d built)",
+                block, i, row.size(), p[i + 1] - p[i]);
+      return EXF_ERR_ARG;
+    }
+  }
+  return EXF_OK;
+}
+
+static int need_transfers(const exf_sys *s) {
+  if (transfers_ready(s)) return EXF_OK;
+  set_error("the transfer operators are not set (exf_sys_set_transfer for every level and block)");
+  return EXF_ERR_STATE;
+}
+
 int exf_sys_get_prol(exf_sys *s, int lev, long *nnz, int *rowptr, int *col, double *val) {
   CHECK_LEV(s, lev);
   if (lev == 0) {
     set_error("no prolongation into level 0");
     return EXF_ERR_ARG;
   }
+  EXF_TRY(need_transfers(s));
   const SysLevel &F = s->L[lev], &C = s->L[lev - 1];
   std::vector<int> p, c;
   std::vector<double> v;
@@ -623,6 +689,7 @@ int exf_sys_get_rest(exf_sys *s, int lev, long *nnz, int *rowptr, int *col, doub
     set_error("no restriction from above the top level");
     return EXF_ERR_ARG;
   }
+  EXF_TRY(need_transfers(s));
   const SysLevel &C = s->L[lev], &F = s->L[lev + 1];
   std::vector<double> mask(C.ndof);
   EXF_CUDA(cudaMemcpyAsync(mask.data(), C.rmask.p, C.ndof * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
@@ -714,15 +781,6 @@ int exf_gen_mat_rhs(exf_sys *s, const exf_phys *ph, int lev, int mode) {
   CHECK_LEV(s, lev);
   if (!ph || (mode != 0 && mode != 1)) return EXF_ERR_ARG;
   if (s->kind == EXF_KIND_NS && s->mesh->dim == 3 && s->nv2 != 3) return EXF_ERR_STATE;
-  // a natural side with nonzero NS boundary flag would need the Neumann branch
-  if (s->kind == EXF_KIND_NS) {
-    const SysLevel &T = s->L[s->nlev - 1];
-    for (size_t i = 0; i < (size_t)s->nv2 * T.N; i++)
-      if (s->bc0[i] != 0 && s->bc1[i] != 0 && s->bc1[i] != 1) {
-        set_error("NS Neumann/traction flags are not supported (dof %zu flag %d)", i, s->bc1[i]);
-        return EXF_ERR_UNSUPPORTED;
-      }
-  }
   EXF_TRY(assemble_level(s, ph, lev, mode));
   EXF_TRY(sync_fp32(s, lev));
   if (lev == 0) s->coarse_ok = 0;
@@ -800,6 +858,7 @@ static unsigned long long params_key(const exf_mg_params *p) {
   mix((unsigned long long)p->vanka_kernel);
   mix((unsigned long long)p->cond_corr);
   mix((unsigned long long)p->stop_test);
+  mix((unsigned long long)p->fp32_blocks);
   return h | 1ull;
 }
 
@@ -841,6 +900,99 @@ static int cycle_graph(exf_sys *s, const exf_mg_params *p, double *dnr) {
   return EXF_OK;
 }
 
+// The check at the end of every device-loop iteration: record the cycle's relative
+// residual, apply the stop test and set the WHILE condition (continue while not converged,
+// finite and below max_cycles).
+__global__ void k_cycle_check(cudaGraphConditionalHandle h, LoopDev *st, const double *r2, const double *acc2) {
+  const double rel = sqrt(*r2) / st->den;
+  const int c = st->cycles;
+  if (c < 256) st->hist[c] = rel;
+  st->cycles = c + 1;
+  st->rel = rel;
+  const double acc = (acc2 && !st->mixed) ? sqrt(*acc2) / st->den : rel;
+  st->last_acc = acc;
+  const bool done = st->ref_stop ? acc < st->lim : rel <= st->lim;
+  const bool go = isfinite(rel) && !done && c + 1 < st->max_cycles;
+  cudaGraphSetConditional(h, go ? 1u : 0u);
+}
+
+// Cycles until convergence inside one graph launch: a conditional WHILE node whose body is
+// the captured V-cycle followed by k_cycle_check.  Returns EXF_ERR_UNSUPPORTED (and never
+// tries again for this system) when the runtime does not build such a graph; the caller
+// then loops on the host.
+static int cycle_body(exf_sys *s, const exf_mg_params *p, double *dnr);
+static unsigned long long params_key(const exf_mg_params *p);
+static int device_loop(exf_sys *s, const exf_mg_params *p, exf_solve_stats *st, double den, double lim,
+                       bool ref_stop, double *dnr) {
+  const int gi = p->precision == EXF_PREC_MIXED ? 1 : 0;
+  const unsigned long long key = params_key(p);
+  if (!s->loop_dev.p) EXF_TRY(s->loop_dev.alloc(1));
+  if (!s->loop_graph[gi] || s->loop_key[gi] != key || s->loop_epoch[gi] != s->buf_epoch) {
+    if (s->loop_graph[gi]) {
+      cudaGraphExecDestroy(s->loop_graph[gi]);
+      s->loop_graph[gi] = nullptr;
+    }
+    cudaGraph_t g = nullptr;
+    cudaGraphConditionalHandle h;
+    cudaGraphNodeParams np = {};
+    cudaGraphNode_t node;
+    bool ok = cudaGraphCreate(&g, 0) == cudaSuccess &&
+              cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault) == cudaSuccess;
+    if (ok) {
+      np.type = cudaGraphNodeTypeConditional;
+      np.conditional.handle = h;
+      np.conditional.type = cudaGraphCondTypeWhile;
+      np.conditional.size = 1;
+      ok = cudaGraphAddNode(&node, g, nullptr, 0, &np) == cudaSuccess;
+    }
+    cudaGraph_t body = ok ? np.conditional.phGraph_out[0] : nullptr;
+    const long long c0 = exf_launch_count();
+    if (ok) ok = cudaStreamBeginCaptureToGraph(s->stream, body, nullptr, nullptr, 0,
+                                               cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+    int rc = EXF_OK;
+    if (ok) {
+      rc = cycle_body(s, p, dnr);
+      if (rc == EXF_OK) {
+        const double *acc2 = needs_acc(p) ? s->mg_acc.p + 4 * (s->nlev - 1) + 2 : nullptr;
+        k_cycle_check<<<1, 1, 0, s->stream>>>(h, s->loop_dev.p, dnr, acc2);
+        count_launch(1);
+      }
+      cudaGraph_t cap = body;
+      ok = cudaStreamEndCapture(s->stream, &cap) == cudaSuccess && rc == EXF_OK;
+    }
+    s->loop_launches[gi] = exf_launch_count() - c0;
+    count_launch(-(int)s->loop_launches[gi]);  // captured, not executed
+    if (ok) ok = cudaGraphInstantiate(&s->loop_graph[gi], g, 0) == cudaSuccess;
+    if (g) cudaGraphDestroy(g);
+    cudaGetLastError();
+    if (rc != EXF_OK) return rc;
+    if (!ok) {
+      s->loop_graph[gi] = nullptr;
+      s->loop_unavailable = 1;
+      return EXF_ERR_UNSUPPORTED;
+    }
+    s->loop_key[gi] = key;
+    s->loop_epoch[gi] = s->buf_epoch;
+  }
+  LoopDev hd = {};
+  hd.den = den;
+  hd.lim = lim;
+  hd.max_cycles = p->max_cycles;
+  hd.cycles = st->cycles;
+  hd.ref_stop = ref_stop ? 1 : 0;
+  hd.mixed = p->precision == EXF_PREC_MIXED ? 1 : 0;
+  EXF_CUDA(cudaMemcpyAsync(s->loop_dev.p, &hd, offsetof(LoopDev, hist), cudaMemcpyHostToDevice, s->stream));
+  EXF_CUDA(cudaGraphLaunch(s->loop_graph[gi], s->stream));
+  EXF_CUDA(cudaMemcpyAsync(&hd, s->loop_dev.p, sizeof(LoopDev), cudaMemcpyDeviceToHost, s->stream));
+  EXF_CUDA(cudaStreamSynchronize(s->stream));
+  count_launch((int)(s->loop_launches[gi] * (hd.cycles - st->cycles)));
+  for (int c = st->cycles; c < hd.cycles && c < 256; c++) st->hist[c] = hd.hist[c];
+  st->cycles = hd.cycles;
+  st->rel_res = hd.rel;
+  st->last_acc = hd.last_acc;
+  return EXF_OK;
+}
+
 static int read_scalar(exf_sys *s, const double *d, double *h) {
   EXF_CUDA(cudaMemcpyAsync(h, d, sizeof(double), cudaMemcpyDeviceToHost, s->stream));
   EXF_CUDA(cudaStreamSynchronize(s->stream));
@@ -854,6 +1006,7 @@ int exf_mg_solve(exf_sys *s, const exf_mg_params *p, exf_solve_stats *st) {
     set_error("exf_mg_solve before assembly");
     return EXF_ERR_STATE;
   }
+  EXF_TRY(need_transfers(s));
   if (p->gamma < 1 || p->nu_pre < 0 || p->nu_post < 0 || p->max_cycles < 0 ||
       (p->stop_test != EXF_STOP_RELRES && p->stop_test != EXF_STOP_REFERENCE))
     return EXF_ERR_ARG;
@@ -893,8 +1046,24 @@ int exf_mg_solve(exf_sys *s, const exf_mg_params *p, exf_solve_stats *st) {
     done = true;  // skip the cycle loop
   }
   while (!done && st->cycles < p->max_cycles) {
-    // the first cycle runs eagerly (it sizes every scratch buffer); later cycles replay a
-    // captured CUDA graph of the whole cycle when use_graph is set
+    // the first cycle runs eagerly (it sizes every scratch buffer); with use_graph the
+    // later cycles run on the device until the stop test holds (one graph launch, no host
+    // read per cycle), or, where the runtime cannot build that graph, replay a captured
+    // graph of one cycle per host iteration
+    if (p->use_graph && st->cycles > 0 && !s->loop_unavailable) {
+      const int lrc = device_loop(s, p, st, den, lim, ref_stop, dnr);
+      if (lrc == EXF_OK) {
+        rel = st->rel_res;
+        if (!std::isfinite(rel)) {
+          rc = EXF_ERR_DIVERGED;
+          set_error("multigrid diverged at cycle %d", st->cycles);
+          break;
+        }
+        done = ref_stop ? st->last_acc < lim : rel <= p->eps;
+        continue;
+      }
+      if (lrc != EXF_ERR_UNSUPPORTED) return lrc;
+    }
     if (p->use_graph && st->cycles > 0) {
       EXF_TRY(cycle_graph(s, p, dnr));
     } else {
@@ -948,6 +1117,7 @@ int exf_resid(exf_sys *s, int lev, const double *x, const double *b, double *r) 
 int exf_restrict(exf_sys *s, int lev, const double *r_fine, double *b_coarse) {
   CHECK_LEV(s, lev);
   if (lev >= s->nlev - 1) return EXF_ERR_ARG;
+  EXF_TRY(need_transfers(s));
   SysLevel &C = s->L[lev], &F = s->L[lev + 1];
   DBuf<double> df, dc;
   EXF_TRY(df.alloc(F.ndof));
@@ -960,6 +1130,7 @@ int exf_restrict(exf_sys *s, int lev, const double *r_fine, double *b_coarse) {
 int exf_prolong(exf_sys *s, int lev, const double *x_coarse, double *y_fine) {
   CHECK_LEV(s, lev);
   if (lev == 0) return EXF_ERR_ARG;
+  EXF_TRY(need_transfers(s));
   SysLevel &F = s->L[lev], &C = s->L[lev - 1];
   DBuf<double> df, dc;
   EXF_TRY(df.alloc(F.ndof));
@@ -1027,6 +1198,7 @@ int exf_time_op(exf_sys *s, int what, int lev, const exf_mg_params *p, const exf
   if (!p || !avg_ms || reps < 1) return EXF_ERR_ARG;
   if (what == 2 && !ph) return EXF_ERR_ARG;
   if (what != 2 && !s->assembled) return EXF_ERR_STATE;
+  if (what == 3) EXF_TRY(need_transfers(s));
   if (!s->coarse_ok && what == 3) EXF_TRY(coarse_factor(s));
   SysLevel &L = s->L[lev];
   const bool f32 = p->precision == EXF_PREC_MIXED;

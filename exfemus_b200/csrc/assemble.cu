@@ -42,6 +42,7 @@ struct FETab {
   double sw[FE<DIM>::NSQ];
   double sphi[FE<DIM>::NSQ][FE<DIM>::NSN];
   double sdphi[FE<DIM>::NSQ][FE<DIM>::NSN][DIM - 1];
+  double spsi[FE<DIM>::NSQ][DIM == 2 ? 2 : 4];  // linear shapes on the side's vertices
 };
 
 static double lag1(int a, double x) {
@@ -120,6 +121,11 @@ static void fill_tab(FETab<DIM> &t) {
         double dv = 1.;
         for (int d = 0; d < sdim; d++) dv *= (d == k) ? dlag1(abc[d], xi[d]) : lag1(abc[d], xi[d]);
         t.sdphi[q][s][k] = dv;
+      }
+      if (s < (sdim == 1 ? 2 : 4)) {  // vertices come first on a side
+        double w = 1.;
+        for (int d = 0; d < sdim; d++) w *= lin1(abc[d], xi[d]);
+        t.spsi[q][s] = w;
       }
     }
   }
@@ -438,8 +444,28 @@ __global__ void __launch_bounds__(NT, DIM == 3 ? EXF_ASM_MINB3 : EXF_ASM_MINB2) 
     const int last = sur[F::NSN - 1];
     const double det = jac_sur<DIM>(t, F::NSQ - 1, s_xx, sur);
     const double ipen = det * ph.penalty;
-    double nrm[3];
-    for (int d = 0; d < 3; d++) nrm[d] = (double)A.side.dir[sd][d];
+    // MGFE::normal_g (src/MGFE.C:1601-1646): 2D the tangent from side node 0 to 1 turned
+    // clockwise, 3D (x1 - x0) x (x3 - x0), normalised
+    double nrm[3] = {0., 0., 0.};
+    {
+      double t1[3] = {0., 0., 0.}, t3[3] = {0., 0., 0.};
+      for (int d = 0; d < DIM; d++) {
+        t1[d] = s_xx[d][sur[1]] - s_xx[d][sur[0]];
+        if (DIM == 3) t3[d] = s_xx[d][sur[3]] - s_xx[d][sur[0]];
+      }
+      if (DIM == 2) {
+        nrm[0] = t1[1];
+        nrm[1] = -t1[0];
+      } else {
+        nrm[0] = t1[1] * t3[2] - t1[2] * t3[1];
+        nrm[1] = t1[2] * t3[0] - t1[0] * t3[2];
+        nrm[2] = t1[0] * t3[1] - t1[1] * t3[0];
+      }
+      double mm = 0.;
+      for (int d = 0; d < DIM; d++) mm += nrm[d] * nrm[d];
+      mm = sqrt(mm);
+      for (int d = 0; d < DIM; d++) nrm[d] /= mm;
+    }
     for (int p = tid; p < nv2 * F::NSN; p += NT) {
       const int a = p / F::NSN, k = p % F::NSN;
       const int lv = sur[k];
@@ -465,6 +491,39 @@ __global__ void __launch_bounds__(NT, DIM == 3 ? EXF_ASM_MINB3 : EXF_ASM_MINB2) 
                 ((1 - bc_n) * (1 - bc_tg) * s_uold[a][lv] + bc_n * vdn * nrm[a] +
                  bc_tg * (s_uold[a][lv] - vdn * nrm[a]));
         }
+      } else if (ns && s_bcb[a][last] != 0) {
+        // Neumann / Robin sides (template_appl/nse/SRC/MGSolverNS.C:604-681), alpha_t = 1:
+        // row (a, lv) takes, per surface Gauss point, the tangential / normal Robin term
+        // lumped on its diagonal, the normal-normal coupling to the later components and,
+        // with phys.traction (the reference's MESHNUMBER == 1), the pressure traction
+        // -n_a p_old phi
+        constexpr int NVB = DIM == 2 ? 2 : 4;
+        const int bs = s_bcb[a][lv];
+        const int bc_rhs = (bs & 4) >> 2, bc_tg = (bs & 2) >> 1, bc_n = bs % 2;
+        const int bcv2 = s_bcv[a][lv] % 2;
+        double diag = 0., fr = 0.;
+        for (int q = 0; q < F::NSQ; q++) {
+          const double dt = jac_sur<DIM>(t, q, s_xx, sur) * t->sw[q] * bcv2;
+          const double phii = t->sphi[q][k];
+          double pg = 0.;
+          for (int kv = 0; kv < NVB; kv++) pg += t->spsi[q][kv] * s_uold[DIM][sur[kv]];
+          fr += -1. * bc_rhs * dt * phii * nrm[a] * pg;
+          for (int j = 0; j < F::NSN; j++) {
+            const double phij = t->sphi[q][j];
+            diag += dt * bc_tg * phij * phii + dt * nrm[a] * nrm[a] * phij * phii * (bc_n - bc_tg);
+          }
+        }
+        A.vv[(long)(a * DIM + a) * A.nqq + blk] += diag;
+        for (int b = a + 1; b < DIM; b++)  // normal-normal coupling, one column node at a time
+          for (int j = 0; j < F::NSN; j++) {
+            double o = 0.;
+            for (int q = 0; q < F::NSQ; q++)
+              o += jac_sur<DIM>(t, q, s_xx, sur) * t->sw[q] * bcv2 * nrm[b] * nrm[a] * t->sphi[q][j] *
+                   t->sphi[q][k] * (bc_n - bc_tg);
+            const long bj = qq_ptr[nlv] + A.pos_qq[((long)e * NEN + lv) * NEN + sur[j]];
+            A.vv[(long)(a * DIM + b) * A.nqq + bj] += o;
+          }
+        if (mode == 1 && ph.traction != 0.) A.rhs[(long)a * A.N + nlv] += fr;
       } else if (!ns && s_bcb[0][last] != 0) {
         // Robin: k dT/dn = -h T; the constant terms of the reference are zero
         const int bs = s_bcb[0][lv];
@@ -554,7 +613,7 @@ static int assemble_dim(exf_sys *s, const exf_phys *ph, int lev, int mode) {
   }
   if (mode == 1) EXF_TRY(L.b.zero(st));
   constexpr int NT = DIM == 2 ? 128 : 256;
-  for (int c = 0; c < 8; c++) {
+  for (int c = 0; c + 1 < (int)ml.ecol_off.size(); c++) {
     int n = ml.ecol_off[c + 1] - ml.ecol_off[c];
     if (n == 0) continue;
     a.elist = ml.d_elist.p + ml.ecol_off[c];

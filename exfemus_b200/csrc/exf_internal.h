@@ -127,17 +127,22 @@ struct DBuf {
 };
 
 struct MeshLevel {
-  int nnodes = 0, nel = 0, ne[3] = {1, 1, 1};
+  int nnodes = 0, nel = 0, ne[3] = {1, 1, 1};  // ne: elements per axis (structured boxes)
   std::vector<int> conn, neigh, colour;   // host copies
+  std::vector<int> parent;                // uploaded meshes: parent element on level - 1
   DBuf<int> d_conn, d_neigh;
   DBuf<int> d_elist;                      // elements sorted by colour
-  int ecol_off[9] = {0};
+  std::vector<int> ecol_off;              // [element colours + 1] offsets into d_elist
 };
 
 }  // namespace exf
 
 struct exf_mesh {
   int dim = 2, nlev = 1, nen = 9, nvx = 4, nsides = 4, nsn = 3;
+  // generated box (exf_mesh_create): nodes on an integer lattice, colourings and
+  // transfers from lattice indices; uploaded (exf_mesh_upload): from the arrays
+  bool lattice = true;
+  bool has_parent = false;                // uploaded with parent elements
   int n0[3] = {1, 1, 1}, L[3] = {1, 1, 1};
   int ntop = 0, nvert0 = 0;
   int device = 0;
@@ -232,6 +237,20 @@ struct SysLevel {
   long len32 = 0;                   // length of the FP32 V-cycle vectors
 };
 
+// device state of the device-resident solve loop (cycles 2.. of exf_mg_solve run inside
+// one graph launch whose conditional WHILE node repeats the V-cycle body while the check
+// kernel says so)
+struct LoopDev {
+  double den;       // ||b|| (1 when b = 0)
+  double lim;       // eps, or eps (1 + ||b||) for the reference stop test
+  int max_cycles;
+  int cycles;       // cycles done so far (set before the launch, advanced on the device)
+  int ref_stop;     // 1: stop on the top level's accuracy (FP64 cycles)
+  int mixed;        // 1: mixed precision (the accuracy is the FP64 relative residual)
+  double rel, last_acc;
+  double hist[256];
+};
+
 struct Partials {
   DBuf<double> part;   // per-block partial sums
   DBuf<double> out;    // reduced scalars
@@ -276,6 +295,13 @@ struct exf_sys {
   long long graph_launches[2] = {0, 0};
   unsigned buf_epoch = 1;                   // bumped when a buffer baked into a graph moves
   unsigned graph_epoch[2] = {0, 0};
+  // device-resident solve loop (per precision): WHILE-node graph, its key and epoch
+  cudaGraphExec_t loop_graph[2] = {nullptr, nullptr};
+  unsigned long long loop_key[2] = {0, 0};
+  unsigned loop_epoch[2] = {0, 0};
+  long long loop_launches[2] = {0, 0};     // kernels per loop iteration
+  int loop_unavailable = 0;                 // the runtime refused the conditional graph
+  exf::DBuf<exf::LoopDev> loop_dev;
 };
 
 // Entry-point guards: a null handle is an argument error; otherwise the system's device
@@ -308,9 +334,18 @@ constexpr int spmv_lpr() {
 
 // kernels / launchers implemented in the .cu files
 int build_mesh_host(exf_mesh *m);
+int mesh_finish_levels(exf_mesh *m);  // element colours, colour lists, device copies
+// uploaded meshes: node indices 0..n-1 in (z, y, x) order of their coordinates, and a
+// first-fit colouring of items in that order under the conflict lists cptr/cidx
+std::vector<int> node_zyx_order(const exf_mesh *m, int n);
+int colour_items_greedy(const exf_mesh *m, int nitem, const std::vector<int> &order,
+                        const std::vector<int> &cptr, const std::vector<int> &cidx, std::vector<int> &colour);
 int upload_fe_table(exf_mesh *m);  // FE tables of the mesh's element type, on its device
 int build_patterns(exf_sys *s);
 int build_transfers(exf_sys *s);
+int set_transfer(exf_sys *s, int lev, int kind, int block, const int dim[2], const int *len, const int *pos,
+                 const double *val);
+bool transfers_ready(const exf_sys *s);
 int update_rmask(exf_sys *s);
 int build_colours(exf_sys *s);
 int assemble_level(exf_sys *s, const exf_phys *ph, int lev, int mode);

@@ -13,6 +13,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <algorithm>
 
 #include "exf_internal.h"
 #include "fe_topology.h"
@@ -116,26 +117,39 @@ int build_mesh_host(exf_mesh *m) {
           }
           ml.colour[e] = (ex & 1) | ((ey & 1) << 1) | ((ez & 1) << 2);
         }
-    // element list grouped by colour (stable)
+  }
+  EXF_TRY(m->d_lat.alloc(m->lat.size()));
+  EXF_CUDA(cudaMemcpy(m->d_lat.p, m->lat.data(), m->lat.size() * sizeof(int), cudaMemcpyHostToDevice));
+  return mesh_finish_levels(m);
+}
+
+// Element lists grouped by colour (stable in element order) and the device copies of
+// the connectivity, neighbours and coordinates.  Elements of one colour share no node, so
+// one assembly launch per colour scatters into disjoint rows.
+int mesh_finish_levels(exf_mesh *m) {
+  for (int l = 0; l < m->nlev; l++) {
+    MeshLevel &ml = m->lev[l];
+    int ncol = 0;
+    for (int e = 0; e < ml.nel; e++) ncol = std::max(ncol, ml.colour[e] + 1);
     std::vector<int> elist;
     elist.reserve(ml.nel);
-    for (int c = 0; c < 8; c++) {
+    ml.ecol_off.assign(ncol + 1, 0);
+    for (int c = 0; c < ncol; c++) {
       ml.ecol_off[c] = (int)elist.size();
       for (int e = 0; e < ml.nel; e++)
         if (ml.colour[e] == c) elist.push_back(e);
     }
-    ml.ecol_off[8] = (int)elist.size();
+    ml.ecol_off[ncol] = (int)elist.size();
     EXF_TRY(ml.d_conn.alloc(ml.conn.size()));
     EXF_TRY(ml.d_neigh.alloc(ml.neigh.size()));
     EXF_TRY(ml.d_elist.alloc(elist.size()));
     EXF_CUDA(cudaMemcpy(ml.d_conn.p, ml.conn.data(), ml.conn.size() * sizeof(int), cudaMemcpyHostToDevice));
     EXF_CUDA(cudaMemcpy(ml.d_neigh.p, ml.neigh.data(), ml.neigh.size() * sizeof(int), cudaMemcpyHostToDevice));
-    EXF_CUDA(cudaMemcpy(ml.d_elist.p, elist.data(), elist.size() * sizeof(int), cudaMemcpyHostToDevice));
+    if (!elist.empty())
+      EXF_CUDA(cudaMemcpy(ml.d_elist.p, elist.data(), elist.size() * sizeof(int), cudaMemcpyHostToDevice));
   }
   EXF_TRY(m->d_xyz.alloc(m->xyz.size()));
-  EXF_TRY(m->d_lat.alloc(m->lat.size()));
   EXF_CUDA(cudaMemcpy(m->d_xyz.p, m->xyz.data(), m->xyz.size() * sizeof(double), cudaMemcpyHostToDevice));
-  EXF_CUDA(cudaMemcpy(m->d_lat.p, m->lat.data(), m->lat.size() * sizeof(int), cudaMemcpyHostToDevice));
   return EXF_OK;
 }
 

@@ -356,6 +356,43 @@ __global__ void k_item_colour(const int *lat, int nitem, int step, int dim, int 
   colour[i] = c;
 }
 
+// Uploaded meshes (no lattice): greedy first-fit colouring with items in (z, y, x) order of
+// their node coordinates.  T: nodes sharing an element conflict (qq); NS: pressure
+// vertices whose stars share a node conflict -- the stars holding node n are the vertices
+// of ql(n), so the conflicts of vertex m are the union of ql(n) over n in qq(m).  On a
+// structured box this reproduces the lattice colouring (the conflicts are the items within
+// two lattice steps in every direction, and first fit in lattice order takes
+// i%3 + 3 (j%3) + 9 (k%3)).
+static int colour_general(exf_sys *s, int l, int nitem, std::vector<int> &col) {
+  exf_mesh *m = s->mesh;
+  SysLevel &L = s->L[l];
+  std::vector<int> qp(L.N + 1), qc(L.nqq), lp(L.N + 1), lc(L.nql);
+  EXF_CUDA(cudaMemcpy(qp.data(), L.qq_ptr.p, (L.N + 1) * sizeof(int), cudaMemcpyDeviceToHost));
+  EXF_CUDA(cudaMemcpy(qc.data(), L.qq_col.p, L.nqq * sizeof(int), cudaMemcpyDeviceToHost));
+  EXF_CUDA(cudaMemcpy(lp.data(), L.ql_ptr.p, (L.N + 1) * sizeof(int), cudaMemcpyDeviceToHost));
+  EXF_CUDA(cudaMemcpy(lc.data(), L.ql_col.p, L.nql * sizeof(int), cudaMemcpyDeviceToHost));
+  std::vector<int> cptr(nitem + 1, 0), cidx;
+  if (s->kind == EXF_KIND_T) {
+    cptr.assign(qp.begin(), qp.begin() + nitem + 1);
+    cidx.assign(qc.begin(), qc.begin() + qp[nitem]);
+  } else {
+    std::vector<int> stamp(nitem, -1);
+    for (int v = 0; v < nitem; v++) {
+      for (int k = qp[v]; k < qp[v + 1]; k++) {
+        const int n = qc[k];
+        for (int j = lp[n]; j < lp[n + 1]; j++)
+          if (stamp[lc[j]] != v) {
+            stamp[lc[j]] = v;
+            cidx.push_back(lc[j]);
+          }
+      }
+      cptr[v + 1] = (int)cidx.size();
+    }
+  }
+  const std::vector<int> order = node_zyx_order(m, nitem);
+  return colour_items_greedy(m, nitem, order, cptr, cidx, col);
+}
+
 int build_colours(exf_sys *s) {
   exf_mesh *m = s->mesh;
   cudaStream_t st = s->stream;
@@ -365,12 +402,17 @@ int build_colours(exf_sys *s) {
     int nitem = s->kind == EXF_KIND_T ? L.N : L.NL;
     int step = s->kind == EXF_KIND_T ? sl : 2 * sl;
     EXF_TRY(L.item_colour.alloc(nitem));
-    k_item_colour<<<nblk(nitem, 256), 256, 0, st>>>(m->d_lat.p, nitem, step, m->dim, L.item_colour.p);
-    EXF_LAUNCH_CHECK();
     std::vector<int> col(nitem);
-    EXF_CUDA(cudaMemcpyAsync(col.data(), L.item_colour.p, nitem * sizeof(int), cudaMemcpyDeviceToHost, st));
-    EXF_CUDA(cudaStreamSynchronize(st));
-    L.ncolour = m->dim == 2 ? 9 : 27;
+    if (m->lattice) {
+      k_item_colour<<<nblk(nitem, 256), 256, 0, st>>>(m->d_lat.p, nitem, step, m->dim, L.item_colour.p);
+      EXF_LAUNCH_CHECK();
+      EXF_CUDA(cudaMemcpyAsync(col.data(), L.item_colour.p, nitem * sizeof(int), cudaMemcpyDeviceToHost, st));
+      EXF_CUDA(cudaStreamSynchronize(st));
+      L.ncolour = m->dim == 2 ? 9 : 27;
+    } else {
+      L.ncolour = colour_general(s, l, nitem, col);
+      EXF_CUDA(cudaMemcpy(L.item_colour.p, col.data(), nitem * sizeof(int), cudaMemcpyHostToDevice));
+    }
     L.col_off.assign(L.ncolour + 1, 0);
     for (int i = 0; i < nitem; i++) L.col_off[col[i] + 1]++;
     for (int c = 0; c < L.ncolour; c++) L.col_off[c + 1] += L.col_off[c];
@@ -388,16 +430,19 @@ int build_colours(exf_sys *s) {
       EXF_CUDA(cudaMemcpy(lp.data(), L.ql_ptr.p, (L.N + 1) * sizeof(int), cudaMemcpyDeviceToHost));
       EXF_CUDA(cudaMemcpy(lc.data(), L.ql_col.p, L.nql * sizeof(int), cudaMemcpyDeviceToHost));
       // lattice of this level (Q2 nodes): the node at each lattice point, and the offset of
-      // every block's column from its row node as an index step in a 9^d tile
+      // every block's column from its row node as an index step in a 9^d tile (TILE
+      // kernels; uploaded meshes have no lattice: codes zero, the TILE kernels refused)
       const int dim = m->dim;
-      for (int d = 0; d < 3; d++) L.Ll[d] = d < dim ? 2 * m->lev[l].ne[d] + 1 : 1;
+      const bool lat = m->lattice;
+      for (int d = 0; d < 3; d++) L.Ll[d] = (lat && d < dim) ? 2 * m->lev[l].ne[d] + 1 : 1;
       if (L.Ll[0] > 2048 || L.Ll[1] > 2048 || L.Ll[2] > 1024) {
         set_error("build_colours: level lattice %dx%dx%d exceeds the packed patch origin", L.Ll[0], L.Ll[1], L.Ll[2]);
         return EXF_ERR_UNSUPPORTED;
       }
-      auto latl = [&](int n, int d) { return d < dim ? m->lat[3 * (size_t)n + d] / sl : 0; };
-      std::vector<int> lnode(L.N);
-      for (int n = 0; n < L.N; n++) lnode[((size_t)latl(n, 2) * L.Ll[1] + latl(n, 1)) * L.Ll[0] + latl(n, 0)] = n;
+      auto latl = [&](int n, int d) { return (lat && d < dim) ? m->lat[3 * (size_t)n + d] / sl : 0; };
+      std::vector<int> lnode(L.N, 0);
+      if (lat)
+        for (int n = 0; n < L.N; n++) lnode[((size_t)latl(n, 2) * L.Ll[1] + latl(n, 1)) * L.Ll[0] + latl(n, 0)] = n;
       const int tstep[3] = {1, 9, 81};
       bool far = false;
       auto tcode = [&](int n, int c) {
@@ -409,11 +454,12 @@ int build_colours(exf_sys *s) {
         }
         return (int16_t)v;
       };
-      std::vector<int16_t> tq(L.nqq), tl(L.nql);
-      for (int n = 0; n < L.N; n++) {
-        for (int k = qp[n]; k < qp[n + 1]; k++) tq[k] = tcode(n, qc[k]);
-        for (int k = lp[n]; k < lp[n + 1]; k++) tl[k] = tcode(n, lc[k]);
-      }
+      std::vector<int16_t> tq(L.nqq, 0), tl(L.nql, 0);
+      if (lat)
+        for (int n = 0; n < L.N; n++) {
+          for (int k = qp[n]; k < qp[n + 1]; k++) tq[k] = tcode(n, qc[k]);
+          for (int k = lp[n]; k < lp[n + 1]; k++) tl[k] = tcode(n, lc[k]);
+        }
       if (far) {
         set_error("build_colours: a block couples nodes more than 2 lattice steps apart");
         return EXF_ERR_UNSUPPORTED;
@@ -429,7 +475,14 @@ int build_colours(exf_sys *s) {
       // one ended and finds the star rows both read still in L2 (the order inside a
       // colour does not change its result: its patches are independent)
       std::vector<int> sweep(items);
+      std::vector<long long> rank;
+      if (!lat) {  // (z, y, x) order of the vertex coordinates
+        const std::vector<int> ord = node_zyx_order(m, nitem);
+        rank.assign(nitem, 0);
+        for (int i = 0; i < nitem; i++) rank[ord[i]] = i;
+      }
       auto lkey = [&](int v) {
+        if (!lat) return rank[v];
         return ((long long)latl(v, 2) * L.Ll[1] + latl(v, 1)) * L.Ll[0] + latl(v, 0);
       };
       for (int c = 0; c < L.ncolour; c++) {
@@ -476,7 +529,7 @@ int build_colours(exf_sys *s) {
         pin[2 * t + 1] = make_int4(K, lp[mm + 1] - lp[mm], latl(mm, 0) | (latl(mm, 1) << 11) | (latl(mm, 2) << 22), 0);
       }
       const int smax = dim == 3 ? 125 : 25;
-      L.tile_ok = kmax <= smax && rmax <= smax;
+      L.tile_ok = lat && kmax <= smax && rmax <= smax;
       EXF_TRY(L.vrinfo.alloc(vri.size()));
       EXF_CUDA(cudaMemcpy(L.vrinfo.p, vri.data(), vri.size() * sizeof(int4), cudaMemcpyHostToDevice));
       if (dim == 3) {  // star-major record offsets of the BULK smoother
@@ -559,6 +612,67 @@ static void build_prol_host(const exf_mesh *m, int l, bool quad, Transfer &P) {
   }
 }
 
+// Uploaded meshes: the same rows from the parent elements.  A fine element lies in the
+// sub-cell of its parent at the corner it shares with the parent: its local vertex k is
+// the parent's vertex k (uniform refinement keeps the parent's orientation), so its local
+// node with offsets (a,b,c) sits at xi = -1 + (2 pos + (a,b,c)) / 2 in the parent, pos =
+// (parent vertex k's offsets) / 2.  Returns false when an element breaks that rule or the
+// rows do not reproduce the fine node coordinates (both exact for affine refinement).
+static bool build_prol_parent(const exf_mesh *m, int l, bool quad, Transfer &P) {
+  const int dim = m->dim, nen = m->nen, nvx = m->nvx;
+  const MeshLevel &fl = m->lev[l], &cl = m->lev[l - 1];
+  const int nrow = quad ? fl.nnodes : cl.nnodes;
+  std::vector<int> own(fl.nnodes, -1), ownk(fl.nnodes, -1);
+  for (int e = 0; e < fl.nel; e++)
+    for (int k = 0; k < nen; k++) {
+      const int nd = fl.conn[(size_t)e * nen + k];
+      if (own[nd] < 0) {
+        own[nd] = e;
+        ownk[nd] = k;
+      }
+    }
+  P.nrow = nrow;
+  P.h_ptr.assign(nrow + 1, 0);
+  P.h_col.clear();
+  P.h_val.clear();
+  for (int i = 0; i < nrow; i++) {
+    const int e = own[i];
+    if (e < 0) return false;
+    const int pel = fl.parent[e];
+    const int *fc = &fl.conn[(size_t)e * nen];
+    const int *pc = &cl.conn[(size_t)pel * nen];
+    int corner = -1;
+    for (int k = 0; k < nvx; k++)
+      if (fc[k] == pc[k]) corner = corner < 0 ? k : -2;
+    if (corner < 0) return false;
+    const int *cabc = dim == 2 ? Q9_ABC[corner] : H27_ABC[corner];
+    const int *fabc = dim == 2 ? Q9_ABC[ownk[i]] : H27_ABC[ownk[i]];
+    double xi[3] = {0, 0, 0};
+    for (int d = 0; d < dim; d++) xi[d] = -1. + (double)(cabc[d] + fabc[d]) / 2.;
+    std::vector<std::pair<int, double>> ent;
+    const int nsh = quad ? nen : nvx;
+    double xr[3] = {0, 0, 0};
+    for (int kj = 0; kj < nsh; kj++) {
+      const int *abc = dim == 2 ? Q9_ABC[kj] : H27_ABC[kj];
+      double v = 1.;
+      for (int d = 0; d < dim; d++) v *= quad ? lag1(abc[d], xi[d]) : lin1(abc[d], xi[d]);
+      for (int d = 0; d < dim; d++) xr[d] += v * m->xyz[(size_t)pc[kj] + (size_t)d * m->ntop];
+      if (fabs(v) > 1e-8) ent.push_back({pc[kj], v});
+    }
+    for (int d = 0; d < dim; d++) {
+      const double ext = m->box[2 * d + 1] - m->box[2 * d];
+      if (fabs(xr[d] - m->xyz[(size_t)i + (size_t)d * m->ntop]) > 1e-9 * (ext > 0 ? ext : 1.)) return false;
+    }
+    std::sort(ent.begin(), ent.end());
+    for (auto &pv : ent) {
+      P.h_col.push_back(pv.first);
+      P.h_val.push_back(pv.second);
+    }
+    P.h_ptr[i + 1] = (int)P.h_col.size();
+  }
+  return true;
+}
+
 static void transpose_host(const Transfer &P, int ncol, Transfer &R) {
   R.nrow = ncol;
   R.h_ptr.assign(ncol + 1, 0);
@@ -594,23 +708,97 @@ static int upload_transfer(Transfer &T) {
   return EXF_OK;
 }
 
+// Transfers of every level pair: from the lattice (generated boxes), from the parent
+// elements (uploaded with parents), or left empty until exf_sys_set_transfer supplies
+// them (uploaded without parents; solves refuse to start until then).
 int build_transfers(exf_sys *s) {
   exf_mesh *m = s->mesh;
+  if (!m->lattice && !m->has_parent) return EXF_OK;
   for (int l = 1; l < s->nlev; l++) {
     SysLevel &F = s->L[l];
     SysLevel &C = s->L[l - 1];
-    build_prol_host(m, l, true, F.Pq);
-    EXF_TRY(upload_transfer(F.Pq));
-    transpose_host(F.Pq, C.N, C.Rq);
-    EXF_TRY(upload_transfer(C.Rq));
-    if (s->nv1) {
-      build_prol_host(m, l, false, F.Pl);
-      EXF_TRY(upload_transfer(F.Pl));
-      transpose_host(F.Pl, C.NL, C.Rl);
-      EXF_TRY(upload_transfer(C.Rl));
+    for (int q = 0; q < (s->nv1 ? 2 : 1); q++) {
+      const bool quad = q == 0;
+      Transfer &P = quad ? F.Pq : F.Pl;
+      Transfer &R = quad ? C.Rq : C.Rl;
+      if (m->lattice) {
+        build_prol_host(m, l, quad, P);
+      } else if (!build_prol_parent(m, l, quad, P)) {
+        set_error("build_transfers: level %d: a child element is not a sub-cell of its parent with the parent's "
+                  "orientation, or the prolongation does not reproduce the node coordinates", l);
+        return EXF_ERR_ARG;
+      }
+      EXF_TRY(upload_transfer(P));
+      transpose_host(P, quad ? C.N : C.NL, R);
+      EXF_TRY(upload_transfer(R));
     }
   }
   return EXF_OK;
+}
+
+// one block of a transfer operator in gencase's dataset layout (rows, columns, cumulative
+// row offsets, level-local column nodes, values): columns sorted per row, uploaded
+int set_transfer(exf_sys *s, int lev, int kind, int block, const int dim[2], const int *len, const int *pos,
+                 const double *val) {
+  if (lev < 0 || lev >= s->nlev || (kind != 0 && kind != 1) || (block != 1 && block != 2) || !dim || !len ||
+      (!pos && dim[0] > 0) || (block == 1 && !s->nv1)) {
+    set_error("exf_sys_set_transfer: bad argument");
+    return EXF_ERR_ARG;
+  }
+  const int other = kind == 0 ? lev - 1 : lev + 1;
+  if (other < 0 || other >= s->nlev) {
+    set_error("exf_sys_set_transfer: no level %d next to level %d", other, lev);
+    return EXF_ERR_ARG;
+  }
+  SysLevel &L = s->L[lev], &O = s->L[other];
+  const int nrow = block == 2 ? L.N : L.NL, ncol = block == 2 ? O.N : O.NL;
+  if (dim[0] != nrow || dim[1] != ncol) {
+    set_error("exf_sys_set_transfer: block is %dx%d, level %d needs %dx%d", dim[0], dim[1], lev, nrow, ncol);
+    return EXF_ERR_ARG;
+  }
+  if (len[0] != 0) {
+    set_error("exf_sys_set_transfer: row offsets must start at 0");
+    return EXF_ERR_ARG;
+  }
+  Transfer T;
+  T.nrow = nrow;
+  T.h_ptr.assign(len, len + nrow + 1);
+  for (int i = 0; i < nrow; i++) {
+    if (len[i + 1] < len[i]) {
+      set_error("exf_sys_set_transfer: row offsets decrease at row %d", i);
+      return EXF_ERR_ARG;
+    }
+    std::vector<std::pair<int, double>> ent;
+    for (int q = len[i]; q < len[i + 1]; q++) {
+      if (pos[q] < 0 || pos[q] >= ncol) {
+        set_error("exf_sys_set_transfer: column %d of row %d outside 0..%d", pos[q], i, ncol - 1);
+        return EXF_ERR_ARG;
+      }
+      ent.push_back({pos[q], val ? val[q] : 0.});
+    }
+    std::stable_sort(ent.begin(), ent.end(), [](const std::pair<int, double> &a, const std::pair<int, double> &b) {
+      return a.first < b.first;
+    });
+    for (auto &e : ent) {
+      T.h_col.push_back(e.first);
+      T.h_val.push_back(e.second);
+    }
+  }
+  EXF_TRY(upload_transfer(T));
+  Transfer &dst = kind == 0 ? (block == 2 ? L.Pq : L.Pl) : (block == 2 ? L.Rq : L.Rl);
+  dst = std::move(T);
+  s->buf_epoch++;
+  return EXF_OK;
+}
+
+// every transfer a V-cycle needs is present
+bool transfers_ready(const exf_sys *s) {
+  for (int l = 1; l < s->nlev; l++) {
+    const SysLevel &F = s->L[l], &C = s->L[l - 1];
+    if (F.Pq.nrow != F.N || C.Rq.nrow != C.N) return false;
+    if (s->nv1 && (F.Pl.nrow != F.NL || C.Rl.nrow != C.NL)) return false;
+  }
+  return true;
 }
 
 // restriction row mask: bc[0][top dof] % 2 (src/MGSolverDA.C:2423-2425)

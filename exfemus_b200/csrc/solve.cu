@@ -1673,7 +1673,8 @@ static int vanka_sweep_rows(exf_sys *s, int lev, const exf_mg_params *p, T *x, c
     // 1.42 ms for the register-pipelined row kernel, so AUTO does not use it
     if constexpr (sizeof(T) == 4 && D == 3) {
       // AUTO: the bulk kernel on the streaming levels (above four waves of rows)
-      if (p->vanka_kernel == EXF_VANKA_BULK || (p->vanka_kernel == EXF_VANKA_AUTO && EXF_AUTO_BULK && big)) {
+      if (!p->fp32_blocks &&
+          (p->vanka_kernel == EXF_VANKA_BULK || (p->vanka_kernel == EXF_VANKA_AUTO && EXF_AUTO_BULK && big))) {
         constexpr int NWC = EXF_BK_NWC, STG = EXF_BK_STG, CAPB = EXF_BK_CAPB, UNR = EXF_BK_UNR,
                       BLPR = EXF_BK_LPR;
         static_assert(CAPB >= 512, "a stage holds the longest row (header, 255 blocks, 255 couplings, pad)");
@@ -1719,7 +1720,7 @@ static int vanka_sweep_rows(exf_sys *s, int lev, const exf_mg_params *p, T *x, c
         EXF_COUNT(2);
         continue;
       }
-      if (p->vanka_kernel == EXF_VANKA_STREAM) {
+      if (p->vanka_kernel == EXF_VANKA_STREAM && !p->fp32_blocks) {
         if (!L.tile_ok) {
           set_error("Vanka row streaming: a row of level %d exceeds 125 blocks", lev);
           return EXF_ERR_UNSUPPORTED;
@@ -1753,16 +1754,22 @@ static int vanka_sweep_rows(exf_sys *s, int lev, const exf_mg_params *p, T *x, c
         continue;
       }
     }
+    bool launched = false;
     if constexpr (sizeof(T) == 4) {  // FP32 V-cycle: row-scaled FP16 velocity blocks
-      using VB = Packed16<D>;
-      const VB vb{L.qq_col.p, L.h16.p, L.h16cx.p};
-      auto kern = big   ? k_vanka_rows<T, D, LPR_S, NTR, I4, UNR_S, MINB_S, VB>
-                  : mid ? k_vanka_rows<T, D, LPR, NTR, I4, UNR_M, MINB_M, VB>
-                        : k_vanka_rows<T, D, LPR, NTR, I4, UNR_L, 1, VB>;
-      EXF_CUDA(launch_pdl(kern, dim3(nblk(big ? nthr_s : nthr, NTR)), dim3(NTR), 0, s->stream, L.vrinfo.p + L.vrow_off[c], nr,
-                          L.vrow_off[c], pin, n, L.N, vb, (const T *)L.vsc.p, L.qq_col.p, L.ql_col.p, L.nql, L.nqqL,
-                          VT<T>::vp(L), VT<T>::pv(L), VT<T>::pp(L), x, b, res, pres_off));
-    } else {
+      if (!p->fp32_blocks) {
+        using VB = Packed16<D>;
+        const VB vb{L.qq_col.p, L.h16.p, L.h16cx.p};
+        auto kern = big   ? k_vanka_rows<T, D, LPR_S, NTR, I4, UNR_S, MINB_S, VB>
+                    : mid ? k_vanka_rows<T, D, LPR, NTR, I4, UNR_M, MINB_M, VB>
+                          : k_vanka_rows<T, D, LPR, NTR, I4, UNR_L, 1, VB>;
+        EXF_CUDA(launch_pdl(kern, dim3(nblk(big ? nthr_s : nthr, NTR)), dim3(NTR), 0, s->stream,
+                            L.vrinfo.p + L.vrow_off[c], nr, L.vrow_off[c], pin, n, L.N, vb, (const T *)L.vsc.p,
+                            L.qq_col.p, L.ql_col.p, L.nql, L.nqqL, VT<T>::vp(L), VT<T>::pv(L), VT<T>::pp(L), x, b,
+                            res, pres_off));
+        launched = true;
+      }
+    }
+    if (!launched) {  // FP64, or FP32 storage of the blocks in the FP32 V-cycle
       using VB = PlanarBlocks<T, D * D>;
       const VB vb{L.qq_col.p, VT<T>::vv(L), L.nqq};
       auto kern = big ? k_vanka_rows<T, D, LPR, NTR, I4, UNR_S, MINB_S, VB>
@@ -1846,7 +1853,8 @@ static int vanka_sweep_tile(exf_sys *s, int lev, const exf_mg_params *p, T *x, c
 template <class T, int D>
 static int vanka_sweep(exf_sys *s, int lev, const exf_mg_params *p, T *x, const T *b) {
   SysLevel &L = s->L[lev];
-  if (p->vanka_kernel == EXF_VANKA_TILE) {
+  // FP32 blocks in the FP32 V-cycle are read by the row kernel only
+  if (p->vanka_kernel == EXF_VANKA_TILE && !(sizeof(T) == 4 && p->fp32_blocks)) {
     if (!L.tile_ok) {
       set_error("Vanka tile kernel: a star or row of level %d exceeds the 5^d-node patch", lev);
       return EXF_ERR_UNSUPPORTED;

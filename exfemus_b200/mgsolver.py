@@ -60,6 +60,31 @@ class Mesh:
         check(L.exf_mesh_create(C.byref(d), C.byref(h)))
         self.h, self.L, self.dim, self.nlev = h, L, dim, nlev
 
+    @classmethod
+    def upload(cls, dim, nnodes, nvert0, xyz, conn, neigh, parent=None, device=0):
+        """A hierarchy from host arrays, as MGMesh::read_c holds it (src/MGMesh.C:493-908):
+        nnodes[L] Q2 nodes per level (level-nested numbering), nvert0 vertices of level 0,
+        xyz [dim][ntop], conn[L] [nel][9|27] top node numbers, neigh[L] [nel][4|6]
+        level-local neighbours (-1 boundary), parent[L] (L >= 1) parent elements or None."""
+        L = load()
+        nlev = len(nnodes)
+        d = _lib.ExfMeshData()
+        keep = [np.ascontiguousarray(nnodes, np.int32), np.ascontiguousarray(xyz, np.float64).ravel(),
+                np.ascontiguousarray([len(c) for c in conn], np.int32),
+                np.ascontiguousarray(np.concatenate([np.asarray(c, np.int32).ravel() for c in conn])),
+                np.ascontiguousarray(np.concatenate([np.asarray(c, np.int32).ravel() for c in neigh]))]
+        if parent is not None:
+            keep.append(np.ascontiguousarray(np.concatenate([np.asarray(p, np.int32).ravel() for p in parent[1:]])))
+        d.dim, d.nlev, d.device, d.nvert0 = dim, nlev, device, nvert0
+        d.nnodes, d.xyz, d.nel = keep[0].ctypes.data, keep[1].ctypes.data, keep[2].ctypes.data
+        d.conn, d.neigh = keep[3].ctypes.data, keep[4].ctypes.data
+        d.parent = keep[5].ctypes.data if parent is not None else None
+        h = C.c_void_p()
+        check(L.exf_mesh_upload(C.byref(d), C.byref(h)))
+        self = cls.__new__(cls)
+        self.h, self.L, self.dim, self.nlev = h, L, dim, nlev
+        return self
+
     def close(self):
         if getattr(self, "h", None):
             self.L.exf_mesh_destroy(self.h)
@@ -199,6 +224,21 @@ class MGSolBase:
         nc = C.c_int()
         check(self.L.exf_sys_get_colours(self.h, lev, C.byref(nc), iptr(out)))
         return nc.value, out
+
+    def set_transfer(self, lev, kind, block, dim, length, pos, val):
+        """One block of a Prol/Rest operator in gencase's dataset layout (DIM0/LEN0/POS0/VAL0)."""
+        a = np.ascontiguousarray(dim, np.int32)
+        b = np.ascontiguousarray(length, np.int32)
+        c = np.ascontiguousarray(pos, np.int32)
+        v = np.ascontiguousarray(val, np.float64)
+        check(self.L.exf_sys_set_transfer(self.h, lev, kind, block, iptr(a), iptr(b), iptr(c), dptr(v)))
+
+    def check_pattern(self, lev, block, dim, length, pos):
+        """Status of exf_sys_check_pattern for one block of gencase's matrix datasets."""
+        a = np.ascontiguousarray(dim, np.int32)
+        b = np.ascontiguousarray(length, np.int32)
+        c = np.ascontiguousarray(pos, np.int32)
+        return self.L.exf_sys_check_pattern(self.h, lev, block, iptr(a), iptr(b), iptr(c))
 
     def couple(self, other):
         check(self.L.exf_sys_couple(self.h, other.h if other is not None else None))

@@ -39,7 +39,7 @@ extern "C" {
 #define EXF_ERR_NOT_CONVERGED 5 /* max_cycles reached above the tolerance           */
 #define EXF_ERR_SINGULAR 6      /* zero pivot in the coarsest direct factorisation  */
 #define EXF_ERR_NOMEM 7         /* device allocation failed                         */
-#define EXF_ERR_UNSUPPORTED 8   /* boundary flag or option not implemented         */
+#define EXF_ERR_UNSUPPORTED 8   /* option not implemented for this system or kernel */
 
 /* system kinds: MGSolT (one quadratic variable) and coupled MGSolNS (NS_EQUATIONS==1:
  * dim quadratic velocity components + one linear pressure) */
@@ -93,6 +93,8 @@ typedef struct {
   double ifr;       /* _IFr                                                        */
   double dirg[3];   /* _dirg                                                       */
   double buoy;      /* Boussinesq source coefficient: f += buoy*T*dirg             */
+  double traction;  /* 1: natural NS sides whose bc1 has bit 2 get the pressure    */
+                    /* traction rhs -n_a p_old phi (the reference's MESHNUMBER 1) */
 } exf_phys;
 
 typedef struct {
@@ -112,6 +114,9 @@ typedef struct {
   int use_graph;       /* 1: replay each V-cycle from a captured CUDA graph        */
   int vanka_kernel;    /* EXF_VANKA_*                                              */
   int stop_test;       /* EXF_STOP_*                                               */
+  int fp32_blocks;     /* mixed precision: 1 = the Vanka sweeps read the FP32 velocity */
+                       /* blocks (FP32 storage throughout the V-cycle) with the row    */
+                       /* kernel; 0 = row-scaled FP16 block records (default)          */
 } exf_mg_params;
 
 /* stop tests of exf_mg_solve.  A level's accuracy is what the reference's level solver
@@ -142,6 +147,42 @@ EXF_API const char *exf_version(void);
  * replaces MGMesh::read_c (src/MGMesh.C:493-908) for generated boxes */
 EXF_API int exf_mesh_create(const exf_mesh_desc *desc, exf_mesh **out);
 EXF_API int exf_mesh_destroy(exf_mesh *m);
+/* --- mesh from host arrays: the hierarchy MGMesh::read_c holds (src/MGMesh.C:493-908)
+ * after reading gencase's mesh file, one subdomain (the LASPACK path is single-process):
+ *   nnodes[L]   _NoNodes[L]: Q2 nodes of level L.  Nodes are numbered level-nested as
+ *               init_dof requires (src/MGSolverDA.C:880-951): the nodes of level L are the
+ *               top nodes 0..nnodes[L]-1, so the Q1 (pressure) nodes of level L are the Q2
+ *               nodes of level L-1, and those of level 0 are the first nvert0 nodes
+ *   nvert0      _NoNodes of the linear coarse mesh: vertices of level 0
+ *   xyz         _xyz, [dim][nnodes[nlev-1]] component-major
+ *   nel[L]      _NoElements[0][L]
+ *   conn        _el_map[0]: the volume elements of every level, level after level
+ *               (_off_el[0]), [sum nel][9 | 27] top node numbers in libMesh Quad9/Hex27
+ *               local order, vertices first
+ *   neigh       _el_neighbor[0]: [sum nel][4 | 6] level-local index of the element across
+ *               each side (libMesh side order), -1 on the boundary
+ *   parent      [sum_{L>=1} nel[L]] level-local index of each element's parent on level
+ *               L-1 (gencase's elem_sto parent, USER_APPL/gencase/src/MGGenCase.C:306-346);
+ *               NULL when the transfer operators come from exf_sys_set_transfer instead
+ * The children of an element must be the 2^dim sub-cells of its reference element with
+ * the parent's orientation (uniform refinement); the library places each child by the
+ * parent vertex it contains and checks that the prolongation reproduces the fine node
+ * coordinates (EXF_ERR_ARG otherwise).  Smoother and assembly colourings are greedy
+ * first-fit colourings taken in (z, y, x) coordinate order; on a structured box they
+ * equal the colourings of exf_mesh_create, so both give the same bits. */
+typedef struct {
+  int dim;
+  int nlev;
+  int device;
+  const int *nnodes;
+  int nvert0;
+  const double *xyz;
+  const int *nel;
+  const int *conn;
+  const int *neigh;
+  const int *parent;
+} exf_mesh_data;
+EXF_API int exf_mesh_upload(const exf_mesh_data *d, exf_mesh **out);
 EXF_API int exf_mesh_info(const exf_mesh *m, int lev, int *nnodes, int *nel, int *nvert0);
 EXF_API int exf_mesh_get_xyz(const exf_mesh *m, double *xyz);               /* [dim][ntop]    */
 EXF_API int exf_mesh_get_conn(const exf_mesh *m, int lev, int *conn, int *neigh, int *colour);
@@ -160,6 +201,26 @@ EXF_API int exf_sys_get_pattern(exf_sys *s, int lev, int *rowptr, int *col); /* 
 EXF_API int exf_sys_get_prol(exf_sys *s, int lev, long *nnz, int *rowptr, int *col, double *val);
 EXF_API int exf_sys_get_rest(exf_sys *s, int lev, long *nnz, int *rowptr, int *col, double *val);
 EXF_API int exf_sys_get_colours(exf_sys *s, int lev, int *ncolours, int *colour_of_item);
+/* transfer operators from gencase's operator datasets (ReadProl src/MGSolverDA.C:2011-2230,
+ * ReadRest :2236-2444; written by compute_prol_qq / compute_res_qq,
+ * USER_APPL/gencase/src/MGGenCase.C:2308-2569; datasets DIM0<b>, LEN0<b>, POS0<b>, VAL0<b>
+ * of the Prol<L-1>_<L> / Rest<L+1>_<L> files, contrib/matrix/sparse_MmatrixM.C:194-264):
+ *   kind  0 = prolongation into level lev (rows: nodes of lev, columns: nodes of lev-1),
+ *         1 = restriction into level lev (rows: nodes of lev, columns: nodes of lev+1)
+ *   block 2 = the quadratic (Q2 node) block "22", 1 = the linear (Q1 node) block "11"
+ *   dim   DIM0<b>: {rows, columns}; len LEN0<b>: rows+1 cumulative row offsets;
+ *   pos   POS0<b>: level-local column nodes; val VAL0<b>: the entries
+ * Every variable of the block uses the node operator, as in the reference.  Restriction rows
+ * are scaled by bc0 % 2 of their top-level DOF when applied (:2423-2425), so the flags may
+ * change later.  Columns are sorted per row; entries are kept as given. */
+EXF_API int exf_sys_set_transfer(exf_sys *s, int lev, int kind, int block, const int dim[2], const int *len,
+                                 const int *pos, const double *val);
+/* check a level's sparsity against gencase's matrix datasets (ReadMatrix,
+ * src/MGSolverDA.C:1785-2009; LEN0<b>/POS0<b> of block b = 22 (Q2 rows, Q2 columns) or 21
+ * (Q2 rows, Q1 columns)): EXF_OK when every row holds exactly the node columns the library
+ * built from the elements (in any order, as LASPACK sorts them, operats.c:813),
+ * EXF_ERR_ARG with the first differing row otherwise */
+EXF_API int exf_sys_check_pattern(exf_sys *s, int lev, int block, const int dim[2], const int *len, const int *pos);
 /* coupling: T reads the NS velocity, NS reads T for buoyancy (get_el_sol of the
  * other equation, src/MGSolverBase.C:336-354) */
 EXF_API int exf_sys_couple(exf_sys *s, exf_sys *other);

@@ -14,6 +14,7 @@
 #include "errhandl.h"
 #include "itersolv.h"
 #include "operats.h"
+#include "precond.h"
 #include "qmatrix.h"
 #include "qvector.h"
 #include "rtc.h"
@@ -51,10 +52,29 @@ int lpb_spmv(int n, const int *ptr, const int *col, const double *val, const dou
   return rc;
 }
 
-/* unpreconditioned GMRES(restart) to relative accuracy tol (itersolv.c:1341);
- * transpose != 0 solves A^T x = b through Transp_Q (operats.c:1325). */
-int lpb_gmres(int n, const int *ptr, const int *col, const double *val, const double *b, double *x, double tol,
-              int maxit, int restart, int transpose, int *iters, double *acc) {
+/* y = A^T x through Transp_Q (operats.c:1325) and Mul_QV */
+int lpb_spmv_t(int n, const int *ptr, const int *col, const double *val, const double *x, double *y) {
+  QMatrix A;
+  QVector X, Y;
+  fill_q(&A, n, ptr, col, val);
+  fill_v(&X, "x", n, x);
+  fill_v(&Y, "y", n, NULL);
+  Asgn_VV(&Y, Mul_QV(Transp_Q(&A), &X));
+  get_v(&Y, n, y);
+  int rc = LASResult() == LASOK ? 0 : 1;
+  V_Destr(&X);
+  V_Destr(&Y);
+  Q_Destr(&A);
+  return rc;
+}
+
+/* GMRES(restart) to relative accuracy tol (itersolv.c:1341), unpreconditioned
+ * (precond 0) or with LASPACK's ILU(0) (precond 1, ILUPrecond, precond.c; the default
+ * level solver of the reference's LASPACK backend is GMRES + ILU,
+ * contrib/matrix/linear_solverM.h:200-205); transpose != 0 solves A^T x = b through
+ * Transp_Q (operats.c:1325). */
+int lpb_gmres_pc(int n, const int *ptr, const int *col, const double *val, const double *b, double *x, double tol,
+                 int maxit, int restart, int transpose, int precond, int *iters, double *acc) {
   QMatrix A;
   QVector X, B;
   fill_q(&A, n, ptr, col, val);
@@ -62,11 +82,12 @@ int lpb_gmres(int n, const int *ptr, const int *col, const double *val, const do
   fill_v(&B, "b", n, b);
   SetRTCAccuracy(tol);
   SetGMRESRestart(restart);
+  PrecondProcType pc = precond == 1 ? ILUPrecond : NULL;
   if (transpose) {
     QMatrix *At = Transp_Q(&A);
-    GMRESIter(At, &X, &B, maxit, NULL, 1.);
+    GMRESIter(At, &X, &B, maxit, pc, 1.);
   } else {
-    GMRESIter(&A, &X, &B, maxit, NULL, 1.);
+    GMRESIter(&A, &X, &B, maxit, pc, 1.);
   }
   get_v(&X, n, x);
   *iters = GetLastNoIter();
@@ -76,6 +97,11 @@ int lpb_gmres(int n, const int *ptr, const int *col, const double *val, const do
   V_Destr(&B);
   Q_Destr(&A);
   return rc;
+}
+
+int lpb_gmres(int n, const int *ptr, const int *col, const double *val, const double *b, double *x, double tol,
+              int maxit, int restart, int transpose, int *iters, double *acc) {
+  return lpb_gmres_pc(n, ptr, col, val, b, x, tol, maxit, restart, transpose, 0, iters, acc);
 }
 
 /* forward SOR sweeps (itersolv.c:850-894), omega = 1 is lexicographic Gauss-Seidel */

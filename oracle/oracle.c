@@ -241,6 +241,7 @@ typedef struct {
   double sw[9];
   double sphi[9][9];
   double sdphi[9][9][2];
+  double spsi[9][4];        /* linear surface shapes on the side's vertices */
 } fe_tab;
 
 /* Gauss points: x-major then y then z (src/MGFE.C:214-227), weights 5/9, 8/9, 5/9. */
@@ -319,6 +320,11 @@ static void fe_init(fe_tab *t, int dim) {
         double dv = 1.;
         for (int d = 0; d < sdim; d++) dv *= (d == k) ? dlag1(abc[d], xi[d]) : lag1(abc[d], xi[d]);
         t->sdphi[q][s][k] = dv;
+      }
+      if (s < (sdim == 1 ? 2 : 4)) { /* vertices come first on a side */
+        double w = 1.;
+        for (int d = 0; d < sdim; d++) w *= lin1(abc[d], xi[d]);
+        t->spsi[q][s] = w;
       }
     }
   }
@@ -923,9 +929,27 @@ static double upwind_f(double up, double rho, double mod, double h, double diff)
   return up * rho * 0.5 * (1. / tanh(pe) - 1. / pe) * h / mod;
 }
 
-static void side_normal(int dim, int sd, double *nrm) {
-  const int *dir = dim == 2 ? Q9_SIDE_DIR[sd] : H27_FACE_DIR[sd];
-  for (int d = 0; d < 3; d++) nrm[d] = (double)dir[d];
+/* MGFE::normal_g (src/MGFE.C:1601-1646) on the side's coordinates xb [dim][nsn]: 2D the
+ * tangent from side node 0 to 1 turned clockwise, 3D (x1 - x0) x (x3 - x0), normalised */
+static void side_normal(int dim, const double *xb, int nsn, double *nrm) {
+  double t1[3] = {0, 0, 0}, t3[3] = {0, 0, 0};
+  for (int d = 0; d < dim; d++) {
+    t1[d] = xb[d * nsn + 1] - xb[d * nsn + 0];
+    if (dim == 3) t3[d] = xb[d * nsn + 3] - xb[d * nsn + 0];
+  }
+  nrm[2] = 0.;
+  if (dim == 2) {
+    nrm[0] = t1[1];
+    nrm[1] = -t1[0];
+  } else {
+    nrm[0] = t1[1] * t3[2] - t1[2] * t3[1];
+    nrm[1] = t1[2] * t3[0] - t1[0] * t3[2];
+    nrm[2] = t1[0] * t3[1] - t1[1] * t3[0];
+  }
+  double mm = 0.;
+  for (int d = 0; d < dim; d++) mm += nrm[d] * nrm[d];
+  mm = sqrt(mm);
+  for (int d = 0; d < dim; d++) nrm[d] /= mm;
 }
 
 /* One element of MGSolT::GenMatRhs (template_appl/nse/SRC/MGSolverT.C:93-525) or
@@ -1063,7 +1087,7 @@ static void asm_element(or_sys *s, int lev, int mode, const or_phys *ph, const d
     for (int k = 0; k < nsn; k++)
       for (int d = 0; d < dim; d++) xb[d * nsn + k] = xx[d * nen + sur[k]];
     double nrm[3];
-    side_normal(dim, sd, nrm);
+    side_normal(dim, xb, nsn, nrm);
     int last = sur[nsn - 1];
     for (int a = 0; a < nv2; a++) {
       if (bcv[a][last] == 0) {
@@ -1092,6 +1116,33 @@ static void asm_element(or_sys *s, int lev, int mode, const or_phys *ph, const d
                 ((1 - bc_n) * (1 - bc_tg) + bc_tg) * ipen + ipen * nrm[a] * nrm[a] * (bc_n - bc_tg);
             for (int b = a + 1; b < dim; b++)
               Ke[row * nloc + b * nen + lv] += ipen * nrm[b] * nrm[a] * (bc_n - bc_tg);
+          }
+        }
+      } else if (s->kind == 1 && bcb[a][last] != 0) {
+        /* Neumann / Robin sides of MGSolNS::GenMatRhs (template_appl/nse/SRC/MGSolverNS.C:
+         * 604-681), alpha_t = 1: per surface Gauss point and side node i (row a, i) with
+         * flags bit0 normal, bit1 tangential, bit2 rhs, the tangential / normal Robin term
+         * lumped on the diagonal, the normal-normal coupling to the later components, and
+         * (MESHNUMBER == 1) the pressure traction -n_a p_old phi_i */
+        const int nvb = dim == 2 ? 2 : 4;
+        for (int q = 0; q < t->sng; q++) {
+          double JxW = jac_sur(t, q, xb, nsn) * t->sw[q];
+          double pg = 0.;
+          for (int k = 0; k < nvb; k++) pg += t->spsi[q][k] * uold[dim][sur[k]];
+          for (int i = 0; i < nsn; i++) {
+            int lei = sur[i];
+            int row = a * nen + lei;
+            int bs = bcb[a][lei];
+            double dt = JxW * (bcv[a][lei] % 2);
+            int bc_rhs = (bs & 4) >> 2, bc_tg = (bs & 2) >> 1, bc_n = bs % 2;
+            double phii = t->sphi[q][i];
+            if (mode == 1 && ph->traction != 0.) Fe[row] += -1. * bc_rhs * dt * phii * nrm[a] * pg;
+            for (int j = 0; j < nsn; j++) {
+              double phij = t->sphi[q][j];
+              Ke[row * nloc + row] += dt * bc_tg * phij * phii + dt * nrm[a] * nrm[a] * phij * phii * (bc_n - bc_tg);
+              for (int b = a + 1; b < dim; b++)
+                Ke[row * nloc + b * nen + sur[j]] += dt * nrm[b] * nrm[a] * phij * phii * (bc_n - bc_tg);
+            }
           }
         }
       } else if (s->kind == 0 && bcb[0][last] != 0) {

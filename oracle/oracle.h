@@ -35,6 +35,8 @@ typedef struct {
   double ifr;        /* _IFr gravity factor                                       */
   double dirg[3];    /* _dirg gravity direction                                   */
   double buoy;       /* Boussinesq source: f += buoy*T*dirg                       */
+  double traction;   /* 1: natural NS sides with bc1 bit 2 get the pressure traction */
+                     /* rhs -n_a p_old phi_i (the reference's MESHNUMBER == 1)      */
 } or_phys;
 
 typedef struct {

@@ -23,7 +23,7 @@ class OrPhys(C.Structure):
     _fields_ = [("inv_re", C.c_double), ("inv_prdl", C.c_double), ("rho", C.c_double),
                 ("rhocp", C.c_double), ("inv_dt", C.c_double), ("penalty", C.c_double),
                 ("upwind_ns", C.c_double), ("upwind_t", C.c_double), ("ifr", C.c_double),
-                ("dirg", C.c_double * 3), ("buoy", C.c_double)]
+                ("dirg", C.c_double * 3), ("buoy", C.c_double), ("traction", C.c_double)]
 
 
 class OrMgParams(C.Structure):
@@ -297,9 +297,12 @@ class Laspack:
             dp = np.ctypeslib.ndpointer(np.float64, flags="C")
             I = C.c_int
             L.lpb_spmv.argtypes = [I, ip, ip, dp, dp, dp]
+            L.lpb_spmv_t.argtypes = [I, ip, ip, dp, dp, dp]
             L.lpb_gmres.argtypes = [I, ip, ip, dp, dp, dp, C.c_double, I, I, I, C.POINTER(I),
                                     C.POINTER(C.c_double)]
             L.lpb_sorforw.argtypes = [I, ip, ip, dp, dp, dp, I, C.c_double, C.POINTER(C.c_double)]
+            L.lpb_gmres_pc.argtypes = [I, ip, ip, dp, dp, dp, C.c_double, I, I, I, I, C.POINTER(I),
+                                       C.POINTER(C.c_double)]
             _LP = L
         self.L = _LP
 
@@ -308,13 +311,20 @@ class Laspack:
         self.L.lpb_spmv(len(rp) - 1, rp, col, val, np.ascontiguousarray(x, np.float64), y)
         return y
 
-    def gmres(self, rp, col, val, b, x0=None, tol=1e-12, maxit=2000, restart=30, transpose=False):
+    def spmv_t(self, rp, col, val, x):
+        """A^T x through the reference's Transp_Q and Mul_QV."""
+        y = np.zeros(len(rp) - 1)
+        self.L.lpb_spmv_t(len(rp) - 1, rp, col, val, np.ascontiguousarray(x, np.float64), y)
+        return y
+
+    def gmres(self, rp, col, val, b, x0=None, tol=1e-12, maxit=2000, restart=30, transpose=False, ilu=False):
+        """LASPACK GMRESIter (optionally ILU(0)-preconditioned) on A or Transp_Q(A)."""
         n = len(rp) - 1
         x = np.zeros(n) if x0 is None else np.array(x0, np.float64)
         it = C.c_int(0)
         acc = C.c_double(0)
-        self.L.lpb_gmres(n, rp, col, val, np.ascontiguousarray(b, np.float64), x, tol, maxit, restart,
-                         1 if transpose else 0, C.byref(it), C.byref(acc))
+        self.L.lpb_gmres_pc(n, rp, col, val, np.ascontiguousarray(b, np.float64), x, tol, maxit, restart,
+                            1 if transpose else 0, 1 if ilu else 0, C.byref(it), C.byref(acc))
         return x, it.value, acc.value
 
     def sorforw(self, rp, col, val, b, x0, nsweeps, omega=1.0):

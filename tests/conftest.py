@@ -11,6 +11,7 @@ if ROOT not in sys.path:
 
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA device (B200) and the built CUDA library")
+    config.addinivalue_line("markers", "slow: a workload at its full size (minutes; still part of -m gpu)")
 
 
 @pytest.fixture(scope="session")

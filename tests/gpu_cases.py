@@ -12,7 +12,12 @@ CASES = {
     "cavity2d": (2, 3, (4, 4), (0, 1, 0, 1), 1, _lib.BC_CAVITY, dict(inv_re=1 / 400.)),
     "channel3d": (3, 2, (4, 2, 2), (0, 4, 0, 1, 0, 1), 1, _lib.BC_CHANNEL, dict(inv_re=0.01)),
     "heat3d": (3, 2, (2, 2, 2), (0, 1, 0, 1, 0, 1), 0, _lib.BC_HEAT_DIRICHLET, dict()),
+    # the channel with Neumann / Robin outlet sides (MGSolverNS.C:604-681): velocity flags
+    # normal + rhs, tangential, tangential + rhs, and the pressure traction on
+    "outlet3d": (3, 2, (4, 2, 2), (0, 4, 0, 1, 0, 1), 1, _lib.BC_CHANNEL, dict(inv_re=0.01, traction=1.0)),
 }
+# natural-side flags per velocity component on the outlet (nodes off the walls)
+OUTLET_FLAGS = {"outlet3d": (5, 2, 6)}
 
 
 def initial(name, mesh_xyz, ntop, ndof, preset):
@@ -33,6 +38,15 @@ def make(name, oracle):
     osys.bc_preset(preset)
     xyz = om.xyz()
     top = nlev - 1
+    if name in OUTLET_FLAGS:
+        b0, b1 = osys.bc()
+        N = om.ntop
+        outlet = np.abs(xyz[0] - box[1]) < 1e-12
+        for a, f in enumerate(OUTLET_FLAGS[name]):
+            sel = outlet & (b0[a * N:(a + 1) * N] != 0)
+            b1[a * N:(a + 1) * N][sel] = f
+        osys.set_bc(b0, b1)
+        gs.set_bc(b0, b1)
     xold = initial(name, xyz, om.ntop, osys.ndof(top), preset)
     if kind == 1:
         # a non-trivial advecting field: the Dirichlet data plus a smooth interior field
@@ -41,6 +55,9 @@ def make(name, oracle):
         for a in range(dim):
             free = b0[a * N:(a + 1) * N] != 0
             xold[a * N:(a + 1) * N][free] += 0.3 * np.sin(3 * xyz[0][free] + a) * np.cos(2 * xyz[1][free])
+        if name in OUTLET_FLAGS:  # a pressure for the traction term
+            NL = om.nnodes(top - 1)
+            xold[dim * N:] = 0.5 - 0.1 * xyz[0][:NL] + 0.05 * xyz[1][:NL]
     qe = None
     if kind == 0:
         qe = workloads.heat_source(om.nel(top), seed=0)

@@ -210,6 +210,47 @@ def test_mixed_precision_matches_fp64_oracle(case, oracle_mod, vk):
     assert rel(gs.x(), xo) < 1e-9
 
 
+def test_mixed_fp32_block_storage_matches_fp64_oracle(case, oracle_mod):
+    """Mixed precision with FP32 storage of every V-cycle matrix (the Vanka sweeps read the
+    FP32 velocity blocks instead of the row-scaled FP16 records): the solution at 1e-12
+    is within 1e-9 of the FP64 oracle's."""
+    _assemble_both(case)
+    gs, os_ = case["gs"], case["os"]
+    ns = case["kind"] == 1
+    nu = (3, 3) if ns else (2, 2)
+    gp = ex.mg_params(eps=1e-12, max_cycles=120, nu_pre=nu[0], nu_post=nu[1],
+                      smoother=_lib.SMOOTH_VANKA if ns else _lib.SMOOTH_GS, omega=0.4,
+                      precision=_lib.PREC_MIXED, fp32_blocks=1)
+    op = or_mg(oracle_mod, eps=1e-13, max_cycles=150, nu_pre=nu[0], nu_post=nu[1], smoother=1 if ns else 0,
+               omega=0.4)
+    x0 = case["xold"]
+    gs.set_x(x0)
+    st = gs.solve(gp)
+    xo, _ = os_.mg_solve(op, x0=x0)
+    assert st.converged and st.rel_res <= 1e-12
+    assert rel(gs.x(), xo) < 1e-9
+
+
+def test_device_loop_matches_host_loop(case):
+    """Cycles run on the device (one graph launch with a conditional WHILE node, use_graph)
+    and cycles driven from the host (use_graph off) give the same bits: the same cycle
+    count, per-cycle residuals and solution."""
+    _assemble_both(case)
+    gs = case["gs"]
+    ns = case["kind"] == 1
+    out = []
+    for graph in (0, 1):
+        for prec in (_lib.PREC_FP64, _lib.PREC_MIXED):
+            gs.set_x(case["xold"])
+            st = gs.solve(ex.mg_params(eps=1e-11, max_cycles=80, nu_pre=3 if ns else 2, nu_post=3 if ns else 2,
+                                       smoother=_lib.SMOOTH_VANKA if ns else _lib.SMOOTH_GS, omega=0.4,
+                                       precision=prec, use_graph=graph))
+            assert st.converged
+            out.append((st.cycles, list(st.hist[:st.cycles]), gs.x()))
+    for a, b in zip(out[:2], out[2:]):
+        assert a[0] == b[0] and a[1] == b[1] and np.array_equal(a[2], b[2])
+
+
 def test_solve_is_deterministic(case):
     _assemble_both(case)
     gs = case["gs"]

@@ -1,0 +1,252 @@
+"""Meshes and operators from host arrays (needs a B200).
+
+exf_mesh_upload takes the hierarchy MGMesh::read_c holds (coordinates, per-level element
+connectivity in top node numbers, neighbours, and the parent elements gencase records);
+exf_sys_set_transfer takes the transfer operators in gencase's dataset layout; and
+exf_sys_check_pattern checks a level's sparsity against gencase's matrix datasets.
+
+  * the structured box pushed through the upload path gives the same bits as
+    exf_mesh_create (colourings, patterns, transfers, matrices, solutions);
+  * a copy with nodes permuted inside each nesting class and elements permuted inside
+    each level gives the permuted solution (within 1e-12);
+  * transfers supplied as gencase blocks give the same bits as those built from parents,
+    and solves refuse to start before they are set;
+  * gencase-ordered (unsorted) pattern rows are accepted, a row missing a coupling is not.
+"""
+import numpy as np
+import pytest
+
+import exfemus_b200 as ex
+from exfemus_b200 import _lib, workloads
+
+from conftest import rel
+
+pytestmark = pytest.mark.gpu
+
+CASES = {
+    "heat2d": (2, 3, (4, 4), (0, 1, 0, 1), _lib.KIND_T, _lib.BC_HEAT_DIRICHLET, dict()),
+    "cavity2d": (2, 3, (4, 4), (0, 1, 0, 1), _lib.KIND_NS, _lib.BC_CAVITY, dict(inv_re=1 / 400.)),
+    "channel3d": (3, 2, (4, 2, 2), (0, 4, 0, 1, 0, 1), _lib.KIND_NS, _lib.BC_CHANNEL, dict(inv_re=0.01)),
+}
+
+
+def structured_arrays(gm, n0):
+    """The upload arrays of a generated box, with the parent of element (ex, ey, ez) the
+    coarse element (ex/2, ey/2, ez/2)."""
+    dim, nlev = gm.dim, gm.nlev
+    conn, neigh, parent = [], [], [None]
+    for lev in range(nlev):
+        c, nb, _ = gm.conn(lev)
+        conn.append(c)
+        neigh.append(nb)
+        if lev > 0:
+            ne = [(n0[d] << lev) if d < dim else 1 for d in range(3)]
+            nc = [(n0[d] << (lev - 1)) if d < dim else 1 for d in range(3)]
+            e = np.arange(c.shape[0])
+            ex_, ey_, ez_ = e % ne[0], (e // ne[0]) % ne[1], e // (ne[0] * ne[1])
+            parent.append(((ez_ // 2) * nc[1] + ey_ // 2) * nc[0] + ex_ // 2)
+    return dict(dim=dim, nnodes=[gm.nnodes(l) for l in range(nlev)], nvert0=gm.nvert0, xyz=gm.xyz(), conn=conn,
+                neigh=neigh, parent=parent)
+
+
+def make_sys(mesh, name, xold_of=None):
+    dim, nlev, n0, box, kind, preset, pk = CASES[name]
+    s = (ex.MGSolNS if kind == _lib.KIND_NS else ex.MGSolT)(mesh)
+    s.GenBc(preset)
+    s.phys = ex.phys(**pk)
+    xyz = mesh.xyz()
+    if kind == _lib.KIND_NS:
+        x0 = workloads.ns_initial(dict(box=box, bc=preset), xyz, mesh.ntop, s.ntop_dof)
+        N = mesh.ntop
+        for a in range(dim):  # a smooth interior field, so the advection terms are exercised
+            x0[a * N:(a + 1) * N] += 0.3 * np.sin(3 * xyz[0] + a) * np.cos(2 * xyz[1])
+        b0, _ = s.bc()
+        x0[:dim * N][b0[:dim * N] == 0] = workloads.ns_initial(dict(box=box, bc=preset), xyz, N,
+                                                               s.ntop_dof)[:dim * N][b0[:dim * N] == 0]
+    else:
+        x0 = np.zeros(s.ntop_dof)
+        c, _, _ = mesh.conn(nlev - 1)  # a source that follows the element's position
+        cx, cy = xyz[0][c[:, :4]].mean(axis=1), xyz[1][c[:, :4]].mean(axis=1)
+        s.set_source(1.0 + 0.1 * np.sin(7 * cx) * np.cos(5 * cy))
+    s.set_xold(x0)
+    return s, x0
+
+
+def params(name, **kw):
+    ns = CASES[name][4] == _lib.KIND_NS
+    return ex.mg_params(eps=kw.pop("eps", 1e-11), max_cycles=200, nu_pre=3 if ns else 2, nu_post=3 if ns else 2,
+                        smoother=_lib.SMOOTH_VANKA if ns else _lib.SMOOTH_GS, omega=0.4, **kw)
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_structured_box_through_upload_is_bit_identical(name, gpu_lib):
+    dim, nlev, n0, box, kind, preset, pk = CASES[name]
+    gm = ex.Mesh(dim, nlev, n0, box)
+    um = ex.Mesh.upload(**structured_arrays(gm, n0))
+    for lev in range(nlev):
+        for a, b in zip(gm.conn(lev), um.conn(lev)):
+            assert np.array_equal(a, b)
+    gs, x0 = make_sys(gm, name)
+    us, ux0 = make_sys(um, name)
+    assert np.array_equal(x0, ux0)
+    for a, b in zip(gs.bc(), us.bc()):
+        assert np.array_equal(a, b)
+    for lev in range(nlev):
+        assert gs.colours(lev)[0] == us.colours(lev)[0]
+        assert np.array_equal(gs.colours(lev)[1], us.colours(lev)[1])
+        for a, b in zip(gs.pattern(lev), us.pattern(lev)):
+            assert np.array_equal(a, b)
+        if lev > 0:
+            for a, b in zip(gs.prol(lev), us.prol(lev)):
+                assert np.array_equal(a, b)
+        if lev < nlev - 1:
+            for a, b in zip(gs.rest(lev), us.rest(lev)):
+                assert np.array_equal(a, b)
+    gs.assemble_all()
+    us.assemble_all()
+    for lev in range(nlev):
+        assert np.array_equal(gs.matrix(lev), us.matrix(lev))
+    assert np.array_equal(gs.rhs(), us.rhs())
+    for prec in (_lib.PREC_FP64, _lib.PREC_MIXED):
+        out = []
+        for s in (gs, us):
+            s.set_x(x0)
+            st = s.solve(params(name, precision=prec))
+            assert st.converged
+            out.append((s.x(), list(st.hist[:st.cycles])))
+        assert np.array_equal(out[0][0], out[1][0])
+        assert out[0][1] == out[1][1]
+
+
+def permuted_arrays(arr, seed):
+    """Nodes permuted inside each nesting class ([0, nvert0), [nvert0, nnodes[0]),
+    [nnodes[L-1], nnodes[L])) and elements inside each level; returns the arrays and the
+    node permutation (new index of old node i)."""
+    rng = np.random.default_rng(seed)
+    bounds = [0, arr["nvert0"]] + list(arr["nnodes"])
+    pi = np.arange(bounds[-1])
+    for a, b in zip(bounds[:-1], bounds[1:]):
+        pi[a:b] = a + rng.permutation(b - a)
+    xyz = np.zeros_like(arr["xyz"])
+    xyz[:, pi] = arr["xyz"]
+    conn, neigh, parent, sig = [], [], [None], []
+    for lev, (c, nb) in enumerate(zip(arr["conn"], arr["neigh"])):
+        s = rng.permutation(c.shape[0])  # new index of old element e
+        sig.append(s)
+        cn = np.empty_like(c)
+        cn[s] = pi[c]
+        nn = np.empty_like(nb)
+        nn[s] = np.where(nb >= 0, s[np.maximum(nb, 0)], -1)
+        conn.append(cn)
+        neigh.append(nn)
+        if lev > 0:
+            pn = np.empty(c.shape[0], np.int64)
+            pn[s] = sig[lev - 1][arr["parent"][lev]]
+            parent.append(pn)
+    return dict(arr, xyz=xyz, conn=conn, neigh=neigh, parent=parent), pi
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_permuted_copy_gives_the_permuted_solution(name, gpu_lib):
+    dim, nlev, n0, box, kind, preset, pk = CASES[name]
+    gm = ex.Mesh(dim, nlev, n0, box)
+    arr = structured_arrays(gm, n0)
+    parr, pi = permuted_arrays(arr, seed=5)
+    pm = ex.Mesh.upload(**parr)
+    gs, x0 = make_sys(gm, name)
+    ps, px0 = make_sys(pm, name)
+    N, top = gm.ntop, nlev - 1
+    # DOF permutation of the top level: component blocks of N nodes, then the pressure
+    nv2 = dim if kind == _lib.KIND_NS else 1
+    dperm = np.concatenate([a * N + pi for a in range(nv2)] +
+                           ([nv2 * N + pi[:gm.nnodes(top - 1)]] if kind == _lib.KIND_NS else []))
+    assert np.array_equal(px0[dperm], x0)
+    for a, b in zip(gs.bc(), ps.bc()):
+        assert np.array_equal(b[dperm], a)
+    gs.assemble_all()
+    ps.assemble_all()
+    assert rel(ps.rhs()[dperm], gs.rhs()) < 1e-14
+    for s, x in ((gs, x0), (ps, px0)):
+        s.set_x(x)
+        assert s.solve(params(name, eps=1e-12)).converged
+    assert rel(ps.x()[dperm], gs.x()) < 1e-12
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_transfers_from_gencase_blocks(name, gpu_lib):
+    dim, nlev, n0, box, kind, preset, pk = CASES[name]
+    gm = ex.Mesh(dim, nlev, n0, box)
+    arr = structured_arrays(gm, n0)
+    ref_mesh = ex.Mesh.upload(**arr)
+    bare = ex.Mesh.upload(**dict(arr, parent=None))
+    rs, x0 = make_sys(ref_mesh, name)
+    bs, _ = make_sys(bare, name)
+    bs.assemble_all()
+    with pytest.raises(ex.ExfError) as e:
+        bs.solve(params(name))
+    assert e.value.code == _lib.EXF_ERR_STATE
+    nv2 = dim if kind == _lib.KIND_NS else 1
+    for lev in range(1, nlev):
+        rp, col, val = rs.prol(lev)
+        Nf, Nc = gm.nnodes(lev), gm.nnodes(lev - 1)
+        NLf = gm.nnodes(lev - 1)
+        NLc = gm.nnodes(lev - 2) if lev >= 2 else gm.nvert0
+        import scipy.sparse as sp
+        P = sp.csr_matrix((val, col, rp), shape=(rs.ndof(lev), rs.ndof(lev - 1)))
+        blocks = [(2, P[:Nf, :Nc], Nf, Nc)]
+        if kind == _lib.KIND_NS:
+            blocks.append((1, P[nv2 * Nf:nv2 * Nf + NLf, nv2 * Nc:nv2 * Nc + NLc], NLf, NLc))
+        for block, B, nr, nc in blocks:
+            B = sp.csr_matrix(B)
+            # gencase writes rows in its own column order: reverse each row
+            pos = np.concatenate([B.indices[B.indptr[i]:B.indptr[i + 1]][::-1] for i in range(nr)])
+            vals = np.concatenate([B.data[B.indptr[i]:B.indptr[i + 1]][::-1] for i in range(nr)])
+            bs.set_transfer(lev, 0, block, (nr, nc), B.indptr, pos, vals)
+            R = sp.csr_matrix(B.T)  # compute_res_qq: the transposed embedding, |v| > 1e-6
+            R.data[np.abs(R.data) <= 1e-6] = 0.0
+            R.eliminate_zeros()
+            R.sort_indices()
+            bs.set_transfer(lev - 1, 1, block, (nc, nr), R.indptr, R.indices, R.data)
+    for lev in range(nlev):
+        if lev > 0:
+            for a, b in zip(rs.prol(lev), bs.prol(lev)):
+                assert np.array_equal(a, b)
+        if lev < nlev - 1:
+            for a, b in zip(rs.rest(lev), bs.rest(lev)):
+                assert np.array_equal(a, b)
+    rs.assemble_all()
+    out = []
+    for s in (rs, bs):
+        s.set_x(x0)
+        st = s.solve(params(name))
+        assert st.converged
+        out.append(s.x())
+    assert np.array_equal(out[0], out[1])
+
+
+@pytest.mark.parametrize("name", ["heat2d", "cavity2d"])
+def test_pattern_check_against_gencase_blocks(name, gpu_lib):
+    dim, nlev, n0, box, kind, preset, pk = CASES[name]
+    gm = ex.Mesh(dim, nlev, n0, box)
+    s, _ = make_sys(gm, name)
+    rng = np.random.default_rng(2)
+    for lev in range(nlev):
+        rp, col = s.pattern(lev)
+        N = gm.nnodes(lev)
+        NL = gm.nnodes(lev - 1) if lev else gm.nvert0
+        nv2 = dim if kind == _lib.KIND_NS else 1
+        blocks = {22: (0, N, 0, N)}
+        if kind == _lib.KIND_NS:
+            blocks.update({21: (0, N, nv2 * N, NL), 12: (nv2 * N, NL, 0, N), 11: (nv2 * N, NL, nv2 * N, NL)})
+        for block, (r0, nr, c0, nc) in blocks.items():
+            rows = []
+            for i in range(nr):
+                c = col[rp[r0 + i]:rp[r0 + i + 1]]
+                c = c[(c >= c0) & (c < c0 + nc)] - c0
+                rows.append(rng.permutation(c))
+            length = np.concatenate([[0], np.cumsum([len(r) for r in rows])])
+            pos = np.concatenate(rows)
+            assert s.check_pattern(lev, block, (nr, nc), length, pos) == _lib.EXF_OK
+            bad = np.concatenate([rows[0][1:]] + rows[1:])
+            blen = np.concatenate([[0], np.cumsum([len(rows[0]) - 1] + [len(r) for r in rows[1:]])])
+            assert s.check_pattern(lev, block, (nr, nc), blen, bad) == _lib.EXF_ERR_ARG

@@ -294,3 +294,88 @@ def test_ns_operator_reproduces_quadratic_flow(oracle_mod, dim):
         ref = expect[a][interior]
         assert np.abs(got - ref).max() <= 1e-12 * np.abs(ref).max(), (a, np.abs(got - ref).max())
     assert np.abs(y[dim * N:]).max() <= 1e-13 * np.abs(y[:dim * N]).max()
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+def test_ns_neumann_sides(oracle_mod, dim):
+    """The natural-side branch of MGSolNS::GenMatRhs (template_appl/nse/SRC/MGSolverNS.C:
+    604-681) on the outlet x = L of a box, every other wall Dirichlet:
+      bc1 = 1 (normal):     velocity row a gains n_a^2 int_side phi_i   (lumped Robin)
+      bc1 = 2 (tangential): row a gains (1 - n_a^2) int_side phi_i
+      bc1 = 4 (rhs) with traction on: rhs row a gains -n_a int_side phi_i p_old
+    with n the outward normal (1, 0, 0); rows of nodes on a Dirichlet wall take nothing."""
+    n0 = (2, 2) if dim == 2 else (2, 1, 1)
+    box = (0, 2, 0, 1) if dim == 2 else (0, 2, 0, 1, 0, 1)
+    m = oracle_mod.OrMesh(dim, 2, n0, box)
+    X = m.xyz()
+    N = m.nnodes(1)
+    NL = m.nnodes(0)
+    ntop = m.ntop
+    h = [(box[2 * d + 1] - box[2 * d]) / (n0[d] << 1) for d in range(dim)]
+    outlet = np.abs(X[0] - box[1]) < 1e-12
+    wall = np.zeros(ntop, bool)
+    for d in range(dim):
+        wall |= np.abs(X[d] - box[2 * d]) < 1e-12
+        if d > 0:
+            wall |= np.abs(X[d] - box[2 * d + 1]) < 1e-12
+    # int over the outlet face of phi_i: product of the 1D Simpson weights of the face axes
+    W = np.ones(ntop)
+    for d in range(1, dim):
+        k = np.rint((X[d] - box[2 * d]) / (h[d] / 2)).astype(int)
+        kmax = 2 * (n0[d] << 1)
+        w1 = np.where(k % 2 == 1, 4 * h[d] / 6, np.where((k == 0) | (k == kmax), h[d] / 6, 2 * h[d] / 6))
+        W *= w1
+    W[~outlet] = 0.0
+
+    def run(flags, traction, p_old=0.0):
+        s = oracle_mod.OrSys(m, 1)
+        n = s.ndof(1)
+        b0 = np.ones(n, np.int32)
+        b1 = np.zeros(n, np.int32)
+        for a in range(dim):
+            b0[a * N:(a + 1) * N][wall] = 0  # the outlet's corners and edges belong to the walls
+            b1[a * N:(a + 1) * N][outlet & ~wall] = flags[a]
+        s.set_bc(b0, b1)
+        xold = np.zeros(n)
+        xold[dim * N:] = p_old
+        s.assemble(1, 1, or_phys(oracle_mod, inv_re=0.1, traction=traction), xold=xold)
+        rp, col = s.pattern(1)
+        return sp.csr_matrix((s.matrix(1), col, rp), shape=(n, n)), s.rhs(), b0
+
+    A0, r0, b0 = run([0] * dim, 0.0)
+    free = np.concatenate([b0[a * N:(a + 1) * N] for a in range(dim)]).astype(bool)
+    A1, _, _ = run([1] * dim, 0.0)
+    D = (A1 - A0).tocsr()
+    expect = np.concatenate([W * (1.0 if a == 0 else 0.0) for a in range(dim)]) * free
+    assert abs(D - sp.diags(np.concatenate([expect, np.zeros(NL)]))).max() < 1e-14
+    A2, _, _ = run([2] * dim, 0.0)
+    D = (A2 - A0).tocsr()
+    expect = np.concatenate([W * (0.0 if a == 0 else 1.0) for a in range(dim)]) * free
+    assert abs(D - sp.diags(np.concatenate([expect, np.zeros(NL)]))).max() < 1e-14
+    P = 0.75
+    _, r4, _ = run([4] * dim, 1.0, p_old=P)
+    _, r4off, _ = run([4] * dim, 0.0, p_old=P)
+    expect = np.concatenate([-P * W * (1.0 if a == 0 else 0.0) for a in range(dim)]) * free
+    assert np.abs((r4 - r4off)[:dim * N] - expect).max() < 1e-14
+    assert np.abs(r4off - r0).max() == 0.0
+
+
+def test_face0_normal_follows_the_reference_side_order(oracle_mod):
+    """MGFE::normal_g (src/MGFE.C:1601-1646) takes (x1 - x0) x (x3 - x0) on the side's nodes;
+    on the hex27 face {0, 1, 2, 3, ...} of _surf_top (z = z0) that is +z, so the traction
+    term there has the sign of an inward normal (outward on every other face)."""
+    m = oracle_mod.OrMesh(3, 1, (1, 1, 1), (0, 1, 0, 1, 0, 1))
+    X = m.xyz()
+    bottom = np.abs(X[2]) < 1e-12
+    s = oracle_mod.OrSys(m, 1)
+    n = s.ndof(0)
+    N = m.nnodes(0)
+    b0 = np.ones(n, np.int32)
+    b1 = np.zeros(n, np.int32)
+    b1[2 * N:3 * N][bottom] = 4
+    s.set_bc(b0, b1)
+    xold = np.zeros(n)
+    xold[3 * N:] = 1.0
+    s.assemble(0, 1, or_phys(oracle_mod, inv_re=0.1, traction=1.0), xold=xold)
+    r = s.rhs()[2 * N:3 * N]
+    assert r[bottom].sum() < 0 and abs(r[bottom].sum() + 1.0) < 1e-13  # -n_z int p = -(+1)(1)
