@@ -48,6 +48,11 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default=WORKLOAD)
     ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--nlev", type=int, default=None,
+                    help="profiling modes (vcycle, step): levels of the workload's hierarchy (fewer levels, "
+                         "a smaller fine level of the same kernels)")
+    ap.add_argument("--vanka-kernel", type=int, default=None,
+                    help="profiling modes: EXF_VANKA_* kernel of the Vanka sweeps (default AUTO)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--mode", default="bench", choices=["bench", "vcycle", "step", "workloads"],
                     help="vcycle: assemble once and run one mixed and one FP64 V-cycle; step: one Picard "
@@ -145,11 +150,13 @@ def host_info():
 
 def config_dict(ndof, nnz_fine, ws):
     """The workload as both arms report it (identical dicts: same system, same solver)."""
+    from exfemus_b200 import workloads
     return {"workload": WORKLOAD, "mesh": "64x16x16 hex27/hex8, 4 levels (8x2x2 coarsest)", "ndof": int(ndof),
             "nnz_fine": int(nnz_fine),
             "picard_step": "first Picard system every step (x_old = initial field): assembly of all levels + "
                            "coarse factorisation + solve to 1e-10 + x_old update; value = factorisation + solve",
-            "solver": "V-cycle, Vanka 3/3 (doubled below the top), omega 0.4, direct coarse solve",
+            "solver": "V-cycle, Vanka 3/3 (doubled below the top), omega %g, direct coarse solve"
+                      % workloads.vanka_omega(workloads.WORKLOADS[WORKLOAD]),
             "l2": "inputs larger than L2 (fine matrix %.1f M nonzeros, %.2f GB as FP64 CSR)"
                   % (nnz_fine / 1e6, nnz_fine * 12 / 1e9),
             "parallelism": "replicas" if ws > 1 else "single GPU"}
@@ -190,7 +197,7 @@ def cpu_reference(threads):
     t_factor = time.perf_counter() - t0
     mp = oracle.OrMgParams()
     mp.eps, mp.max_cycles, mp.gamma, mp.nu_pre, mp.nu_post = 1e-30, 1, 1, 3, 3
-    mp.double_below_top, mp.smoother, mp.omega, mp.corr_damp = 1, 1, workloads.VANKA_OMEGA, 0.95
+    mp.double_below_top, mp.smoother, mp.omega, mp.corr_damp = 1, 1, workloads.vanka_omega(w), 0.95
     nel = sum(m.nel(l) for l in range(w["nlev"]))
     return dict(t_asm=t_asm, t_factor=t_factor, nel=nel, ndof=s.ndof(top), nnz=s.L.or_sys_nnz(s.h, top),
                 sys=s, mp=mp, x0=x0, threads=oracle.get_threads())
@@ -252,12 +259,14 @@ def run_vcycle(args, local):
     """One assembly and one V-cycle per precision on the workload (kernel profiling)."""
     import exfemus_b200 as ex
     from exfemus_b200 import _lib
-    case = ex.make_case(args.workload, device=local)
+    case = ex.make_case(args.workload, device=local, **({"nlev": args.nlev} if args.nlev else {}))
     ns = case["NS"]
     ns.assemble_all()
     for prec in (_lib.PREC_MIXED, _lib.PREC_FP64):
         p = case["mg_NS"]
         p.precision, p.max_cycles = prec, 1
+        if args.vanka_kernel is not None:
+            p.vanka_kernel = args.vanka_kernel
         st = ns.solve(p)
         print("precision %d: 1 cycle, rel %.3e, %.3f ms" % (prec, st.rel_res, st.seconds * 1e3), flush=True)
 
@@ -266,10 +275,12 @@ def run_step(args, local):
     """One Picard step of the workload from its initial field (kernel launch list)."""
     import exfemus_b200 as ex
     from exfemus_b200 import _lib
-    case = ex.make_case(args.workload, device=local)
+    case = ex.make_case(args.workload, device=local, **({"nlev": args.nlev} if args.nlev else {}))
     ns = case["NS"]
     p = case["mg_NS"]
     p.precision, p.eps = _lib.PREC_MIXED, 1e-10
+    if args.vanka_kernel is not None:
+        p.vanka_kernel = args.vanka_kernel
     ns.assemble_all()
     st = ns.solve(p)
     print("step: %d cycles, rel %.3e, %.3f ms" % (st.cycles, st.rel_res, st.seconds * 1e3), flush=True)
@@ -341,7 +352,7 @@ def run_workloads(args, local):
     g[1:] = 0.1 * np.random.default_rng(1).standard_normal(w["modes"] - 1) / np.arange(2, w["modes"] + 1)
     x0 = workloads.t_initial(w, xyz, t.ntop_dof, g_modes=g)
     wj = np.ascontiguousarray(top_wall_weights(xyz))
-    p = ex.mg_params(eps=1e-12, max_cycles=400, smoother=_lib.SMOOTH_GS, nu_pre=3, nu_post=3)
+    p = ex.mg_params(eps=1e-11, max_cycles=400, smoother=_lib.SMOOTH_GS, nu_pre=3, nu_post=3)
     stf = _lib.ExfSolveStats()
     t.set_xold(x0)
     t.set_source(qe)

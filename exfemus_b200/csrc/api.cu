@@ -1267,12 +1267,12 @@ int exf_level_bytes(exf_sys *s, int lev, int precision, double *spmv_bytes, doub
   auto vrow = [&](int n) {  // bytes of the d velocity rows of node n
     return (double)(qp[n + 1] - qp[n]) * (d * d * vb + 4.) + (double)(lp[n + 1] - lp[n]) * (d * vb + 4.) + 8.;
   };
-  // a star row as the Vanka row kernel reads it: FP16 records in the FP32 smoother
-  // (3D: 16 + 8 bytes per block; 2D: 8 + 4), FP64 planes + column otherwise; pressure
-  // couplings; its descriptor (16) and, for FP16, its d row scales
+  // a star row as the Vanka row kernel reads it: FP16 values and the column in the FP32
+  // smoother (3D: 18 + 4 bytes per block; 2D: 8 + 4), FP64 planes + column otherwise;
+  // pressure couplings; its descriptor (16) and, for FP16, its d row scales
   const bool h16 = precision == EXF_PREC_MIXED;
   auto srow = [&](int n) {
-    const double blk = h16 ? (d == 3 ? 24. : 12.) : d * d * vb + 4.;
+    const double blk = h16 ? (d == 3 ? 22. : 12.) : d * d * vb + 4.;
     return (double)(qp[n + 1] - qp[n]) * blk + (double)(lp[n + 1] - lp[n]) * (d * vb + 4.) + 16. +
            (h16 ? d * 4. : 0.);
   };

@@ -216,9 +216,11 @@ struct SysLevel {
   DBuf<uint2> h16cx;
   DBuf<uint32_t> h16qc;
   DBuf<float> vsc;
-  // BULK smoother (3D FP32): the h16 / h16cx records of every star row copied row after
-  // row in sweep order, each row padded to an even count, so that the rows of a colour are
-  // one contiguous stream; allocated on the first BULK sweep, refreshed after assembly
+  // BULK smoother (3D FP32): every star row as 16-byte records, row after row in sweep
+  // order (row scales and node; counts; the FP16 values 0..7 of each block; the block
+  // columns, 4 per record; the 9th values, 8 per record; the pressure couplings), so that
+  // the rows of a colour are one contiguous stream; allocated on the first BULK sweep,
+  // refreshed after assembly.
   DBuf<long long> soff;        // [nvrows + 2] first record of each star row (last repeated)
   std::vector<long long> soff_h;
   long long nstar = 0;         // soff[nvrows]
@@ -227,7 +229,6 @@ struct SysLevel {
   std::vector<int> bsched_coff;
   int bsched_G = 0;
   DBuf<uint4> sv;
-  DBuf<uint2> scx;
   // transfers: Pq/Pl from level-1 to this level (fine rows), Rq/Rl from this level+1
   Transfer Pq, Pl, Rq, Rl;
   DBuf<double> rmask;    // [ndof] restriction row mask (bc0 % 2 of the top DOF)

@@ -534,8 +534,10 @@ int build_colours(exf_sys *s) {
       EXF_CUDA(cudaMemcpy(L.vrinfo.p, vri.data(), vri.size() * sizeof(int4), cudaMemcpyHostToDevice));
       if (dim == 3) {  // star-major record offsets of the BULK smoother
         std::vector<long long> so(vri.size() + 1, 0);
-        for (size_t g = 0; g < vri.size(); g++)  // row scales, blocks, couplings; even count
-          so[g + 1] = so[g] + ((2 + (vri[g].w & 0xff) + ((vri[g].w >> 8) & 0xff)) & ~1);
+        for (size_t g = 0; g < vri.size(); g++) {  // 2 header records, blocks, columns, 9th values, couplings
+          const int nk = vri[g].w & 0xff, nl = (vri[g].w >> 8) & 0xff;
+          so[g + 1] = so[g] + 2 + nk + ((nk + 3) >> 2) + ((nk + 7) >> 3) + nl;
+        }
         L.nstar = so.back();
         so.push_back(so.back());  // 16-byte copies of offset pairs may read one entry past the end
         EXF_TRY(L.soff.alloc(so.size()));

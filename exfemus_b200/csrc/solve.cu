@@ -1299,19 +1299,22 @@ __global__ void k_vanka_apply(const int *__restrict__ vrows, int nr, long gbase,
   }
 }
 
-// BULK phase 1 for the 3D FP32 smoother.  Each star row is stored star-major (sv, scx:
-// row after row in sweep order) as one self-contained record run: a header {row scales,
-// node} / {nqq | nql << 8}, the FP16 blocks, and the pressure couplings {vp 0..2, column},
-// so a colour's rows are one contiguous stream.  Persistent CTAs own contiguous row
-// ranges, cut on the host into stages of whole rows (at most 32 rows and CAPB records:
-// the schedule, {first row, first record} per stage).  One producer warp fills stage
-// buffers with three bulk copies (values, columns, the rows' record offsets) completed
-// on the stage's "full" mbarrier, with no global load on its path; NWC consumer warps
-// take the stages' row pairs round-robin (16 lanes per row, every column gather of a
-// row issued at once, x gathers mostly L1 hits) and release a stage on its "empty"
-// mbarrier.  Each lane visits the blocks and couplings of its row in the same order as
-// the ROWS kernel, so both give the same sums.  Every wait is bounded: a wait that runs
-// out sets the system's wait flag and the kernel leaves once its copies have landed.
+// BULK phase 1 for the 3D FP32 smoother.  Each star row is stored star-major (sv: row
+// after row in sweep order) as one self-contained run of 16-byte records: {row scales,
+// node}, {nqq | nql << 8}, the FP16 values 0..7 of each block, the block columns (4 per
+// record), the blocks' 9th values (8 per record) and the pressure couplings {vp 0..2,
+// column}: 22 bytes per block, so a colour's rows are one contiguous stream.  (Reading the
+// columns from qq_col through L2 instead, 18 bytes per block in the stream, was slower:
+// 1.16 against 1.07 ms per channel3d fine sweep.)  Persistent CTAs own contiguous row ranges, cut on
+// the host into stages of whole rows (at most 32 rows and CAPB records: the schedule,
+// {first row, first record} per stage).  One producer warp fills stage buffers with two
+// bulk copies (the records and the rows' record offsets) completed on the stage's "full"
+// mbarrier, with no global load on its path; NWC consumer warps take the stages' row pairs
+// round-robin (16 lanes per row, every column gather of a row issued at once, x gathers
+// mostly L1 hits) and release a stage on its "empty" mbarrier.  Each lane visits the
+// blocks and couplings of its row in the same order as the ROWS kernel, so both give the
+// same sums.  Every wait is bounded: a wait that runs out sets the system's wait flag and
+// the kernel leaves once its copies have landed.
 #ifndef EXF_WAIT_TRIES
 #define EXF_WAIT_TRIES (1 << 22)
 #endif
@@ -1351,8 +1354,7 @@ static int star_pack(exf_sys *s, int lev);
 
 template <int STG, int CAPB>
 struct BulkSmem {
-  uint4 val[STG][CAPB];   // row headers, FP16 values 0..7 of each block, couplings
-  uint2 cx[STG][CAPB];    // {nqq | nql << 8, 0}, {column, value 8}, {column, 0}
+  uint4 val[STG][CAPB];   // the stage's star-row records
   long long so[STG][34];  // record offsets of the stage's rows (from an even row index)
   int nrow[STG];          // rows in the stage; 0 ends the stream
   int gfirst[STG];        // colour row index of the stage's first row
@@ -1363,8 +1365,7 @@ template <int NWC, int STG, int CAPB, int UNR, int LPR>
 __global__ void __launch_bounds__(32 * (NWC + 1), 1)
     k_vanka_rows_bulk(const longlong2 *__restrict__ sched, const int *__restrict__ sched_off, int gbase,
                       const int4 *__restrict__ pinfo, int npatch, int N, const long long *__restrict__ soff,
-                      const uint4 *__restrict__ sv, const uint2 *__restrict__ scx,
-                      const int *__restrict__ qq_col, const int *__restrict__ ql_col, long nqqL,
+                      const uint4 *__restrict__ sv, const int *__restrict__ qq_col, const int *__restrict__ ql_col, long nqqL,
                       const float *__restrict__ pv, const float *__restrict__ pp, const float *__restrict__ x,
                       const float *__restrict__ b, float *__restrict__ res, long pres_off,
                       int *__restrict__ wait_flag) {
@@ -1414,16 +1415,13 @@ __global__ void __launch_bounds__(32 * (NWC + 1), 1)
                                           __shfl_sync(0xffffffffu, win.y, it + 1 - wb));
       if (lane == 0) {
         const int r = (int)st.x, m = (int)(en.x - st.x);
-        const unsigned nb = (unsigned)(en.y - st.y);  // records (even)
+        const unsigned nb = (unsigned)(en.y - st.y);  // records
         const long long ga = ((long long)gbase + r) & ~1LL;
         const unsigned ns = (unsigned)((((long long)gbase + r + m + 1 - ga) + 1) & ~1LL);  // offsets, even
         S.nrow[s] = m;
         S.gfirst[s] = r;
-        mbar_arrive_tx(&S.full[s], nb * 24u + ns * 8u);
-        if (nb > 0) {
-          bulk_g2s(&S.val[s][0], sv + st.y, nb * 16u, &S.full[s]);
-          bulk_g2s(&S.cx[s][0], scx + st.y, nb * 8u, &S.full[s]);
-        }
+        mbar_arrive_tx(&S.full[s], nb * 16u + ns * 8u);
+        if (nb > 0) bulk_g2s(&S.val[s][0], sv + st.y, nb * 16u, &S.full[s]);
         bulk_g2s(&S.so[s][0], soff + ga, ns * 8u, &S.full[s]);
       }
       __syncwarp();
@@ -1477,11 +1475,14 @@ __global__ void __launch_bounds__(32 * (NWC + 1), 1)
       const bool valid = j < m;
       float acc[3] = {0.f, 0.f, 0.f};
       const int of = valid ? (int)(S.so[s][d + j] - base) : 0;
-      const uint4 *vr = &S.val[s][of];  // [0]: header; [1, nk]: blocks; then couplings
-      const uint2 *cr = &S.cx[s][of];
+      const uint4 *vr = &S.val[s][of];  // [0], [1]: header; [2, 2 + nk): blocks; columns; 9th values; couplings
       const uint4 hs = vr[0];
-      const int rw = valid ? (int)cr[0].x : 0;
+      const int rw = valid ? (int)vr[1].x : 0;
       const int nk = rw & 0xff, nl = (rw >> 8) & 0xff;
+      const int c4 = (nk + 3) >> 2;
+      const int *qc = reinterpret_cast<const int *>(vr + 2 + nk);  // the row's block columns
+      const __half *v8 = reinterpret_cast<const __half *>(vr + 2 + nk + c4);
+      const uint4 *cpl = vr + 2 + nk + c4 + ((nk + 7) >> 3);
       float4 bv = make_float4(0.f, 0.f, 0.f, 0.f);
       if (valid && hl == 0) bv = reinterpret_cast<const float4 *>(b)[hs.w];
       // the first two pressure couplings of the lane, gathered before the blocks (added
@@ -1489,11 +1490,11 @@ __global__ void __launch_bounds__(32 * (NWC + 1), 1)
       uint4 cq0 = make_uint4(0u, 0u, 0u, 0u), cq1 = cq0;
       float pq0 = 0.f, pq1 = 0.f;
       if (hl < nl) {
-        cq0 = vr[1 + nk + hl];
+        cq0 = cpl[hl];
         pq0 = x4[(int)cq0.w].w;
       }
       if (hl + LPR < nl) {
-        cq1 = vr[1 + nk + hl + LPR];
+        cq1 = cpl[hl + LPR];
         pq1 = x4[(int)cq1.w].w;
       }
       for (int i0 = 0; i0 < nk; i0 += UNR * LPR) {
@@ -1502,7 +1503,7 @@ __global__ void __launch_bounds__(32 * (NWC + 1), 1)
 #pragma unroll
         for (int u = 0; u < UNR; u++) {
           const int i = i0 + u * LPR + hl;
-          c[u] = i < nk ? (int)cr[1 + i].x : -1;
+          c[u] = i < nk ? qc[i] : -1;
         }
 #pragma unroll
         for (int u = 0; u < UNR; u++) xb[u] = c[u] >= 0 ? x4[c[u]] : make_float4(0.f, 0.f, 0.f, 0.f);
@@ -1510,14 +1511,14 @@ __global__ void __launch_bounds__(32 * (NWC + 1), 1)
         for (int u = 0; u < UNR; u++) {
           const int i = i0 + u * LPR + hl;
           if (c[u] >= 0) {
-            const uint4 h = vr[1 + i];
+            const uint4 h = vr[2 + i];
             float v[9];
             float2 f;
             f = h2f(h.x); v[0] = f.x; v[1] = f.y;
             f = h2f(h.y); v[2] = f.x; v[3] = f.y;
             f = h2f(h.z); v[4] = f.x; v[5] = f.y;
             f = h2f(h.w); v[6] = f.x; v[7] = f.y;
-            v[8] = h2f(cr[1 + i].y).x;
+            v[8] = __half2float(v8[i]);
             const float xx[3] = {xb[u].x, xb[u].y, xb[u].z};
 #pragma unroll
             for (int a = 0; a < 3; a++)
@@ -1542,7 +1543,7 @@ __global__ void __launch_bounds__(32 * (NWC + 1), 1)
         acc[2] += __uint_as_float(cq1.z) * pq1;
       }
       for (int i = hl + 2 * LPR; i < nl; i += LPR) {  // further couplings
-        const uint4 q4 = vr[1 + nk + i];
+        const uint4 q4 = cpl[i];
         const float pval = x4[(int)q4.w].w;
         acc[0] += __uint_as_float(q4.x) * pval;
         acc[1] += __uint_as_float(q4.y) * pval;
@@ -1590,7 +1591,7 @@ __global__ void __launch_bounds__(32 * (NWC + 1), 1)
 #define EXF_BK_STG 4
 #endif
 #ifndef EXF_BK_CAPB
-#define EXF_BK_CAPB 2048
+#define EXF_BK_CAPB 3072
 #endif
 #ifndef EXF_BK_UNR
 #define EXF_BK_UNR 8
@@ -1677,7 +1678,8 @@ static int vanka_sweep_rows(exf_sys *s, int lev, const exf_mg_params *p, T *x, c
           (p->vanka_kernel == EXF_VANKA_BULK || (p->vanka_kernel == EXF_VANKA_AUTO && EXF_AUTO_BULK && big))) {
         constexpr int NWC = EXF_BK_NWC, STG = EXF_BK_STG, CAPB = EXF_BK_CAPB, UNR = EXF_BK_UNR,
                       BLPR = EXF_BK_LPR;
-        static_assert(CAPB >= 512, "a stage holds the longest row (header, 255 blocks, 255 couplings, pad)");
+        static_assert(CAPB >= 2 + 255 + 64 + 32 + 255,
+                      "a stage holds the longest row (header, 255 blocks with columns and 9th values, 255 couplings)");
         using SM = BulkSmem<STG, CAPB>;
         auto kern = k_vanka_rows_bulk<NWC, STG, CAPB, UNR, BLPR>;
         // CTAs per SM, per device (threads driving systems on one device may both resolve
@@ -1712,7 +1714,7 @@ static int vanka_sweep_rows(exf_sys *s, int lev, const exf_mg_params *p, T *x, c
         EXF_CUDA(launch_pdl(kern, dim3(grid), dim3(32 * (NWC + 1)), sizeof(SM), s->stream,
                             (const longlong2 *)L.bsched.p, (const int *)(L.bsched_off.p + L.bsched_coff[c]),
                             L.vrow_off[c], pin, n, L.N, (const long long *)L.soff.p, (const uint4 *)L.sv.p,
-                            (const uint2 *)L.scx.p, (const int *)L.qq_col.p, (const int *)L.ql_col.p, L.nqqL,
+                            (const int *)L.qq_col.p, (const int *)L.ql_col.p, L.nqqL,
                             (const float *)VT<T>::pv(L), (const float *)VT<T>::pp(L), (const float *)x,
                             (const float *)b, (float *)res, pres_off, s->wait_flag.p));
         EXF_CUDA(launch_pdl(k_vanka_solve<T, D, NTS, I4, SU>, dim3(n), dim3(NTS), 0, s->stream, pin, L.N, L.vrows.p,
@@ -1911,34 +1913,42 @@ __global__ void k_pack16(int N, const int *__restrict__ qq_ptr, const int *__res
 __global__ void k_pack_star(int nrows, const int4 *__restrict__ rinfo, const long long *__restrict__ soff, int N,
                             const uint4 *__restrict__ h16, const uint2 *__restrict__ cx,
                             const float *__restrict__ vsc, const int *__restrict__ ql_col,
-                            const float *__restrict__ vp, long nql, uint4 *__restrict__ sv,
-                            uint2 *__restrict__ scx) {
+                            const float *__restrict__ vp, long nql, uint4 *__restrict__ sv) {
   const long g = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (g >= nrows) return;
   const int4 ri = rinfo[g];
   const int node = ri.x, k0 = ri.y, l0 = ri.z, nk = ri.w & 0xff, nl = (ri.w >> 8) & 0xff;
+  const int c4 = (nk + 3) >> 2, n8 = (nk + 7) >> 3;
   const long long o = soff[g];
   const int w = (int)(soff[g + 1] - o);
   for (int i = lane; i < w; i += 32) {
     uint4 v = make_uint4(0u, 0u, 0u, 0u);
-    uint2 c = make_uint2(0u, 0u);
     if (i == 0) {
       v = make_uint4(__float_as_uint(vsc[node]), __float_as_uint(vsc[(long)N + node]),
                      __float_as_uint(vsc[2L * N + node]), (unsigned)node);
-      c = make_uint2((unsigned)(nk | (nl << 8)), 0u);
-    } else if (i <= nk) {
-      v = h16[k0 + i - 1];
-      c = cx[k0 + i - 1];
-    } else if (i <= nk + nl) {
-      const long q = l0 + i - 1 - nk;
-      const int col = ql_col[q];
+    } else if (i == 1) {
+      v = make_uint4((unsigned)(nk | (nl << 8)), 0u, 0u, 0u);
+    } else if (i < 2 + nk) {
+      v = h16[k0 + i - 2];
+    } else if (i < 2 + nk + c4) {  // columns of blocks 4 (i - 2 - nk) ..
+      const int b0 = 4 * (i - 2 - nk);
+      unsigned c[4];
+#pragma unroll
+      for (int t = 0; t < 4; t++) c[t] = b0 + t < nk ? cx[k0 + b0 + t].x : 0u;
+      v = make_uint4(c[0], c[1], c[2], c[3]);
+    } else if (i < 2 + nk + c4 + n8) {  // 9th values of blocks 8 (i - 2 - nk - c4) ..
+      const int b0 = 8 * (i - 2 - nk - c4);
+      unsigned h[8];
+#pragma unroll
+      for (int t = 0; t < 8; t++) h[t] = b0 + t < nk ? (cx[k0 + b0 + t].y & 0xffffu) : 0u;
+      v = make_uint4(h[0] | (h[1] << 16), h[2] | (h[3] << 16), h[4] | (h[5] << 16), h[6] | (h[7] << 16));
+    } else {
+      const long q = l0 + i - 2 - nk - c4 - n8;
       v = make_uint4(__float_as_uint(vp[q]), __float_as_uint(vp[nql + q]), __float_as_uint(vp[2 * nql + q]),
-                     (unsigned)col);
-      c = make_uint2((unsigned)col, 0u);
+                     (unsigned)ql_col[q]);
     }
     sv[o + i] = v;
-    scx[o + i] = c;
   }
 }
 
@@ -1949,12 +1959,10 @@ static int star_pack(exf_sys *s, int lev) {
     return EXF_ERR_STATE;
   }
   EXF_TRY(L.sv.ensure((size_t)L.nstar));
-  EXF_TRY(L.scx.ensure((size_t)L.nstar));
   const int nrows = L.vrow_off[L.ncolour];
   if (nrows > 0)
     k_pack_star<<<nblk((long)nrows * 32, 256), 256, 0, s->stream>>>(
-        nrows, L.vrinfo.p, L.soff.p, L.N, L.h16.p, L.h16cx.p, L.vsc.p, L.ql_col.p, L.A32.vp.p, L.nql, L.sv.p,
-        L.scx.p);
+        nrows, L.vrinfo.p, L.soff.p, L.N, L.h16.p, L.h16cx.p, L.vsc.p, L.ql_col.p, L.A32.vp.p, L.nql, L.sv.p);
   EXF_CUDA(cudaGetLastError());
   return EXF_OK;
 }
@@ -2052,8 +2060,9 @@ template int smooth<double>(exf_sys *, int, const exf_mg_params *, int, double *
 template int smooth<float>(exf_sys *, int, const exf_mg_params *, int, float *, const float *);
 
 // -------------------------------------------------- coarsest direct solve
-// In-place Gauss-Jordan inversion with partial pivoting, once per assembly, in ONE
-// cooperative kernel (two grid-wide barriers per pivot).  Pivot rows are not swapped:
+// In-place Gauss-Jordan inversion with partial pivoting, once per assembly: blocked (a
+// single-CTA panel of 16 pivots, then one rank-16 update) where the panel fits shared
+// memory, otherwise ONE cooperative kernel with a grid-wide barrier per pivot.  Pivot rows are not swapped:
 // step k pivots on the largest |a_ik| among unused rows p_k, which leaves
 // W[p_k][j] = A0^{-1}[k][p_j]; the extraction kernel undoes the permutation.  Each coarse
 // solve is then one dense GEMV in FP64.  Pressure-gauge rows become identity rows in the
@@ -2177,6 +2186,267 @@ __global__ void __launch_bounds__(NT)
   }
 }
 
+// ---- blocked Gauss-Jordan: NB pivots per block.  The NB steps of a block change every
+// column outside the block j by W[:, j] += (H - E_P) W[P, j], where P are the block's pivot
+// rows, W[P, j] their values before the block, E_P the unit columns e_{p_t} and H the
+// block's own columns after its NB steps (each step k is W <- (I + g_k e_{p_k}^T) W, and
+// such products stay of the form I + (H - E_P) E_P^T).  One CTA factors the n x NB panel
+// with the same pivot rule as k_gj_coop; a grid-wide kernel then applies the rank-NB
+// change to the other columns.
+//
+// Every row of the panel belongs to one thread, which searches, eliminates and (as the
+// pivot row) scales it.  Per pivot: the warps' candidate keys -> barrier -> every warp
+// reduces the keys itself; the pivot row's owner scales its row and publishes the scaled
+// copy -> barrier -> every thread eliminates its rows against the published copy.  (A
+// one-barrier form that left the pivot row unscaled for the other threads and scaled it
+// one step later gave wrong, run-dependent factors on B200 once a thread held two rows;
+// the published copy with its own barrier is correct at every size.)
+
+// R[t][j] = W[p_t][j]: the block's pivot rows before the block, for the columns outside
+// the block (the block's own columns of W may already hold H); CH loads in flight per
+// thread
+template <int NT, int CH>
+__device__ __forceinline__ void gj_copy_pivot_rows(const double *__restrict__ W, int n, int nb, const int *spiv,
+                                                   double *__restrict__ R) {
+  const long tot = (long)nb * n;
+  for (long q0 = threadIdx.x; q0 < tot; q0 += (long)CH * NT) {
+    double v[CH];
+#pragma unroll
+    for (int c = 0; c < CH; c++) {
+      const long q = q0 + (long)c * NT;
+      v[c] = q < tot ? W[(long)spiv[q / n] * n + q % n] : 0.;
+    }
+#pragma unroll
+    for (int c = 0; c < CH; c++) {
+      const long q = q0 + (long)c * NT;
+      if (q < tot) R[q] = v[c];
+    }
+  }
+}
+
+// the panel in registers: thread tid holds rows tid + r * NT (r < RPT), n <= RPT * NT
+template <int NB, int NT, int RPT>
+__global__ void __launch_bounds__(NT, 1)
+    k_gj_panel_reg(double *__restrict__ W, int n, int k0, int nb, int *__restrict__ pivrow, int *__restrict__ used,
+                   double *__restrict__ Hm, double *__restrict__ R, int *__restrict__ bad) {
+  __shared__ unsigned long long sk[2][NT / 32];
+  __shared__ double srs[2][NB];
+  __shared__ int spiv[NB];
+  const int tid = threadIdx.x, lane = tid & 31;
+  double a[RPT][NB];
+  unsigned ub = 0;  // used (or absent) rows of this thread
+#pragma unroll
+  for (int r = 0; r < RPT; r++) {
+    const int i = tid + r * NT;
+#pragma unroll
+    for (int u = 0; u < NB; u++) a[r][u] = (i < n && u < nb) ? W[(long)i * n + k0 + u] : 0.;
+    if (i >= n || used[i]) ub |= 1u << r;
+  }
+#pragma unroll
+  for (int t = 0; t < NB; t++) {
+    if (t >= nb) break;
+    unsigned long long v = 0;
+#pragma unroll
+    for (int r = 0; r < RPT; r++)
+      if (!((ub >> r) & 1u)) {
+        const unsigned long long c = piv_key(a[r][t], tid + r * NT);
+        v = c > v ? c : v;
+      }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const unsigned long long v2 = __shfl_xor_sync(0xffffffffu, v, o);
+      v = v2 > v ? v2 : v;
+    }
+    if (lane == 0) sk[t & 1][tid >> 5] = v;
+    __syncthreads();
+    unsigned long long m = lane < NT / 32 ? sk[t & 1][lane] : 0ull;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const unsigned long long m2 = __shfl_xor_sync(0xffffffffu, m, o);
+      m = m2 > m ? m2 : m;
+    }
+    if (m == 0) {  // no candidate row left: singular (the same branch in every thread)
+      if (tid == 0) *bad = 1;
+      return;
+    }
+    const int p = 0xFFFFF - (int)(m & 0xFFFFFull);
+    if (p % NT == tid) {
+      const int r0 = p / NT;
+#pragma unroll
+      for (int r = 0; r < RPT; r++)
+        if (r == r0) {
+          const double piv = a[r][t];
+          const double inv = piv != 0. ? 1. / piv : 0.;
+#pragma unroll
+          for (int u = 0; u < NB; u++) {
+            a[r][u] = u == t ? inv : a[r][u] * inv;
+            srs[t & 1][u] = a[r][u];
+          }
+          if (piv == 0.) *bad = 1;
+        }
+      ub |= 1u << r0;
+      spiv[t] = p;
+    }
+    __syncthreads();
+    const double inv = srs[t & 1][t];
+#pragma unroll
+    for (int r = 0; r < RPT; r++) {
+      const int i = tid + r * NT;
+      if (i < n && i != p) {
+        const double ci = a[r][t];
+#pragma unroll
+        for (int u = 0; u < NB; u++) a[r][u] = u == t ? -ci * inv : a[r][u] - ci * srs[t & 1][u];
+      }
+    }
+  }
+  __syncthreads();
+  if (tid < nb) pivrow[k0 + tid] = spiv[tid];
+#pragma unroll
+  for (int r = 0; r < RPT; r++) {
+    const int i = tid + r * NT;
+    if (i < n) {
+      used[i] = (ub >> r) & 1u;
+#pragma unroll
+      for (int u = 0; u < NB; u++)
+        if (u < nb) {
+          W[(long)i * n + k0 + u] = a[r][u];
+          Hm[(long)u * n + i] = a[r][u] - (i == spiv[u] ? 1. : 0.);
+        }
+    }
+  }
+  gj_copy_pivot_rows<NT, 16>(W, n, nb, spiv, R);
+}
+
+// the panel in shared memory ([NB][n], a warp's rows in consecutive words), for levels
+// whose rows exceed RPT * NT of the register form
+template <int NB, int NT>
+__global__ void __launch_bounds__(NT, 1)
+    k_gj_panel(double *__restrict__ W, int n, int k0, int nb, int *__restrict__ pivrow, int *__restrict__ used,
+               double *__restrict__ Hm, double *__restrict__ R, int *__restrict__ bad) {
+  extern __shared__ __align__(16) double sp[];  // [NB][n] panel, then n used flags (bytes)
+  unsigned char *su = reinterpret_cast<unsigned char *>(sp + (size_t)NB * n);
+  __shared__ unsigned long long sk[2][NT / 32];
+  __shared__ double srs[2][NB];
+  __shared__ int spiv[NB];
+  const int tid = threadIdx.x, lane = tid & 31;
+  for (long q = tid; q < (long)n * NB; q += NT) {
+    const int i = (int)(q / NB), t = (int)(q % NB);
+    sp[(long)t * n + i] = t < nb ? W[(long)i * n + k0 + t] : 0.;
+  }
+  for (int i = tid; i < n; i += NT) su[i] = (unsigned char)used[i];
+  __syncthreads();
+  for (int t = 0; t < nb; t++) {
+    unsigned long long v = 0;
+    for (int i = tid; i < n; i += NT)
+      if (!su[i]) {
+        const unsigned long long c = piv_key(sp[(long)t * n + i], i);
+        v = c > v ? c : v;
+      }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const unsigned long long v2 = __shfl_xor_sync(0xffffffffu, v, o);
+      v = v2 > v ? v2 : v;
+    }
+    if (lane == 0) sk[t & 1][tid >> 5] = v;
+    __syncthreads();
+    unsigned long long m = lane < NT / 32 ? sk[t & 1][lane] : 0ull;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const unsigned long long m2 = __shfl_xor_sync(0xffffffffu, m, o);
+      m = m2 > m ? m2 : m;
+    }
+    if (m == 0) {
+      if (tid == 0) *bad = 1;
+      return;
+    }
+    const int p = 0xFFFFF - (int)(m & 0xFFFFFull);
+    if (p % NT == tid) {
+      const double piv = sp[(long)t * n + p];
+      const double inv = piv != 0. ? 1. / piv : 0.;
+      for (int u = 0; u < NB; u++) {
+        const double r = u == t ? inv : sp[(long)u * n + p] * inv;
+        srs[t & 1][u] = r;
+        sp[(long)u * n + p] = r;
+      }
+      su[p] = 1;
+      spiv[t] = p;
+      if (piv == 0.) *bad = 1;
+    }
+    __syncthreads();
+    const double inv = srs[t & 1][t];
+    for (int i = tid; i < n; i += NT) {
+      if (i == p) continue;
+      const double ci = sp[(long)t * n + i];
+#pragma unroll
+      for (int u = 0; u < NB; u++) {
+        double &w = sp[(long)u * n + i];
+        w = u == t ? -ci * inv : w - ci * srs[t & 1][u];
+      }
+    }
+  }
+  __syncthreads();
+  if (tid < nb) pivrow[k0 + tid] = spiv[tid];
+  for (int i = tid; i < n; i += NT) used[i] = su[i];
+  for (long q = tid; q < (long)n * NB; q += NT) {
+    const int i = (int)(q / NB), t = (int)(q % NB);
+    if (t < nb) {
+      const double h = sp[(long)t * n + i];
+      W[(long)i * n + k0 + t] = h;
+      Hm[(long)t * n + i] = h - (i == spiv[t] ? 1. : 0.);
+    }
+  }
+  gj_copy_pivot_rows<NT, 4>(W, n, nb, spiv, R);
+}
+
+// W[i, j] += sum_t Hm[t][i] R[t][j] (Hm = H - E_P) for every column j outside the block:
+// a rank-NB update in 64 x 64 tiles, the tile's Hm and R slices staged in shared memory,
+// a 4 x 4 register tile per thread; each entry sums its NB products in order t = 0, 1, ..
+template <int NB>
+__global__ void __launch_bounds__(256)
+    k_gj_update(double *__restrict__ W, int n, int k0, int nb, const double *__restrict__ Hm,
+                const double *__restrict__ R) {
+  __shared__ __align__(16) double sh[NB][64];
+  __shared__ __align__(16) double sr[NB][64];
+  const int tid = threadIdx.x;
+  const int bi = blockIdx.y * 64, bj = blockIdx.x * 64;
+  for (int q = tid; q < NB * 64; q += 256) {
+    const int t = q / 64, c = q % 64;
+    sh[t][c] = (t < nb && bi + c < n) ? Hm[(long)t * n + bi + c] : 0.;
+    sr[t][c] = (t < nb && bj + c < n) ? R[(long)t * n + bj + c] : 0.;
+  }
+  __syncthreads();
+  const int ti = (tid >> 4) * 4, tj = (tid & 15) * 4;
+  double acc[4][4];
+#pragma unroll
+  for (int a = 0; a < 4; a++)
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+      const int i = bi + ti + a, j = bj + tj + c;
+      acc[a][c] = (i < n && j < n) ? W[(long)i * n + j] : 0.;
+    }
+#pragma unroll
+  for (int t = 0; t < NB; t++) {
+    if (t < nb) {
+      const double2 h0 = *reinterpret_cast<const double2 *>(&sh[t][ti]);
+      const double2 h1 = *reinterpret_cast<const double2 *>(&sh[t][ti + 2]);
+      const double2 r0 = *reinterpret_cast<const double2 *>(&sr[t][tj]);
+      const double2 r1 = *reinterpret_cast<const double2 *>(&sr[t][tj + 2]);
+      const double h[4] = {h0.x, h0.y, h1.x, h1.y}, r[4] = {r0.x, r0.y, r1.x, r1.y};
+#pragma unroll
+      for (int a = 0; a < 4; a++)
+#pragma unroll
+        for (int c = 0; c < 4; c++) acc[a][c] += h[a] * r[c];
+    }
+  }
+#pragma unroll
+  for (int a = 0; a < 4; a++)
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+      const int i = bi + ti + a, j = bj + tj + c;
+      if (i < n && j < n && (j < k0 || j >= k0 + nb)) W[(long)i * n + j] = acc[a][c];
+    }
+}
+
 // inv[k][p_j] = W[p_k][j]
 __global__ void k_extract_inv(const double *W, int n, const int *pivrow, double *inv) {
   const int k = blockIdx.x;
@@ -2198,7 +2468,7 @@ int coarse_factor(exf_sys *s) {
   }
   EXF_TRY(s->coarse_vals.ensure(L.nnz));
   EXF_TRY(s->coarse_work.ensure((size_t)n * n));
-  EXF_TRY(s->coarse_work2.ensure((size_t)n * n));
+  EXF_TRY(s->coarse_work2.ensure(std::max((size_t)n * n, (size_t)n * 32)));  // also the blocked form's H, R
   EXF_TRY(s->coarse_piv.ensure(n));
   EXF_TRY(s->coarse_used.ensure(n));
   EXF_TRY(s->coarse_bad.ensure(1));
@@ -2208,6 +2478,7 @@ int coarse_factor(exf_sys *s) {
   EXF_TRY(used.zero(st));
   EXF_TRY(bad.zero(st));
   EXF_TRY(key.zero(st));
+  EXF_TRY(pivrow.zero(st));  // every entry a valid row, even after a singular pivot
   EXF_TRY(csr_values(s, 0, s->coarse_vals.p));
   double *W = s->coarse_work.p;
   k_dense_from_csr<<<n, 128, 0, st>>>(L.csr_ptr.p, L.csr_col.p, s->coarse_vals.p, n, W);
@@ -2226,16 +2497,36 @@ int coarse_factor(exf_sys *s) {
 #endif
   const int grid = std::max(1, std::min(n, nsm * std::min(per_sm, EXF_GJ_BLOCKS_PER_SM)));  // rows over blocks
   double *W1p = s->coarse_work2.p;
-  void *args[] = {&W, &W1p, (void *)&n, &pivrow.p, &key.p, &used.p, &bad.p};
-  EXF_CUDA(cudaLaunchCooperativeKernel((void *)k_gj_coop<NT>, grid, NT, args, 0, st));
-  EXF_COUNT(3);
-  const double *Wfinal = (n & 1) ? W1p : W;  // step n-1 wrote buffer (n-1)&1 ? W0 : W1
-  if (s->coarse_inv.n != (size_t)n * n) {
-    EXF_TRY(s->coarse_inv.alloc((size_t)n * n));
-    s->buf_epoch++;
+  const double *Wfinal = W;
+  // blocked form while the n x NB panel fits one CTA's shared memory
+  constexpr int GNB = 16, GNT = 1024;
+  const size_t psm = (size_t)n * GNB * sizeof(double) + (((size_t)n + 15) & ~(size_t)15);
+  int smax = 0;
+  EXF_CUDA(cudaDeviceGetAttribute(&smax, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  if (psm + 1024 <= (size_t)smax) {
+    // one value for every caller (the attribute is per function, shared by the threads
+    // that factor systems of different sizes)
+    EXF_CUDA(cudaFuncSetAttribute(k_gj_panel<GNB, GNT>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax - 1024));
+    // H - E_P (NB x n) and the block's pivot rows (NB x n) in the second work buffer
+    double *Hb = W1p, *Rb = W1p + (size_t)n * GNB;
+    const dim3 ugrid((unsigned)((n + 63) / 64), (unsigned)((n + 63) / 64));
+    constexpr int RNT = 512, RPT = 3;
+    for (int k0 = 0; k0 < n; k0 += GNB) {
+      const int nb = std::min(GNB, n - k0);
+      if (n <= RNT * RPT)
+        k_gj_panel_reg<GNB, RNT, RPT><<<1, RNT, 0, st>>>(W, n, k0, nb, pivrow.p, used.p, Hb, Rb, bad.p);
+      else
+        k_gj_panel<GNB, GNT><<<1, GNT, psm, st>>>(W, n, k0, nb, pivrow.p, used.p, Hb, Rb, bad.p);
+      k_gj_update<GNB><<<ugrid, 256, 0, st>>>(W, n, k0, nb, Hb, Rb);
+      EXF_COUNT(2);
+    }
+    EXF_LAUNCH_CHECK();
+  } else {
+    void *args[] = {&W, &W1p, (void *)&n, &pivrow.p, &key.p, &used.p, &bad.p};
+    EXF_CUDA(cudaLaunchCooperativeKernel((void *)k_gj_coop<NT>, grid, NT, args, 0, st));
+    EXF_COUNT(3);
+    Wfinal = (n & 1) ? W1p : W;  // step n-1 wrote buffer (n-1)&1 ? W0 : W1
   }
-  k_extract_inv<<<n, 128, 0, st>>>(Wfinal, n, pivrow.p, s->coarse_inv.p);
-  EXF_LAUNCH_CHECK();
   int hbad = 0;
   EXF_CUDA(cudaMemcpyAsync(&hbad, bad.p, sizeof(int), cudaMemcpyDeviceToHost, st));
   EXF_CUDA(cudaStreamSynchronize(st));
@@ -2243,6 +2534,12 @@ int coarse_factor(exf_sys *s) {
     set_error("coarsest matrix is singular");
     return EXF_ERR_SINGULAR;
   }
+  if (s->coarse_inv.n != (size_t)n * n) {
+    EXF_TRY(s->coarse_inv.alloc((size_t)n * n));
+    s->buf_epoch++;
+  }
+  k_extract_inv<<<n, 128, 0, st>>>(Wfinal, n, pivrow.p, s->coarse_inv.p);
+  EXF_LAUNCH_CHECK();
   s->coarse_ok = 1;
   return EXF_OK;
 }

@@ -5,7 +5,8 @@ prolongation embedding matrices _embedding_matrix_q / _embedding_matrix_l (float
 constants) and the side topology _surf_top.  These are the reference's own numbers
 the restated prolongation/restriction and boundary loops must reproduce.
 
-    python tests/golden/make_golden.py [path/to/reference]
+    python tests/golden/make_golden.py path/to/reference
+    EXFEMUS_REFERENCE=path/to/reference python tests/golden/make_golden.py
 
 The reference tree is only needed to regenerate the fixture; tests read the JSON.
 """
@@ -14,7 +15,9 @@ import os
 import re
 import sys
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+REF = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("EXFEMUS_REFERENCE", "")
+if not REF or not os.path.isdir(REF):
+    sys.exit("make_golden.py: give the reference tree as the argument or in EXFEMUS_REFERENCE")
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "mggeomel.json")
 
 TABLES = {

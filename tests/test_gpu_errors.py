@@ -56,24 +56,36 @@ def test_bad_arguments(heat):
     L = _lib.load()
     n = C.c_int()
     assert L.exf_sys_ndof(heat.h, 99, C.byref(n)) == _lib.EXF_ERR_ARG
-    rc, _ = _solve_rc(heat, cond_corr=1)
-    assert rc in (_lib.EXF_ERR_STATE, _lib.EXF_ERR_UNSUPPORTED)
+    rc, _ = _solve_rc(heat)
+    assert rc == _lib.EXF_ERR_STATE  # not assembled yet
     heat.assemble_all()
-    rc, _ = _solve_rc(heat, cond_corr=1)
-    assert rc == _lib.EXF_ERR_UNSUPPORTED
+    rc, _ = _solve_rc(heat, stop_test=7)
+    assert rc == _lib.EXF_ERR_ARG
+    rc, _ = _solve_rc(heat, nu_pre=-1)
+    assert rc == _lib.EXF_ERR_ARG
 
 
-def test_unsupported_ns_traction_flag(gpu_lib):
-    m = ex.Mesh(2, 2, (2, 2), (0, 1, 0, 1))
-    ns = ex.MGSolNS(m)
-    ns.GenBc(_lib.BC_CHANNEL if False else _lib.BC_CAVITY)
-    b0, b1 = ns.bc()
-    i = int(np.where(b0[:m.ntop] == 1)[0][0])
-    b1[i] = 2  # tangential-traction flag on a natural velocity DOF
-    ns.set_bc(b0, b1)
-    with pytest.raises(_lib.ExfError) as e:
-        ns.assemble_all()
-    assert e.value.code == _lib.EXF_ERR_UNSUPPORTED
+def test_tile_kernels_refused_on_uploaded_meshes(gpu_lib):
+    """The tile kernels need the lattice of a generated box: on an uploaded mesh they are
+    refused with EXF_ERR_UNSUPPORTED and the context keeps working."""
+    gm = ex.Mesh(2, 2, (2, 2), (0, 1, 0, 1))
+    conn = [gm.conn(l)[0] for l in range(2)]
+    neigh = [gm.conn(l)[1] for l in range(2)]
+    e = np.arange(conn[1].shape[0])
+    parent = [None, ((e // 4) // 2) * 2 + (e % 4) // 2]
+    um = ex.Mesh.upload(2, [gm.nnodes(0), gm.nnodes(1)], gm.nvert0, gm.xyz(), conn, neigh, parent)
+    ns = ex.MGSolNS(um)
+    ns.GenBc(_lib.BC_CAVITY)
+    ns.phys = ex.phys(inv_re=1 / 400.)
+    ns.assemble_all()
+    rp, col, val = ns.csr(1)  # a consistent right-hand side b = A x (enclosed flow)
+    xr = np.random.default_rng(0).random(ns.ntop_dof)
+    ns.set_rhs(np.array([val[rp[i]:rp[i + 1]] @ xr[col[rp[i]:rp[i + 1]]] for i in range(ns.ntop_dof)]))
+    st = _lib.ExfSolveStats()
+    p = ex.mg_params(smoother=_lib.SMOOTH_VANKA, vanka_kernel=_lib.VANKA_TILE)
+    assert _lib.load().exf_mg_solve(ns.h, C.byref(p), C.byref(st)) == _lib.EXF_ERR_UNSUPPORTED
+    st = ns.solve(ex.mg_params(smoother=_lib.SMOOTH_VANKA, nu_pre=3, nu_post=3))
+    assert st.converged
 
 
 def test_graph_and_eager_cycles_agree_bitwise(heat):

@@ -6,7 +6,11 @@ exf_sys_set_transfer takes the transfer operators in gencase's dataset layout; a
 exf_sys_check_pattern checks a level's sparsity against gencase's matrix datasets.
 
   * the structured box pushed through the upload path gives the same bits as
-    exf_mesh_create (colourings, patterns, transfers, matrices, solutions);
+    exf_mesh_create (colourings, patterns, transfers, matrices, solutions) for the
+    Navier-Stokes systems; for the temperature system the Gauss-Seidel colouring of the
+    upload path is first fit on the element-sharing graph, which is not the lattice's
+    mod-3 colouring (two midpoints two lattice steps apart share no element), so there the
+    solutions agree within 1e-11 at a tight tolerance;
   * a copy with nodes permuted inside each nesting class and elements permuted inside
     each level gives the permuted solution (within 1e-12);
   * transfers supplied as gencase blocks give the same bits as those built from parents,
@@ -91,9 +95,11 @@ def test_structured_box_through_upload_is_bit_identical(name, gpu_lib):
     assert np.array_equal(x0, ux0)
     for a, b in zip(gs.bc(), us.bc()):
         assert np.array_equal(a, b)
+    same_colours = kind == _lib.KIND_NS
     for lev in range(nlev):
-        assert gs.colours(lev)[0] == us.colours(lev)[0]
-        assert np.array_equal(gs.colours(lev)[1], us.colours(lev)[1])
+        if same_colours:
+            assert gs.colours(lev)[0] == us.colours(lev)[0]
+            assert np.array_equal(gs.colours(lev)[1], us.colours(lev)[1])
         for a, b in zip(gs.pattern(lev), us.pattern(lev)):
             assert np.array_equal(a, b)
         if lev > 0:
@@ -111,11 +117,14 @@ def test_structured_box_through_upload_is_bit_identical(name, gpu_lib):
         out = []
         for s in (gs, us):
             s.set_x(x0)
-            st = s.solve(params(name, precision=prec))
+            st = s.solve(params(name, precision=prec, eps=1e-11 if same_colours else 1e-13))
             assert st.converged
             out.append((s.x(), list(st.hist[:st.cycles])))
-        assert np.array_equal(out[0][0], out[1][0])
-        assert out[0][1] == out[1][1]
+        if same_colours:
+            assert np.array_equal(out[0][0], out[1][0])
+            assert out[0][1] == out[1][1]
+        else:
+            assert rel(out[1][0], out[0][0]) < 1e-11
 
 
 def permuted_arrays(arr, seed):
