@@ -140,14 +140,15 @@ int exf_adjoint_backward(exf_sys *s, const exf_phys *ph, const exf_mg_params *p,
   const long n = T.ndof;
   const long nel = s->mesh->lev[top].nel;
   cudaStream_t stm = s->stream;
-  DBuf<double> x_fwd, b_fwd, xold_sav, qe_sav, wdiag, lam, gq;
-  EXF_TRY(x_fwd.alloc(n));
-  EXF_TRY(b_fwd.alloc(n));
-  EXF_TRY(xold_sav.alloc(n));
-  EXF_TRY(qe_sav.alloc(nel));
-  EXF_TRY(wdiag.alloc(n));
-  EXF_TRY(lam.alloc(n));
-  EXF_TRY(gq.alloc(nel));
+  DBuf<double> &x_fwd = s->adj_x, &b_fwd = s->adj_b, &xold_sav = s->adj_xold, &qe_sav = s->adj_qe,
+                &wdiag = s->adj_w, &lam = s->adj_lam, &gq = s->adj_gq;
+  EXF_TRY(x_fwd.ensure(n));
+  EXF_TRY(b_fwd.ensure(n));
+  EXF_TRY(xold_sav.ensure(n));
+  EXF_TRY(qe_sav.ensure(nel));
+  EXF_TRY(wdiag.ensure(n));
+  EXF_TRY(lam.ensure(n));
+  EXF_TRY(gq.ensure(nel));
   EXF_CUDA(cudaMemcpyAsync(x_fwd.p, T.x.p, n * sizeof(double), cudaMemcpyDeviceToDevice, stm));
   EXF_CUDA(cudaMemcpyAsync(b_fwd.p, T.b.p, n * sizeof(double), cudaMemcpyDeviceToDevice, stm));
   EXF_CUDA(cudaMemcpyAsync(xold_sav.p, s->xold.p, n * sizeof(double), cudaMemcpyDeviceToDevice, stm));

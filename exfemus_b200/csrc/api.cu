@@ -447,9 +447,9 @@ int exf_sys_create(exf_mesh *m, int kind, exf_sys **out) {
 int exf_sys_destroy(exf_sys *s) {
   if (!s) return EXF_OK;
   cudaSetDevice(s->mesh->device);
-  for (int k = 0; k < 2; k++) {
-    if (s->graph[k]) cudaGraphExecDestroy(s->graph[k]);
-    if (s->loop_graph[k]) cudaGraphExecDestroy(s->loop_graph[k]);
+  for (int k = 0; k < exf_sys::kGraphSlots; k++) {
+    if (s->cyc_slot[k].exec) cudaGraphExecDestroy(s->cyc_slot[k].exec);
+    if (s->loop_slot[k].exec) cudaGraphExecDestroy(s->loop_slot[k].exec);
   }
   if (s->stream) cudaStreamSynchronize(s->stream);
   s->L.clear();
@@ -862,14 +862,35 @@ static unsigned long long params_key(const exf_mg_params *p) {
   return h | 1ull;
 }
 
-static int cycle_graph(exf_sys *s, const exf_mg_params *p, double *dnr) {
-  const int gi = p->precision == EXF_PREC_MIXED ? 1 : 0;
-  const unsigned long long key = params_key(p);
-  if (!s->graph[gi] || s->graph_key[gi] != key || s->graph_epoch[gi] != s->buf_epoch) {
-    if (s->graph[gi]) {
-      cudaGraphExecDestroy(s->graph[gi]);
-      s->graph[gi] = nullptr;
+// the slot holding (key, current epoch), or an emptied slot to build it in (*hit false):
+// a free one, else the least recently used
+static exf_sys::GraphSlot *graph_slot(exf_sys *s, exf_sys::GraphSlot *slots, unsigned long long key, bool *hit) {
+  exf_sys::GraphSlot *victim = &slots[0];
+  for (int k = 0; k < exf_sys::kGraphSlots; k++) {
+    exf_sys::GraphSlot &g = slots[k];
+    if (g.exec && g.key == key && g.epoch == s->buf_epoch) {
+      g.used = ++s->graph_clock;
+      *hit = true;
+      return &g;
     }
+    if (!g.exec) {
+      if (victim->exec) victim = &g;
+    } else if (victim->exec && g.used < victim->used) {
+      victim = &g;
+    }
+  }
+  if (victim->exec) cudaGraphExecDestroy(victim->exec);
+  *victim = exf_sys::GraphSlot();
+  victim->used = ++s->graph_clock;
+  *hit = false;
+  return victim;
+}
+
+static int cycle_graph(exf_sys *s, const exf_mg_params *p, double *dnr) {
+  const unsigned long long key = params_key(p);
+  bool hit = false;
+  exf_sys::GraphSlot *gs = graph_slot(s, s->cyc_slot, key, &hit);
+  if (!hit) {
     cudaGraph_t g = nullptr;
     const long long c0 = exf_launch_count();
     EXF_CUDA(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
@@ -883,20 +904,20 @@ static int cycle_graph(exf_sys *s, const exf_mg_params *p, double *dnr) {
       set_error("graph capture failed: %s", cudaGetErrorString(e));
       return EXF_ERR_CUDA;
     }
-    e = cudaGraphInstantiate(&s->graph[gi], g, 0);
+    e = cudaGraphInstantiate(&gs->exec, g, 0);
     cudaGraphDestroy(g);
     if (e != cudaSuccess) {
       set_error("graph instantiation failed: %s", cudaGetErrorString(e));
-      s->graph[gi] = nullptr;
+      gs->exec = nullptr;
       return EXF_ERR_CUDA;
     }
-    s->graph_key[gi] = key;
-    s->graph_epoch[gi] = s->buf_epoch;
-    s->graph_launches[gi] = exf_launch_count() - c0;
-    count_launch(-(int)s->graph_launches[gi]);  // captured, not executed
+    gs->key = key;
+    gs->epoch = s->buf_epoch;
+    gs->launches = exf_launch_count() - c0;
+    count_launch(-(int)gs->launches);  // captured, not executed
   }
-  EXF_CUDA(cudaGraphLaunch(s->graph[gi], s->stream));
-  count_launch((int)s->graph_launches[gi]);
+  EXF_CUDA(cudaGraphLaunch(gs->exec, s->stream));
+  count_launch((int)gs->launches);
   return EXF_OK;
 }
 
@@ -924,14 +945,11 @@ static int cycle_body(exf_sys *s, const exf_mg_params *p, double *dnr);
 static unsigned long long params_key(const exf_mg_params *p);
 static int device_loop(exf_sys *s, const exf_mg_params *p, exf_solve_stats *st, double den, double lim,
                        bool ref_stop, double *dnr) {
-  const int gi = p->precision == EXF_PREC_MIXED ? 1 : 0;
   const unsigned long long key = params_key(p);
   if (!s->loop_dev.p) EXF_TRY(s->loop_dev.alloc(1));
-  if (!s->loop_graph[gi] || s->loop_key[gi] != key || s->loop_epoch[gi] != s->buf_epoch) {
-    if (s->loop_graph[gi]) {
-      cudaGraphExecDestroy(s->loop_graph[gi]);
-      s->loop_graph[gi] = nullptr;
-    }
+  bool hit = false;
+  exf_sys::GraphSlot *gs = graph_slot(s, s->loop_slot, key, &hit);
+  if (!hit) {
     cudaGraph_t g = nullptr;
     cudaGraphConditionalHandle h;
     cudaGraphNodeParams np = {};
@@ -960,19 +978,23 @@ static int device_loop(exf_sys *s, const exf_mg_params *p, exf_solve_stats *st, 
       cudaGraph_t cap = body;
       ok = cudaStreamEndCapture(s->stream, &cap) == cudaSuccess && rc == EXF_OK;
     }
-    s->loop_launches[gi] = exf_launch_count() - c0;
-    count_launch(-(int)s->loop_launches[gi]);  // captured, not executed
-    if (ok) ok = cudaGraphInstantiate(&s->loop_graph[gi], g, 0) == cudaSuccess;
+    gs->launches = exf_launch_count() - c0;
+    count_launch(-(int)gs->launches);  // captured, not executed
+    if (ok) ok = cudaGraphInstantiate(&gs->exec, g, 0) == cudaSuccess;
     if (g) cudaGraphDestroy(g);
     cudaGetLastError();
-    if (rc != EXF_OK) return rc;
+    if (rc != EXF_OK) {
+      if (gs->exec) cudaGraphExecDestroy(gs->exec);
+      gs->exec = nullptr;
+      return rc;
+    }
     if (!ok) {
-      s->loop_graph[gi] = nullptr;
+      gs->exec = nullptr;
       s->loop_unavailable = 1;
       return EXF_ERR_UNSUPPORTED;
     }
-    s->loop_key[gi] = key;
-    s->loop_epoch[gi] = s->buf_epoch;
+    gs->key = key;
+    gs->epoch = s->buf_epoch;
   }
   LoopDev hd = {};
   hd.den = den;
@@ -982,10 +1004,10 @@ static int device_loop(exf_sys *s, const exf_mg_params *p, exf_solve_stats *st, 
   hd.ref_stop = ref_stop ? 1 : 0;
   hd.mixed = p->precision == EXF_PREC_MIXED ? 1 : 0;
   EXF_CUDA(cudaMemcpyAsync(s->loop_dev.p, &hd, offsetof(LoopDev, hist), cudaMemcpyHostToDevice, s->stream));
-  EXF_CUDA(cudaGraphLaunch(s->loop_graph[gi], s->stream));
+  EXF_CUDA(cudaGraphLaunch(gs->exec, s->stream));
   EXF_CUDA(cudaMemcpyAsync(&hd, s->loop_dev.p, sizeof(LoopDev), cudaMemcpyDeviceToHost, s->stream));
   EXF_CUDA(cudaStreamSynchronize(s->stream));
-  count_launch((int)(s->loop_launches[gi] * (hd.cycles - st->cycles)));
+  count_launch((int)(gs->launches * (hd.cycles - st->cycles)));
   for (int c = st->cycles; c < hd.cycles && c < 256; c++) st->hist[c] = hd.hist[c];
   st->cycles = hd.cycles;
   st->rel_res = hd.rel;

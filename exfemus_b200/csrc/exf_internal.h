@@ -288,19 +288,27 @@ struct exf_sys {
   // post-smoothing sweep (coarsest: after the solve), -}: the accuracies the reference's
   // level solver reports, for the conditional correction and the reference stop test
   exf::DBuf<double> mg_acc;
+  // scratch of exf_adjoint_backward, kept between calls: the forward x and b, x_old, the
+  // element sources, dB/dx_old, the adjoint state, the source gradient
+  exf::DBuf<double> adj_x, adj_b, adj_xold, adj_qe, adj_w, adj_lam, adj_gq;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   cudaEvent_t user_ev[8] = {nullptr};
-  // captured V-cycle graphs (per precision)
-  cudaGraphExec_t graph[2] = {nullptr, nullptr};
-  unsigned long long graph_key[2] = {0, 0};
-  long long graph_launches[2] = {0, 0};
+  // captured graphs, a few per system so that alternating parameter sets (a forward and
+  // an adjoint solve, the two precisions) each keep theirs: one V-cycle per launch, and
+  // the device-resident solve loop (a WHILE node whose body is the V-cycle and the stop
+  // test); each keyed by the multigrid parameters and the buffer epoch, least recently
+  // used replaced
+  static constexpr int kGraphSlots = 4;
+  struct GraphSlot {
+    cudaGraphExec_t exec = nullptr;
+    unsigned long long key = 0;
+    unsigned epoch = 0;
+    long long launches = 0;                 // kernels per launch (loop: per iteration)
+    unsigned long long used = 0;
+  };
+  GraphSlot cyc_slot[kGraphSlots], loop_slot[kGraphSlots];
+  unsigned long long graph_clock = 0;
   unsigned buf_epoch = 1;                   // bumped when a buffer baked into a graph moves
-  unsigned graph_epoch[2] = {0, 0};
-  // device-resident solve loop (per precision): WHILE-node graph, its key and epoch
-  cudaGraphExec_t loop_graph[2] = {nullptr, nullptr};
-  unsigned long long loop_key[2] = {0, 0};
-  unsigned loop_epoch[2] = {0, 0};
-  long long loop_launches[2] = {0, 0};     // kernels per loop iteration
   int loop_unavailable = 0;                 // the runtime refused the conditional graph
   exf::DBuf<exf::LoopDev> loop_dev;
 };

@@ -1594,7 +1594,7 @@ __global__ void __launch_bounds__(32 * (NWC + 1), 1)
 #define EXF_BK_CAPB 3072
 #endif
 #ifndef EXF_BK_UNR
-#define EXF_BK_UNR 8
+#define EXF_BK_UNR 6
 #endif
 #ifndef EXF_BK_LPR
 #define EXF_BK_LPR 16
