@@ -788,10 +788,16 @@ int exf_gen_mat_rhs(exf_sys *s, const exf_phys *ph, int lev, int mode) {
   return EXF_OK;
 }
 
+// GenMatRhs of every level (the top one with its rhs), the levels' elements of one colour
+// in one launch
 int exf_assemble_all(exf_sys *s, const exf_phys *ph) {
   CHECK_SYS(s);
-  EXF_TRY(exf_gen_mat_rhs(s, ph, s->nlev - 1, 1));
-  for (int l = 0; l < s->nlev - 1; l++) EXF_TRY(exf_gen_mat_rhs(s, ph, l, 0));
+  if (!ph) return EXF_ERR_ARG;
+  if (s->kind == EXF_KIND_NS && s->mesh->dim == 3 && s->nv2 != 3) return EXF_ERR_STATE;
+  EXF_TRY(assemble_all_levels(s, ph));
+  for (int l = 0; l < s->nlev; l++) EXF_TRY(sync_fp32(s, l));
+  s->coarse_ok = 0;
+  s->assembled = 1;
   return EXF_OK;
 }
 
@@ -1232,7 +1238,7 @@ int exf_time_op(exf_sys *s, int what, int lev, const exf_mg_params *p, const exf
       case 1:
         return f32 ? smooth<float>(s, lev, p, 1, L.x32.p, L.b32.p) : smooth<double>(s, lev, p, 1, L.x.p, L.b.p);
       case 2:
-        for (int l = s->nlev - 1; l >= 0; l--) EXF_TRY(assemble_level(s, ph, l, l == s->nlev - 1 ? 1 : 0));
+        EXF_TRY(assemble_all_levels(s, ph));  // the exf_assemble_all path
         return EXF_OK;
       case 3: {
         SysLevel &T = s->L[s->nlev - 1];

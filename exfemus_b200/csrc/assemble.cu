@@ -191,12 +191,14 @@ __device__ double jac_sur(const FETab<DIM> *t, int q, const double (*xx)[FE<DIM>
 #ifndef EXF_ASM_MINB2
 #define EXF_ASM_MINB2 1
 #endif
+// One element of one level (a CTA): element data, Gauss-point fields and coefficients,
+// the volume integrals of every node pair, B / B^T, the rhs (mode 1) and the boundary
+// sides, each added to the level's matrix in place (elements of one colour share no node).
 template <int DIM, int NT>
-__global__ void __launch_bounds__(NT, DIM == 3 ? EXF_ASM_MINB3 : EXF_ASM_MINB2) k_assemble(AsmArgs<DIM> A, int mode) {
+__device__ __forceinline__ void assemble_element(const AsmArgs<DIM> &A, const int e, const int mode) {
   using F = FE<DIM>;
   constexpr int NEN = F::NEN, NVX = F::NVX, NQ = F::NQ;
   const int tid = threadIdx.x;
-  const int e = A.elist[blockIdx.x];
   const bool ns = A.kind == EXF_KIND_NS;
   const int nv2 = ns ? DIM : 1;
 
@@ -365,6 +367,7 @@ __global__ void __launch_bounds__(NT, DIM == 3 ? EXF_ASM_MINB3 : EXF_ASM_MINB2) 
     const int ni = s_conn[i];
     const long blk = qq_ptr[ni] + A.pos_qq[((long)e * NEN + i) * NEN + j];
     if (!ns) {
+      const double old = A.vv[blk];  // loaded before the Gauss-point loop hides its latency
       double K = 0.;
 #pragma unroll 1
       for (int q = 0; q < NQ; q++) {
@@ -377,8 +380,10 @@ __global__ void __launch_bounds__(NT, DIM == 3 ? EXF_ASM_MINB3 : EXF_ASM_MINB2) 
         }
         K += pi * (s_cM[q] * pj + adv) + lap;
       }
-      A.vv[blk] += s_bcv[0][i] * K;
+      A.vv[blk] = old + s_bcv[0][i] * K;
     } else {
+      double old[DIM * DIM];  // the pair's entries, loaded before the Gauss-point loop
+      for (int c = 0; c < DIM * DIM; c++) old[c] = A.vv[(long)c * A.nqq + blk];
       double M = 0., T[DIM * DIM];
       for (int k = 0; k < DIM * DIM; k++) T[k] = 0.;
 #pragma unroll 1
@@ -401,7 +406,7 @@ __global__ void __launch_bounds__(NT, DIM == 3 ? EXF_ASM_MINB3 : EXF_ASM_MINB2) 
         const double bcv = s_bcv[a][i];
         for (int b = 0; b < DIM; b++) {
           double v = T[a * DIM + b] + (a == b ? M : 0.);
-          A.vv[(long)(a * DIM + b) * A.nqq + blk] += bcv * v;
+          A.vv[(long)(a * DIM + b) * A.nqq + blk] = old[a * DIM + b] + bcv * v;
         }
       }
     }
@@ -410,29 +415,36 @@ __global__ void __launch_bounds__(NT, DIM == 3 ? EXF_ASM_MINB3 : EXF_ASM_MINB2) 
     // E_b(iv, j) = sum_q JxW psi_iv d_b phi_j : B^T (velocity rows) and B (pressure rows)
     for (int p = tid; p < NVX * NEN; p += NT) {
       const int iv = p / NEN, j = p % NEN;
+      // B^T: row (a, node j), column pressure vertex iv; B: pressure row iv, column (b,
+      // node j); the entries are loaded before the Gauss-point loop
+      const int nj = s_conn[j];
+      const long kq = A.ql_ptr[nj] + A.pos_ql[((long)e * NEN + j) * NVX + iv];
+      const int niv = s_conn[iv];
+      const long kp = qq_ptr[niv] + A.pos_qq[((long)e * NEN + iv) * NEN + j];
+      double oq[DIM], op[DIM];
+      for (int a = 0; a < DIM; a++) {
+        oq[a] = A.vp[(long)a * A.nql + kq];
+        op[a] = A.pv[(long)a * A.nqqL + kp];
+      }
       double E[DIM];
       for (int b = 0; b < DIM; b++) E[b] = 0.;
       for (int q = 0; q < NQ; q++) {
         const double w = s_JxW[q] * s_psi[q][iv];
         for (int b = 0; b < DIM; b++) E[b] += w * s_dphi[q][j][b];
       }
-      // B^T: row (a, node j), column pressure vertex iv
-      const int nj = s_conn[j];
-      const long kq = A.ql_ptr[nj] + A.pos_ql[((long)e * NEN + j) * NVX + iv];
-      for (int a = 0; a < DIM; a++) A.vp[(long)a * A.nql + kq] += s_bcv[a][j] * (-E[a]);
-      // B: pressure row iv, column (b, node j)
-      const int niv = s_conn[iv];
-      const long kp = qq_ptr[niv] + A.pos_qq[((long)e * NEN + iv) * NEN + j];
-      for (int b = 0; b < DIM; b++) A.pv[(long)b * A.nqqL + kp] += ph.rho * E[b];
+      for (int a = 0; a < DIM; a++) A.vp[(long)a * A.nql + kq] = oq[a] + s_bcv[a][j] * (-E[a]);
+      for (int b = 0; b < DIM; b++) A.pv[(long)b * A.nqqL + kp] = op[b] + ph.rho * E[b];
     }
   }
   // rhs
   if (mode == 1) {
     for (int p = tid; p < nv2 * NEN; p += NT) {
       const int a = p / NEN, i = p % NEN;
+      double &r = A.rhs[(long)a * A.N + s_conn[i]];
+      const double old = r;
       double F = 0.;
       for (int q = 0; q < NQ; q++) F += s_phi[q][i] * s_cR[q][a];
-      A.rhs[(long)a * A.N + s_conn[i]] += s_bcv[a][i] * F;
+      r = old + s_bcv[a][i] * F;
     }
   }
   __syncthreads();
@@ -541,6 +553,27 @@ __global__ void __launch_bounds__(NT, DIM == 3 ? EXF_ASM_MINB3 : EXF_ASM_MINB2) 
   }
 }
 
+template <int DIM, int NT>
+__global__ void __launch_bounds__(NT, DIM == 3 ? EXF_ASM_MINB3 : EXF_ASM_MINB2) k_assemble(AsmArgs<DIM> A, int mode) {
+  assemble_element<DIM, NT>(A, A.elist[blockIdx.x], mode);
+}
+
+// One colour of every level in one launch: work item {level, element}, the level's
+// arguments copied to shared memory (levels write separate matrices, so their elements of
+// one colour run together; each entry still receives its elements in colour order)
+template <int DIM, int NT>
+__global__ void __launch_bounds__(NT, DIM == 3 ? EXF_ASM_MINB3 : EXF_ASM_MINB2)
+    k_assemble_levels(const AsmArgs<DIM> *__restrict__ args, const int2 *__restrict__ work) {
+  __shared__ AsmArgs<DIM> sA;
+  static_assert(sizeof(AsmArgs<DIM>) % 4 == 0, "argument block copied in words");
+  const int2 w = work[blockIdx.x];
+  const int *src = reinterpret_cast<const int *>(args + w.x);
+  int *dst = reinterpret_cast<int *>(&sA);
+  for (int k = threadIdx.x; k < (int)(sizeof(AsmArgs<DIM>) / 4); k += NT) dst[k] = src[k];
+  __syncthreads();
+  assemble_element<DIM, NT>(sA, w.y, sA.rhs ? 1 : 0);
+}
+
 template <int DIM>
 static int upload_tab(exf_mesh *m) {
   FETab<DIM> h;
@@ -554,20 +587,20 @@ static int upload_tab(exf_mesh *m) {
 // devices (driven from different threads) never share or replace them
 int upload_fe_table(exf_mesh *m) { return m->dim == 2 ? upload_tab<2>(m) : upload_tab<3>(m); }
 
+// the arguments of level lev's assembly, its matrix (and rhs for mode 1) zeroed on the stream
 template <int DIM>
-static int assemble_dim(exf_sys *s, const exf_phys *ph, int lev, int mode) {
+static int level_args(exf_sys *s, const exf_phys *ph, int lev, int mode, AsmArgs<DIM> &a) {
   exf_mesh *m = s->mesh;
   if (!m->d_fetab.p || m->d_fetab.n != sizeof(FETab<DIM>)) {
     set_error("assembly: the mesh has no FE tables of dimension %d", DIM);
     return EXF_ERR_STATE;
   }
-  const FETab<DIM> *d_tab = reinterpret_cast<const FETab<DIM> *>(m->d_fetab.p);
   SysLevel &L = s->L[lev];
   const MeshLevel &ml = m->lev[lev];
   const int top = s->nlev - 1;
   cudaStream_t st = s->stream;
-  AsmArgs<DIM> a;
-  a.tab = d_tab;
+  memset(&a, 0, sizeof(a));
+  a.tab = reinterpret_cast<const FETab<DIM> *>(m->d_fetab.p);
   for (int sd = 0; sd < FE<DIM>::NSIDE; sd++) {
     for (int k = 0; k < FE<DIM>::NSN; k++) a.side.nodes[sd][k] = DIM == 2 ? Q9_SIDE[sd][k] : H27_FACE[sd][k];
     for (int d = 0; d < 3; d++) a.side.dir[sd][d] = DIM == 2 ? Q9_SIDE_DIR[sd][d] : H27_FACE_DIR[sd][d];
@@ -612,17 +645,78 @@ static int assemble_dim(exf_sys *s, const exf_phys *ph, int lev, int mode) {
     EXF_TRY(L.A.pp.zero(st));
   }
   if (mode == 1) EXF_TRY(L.b.zero(st));
+  return EXF_OK;
+}
+
+template <int DIM>
+static int assemble_dim(exf_sys *s, const exf_phys *ph, int lev, int mode) {
+  AsmArgs<DIM> a;
+  EXF_TRY(level_args<DIM>(s, ph, lev, mode, a));
+  const MeshLevel &ml = s->mesh->lev[lev];
   constexpr int NT = DIM == 2 ? 128 : 256;
   for (int c = 0; c + 1 < (int)ml.ecol_off.size(); c++) {
     int n = ml.ecol_off[c + 1] - ml.ecol_off[c];
     if (n == 0) continue;
     a.elist = ml.d_elist.p + ml.ecol_off[c];
     a.nel_c = n;
-    k_assemble<DIM, NT><<<n, NT, 0, st>>>(a, mode);
+    k_assemble<DIM, NT><<<n, NT, 0, s->stream>>>(a, mode);
     EXF_LAUNCH_CHECK();
     EXF_COUNT(1);
   }
   return EXF_OK;
+}
+
+// every level (the top one with its rhs) in one launch per colour: the work list of
+// colour c is {level, element} for every level's elements of colour c, top level first,
+// built once per system
+template <int DIM>
+static int assemble_all_dim(exf_sys *s, const exf_phys *ph) {
+  const int nl = s->nlev, top = nl - 1;
+  exf_mesh *m = s->mesh;
+  if (s->asm_work_off.empty()) {
+    int ncol = 0;
+    for (int l = 0; l < nl; l++) ncol = std::max(ncol, (int)m->lev[l].ecol_off.size() - 1);
+    std::vector<int2> work;
+    std::vector<int> off(1, 0);
+    for (int c = 0; c < ncol; c++) {
+      for (int l = top; l >= 0; l--) {
+        const MeshLevel &ml = m->lev[l];
+        if (c + 1 >= (int)ml.ecol_off.size()) continue;
+        std::vector<int> el(ml.ecol_off[c + 1] - ml.ecol_off[c]);
+        if (!el.empty())
+          EXF_CUDA(cudaMemcpy(el.data(), ml.d_elist.p + ml.ecol_off[c], el.size() * sizeof(int),
+                              cudaMemcpyDeviceToHost));
+        for (int e : el) work.push_back(make_int2(l, e));
+      }
+      off.push_back((int)work.size());
+    }
+    EXF_TRY(s->asm_work.alloc(std::max<size_t>(1, work.size()) * sizeof(int2)));
+    if (!work.empty())
+      EXF_CUDA(cudaMemcpy(s->asm_work.p, work.data(), work.size() * sizeof(int2), cudaMemcpyHostToDevice));
+    s->asm_work_off = off;
+  }
+  std::vector<AsmArgs<DIM>> args(nl);
+  for (int l = 0; l < nl; l++) EXF_TRY(level_args<DIM>(s, ph, l, l == top ? 1 : 0, args[l]));
+  EXF_TRY(s->asm_args.ensure(nl * sizeof(AsmArgs<DIM>)));
+  EXF_CUDA(cudaMemcpyAsync(s->asm_args.p, args.data(), nl * sizeof(AsmArgs<DIM>), cudaMemcpyHostToDevice, s->stream));
+  constexpr int NT = DIM == 2 ? 128 : 256;
+  const AsmArgs<DIM> *d_args = reinterpret_cast<const AsmArgs<DIM> *>(s->asm_args.p);
+  const int2 *d_work = reinterpret_cast<const int2 *>(s->asm_work.p);
+  for (int c = 0; c + 1 < (int)s->asm_work_off.size(); c++) {
+    const int n = s->asm_work_off[c + 1] - s->asm_work_off[c];
+    if (n == 0) continue;
+    k_assemble_levels<DIM, NT><<<n, NT, 0, s->stream>>>(d_args, d_work + s->asm_work_off[c]);
+    EXF_LAUNCH_CHECK();
+    EXF_COUNT(1);
+  }
+  // `args` is pageable host memory: the asynchronous copy has staged it by the time the
+  // call returned, so it may go out of scope while the launches read the device copy
+  return EXF_OK;
+}
+
+int assemble_all_levels(exf_sys *s, const exf_phys *ph) {
+  if (s->mesh->dim == 2) return assemble_all_dim<2>(s, ph);
+  return assemble_all_dim<3>(s, ph);
 }
 
 int assemble_level(exf_sys *s, const exf_phys *ph, int lev, int mode) {

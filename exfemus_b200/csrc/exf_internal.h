@@ -291,6 +291,10 @@ struct exf_sys {
   // scratch of exf_adjoint_backward, kept between calls: the forward x and b, x_old, the
   // element sources, dB/dx_old, the adjoint state, the source gradient
   exf::DBuf<double> adj_x, adj_b, adj_xold, adj_qe, adj_w, adj_lam, adj_gq;
+  // exf_assemble_all: per colour the {level, element} work list of every level (top level
+  // first) and the levels' argument blocks
+  exf::DBuf<unsigned char> asm_work, asm_args;
+  std::vector<int> asm_work_off;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   cudaEvent_t user_ev[8] = {nullptr};
   // captured graphs, a few per system so that alternating parameter sets (a forward and
@@ -358,6 +362,7 @@ bool transfers_ready(const exf_sys *s);
 int update_rmask(exf_sys *s);
 int build_colours(exf_sys *s);
 int assemble_level(exf_sys *s, const exf_phys *ph, int lev, int mode);
+int assemble_all_levels(exf_sys *s, const exf_phys *ph);  // every level, one launch per colour
 int sync_fp32(exf_sys *s, int lev);  // FP32 copy + smoother coefficients after a matrix change
 int vanka_prep(exf_sys *s, int lev);
 int csr_values(exf_sys *s, int lev, double *d_out);         // NB -> CSR order (device)

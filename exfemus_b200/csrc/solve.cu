@@ -1585,7 +1585,7 @@ __global__ void __launch_bounds__(32 * (NWC + 1), 1)
 #define EXF_ST_SLOTS 2
 #endif
 #ifndef EXF_BK_NWC
-#define EXF_BK_NWC 19
+#define EXF_BK_NWC 23
 #endif
 #ifndef EXF_BK_STG
 #define EXF_BK_STG 4
@@ -1594,7 +1594,7 @@ __global__ void __launch_bounds__(32 * (NWC + 1), 1)
 #define EXF_BK_CAPB 3072
 #endif
 #ifndef EXF_BK_UNR
-#define EXF_BK_UNR 6
+#define EXF_BK_UNR 4
 #endif
 #ifndef EXF_BK_LPR
 #define EXF_BK_LPR 16

@@ -237,7 +237,9 @@ EXF_API int exf_sys_get_rhs(exf_sys *s, double *b);
 
 /* --- assembly: GenMatRhs (MGSolverNS.C:108-717, MGSolverT.C:93-525) ----------------- */
 EXF_API int exf_gen_mat_rhs(exf_sys *s, const exf_phys *ph, int lev, int mode);
-EXF_API int exf_assemble_all(exf_sys *s, const exf_phys *ph);   /* top mode 1, others mode 0 */
+/* every level, top mode 1, others mode 0: the same matrices and rhs, bit for bit, as
+ * exf_gen_mat_rhs level by level, in one launch per element colour for all levels */
+EXF_API int exf_assemble_all(exf_sys *s, const exf_phys *ph);
 EXF_API int exf_get_matrix(exf_sys *s, int lev, double *val);   /* values in pattern order  */
 EXF_API int exf_set_matrix(exf_sys *s, int lev, const double *val);
 

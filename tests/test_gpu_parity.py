@@ -84,6 +84,22 @@ def test_assembly_matches_oracle(case):
     assert np.abs(g - o).max() <= 1e-12 * max(np.abs(o).max(), 1e-300)
 
 
+def test_assemble_all_equals_per_level_gen_mat_rhs(case):
+    """exf_assemble_all (every level's elements of one colour in one launch) gives the bits
+    of GenMatRhs called level by level (top level with its rhs): each entry receives the
+    same element contributions in the same colour order."""
+    gs = case["gs"]
+    nlev = case["nlev"]
+    gs.assemble_all()
+    m_all = [gs.matrix(lev) for lev in range(nlev)]
+    b_all = gs.rhs()
+    for lev in range(nlev):
+        gs.GenMatRhs(0.0, lev, 1 if lev == nlev - 1 else 0)
+    for lev in range(nlev):
+        assert np.array_equal(gs.matrix(lev), m_all[lev]), lev
+    assert np.array_equal(gs.rhs(), b_all)
+
+
 def test_solver_operations_match_oracle(case):
     _assemble_both(case)
     gs, os_ = case["gs"], case["os"]
