@@ -1654,9 +1654,26 @@ static int vanka_sweep_rows(exf_sys *s, int lev, const exf_mg_params *p, T *x, c
   constexpr int LPR_S = (D == 3 && sizeof(T) == 4) ? EXF_LPR_BIG32 : LPR;
   constexpr int MINB_S = sizeof(T) == 4 ? EXF_MINB_BIG32 : EXF_MINB_BIG64;
   // 3D FP32 levels of one to four waves: two blocks per lane, 64 registers
-  constexpr int UNR_M = (D == 3 && sizeof(T) == 4) ? 2 : UNR_S;
-  constexpr int MINB_M = (D == 3 && sizeof(T) == 4) ? 4 : MINB_S;
-  constexpr int UNR_L = (D == 3 && sizeof(T) == 4) ? 4 : 2;
+#ifndef EXF_UNR_MID32
+#define EXF_UNR_MID32 2
+#endif
+#ifndef EXF_MINB_MID32
+#define EXF_MINB_MID32 4
+#endif
+#ifndef EXF_LPR_MID32
+#define EXF_LPR_MID32 32
+#endif
+#ifndef EXF_UNR_SMALL32
+#define EXF_UNR_SMALL32 2
+#endif
+#ifndef EXF_LPR_SMALL32
+#define EXF_LPR_SMALL32 32
+#endif
+  constexpr int UNR_M = (D == 3 && sizeof(T) == 4) ? EXF_UNR_MID32 : UNR_S;
+  constexpr int MINB_M = (D == 3 && sizeof(T) == 4) ? EXF_MINB_MID32 : MINB_S;
+  constexpr int LPR_M = (D == 3 && sizeof(T) == 4) ? EXF_LPR_MID32 : LPR;
+  constexpr int UNR_L = (D == 3 && sizeof(T) == 4) ? EXF_UNR_SMALL32 : 2;
+  constexpr int LPR_L = (D == 3 && sizeof(T) == 4) ? EXF_LPR_SMALL32 : LPR;
   T *res = VK<T>::res(L);
   const long pres_off = (long)L.vrow_off[L.ncolour] * D;
   for (int cc = 0; cc < L.ncolour; cc++) {
@@ -1762,9 +1779,10 @@ static int vanka_sweep_rows(exf_sys *s, int lev, const exf_mg_params *p, T *x, c
         using VB = Packed16<D>;
         const VB vb{L.qq_col.p, L.h16.p, L.h16cx.p};
         auto kern = big   ? k_vanka_rows<T, D, LPR_S, NTR, I4, UNR_S, MINB_S, VB>
-                    : mid ? k_vanka_rows<T, D, LPR, NTR, I4, UNR_M, MINB_M, VB>
-                          : k_vanka_rows<T, D, LPR, NTR, I4, UNR_L, 1, VB>;
-        EXF_CUDA(launch_pdl(kern, dim3(nblk(big ? nthr_s : nthr, NTR)), dim3(NTR), 0, s->stream,
+                    : mid ? k_vanka_rows<T, D, LPR_M, NTR, I4, UNR_M, MINB_M, VB>
+                          : k_vanka_rows<T, D, LPR_L, NTR, I4, UNR_L, 1, VB>;
+        const long nthr_k = big ? nthr_s : (long)(nr + n) * (mid ? LPR_M : LPR_L);
+        EXF_CUDA(launch_pdl(kern, dim3(nblk(nthr_k, NTR)), dim3(NTR), 0, s->stream,
                             L.vrinfo.p + L.vrow_off[c], nr, L.vrow_off[c], pin, n, L.N, vb, (const T *)L.vsc.p,
                             L.qq_col.p, L.ql_col.p, L.nql, L.nqqL, VT<T>::vp(L), VT<T>::pv(L), VT<T>::pp(L), x, b,
                             res, pres_off));

@@ -99,6 +99,34 @@ def test_graph_and_eager_cycles_agree_bitwise(heat):
     assert np.array_equal(xs[0], xs[1])
 
 
+def test_graph_cache_eviction_keeps_results(gpu_lib):
+    """Six parameter sets on one system (more than its four cached solve graphs, so graphs
+    are evicted and rebuilt) solved twice in turn: every solve gives the bits of the same
+    parameters solved on a fresh system."""
+    def make():
+        m = ex.Mesh(2, 3, (4, 4), (0, 1, 0, 1))
+        t = ex.MGSolT(m)
+        t.GenBc(_lib.BC_HEAT_DIRICHLET)
+        t.set_source(np.ones(m.nel(2)))
+        t.assemble_all()
+        return m, t
+
+    sets = [dict(nu_pre=a, nu_post=a, precision=pr, reverse_colours=rv, eps=1e-11)
+            for a in (1, 2, 3) for pr, rv in ((_lib.PREC_FP64, 0), (_lib.PREC_MIXED, 1))]
+    fresh = []
+    for kw in sets:
+        m, t = make()
+        t.set_x(np.zeros(t.ntop_dof))
+        st = t.solve(ex.mg_params(**kw))
+        fresh.append((st.cycles, t.x()))
+    m, t = make()
+    for _ in range(2):
+        for kw, (cyc, x) in zip(sets, fresh):
+            t.set_x(np.zeros(t.ntop_dof))
+            st = t.solve(ex.mg_params(**kw))
+            assert st.cycles == cyc and np.array_equal(t.x(), x), kw
+
+
 def test_timing_probes_and_refactorisation(heat):
     """exf_time_op 4 (coarse refactorisation) and 5 (FP64 FMA probe) run on an assembled
     system; a solve after a refactorisation gives the same bits as before it."""
