@@ -631,7 +631,7 @@ template <class T, int D, int NT, bool I4, int SU>
 __global__ void __launch_bounds__(NT)
     k_vanka_solve(const int4 *__restrict__ pinfo, int N, const int *__restrict__ vrows, const T *__restrict__ vk,
                   const T *__restrict__ pk, const T *__restrict__ res, long pres_off, T *__restrict__ x, T omega) {
-  __shared__ double s_red[NT / 32], s_bc[2];
+  __shared__ double s_red[NT / 32];
   // the patch's coefficients and star rows do not change during a sweep: load them
   // before waiting for the row kernel
   const int4 pi = pinfo[2 * blockIdx.x];
@@ -653,8 +653,7 @@ __global__ void __launch_bounds__(NT)
       ix[u] = Lay<I4>::v(t % D, vrows[g0 + t / D], N);
     }
   }
-  double Sd = 0.;
-  if (threadIdx.x == 0) Sd = (double)pk[2 * m];
+  const double Sd = (double)pk[2 * m];
   EXF_PDL_WAIT();  // residuals and iterate come from the previous kernels
 #pragma unroll
   for (int u = 0; u < SU; u++)
@@ -662,11 +661,9 @@ __global__ void __launch_bounds__(NT)
       r_[u] = rr[threadIdx.x + u * NT];
       xv[u] = x[ix[u]];
     }
-  T rp = T(0), xp = T(0);
-  if (threadIdx.x == 0) {
-    rp = res[pres_off + m];
-    xp = x[Lay<I4>::p(m, N, D)];
-  }
+  const T rp = res[pres_off + m];
+  T xp = T(0);
+  if (threadIdx.x == 0) xp = x[Lay<I4>::p(m, N, D)];
   double tsum = 0.;
 #pragma unroll
   for (int u = 0; u < SU; u++)
@@ -675,14 +672,11 @@ __global__ void __launch_bounds__(NT)
   for (int o = 16; o > 0; o >>= 1) tsum += __shfl_down_sync(0xffffffffu, tsum, o);
   if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = tsum;
   __syncthreads();
-  if (threadIdx.x == 0) {
-    double Tt = 0.;
-    for (int k = 0; k < NT / 32; k++) Tt += s_red[k];
-    s_bc[0] = Tt - (double)rp;
-    s_bc[1] = Sd;
-  }
-  __syncthreads();
-  const double num = s_bc[0], den = s_bc[1];
+  // every thread sums the warps' partials in warp order (the same value everywhere)
+  double Tt = 0.;
+#pragma unroll
+  for (int k = 0; k < NT / 32; k++) Tt += s_red[k];
+  const double num = Tt - (double)rp, den = Sd;
   const T dp = (T)(fabs(den) > 1e-300 ? num / den : 0.);
 #pragma unroll
   for (int u = 0; u < SU; u++)
