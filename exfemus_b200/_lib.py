@@ -137,6 +137,7 @@ SIGNATURES = [
     ("exf_resid_norm_static", _I, [_P, _I, _P, _P, _P, _P]),
     ("exf_mesh_upload", _I, [C.POINTER(ExfMeshData), C.POINTER(_P)]),
     ("exf_sys_set_transfer", _I, [_P, _I, _I, _I, _IP, _IP, _IP, _DP]),
+    ("exf_sys_get_transfer", _I, [_P, _I, _I, _I, _IP, _LP, _IP, _IP, _DP]),
     ("exf_sys_check_pattern", _I, [_P, _I, _I, _IP, _IP, _IP]),
 ]
 

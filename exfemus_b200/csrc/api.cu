@@ -625,6 +625,35 @@ int exf_sys_set_transfer(exf_sys *s, int lev, int kind, int block, const int dim
   return set_transfer(s, lev, kind, block, dim, len, pos, val);
 }
 
+int exf_sys_get_transfer(exf_sys *s, int lev, int kind, int block, int dim[2], long *nnz, int *len, int *pos,
+                         double *val) {
+  CHECK_LEV(s, lev);
+  if ((kind != 0 && kind != 1) || (block != 1 && block != 2) || !dim || !nnz || (block == 1 && !s->nv1)) {
+    set_error("exf_sys_get_transfer: bad argument");
+    return EXF_ERR_ARG;
+  }
+  const int other = kind == 0 ? lev - 1 : lev + 1;
+  if (other < 0 || other >= s->nlev) {
+    set_error("exf_sys_get_transfer: no level %d next to level %d", other, lev);
+    return EXF_ERR_ARG;
+  }
+  const SysLevel &L = s->L[lev], &O = s->L[other];
+  const Transfer &T = kind == 0 ? (block == 2 ? L.Pq : L.Pl) : (block == 2 ? L.Rq : L.Rl);
+  const int nrow = block == 2 ? L.N : L.NL, ncol = block == 2 ? O.N : O.NL;
+  if (T.nrow != nrow || (int)T.h_ptr.size() != nrow + 1) {
+    set_error("exf_sys_get_transfer: the %s block %d of level %d has not been built or supplied",
+              kind == 0 ? "prolongation" : "restriction", block, lev);
+    return EXF_ERR_STATE;
+  }
+  dim[0] = nrow;
+  dim[1] = ncol;
+  *nnz = T.h_ptr[nrow];
+  if (len) std::copy(T.h_ptr.begin(), T.h_ptr.end(), len);
+  if (pos) std::copy(T.h_col.begin(), T.h_col.end(), pos);
+  if (val) std::copy(T.h_val.begin(), T.h_val.end(), val);
+  return EXF_OK;
+}
+
 int exf_sys_check_pattern(exf_sys *s, int lev, int block, const int dim[2], const int *len, const int *pos) {
   CHECK_LEV(s, lev);
   SysLevel &L = s->L[lev];

@@ -233,6 +233,18 @@ class MGSolBase:
         v = np.ascontiguousarray(val, np.float64)
         check(self.L.exf_sys_set_transfer(self.h, lev, kind, block, iptr(a), iptr(b), iptr(c), dptr(v)))
 
+    def get_transfer(self, lev, kind, block):
+        """One block of a Prol/Rest operator in gencase's dataset layout: (dim, len, pos, val)."""
+        dim = np.zeros(2, np.int32)
+        nnz = C.c_long()
+        check(self.L.exf_sys_get_transfer(self.h, lev, kind, block, iptr(dim), C.byref(nnz), None, None, None))
+        ln = np.zeros(dim[0] + 1, np.int32)
+        pos = np.zeros(nnz.value, np.int32)
+        val = np.zeros(nnz.value)
+        check(self.L.exf_sys_get_transfer(self.h, lev, kind, block, iptr(dim), C.byref(nnz), iptr(ln), iptr(pos),
+                                          dptr(val)))
+        return dim, ln, pos, val
+
     def check_pattern(self, lev, block, dim, length, pos):
         """Status of exf_sys_check_pattern for one block of gencase's matrix datasets."""
         a = np.ascontiguousarray(dim, np.int32)

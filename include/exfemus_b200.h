@@ -215,6 +215,15 @@ EXF_API int exf_sys_get_colours(exf_sys *s, int lev, int *ncolours, int *colour_
  * change later.  Columns are sorted per row; entries are kept as given. */
 EXF_API int exf_sys_set_transfer(exf_sys *s, int lev, int kind, int block, const int dim[2], const int *len,
                                  const int *pos, const double *val);
+/* the writer side of exf_sys_set_transfer: one block of a level's transfer operator in
+ * gencase's dataset layout (what compute_prol_qq / compute_res_qq write,
+ * USER_APPL/gencase/src/MGGenCase.C:2308-2569), for the caller to store as DIM0<b>, LEN0<b>,
+ * POS0<b>, VAL0<b>; kind and block as for exf_sys_set_transfer.  dim receives {rows,
+ * columns} and *nnz the entry count; len (rows + 1), pos and val (nnz each) are filled when
+ * not NULL (a first call with NULL arrays sizes them).  Columns are sorted per row.
+ * EXF_ERR_STATE when the block has not been built or supplied yet. */
+EXF_API int exf_sys_get_transfer(exf_sys *s, int lev, int kind, int block, int dim[2], long *nnz, int *len, int *pos,
+                                 double *val);
 /* check a level's sparsity against gencase's matrix datasets (ReadMatrix,
  * src/MGSolverDA.C:1785-2009; LEN0<b>/POS0<b> of block b = 22 (Q2 rows, Q2 columns) or 21
  * (Q2 rows, Q1 columns)): EXF_OK when every row holds exactly the node columns the library

@@ -233,6 +233,62 @@ def test_transfers_from_gencase_blocks(name, gpu_lib):
     assert np.array_equal(out[0], out[1])
 
 
+@pytest.mark.parametrize("name", list(CASES))
+def test_transfer_blocks_written_and_read_back(name, gpu_lib):
+    """exf_sys_get_transfer writes each Prol/Rest block in gencase's layout: the blocks
+    equal the node blocks of the DOF-level operators, and supplied to an uploaded mesh
+    without parents they give that system the same operators and solution."""
+    import scipy.sparse as sp
+    dim, nlev, n0, box, kind, preset, pk = CASES[name]
+    gm = ex.Mesh(dim, nlev, n0, box)
+    gs, x0 = make_sys(gm, name)
+    bare = ex.Mesh.upload(**dict(structured_arrays(gm, n0), parent=None))
+    bs, _ = make_sys(bare, name)
+    blocks = (2, 1) if kind == _lib.KIND_NS else (2,)
+    for lev in range(nlev):
+        for kk in (0, 1):
+            if (kk == 0 and lev == 0) or (kk == 1 and lev == nlev - 1):
+                continue
+            rp, col, val = gs.prol(lev) if kk == 0 else gs.rest(lev)
+            other = lev - 1 if kk == 0 else lev + 1
+            D = sp.csr_matrix((val, col, rp), shape=(gs.ndof(lev), gs.ndof(other)))
+            for block in blocks:
+                dm, ln, pos, v = gs.get_transfer(lev, kk, block)
+                B = sp.csr_matrix((v, pos, ln), shape=tuple(dm))
+                if block == 2:
+                    R = D[:dm[0], :dm[1]]
+                else:
+                    r0, c0 = dim * gm.nnodes(lev), dim * gm.nnodes(other)
+                    R = D[r0:r0 + dm[0], c0:c0 + dm[1]]
+                if kk == 1:  # the DOF-level restriction carries the bc0 % 2 row mask
+                    keep = np.asarray(abs(R).sum(axis=1)).ravel() > 0
+                    B = sp.diags(keep.astype(float)) @ B
+                assert abs(B - R).max() == 0.0, (lev, kk, block)
+                bs.set_transfer(lev, kk, block, dm, ln, pos, v)
+    for lev in range(nlev):
+        if lev > 0:
+            for a, b in zip(gs.prol(lev), bs.prol(lev)):
+                assert np.array_equal(a, b)
+        if lev < nlev - 1:
+            for a, b in zip(gs.rest(lev), bs.rest(lev)):
+                assert np.array_equal(a, b)
+    gs.assemble_all()
+    bs.assemble_all()
+    out = []
+    for s_ in (gs, bs):
+        s_.set_x(x0)
+        st = s_.solve(params(name))
+        assert st.converged
+        out.append(s_.x())
+    if kind == _lib.KIND_NS:
+        assert np.array_equal(out[0], out[1])
+    else:  # the uploaded T system colours its Gauss-Seidel sweep differently
+        assert rel(out[1], out[0]) < 1e-9
+    with pytest.raises(ex.ExfError) as e:
+        bs.get_transfer(0, 0, 2)  # level 0 has no prolongation
+    assert e.value.code == _lib.EXF_ERR_ARG
+
+
 @pytest.mark.parametrize("name", ["heat2d", "cavity2d"])
 def test_pattern_check_against_gencase_blocks(name, gpu_lib):
     dim, nlev, n0, box, kind, preset, pk = CASES[name]
