@@ -48,6 +48,11 @@ class ExfMeshData(C.Structure):
                 ("neigh", C.c_void_p), ("parent", C.c_void_p)]
 
 
+class ExfMeshCoarse(C.Structure):
+    _fields_ = [("dim", C.c_int), ("nlev", C.c_int), ("device", C.c_int), ("nnode0", C.c_int),
+                ("nvert0", C.c_int), ("xyz0", C.c_void_p), ("nel0", C.c_int), ("conn0", C.c_void_p)]
+
+
 class ExfPhys(C.Structure):
     _fields_ = [("inv_re", C.c_double), ("inv_prdl", C.c_double), ("rho", C.c_double),
                 ("rhocp", C.c_double), ("inv_dt", C.c_double), ("penalty", C.c_double),
@@ -136,6 +141,9 @@ SIGNATURES = [
     ("exf_level_bytes", _I, [_P, _I, _I, _DP, _DP]),
     ("exf_resid_norm_static", _I, [_P, _I, _P, _P, _P, _P]),
     ("exf_mesh_upload", _I, [C.POINTER(ExfMeshData), C.POINTER(_P)]),
+    ("exf_mesh_refine_arrays", _I, [C.POINTER(ExfMeshCoarse), C.POINTER(ExfMeshData)]),
+    ("exf_mesh_data_free", None, [C.POINTER(ExfMeshData)]),
+    ("exf_mesh_refine", _I, [C.POINTER(ExfMeshCoarse), C.POINTER(_P)]),
     ("exf_sys_set_transfer", _I, [_P, _I, _I, _I, _IP, _IP, _IP, _DP]),
     ("exf_sys_get_transfer", _I, [_P, _I, _I, _I, _IP, _LP, _IP, _IP, _DP]),
     ("exf_sys_check_pattern", _I, [_P, _I, _I, _IP, _IP, _IP]),

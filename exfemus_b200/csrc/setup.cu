@@ -619,7 +619,9 @@ static void build_prol_host(const exf_mesh *m, int l, bool quad, Transfer &P) {
 // the parent's vertex k (uniform refinement keeps the parent's orientation), so its local
 // node with offsets (a,b,c) sits at xi = -1 + (2 pos + (a,b,c)) / 2 in the parent, pos =
 // (parent vertex k's offsets) / 2.  Returns false when an element breaks that rule or the
-// rows do not reproduce the fine node coordinates (both exact for affine refinement).
+// quadratic rows do not reproduce the fine node coordinates (the parent's Q2 map places a
+// uniform refinement's nodes, curved elements included; the linear rows share the
+// placement, and a bilinear interpolation of curved coordinates is not expected to match).
 static bool build_prol_parent(const exf_mesh *m, int l, bool quad, Transfer &P) {
   const int dim = m->dim, nen = m->nen, nvx = m->nvx;
   const MeshLevel &fl = m->lev[l], &cl = m->lev[l - 1];
@@ -661,7 +663,7 @@ static bool build_prol_parent(const exf_mesh *m, int l, bool quad, Transfer &P) 
       for (int d = 0; d < dim; d++) xr[d] += v * m->xyz[(size_t)pc[kj] + (size_t)d * m->ntop];
       if (fabs(v) > 1e-8) ent.push_back({pc[kj], v});
     }
-    for (int d = 0; d < dim; d++) {
+    for (int d = 0; quad && d < dim; d++) {
       const double ext = m->box[2 * d + 1] - m->box[2 * d];
       if (fabs(xr[d] - m->xyz[(size_t)i + (size_t)d * m->ntop]) > 1e-9 * (ext > 0 ? ext : 1.)) return false;
     }

@@ -85,6 +85,55 @@ class Mesh:
         self.h, self.L, self.dim, self.nlev = h, L, dim, nlev
         return self
 
+    @staticmethod
+    def _coarse(dim, nlev, nvert0, xyz0, conn0, device):
+        xyz0 = np.ascontiguousarray(xyz0, np.float64)
+        conn0 = np.ascontiguousarray(conn0, np.int32)
+        c = _lib.ExfMeshCoarse()
+        c.dim, c.nlev, c.device, c.nvert0 = dim, nlev, device, nvert0
+        c.nnode0, c.nel0 = xyz0.shape[1], conn0.shape[0]
+        c.xyz0, c.conn0 = xyz0.ctypes.data, conn0.ctypes.data
+        return c, (xyz0, conn0)
+
+    @classmethod
+    def refine(cls, dim, nlev, nvert0, xyz0, conn0, device=0):
+        """A hierarchy by uniform refinement of a coarse quad9 / hex27 mesh (gencase's role):
+        xyz0 [dim][nnode0] with the nvert0 vertices first, conn0 [nel0][9|27] libMesh order."""
+        L = load()
+        c, keep = cls._coarse(dim, nlev, nvert0, xyz0, conn0, device)
+        h = C.c_void_p()
+        check(L.exf_mesh_refine(C.byref(c), C.byref(h)))
+        self = cls.__new__(cls)
+        self.h, self.L, self.dim, self.nlev = h, L, dim, nlev
+        return self
+
+    @staticmethod
+    def refine_arrays(dim, nlev, nvert0, xyz0, conn0):
+        """The refined hierarchy as host arrays (no device work): dict of nnodes, nel, xyz
+        [dim][ntop], conn, neigh and parent per level."""
+        L = load()
+        c, keep = Mesh._coarse(dim, nlev, nvert0, xyz0, conn0, 0)
+        d = _lib.ExfMeshData()
+        check(L.exf_mesh_refine_arrays(C.byref(c), C.byref(d)))
+        try:
+            nnodes = np.ctypeslib.as_array(C.cast(d.nnodes, C.POINTER(C.c_int)), (nlev,)).copy()
+            nel = np.ctypeslib.as_array(C.cast(d.nel, C.POINTER(C.c_int)), (nlev,)).copy()
+            ntop = int(nnodes[-1])
+            xyz = np.ctypeslib.as_array(C.cast(d.xyz, C.POINTER(C.c_double)), (dim, ntop)).copy()
+            nen, ns = (9, 4) if dim == 2 else (27, 6)
+            tot = int(nel.sum())
+            conn = np.ctypeslib.as_array(C.cast(d.conn, C.POINTER(C.c_int)), (tot, nen)).copy()
+            neigh = np.ctypeslib.as_array(C.cast(d.neigh, C.POINTER(C.c_int)), (tot, ns)).copy()
+            parent = (np.ctypeslib.as_array(C.cast(d.parent, C.POINTER(C.c_int)), (tot - int(nel[0]),)).copy()
+                      if nlev > 1 else np.zeros(0, np.int32))
+        finally:
+            L.exf_mesh_data_free(C.byref(d))
+        off = np.concatenate([[0], np.cumsum(nel)])
+        return dict(nnodes=nnodes, nel=nel, nvert0=nvert0, xyz=xyz,
+                    conn=[conn[off[l]:off[l + 1]] for l in range(nlev)],
+                    neigh=[neigh[off[l]:off[l + 1]] for l in range(nlev)],
+                    parent=[None] + [parent[off[l] - off[1]:off[l + 1] - off[1]] for l in range(1, nlev)])
+
     def close(self):
         if getattr(self, "h", None):
             self.L.exf_mesh_destroy(self.h)

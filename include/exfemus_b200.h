@@ -183,6 +183,33 @@ typedef struct {
   const int *parent;
 } exf_mesh_data;
 EXF_API int exf_mesh_upload(const exf_mesh_data *d, exf_mesh **out);
+/* --- mesh by uniform refinement of a coarse quad9 / hex27 mesh (the role of gencase:
+ * libMesh uniformly_refine(nlev - 1) and printMesh's level-nested numbering,
+ * USER_APPL/gencase/src/MGGenCase.C:176-181, 234-...):
+ *   nnode0, xyz0  the coarse mesh's Q2 nodes, [dim][nnode0] component-major; its nvert0
+ *                 vertices are nodes 0..nvert0-1
+ *   nel0, conn0   its elements, [nel0][9 | 27] in libMesh Quad9/Hex27 local order
+ * Every element splits into the 2^dim sub-cells of its reference element with its own
+ * orientation; new nodes take the element's triquadratic (biquadratic) map at their
+ * reference coordinates, so curved elements stay curved, and points on shared edges and
+ * faces are created once.  Level L+1 keeps the nodes of level L with their numbers and
+ * appends its new ones; neighbours are matched by side vertices; the parent of child
+ * e * 2^dim + c is e.  exf_mesh_refine_arrays returns the hierarchy as exf_mesh_upload
+ * takes it (host arrays owned by the library, released by exf_mesh_data_free);
+ * exf_mesh_refine uploads it, transfers from the parents. */
+typedef struct {
+  int dim;
+  int nlev;
+  int device;
+  int nnode0;
+  int nvert0;
+  const double *xyz0;
+  int nel0;
+  const int *conn0;
+} exf_mesh_coarse;
+EXF_API int exf_mesh_refine_arrays(const exf_mesh_coarse *c, exf_mesh_data *out);
+EXF_API void exf_mesh_data_free(exf_mesh_data *d);
+EXF_API int exf_mesh_refine(const exf_mesh_coarse *c, exf_mesh **out);
 EXF_API int exf_mesh_info(const exf_mesh *m, int lev, int *nnodes, int *nel, int *nvert0);
 EXF_API int exf_mesh_get_xyz(const exf_mesh *m, double *xyz);               /* [dim][ntop]    */
 EXF_API int exf_mesh_get_conn(const exf_mesh *m, int lev, int *conn, int *neigh, int *colour);

@@ -315,3 +315,116 @@ def test_pattern_check_against_gencase_blocks(name, gpu_lib):
             bad = np.concatenate([rows[0][1:]] + rows[1:])
             blen = np.concatenate([[0], np.cumsum([len(rows[0]) - 1] + [len(r) for r in rows[1:]])])
             assert s.check_pattern(lev, block, (nr, nc), blen, bad) == _lib.EXF_ERR_ARG
+
+
+def coord_match(xa, xb):
+    """sigma with xb[:, sigma[i]] == xa[:, i] (both point sets equal up to 1e-12)."""
+    def order(x):
+        r = np.round(np.asarray(x, float).T, 12)
+        return np.lexsort(r.T[::-1])
+    oa, ob = order(xa), order(xb)
+    assert np.abs(xa[:, oa] - xb[:, ob]).max() < 1e-12
+    sigma = np.empty(xa.shape[1], dtype=np.int64)
+    sigma[oa] = ob
+    return sigma
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_refined_box_solves_like_the_generated_box(name, gpu_lib):
+    """exf_mesh_refine on a generated box's level-0 mesh: the refined hierarchy (its own
+    node numbering) gives the generated box's solution, matched node by node by
+    coordinates, within 1e-10."""
+    dim, nlev, n0, box, kind, preset, pk = CASES[name]
+    gm = ex.Mesh(dim, nlev, n0, box)
+    c0 = gm.conn(0)[0]
+    rm = ex.Mesh.refine(dim, nlev, gm.nvert0, gm.xyz()[:, :gm.nnodes(0)], c0)
+    assert [rm.nnodes(l) for l in range(nlev)] == [gm.nnodes(l) for l in range(nlev)]
+    gs, x0 = make_sys(gm, name)
+    rs, rx0 = make_sys(rm, name)
+    sigma = coord_match(gm.xyz(), rm.xyz())
+    N = gm.ntop
+    nv2 = dim if kind == _lib.KIND_NS else 1
+    dmap = np.concatenate([a * N + sigma for a in range(nv2)] +
+                          ([nv2 * N + sigma[:gm.nnodes(nlev - 2)]] if kind == _lib.KIND_NS else []))
+    assert np.all(sigma[:gm.nnodes(nlev - 2)] < gm.nnodes(nlev - 2))  # nesting kept
+    for a, b in zip(gs.bc(), rs.bc()):
+        assert np.array_equal(b[dmap], a)
+    assert np.array_equal(rx0[dmap], x0)
+    gs.assemble_all()
+    rs.assemble_all()
+    assert rel(rs.rhs()[dmap], gs.rhs()) < 1e-13
+    for s_, x in ((gs, x0), (rs, rx0)):
+        s_.set_x(x)
+        assert s_.solve(params(name, eps=1e-12)).converged
+    assert rel(rs.x()[dmap], gs.x()) < 1e-10
+
+
+Q9_ABC = [(0, 0, 0), (2, 0, 0), (2, 2, 0), (0, 2, 0), (1, 0, 0), (2, 1, 0), (1, 2, 0), (0, 1, 0), (1, 1, 0)]
+H27_ABC = [(0, 0, 0), (2, 0, 0), (2, 2, 0), (0, 2, 0), (0, 0, 2), (2, 0, 2), (2, 2, 2), (0, 2, 2),
+           (1, 0, 0), (2, 1, 0), (1, 2, 0), (0, 1, 0), (0, 0, 1), (2, 0, 1), (2, 2, 1), (0, 2, 1),
+           (1, 0, 2), (2, 1, 2), (1, 2, 2), (0, 1, 2), (1, 1, 0), (1, 0, 1), (2, 1, 1), (1, 2, 1),
+           (0, 1, 1), (1, 1, 2), (1, 1, 1)]
+Q9_SIDE = [[0, 1, 4], [1, 2, 5], [2, 3, 6], [3, 0, 7]]
+H27_FACE = [[0, 1, 2, 3, 8, 9, 10, 11, 20], [0, 1, 5, 4, 8, 13, 16, 12, 21], [1, 2, 6, 5, 9, 14, 17, 13, 22],
+            [2, 3, 7, 6, 10, 15, 18, 14, 23], [3, 0, 4, 7, 11, 12, 19, 15, 24], [4, 5, 6, 7, 16, 17, 18, 19, 25]]
+
+
+def skewed_coarse(dim, ne, corners):
+    """A coarse grid of ne elements per axis mapped by the (tri)linear map of `corners`
+    (2^dim points, lexicographic): straight-sided elements that are not parallelograms.
+    Returns nvert0, xyz0 [dim][n], conn0 [nel][9 | 27] with the vertices numbered first."""
+    abc = Q9_ABC if dim == 2 else H27_ABC
+    ne3 = list(ne) + [1] * (3 - dim)
+    lat = [(i, j, k) for k in range(2 * ne3[2] + 1 if dim == 3 else 1)
+           for j in range(2 * ne3[1] + 1) for i in range(2 * ne3[0] + 1)]
+    lat.sort(key=lambda p: (any(v % 2 for v in p[:dim]), p[2], p[1], p[0]))  # vertices first
+    idx = {p: n for n, p in enumerate(lat)}
+    nvert0 = sum(1 for p in lat if not any(v % 2 for v in p[:dim]))
+    C = np.asarray(corners, float)
+    xyz0 = np.zeros((dim, len(lat)))
+    for n, p in enumerate(lat):
+        t = [p[d] / (2.0 * ne3[d]) for d in range(dim)]
+        w = []
+        for m in range(2 ** dim):
+            b = [(m >> d) & 1 for d in range(dim)]
+            w.append(np.prod([t[d] if b[d] else 1 - t[d] for d in range(dim)]))
+        xyz0[:, n] = np.asarray(w) @ C
+    conn = []
+    for ez in range(ne3[2]):
+        for ey in range(ne3[1]):
+            for ex_ in range(ne3[0]):
+                o = (2 * ex_, 2 * ey, 2 * ez)
+                conn.append([idx[(o[0] + a, o[1] + b, o[2] + (c if dim == 3 else 0))] for a, b, c in abc])
+    return nvert0, xyz0, np.array(conn)
+
+
+@pytest.mark.parametrize("dim,nlev,ne,corners", [
+    (2, 4, (2, 2), [(0.0, 0.0), (2.0, 0.1), (0.3, 1.2), (1.7, 1.5)]),
+    (3, 3, (2, 1, 1), [(0, 0, 0), (2, 0, 0.2), (0, 1, 0), (1.8, 1.1, 0), (0.1, 0, 1), (2.1, 0, 1.2),
+                       (0, 1.3, 1), (2, 1, 0.9)]),
+])
+def test_refined_skewed_mesh_reproduces_a_linear_field(dim, nlev, ne, corners, gpu_lib):
+    """Heat with Dirichlet data from a linear field and no source on a refined non-affine
+    mesh: isoparametric Q2 elements reproduce the field at every node."""
+    nvert0, xyz0, conn0 = skewed_coarse(dim, ne, corners)
+    m = ex.Mesh.refine(dim, nlev, nvert0, xyz0, conn0)
+    t = ex.MGSolT(m)
+    top = nlev - 1
+    c, nb, _ = m.conn(top)
+    sides = Q9_SIDE if dim == 2 else H27_FACE
+    bnd = np.zeros(m.ntop, bool)
+    for e, s in zip(*np.nonzero(nb < 0)):
+        bnd[c[e, sides[s]]] = True
+    b0 = np.where(bnd, 0, 1).astype(np.int32)
+    b1 = np.ones(m.ntop, np.int32)
+    t.set_bc(b0, b1)
+    xyz = m.xyz()
+    g = 0.3 + 0.7 * xyz[0] - 0.4 * xyz[1] + (0.2 * xyz[2] if dim == 3 else 0.0)
+    t.set_xold(g)
+    t.set_source(np.zeros(m.nel(top)))
+    t.phys = ex.phys()
+    t.assemble_all()
+    t.set_x(np.zeros(t.ntop_dof))
+    st = t.solve(ex.mg_params(eps=1e-13, max_cycles=200, smoother=_lib.SMOOTH_GS, nu_pre=2, nu_post=2))
+    assert st.converged
+    assert np.abs(t.x() - g).max() < 1e-9 * np.abs(g).max()
