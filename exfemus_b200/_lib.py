@@ -16,6 +16,7 @@ EXF_ERR_NOT_CONVERGED = 5
 EXF_ERR_SINGULAR = 6
 EXF_ERR_NOMEM = 7
 EXF_ERR_UNSUPPORTED = 8
+EXF_ERR_IO = 9
 
 KIND_T = 0
 KIND_NS = 1
@@ -51,6 +52,17 @@ class ExfMeshData(C.Structure):
 class ExfMeshCoarse(C.Structure):
     _fields_ = [("dim", C.c_int), ("nlev", C.c_int), ("device", C.c_int), ("nnode0", C.c_int),
                 ("nvert0", C.c_int), ("xyz0", C.c_void_p), ("nel0", C.c_int), ("conn0", C.c_void_p)]
+
+
+class ExfSolnOut(C.Structure):
+    _fields_ = [("dir", C.c_char_p), ("basesol", C.c_char_p), ("basemesh", C.c_char_p),
+                ("connlin", C.c_char_p), ("ndigits", C.c_int), ("t_step", C.c_int), ("time", C.c_double)]
+
+
+class ExfNodeFields(C.Structure):
+    _fields_ = [("dim", C.c_int), ("nnodes", C.c_int), ("xyz", C.c_void_p), ("nel", C.c_int),
+                ("conn", C.c_void_p), ("nvars", C.c_int), ("names", C.POINTER(C.c_char_p)),
+                ("order", C.c_void_p), ("vals", C.c_void_p)]
 
 
 class ExfPhys(C.Structure):
@@ -147,6 +159,8 @@ SIGNATURES = [
     ("exf_sys_set_transfer", _I, [_P, _I, _I, _I, _IP, _IP, _IP, _DP]),
     ("exf_sys_get_transfer", _I, [_P, _I, _I, _I, _IP, _LP, _IP, _IP, _DP]),
     ("exf_sys_check_pattern", _I, [_P, _I, _I, _IP, _IP, _IP]),
+    ("exf_write_xdmf", _I, [C.POINTER(ExfNodeFields), C.POINTER(ExfSolnOut)]),
+    ("exf_print_soln", _I, [C.POINTER(_P), _I, C.POINTER(C.c_char_p), _DP, C.POINTER(ExfSolnOut)]),
 ]
 
 

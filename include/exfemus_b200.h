@@ -40,6 +40,7 @@ extern "C" {
 #define EXF_ERR_SINGULAR 6      /* zero pivot in the coarsest direct factorisation  */
 #define EXF_ERR_NOMEM 7         /* device allocation failed                         */
 #define EXF_ERR_UNSUPPORTED 8   /* option not implemented for this system or kernel */
+#define EXF_ERR_IO 9            /* an output file could not be written              */
 
 /* system kinds: MGSolT (one quadratic variable) and coupled MGSolNS (NS_EQUATIONS==1:
  * dim quadratic velocity components + one linear pressure) */
@@ -290,6 +291,50 @@ EXF_API int exf_mg_solve(exf_sys *s, const exf_mg_params *p, exf_solve_stats *st
  * failing solve and returns its status. */
 EXF_API int exf_timestep_loop(exf_sys *const *sys, int nsys, const exf_phys *phys, const exf_mg_params *params,
                               int nsteps, int *cycles, double *seconds);
+
+/* --- solution output (MGEquationsSystem::print_soln, src/MGEquationsSystem.C:606-721,
+ * with MGMesh::print_conn_lin_hf5 / print_xmf_topology / print_xmf_geometry,
+ * src/MGMesh.C:439-477, 1074-1195, and MGSolDA::print_u / print_xml_attrib,
+ * src/MGSolverDA.C:1184-1290).  HDF5 is replaced by raw little-endian binary files that the
+ * XDMF file addresses by byte offset (Format="Binary", Seek), one file per HDF5 file of the
+ * reference, datasets in the reference's order:
+ *   <dir>/<basemesh><connlin>.bin       MSH0CONN: int32 [nel * 2^dim][4 | 8], each Q2
+ *                                       element as its 2^dim linear sub-cells
+ *   <dir>/<basemesh>.<step>.bin         X1, X2, X3: float64 [nnodes] each (X3 = 0 in 2D)
+ *   <dir>/<basesol>.<step>.bin          one float64 [nnodes] dataset per variable
+ *   <dir>/<basesol>.<step>.xmf          Grid "Mesh": Time, Topology (Quadrilateral |
+ *                                       Hexahedron), Geometry X_Y_Z, one node Attribute
+ *                                       per variable
+ * <step> is t_step zero-padded to ndigits.  Quadratic variables are written at every node;
+ * linear ones (pressure) are read at the element vertices and interpolated to the other
+ * nodes with the element's linear basis, as print_u does. */
+typedef struct {
+  const char *dir;       /* _inout_dir: directory of every file ("" or NULL: current)  */
+  const char *basesol;   /* BASESOL: stem of the solution files, e.g. "sol"            */
+  const char *basemesh;  /* BASEMESH: stem of the mesh files, e.g. "mesh"              */
+  const char *connlin;   /* CONNLIN: suffix of the sub-cell connectivity, "_conn_lin"  */
+  int ndigits;           /* digits of the step number in file names (1..9)             */
+  int t_step;            /* step number (>= 0)                                         */
+  double time;           /* <Time Value> (the reference writes t_step * dt)            */
+} exf_soln_out;
+/* one top-level mesh with node fields, for exf_write_xdmf (host arrays only) */
+typedef struct {
+  int dim;               /* 2 (quad9) or 3 (hex27)                                      */
+  int nnodes;
+  const double *xyz;     /* [dim][nnodes] component-major                              */
+  int nel;
+  const int *conn;       /* [nel][9 | 27] libMesh local order, vertices first          */
+  int nvars;
+  const char *const *names;  /* [nvars] dataset and attribute names                    */
+  const int *order;      /* [nvars] 2: quadratic (every node), 1: linear (vertices)    */
+  const double *vals;    /* [nvars][nnodes]; a linear variable is read at vertices only */
+} exf_node_fields;
+EXF_API int exf_write_xdmf(const exf_node_fields *f, const exf_soln_out *o);
+/* print_soln of nsys systems on one mesh: every variable of every system in order
+ * (MGSolNS: u, v[, w], p; MGSolT: T unless names are given), each scaled by
+ * refvalue[var] (NULL: 1), from x of the top level. */
+EXF_API int exf_print_soln(exf_sys *const *sys, int nsys, const char *const *names, const double *refvalue,
+                           const exf_soln_out *o);
 /* unit-level operations on host buffers (NumericVectorM::resid / matrix_mult);
  * exf_resid with b == NULL returns r = A x */
 EXF_API int exf_resid(exf_sys *s, int lev, const double *x, const double *b, double *r);

@@ -2,8 +2,10 @@
 
 Reads the reference's src/MGGeomEl.C (Hex27 family, DIMENSION 2 and 3 blocks): the
 prolongation embedding matrices _embedding_matrix_q / _embedding_matrix_l (float
-constants) and the side topology _surf_top.  These are the reference's own numbers
-the restated prolongation/restriction and boundary loops must reproduce.
+constants), the side topology _surf_top and the linear-in-quadratic element map Prol;
+and from src/MGMesh.C (MGMesh::print_conn_lin_hf5) the split of a Quad9 / Hex27 into its
+linear sub-cells for output.  These are the reference's own numbers the restated
+prolongation/restriction, boundary loops and output must reproduce.
 
     python tests/golden/make_golden.py path/to/reference
     EXFEMUS_REFERENCE=path/to/reference python tests/golden/make_golden.py
@@ -27,7 +29,11 @@ TABLES = {
     "hex27_embedding_q": ("_embedding_matrix_q[8][27][27]", (8, 27, 27)),
     "hex8_embedding_l": ("_embedding_matrix_l[8][8][8]", (8, 8, 8)),
     "hex27_surf_top": ("_surf_top[54]", (6, 9)),
+    "quad9_prol": ("Prol[9*4]", (9, 4)),
+    "hex27_prol": ("Prol[27*8]", (27, 8)),
 }
+# case label of MGMesh::print_conn_lin_hf5 -> (key, sub-cells, corners)
+CONN_LIN = {"9": ("quad9_conn_lin", 4, 4), "27": ("hex27_conn_lin", 8, 8)}
 NUM = re.compile(r"[-+]?(?:\d+\.\d*|\.\d+|\d+)(?:[eE][-+]?\d+)?")
 
 
@@ -49,7 +55,7 @@ def main():
     src = open(os.path.join(REF, "src", "MGGeomEl.C")).read()
     out = {"source": "src/MGGeomEl.C (ELTYPE 27 blocks)"}
     for key, (decl, shape) in TABLES.items():
-        blk = re.sub(r"//[^\n]*", "", block_after(src, decl))
+        blk = re.sub(r"//[^\n]*", "", re.sub(r"/\*.*?\*/", "", block_after(src, decl), flags=re.S))
         vals = [float(v) for v in NUM.findall(blk)]
         n = 1
         for s in shape:
@@ -59,6 +65,18 @@ def main():
         if "surf_top" in key:
             vals = [int(v) for v in vals]
         out[key] = {"shape": shape, "data": vals}
+    mesh = open(os.path.join(REF, "src", "MGMesh.C")).read()
+    fn = mesh[mesh.index("void MGMesh::print_conn_lin_hf5"):]
+    for label, (key, nsub, ncorner) in CONN_LIN.items():
+        case = fn[re.search(r"case\s+%s\s*:" % label, fn).end():]
+        case = re.sub(r"//[^\n]*", "", case[:case.index("break;")])
+        tab = [[None] * ncorner for _ in range(nsub)]
+        for a, b, v in re.findall(r"conn\[(\d+)\]\[(\d+)\]\s*=\s*(\d+)", case):
+            tab[int(a)][int(b)] = int(v)
+        if any(v is None for r in tab for v in r):
+            raise ValueError(key)
+        out[key] = {"shape": (nsub, ncorner), "data": [v for r in tab for v in r]}
+    out["source"] += "; src/MGMesh.C (print_conn_lin_hf5)"
     with open(OUT, "w") as f:
         json.dump(out, f, separators=(",", ":"))
     print("wrote", OUT)
