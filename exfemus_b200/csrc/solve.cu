@@ -410,7 +410,9 @@ struct PlanarBlocks {
   const int *__restrict__ col;
   const T *__restrict__ v;
   long stride;
-  __device__ __forceinline__ void load(long k, int &c, T (&o)[NQ]) const {
+  template <int M>  // into the first NQ entries of o
+  __device__ __forceinline__ void load(long k, int &c, T (&o)[M]) const {
+    static_assert(M >= NQ, "block buffer too small");
     c = col[k];
 #pragma unroll
     for (int q = 0; q < NQ; q++) o[q] = v[(long)q * stride + k];
@@ -429,7 +431,9 @@ struct Packed16 {
   const int *__restrict__ col;
   const void *__restrict__ h;
   const uint2 *__restrict__ cx;
-  __device__ __forceinline__ void load(long k, int &c, float (&o)[D * D]) const {
+  template <int M>
+  __device__ __forceinline__ void load(long k, int &c, float (&o)[M]) const {
+    static_assert(M >= D * D, "block buffer too small");
     float2 f;
     if constexpr (D == 3) {
       const uint4 r = reinterpret_cast<const uint4 *>(h)[k];
@@ -454,26 +458,44 @@ struct Packed16 {
 // blocks per lane in flight: all columns and values of a chunk are loaded before the
 // first gather; the pressure couplings (at most LPR per row on these meshes) are loaded
 // up front with them.  rsc undoes a row scaling of the blocks on each lane's sum.
-template <class T, int D, int LPR, int UNR, bool I4, int RA, class BL>
-__device__ __forceinline__ void patch_row_dot(int lane, int N, int k0, int nk, int l0, int nl, const BL &bl,
-                                              const int *__restrict__ ql_col, long lstride,
-                                              const T *__restrict__ lv, const T *__restrict__ x, T acc[D],
-                                              const T (&rsc)[D]) {
-  int lc = -1;
-  T lw[RA];
+// patch_row_first loads what does not change during a sweep (the couplings and the
+// first chunk), so a kernel can issue it before waiting for the iterate;
+// patch_row_rest gathers, multiplies and walks the remaining chunks.  LW >= RA and
+// VW >= RA * D are the caller's buffer widths.
+template <class T, int D, int LPR, int UNR, int RA, class BL, int LW, int VW>
+__device__ __forceinline__ void patch_row_first(int lane, int k0, int nk, int l0, int nl, const BL &bl,
+                                                const int *__restrict__ ql_col, long lstride,
+                                                const T *__restrict__ lv, int &lc, T (&lw)[LW], int (&c)[UNR],
+                                                T (&v)[UNR][VW]) {
+  static_assert(LW >= RA && VW >= RA * D, "row buffers too small");
+  lc = -1;
   if (lane < nl) {
     lc = ql_col[l0 + lane];
 #pragma unroll
     for (int a = 0; a < RA; a++) lw[a] = lv[(long)a * lstride + l0 + lane];
   }
-  for (int base = 0; base < nk; base += UNR * LPR) {
-    int c[UNR];
-    T v[UNR][RA * D];
 #pragma unroll
-    for (int u = 0; u < UNR; u++) {
-      const int i = base + u * LPR + lane;
-      c[u] = -1;
-      if (i < nk) bl.load(k0 + i, c[u], v[u]);
+  for (int u = 0; u < UNR; u++) {
+    const int i = u * LPR + lane;
+    c[u] = -1;
+    if (i < nk) bl.load(k0 + i, c[u], v[u]);
+  }
+}
+
+template <class T, int D, int LPR, int UNR, bool I4, int RA, class BL, int LW, int VW>
+__device__ __forceinline__ void patch_row_rest(int lane, int N, int k0, int nk, int l0, int nl, const BL &bl,
+                                               const int *__restrict__ ql_col, long lstride,
+                                               const T *__restrict__ lv, const T *__restrict__ x, T acc[D],
+                                               const T (&rsc)[D], int lc, const T (&lw)[LW], int (&c)[UNR],
+                                               T (&v)[UNR][VW]) {
+  for (int base = 0; base < nk; base += UNR * LPR) {
+    if (base > 0) {
+#pragma unroll
+      for (int u = 0; u < UNR; u++) {
+        const int i = base + u * LPR + lane;
+        c[u] = -1;
+        if (i < nk) bl.load(k0 + i, c[u], v[u]);
+      }
     }
     T xb[UNR][D];
 #pragma unroll
@@ -513,6 +535,18 @@ __device__ __forceinline__ void patch_row_dot(int lane, int N, int k0, int nk, i
   }
 }
 
+template <class T, int D, int LPR, int UNR, bool I4, int RA, class BL>
+__device__ __forceinline__ void patch_row_dot(int lane, int N, int k0, int nk, int l0, int nl, const BL &bl,
+                                              const int *__restrict__ ql_col, long lstride,
+                                              const T *__restrict__ lv, const T *__restrict__ x, T acc[D],
+                                              const T (&rsc)[D]) {
+  int lc, c[UNR];
+  T lw[RA], v[UNR][RA * D];
+  patch_row_first<T, D, LPR, UNR, RA>(lane, k0, nk, l0, nl, bl, ql_col, lstride, lv, lc, lw, c, v);
+  patch_row_rest<T, D, LPR, UNR, I4, RA>(lane, N, k0, nk, l0, nl, bl, ql_col, lstride, lv, x, acc, rsc, lc, lw, c,
+                                         v);
+}
+
 // ROWS phase 1: residuals of the star rows (g < nrows) and of the patches' pressure
 // rows (g >= nrows), LPR lanes per row, written in patch order.  rinfo per star row:
 // {node, qq_ptr[node], ql_ptr[node], nqq | nql << 8 | tile index << 16}; pinfo per patch
@@ -528,43 +562,46 @@ __global__ void __launch_bounds__(NT, MINB)
   const long g = ((long)blockIdx.x * NT + threadIdx.x) / LPR;
   const bool vel = g < nrows;
   const bool prs = !vel && g < (long)nrows + npatch;
-  // the row descriptors do not change during a sweep: on the latency-bound levels
-  // (MINB 1) load them before the wait
+  // the row descriptors, scales, couplings and the first chunk of blocks do not change
+  // during a sweep (only kernels that complete before their dependents start write
+  // them): load them before waiting for the iterate
   int4 q0 = make_int4(0, 0, 0, 0), q1 = q0;
-  auto desc = [&]() {
-    if (vel) {
-      q0 = rinfo[g];
-    } else if (prs) {
-      q0 = pinfo[2 * (g - nrows)];
-      q1 = pinfo[2 * (g - nrows) + 1];
-    }
-  };
-  if constexpr (MINB == 1) desc();
+  if (vel) {
+    q0 = rinfo[g];
+  } else if (prs) {
+    q0 = pinfo[2 * (g - nrows)];
+    q1 = pinfo[2 * (g - nrows) + 1];
+  }
+  const PlanarBlocks<T, D> pb{qq_col, pv, nqqL};
+  int lc = -1, c[UNR];
+  T lw[D], v[UNR][D * D], sc[D];
+#pragma unroll
+  for (int u = 0; u < UNR; u++) c[u] = -1;
+  const int node = q0.x;
+  if (vel) {
+#pragma unroll
+    for (int a = 0; a < D; a++) sc[a] = VB::scaled ? vsc[(long)a * N + node] : T(1);
+    patch_row_first<T, D, LPR, UNR, D>(lane, q0.y, q0.w & 0xff, q0.z, (q0.w >> 8) & 0xff, vb, ql_col, nql, vp, lc,
+                                       lw, c, v);
+  } else if (prs) {
+    patch_row_first<T, D, LPR, UNR, 1>(lane, q0.z, q1.x, q0.w, q1.y, pb, ql_col, 0, pp, lc, lw, c, v);
+  }
   EXF_PDL_WAIT();
-  if constexpr (MINB != 1) desc();
   T acc[D], bv[D];
 #pragma unroll
   for (int a = 0; a < D; a++) acc[a] = bv[a] = T(0);
-  int node = 0;
   if (vel) {
-    const int4 ri = q0;
-    node = ri.x;
     if (lane == 0) {
 #pragma unroll
       for (int a = 0; a < D; a++) bv[a] = b[Lay<I4>::v(a, node, N)];
     }
-    T sc[D];
-#pragma unroll
-    for (int a = 0; a < D; a++) sc[a] = VB::scaled ? vsc[(long)a * N + node] : T(1);
-    patch_row_dot<T, D, LPR, UNR, I4, D>(lane, N, ri.y, ri.w & 0xff, ri.z, (ri.w >> 8) & 0xff, vb, ql_col, nql, vp,
-                                         x, acc, sc);
+    patch_row_rest<T, D, LPR, UNR, I4, D>(lane, N, q0.y, q0.w & 0xff, q0.z, (q0.w >> 8) & 0xff, vb, ql_col, nql, vp,
+                                          x, acc, sc, lc, lw, c, v);
   } else if (prs) {
-    const int4 pi = q0, pj = q1;
-    node = pi.x;
     if (lane == 0) bv[0] = b[Lay<I4>::p(node, N, D)];
     const T one[D] = {};
-    const PlanarBlocks<T, D> pb{qq_col, pv, nqqL};
-    patch_row_dot<T, D, LPR, UNR, I4, 1>(lane, N, pi.z, pj.x, pi.w, pj.y, pb, ql_col, 0, pp, x, acc, one);
+    patch_row_rest<T, D, LPR, UNR, I4, 1>(lane, N, q0.z, q1.x, q0.w, q1.y, pb, ql_col, 0, pp, x, acc, one, lc, lw, c,
+                                          v);
   }
 #pragma unroll
   for (int a = 0; a < D; a++)
