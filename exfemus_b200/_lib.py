@@ -27,6 +27,7 @@ BC_BOUSS_NS = 4
 BC_BOUSS_T = 5
 SMOOTH_GS = 0
 SMOOTH_VANKA = 1
+SMOOTH_GMRES_ILU = 2
 PREC_FP64 = 0
 PREC_MIXED = 1
 VANKA_AUTO = 0
@@ -140,6 +141,7 @@ SIGNATURES = [
     ("exf_prolong", _I, [_P, _I, _DP, _DP]),
     ("exf_smooth", _I, [_P, _I, C.POINTER(ExfMgParams), _I, _DP, _DP]),
     ("exf_coarse_solve", _I, [_P, _DP, _DP]),
+    ("exf_ilu_apply", _I, [_P, _I, _DP, _DP]),
     ("exf_sys_transpose", _I, [_P]),
     ("exf_adjoint_forward", _I, [_P, C.POINTER(ExfPhys), C.POINTER(ExfMgParams), C.POINTER(ExfSolveStats)]),
     ("exf_adjoint_backward", _I, [_P, C.POINTER(ExfPhys), C.POINTER(ExfMgParams), _DP, _DP, _DP,

@@ -99,6 +99,7 @@ int sync_fp32(exf_sys *s, int lev) {
   cp(L.A.pv, L.A32.pv);
   cp(L.A.pp, L.A32.pp);
   EXF_LAUNCH_CHECK();
+  L.ilu_ok = false;  // the matrix changed: refactor before the next GMRES + ILU call
   return vanka_prep(s, lev);
 }
 
@@ -217,8 +218,12 @@ static bool needs_acc(const exf_mg_params *p) { return p->cond_corr || p->stop_t
 // stationary iterations evaluate ||r||/||b|| on a residual refreshed only while
 // Iter < MaxIter (SORForwIter, contrib/laspack/itersolv.c:850-894; LastAcc,
 // contrib/laspack/rtc.c:48-70), i.e. the residual of the iterate before the last sweep.
+// GMRESIter reports the residual of its last test, taken after its last restart cycle.
 template <class T>
 static int smooth_acc(exf_sys *s, int lev, const exf_mg_params *p, int nsw, T *x, const T *b, T *r, double *slot) {
+  if constexpr (sizeof(T) == 8) {
+    if (p->smoother == EXF_SMOOTH_GMRES_ILU) return gmres_smooth(s, lev, p->eps, nsw, x, b, slot);
+  }
   if (!slot) return smooth<T>(s, lev, p, nsw, x, b);
   if (nsw > 0) EXF_TRY(smooth<T>(s, lev, p, nsw - 1, x, b));
   EXF_TRY(spmv_resid<T>(s, lev, x, b, r, slot));
@@ -1075,6 +1080,13 @@ int exf_mg_solve(exf_sys *s, const exf_mg_params *p, exf_solve_stats *st) {
   memset(st, 0, sizeof(*st));
   SysLevel &T = s->L[s->nlev - 1];
   double *dnb = s->red.out.p, *dnr = s->red.out.p + 1;
+  if (p->smoother == EXF_SMOOTH_GMRES_ILU) {
+    if (p->precision != EXF_PREC_FP64) {
+      set_error("GMRES + ILU smoothing runs in FP64 precision only");
+      return EXF_ERR_UNSUPPORTED;
+    }
+    for (int l = 1; l < s->nlev; l++) EXF_TRY(ilu_ready(s, l));  // ILUFactor once per assembly
+  }
   if (!s->coarse_ok) EXF_TRY(coarse_factor(s));
   EXF_CUDA(cudaEventRecord(s->ev0, s->stream));
   EXF_TRY(norm2(s, T.b.p, T.ndof, dnb));
@@ -1211,6 +1223,18 @@ int exf_smooth(exf_sys *s, int lev, const exf_mg_params *p, int nsweeps, double 
   return d2h(s, x, dx.p, L.ndof);
 }
 
+int exf_ilu_apply(exf_sys *s, int lev, const double *c, double *y) {
+  CHECK_LEV(s, lev);
+  if (!c || !y) return EXF_ERR_ARG;
+  SysLevel &L = s->L[lev];
+  DBuf<double> dc;
+  EXF_TRY(dc.alloc(L.ndof));
+  EXF_TRY(h2d(s, dc.p, c, L.ndof));
+  EXF_TRY(ilu_apply(s, lev, dc.p, dc.p));
+  EXF_TRY(device_wait_status(s));
+  return d2h(s, y, dc.p, L.ndof);
+}
+
 int exf_coarse_solve(exf_sys *s, const double *b, double *x) {
   CHECK_SYS(s);
   SysLevel &L = s->L[0];
@@ -1268,6 +1292,7 @@ int exf_time_op(exf_sys *s, int what, int lev, const exf_mg_params *p, const exf
         return f32 ? smooth<float>(s, lev, p, 1, L.x32.p, L.b32.p) : smooth<double>(s, lev, p, 1, L.x.p, L.b.p);
       case 2:
         EXF_TRY(assemble_all_levels(s, ph));  // the exf_assemble_all path
+        for (int l = 0; l < s->nlev; l++) s->L[l].ilu_ok = false;
         return EXF_OK;
       case 3: {
         SysLevel &T = s->L[s->nlev - 1];

@@ -232,6 +232,15 @@ struct SysLevel {
   // transfers: Pq/Pl from level-1 to this level (fine rows), Rq/Rl from this level+1
   Transfer Pq, Pl, Rq, Rl;
   DBuf<double> rmask;    // [ndof] restriction row mask (bc0 % 2 of the top DOF)
+  // GMRES + ILU level solver (scalar systems): the factor on the qq pattern and the
+  // inverse of its diagonal, per-row publication flags and {ticket, generation, zero
+  // pivot}; the Krylov vectors, two scratch vectors, the scalars and a control word
+  DBuf<double> ilu_f, ilu_inv;
+  DBuf<int> ilu_flag, ilu_ctl;
+  bool ilu_ok = false;
+  int ilu_maxl = 0;
+  DBuf<double> gm_V, gm_w, gm_t, gm_sc, gm_part;
+  DBuf<int> gm_ctl;
   // vectors
   DBuf<double> x, b, r, dx;     // dx: smoother scratch (Vanka star-row residuals)
   DBuf<float> x32, b32, r32, dx32;  // NS: node-interleaved float4 per node (4N floats)
@@ -381,6 +390,10 @@ template <class T>
 int smooth(exf_sys *s, int lev, const exf_mg_params *p, int nsweeps, T *x, const T *b);
 // EXF_ERR_CUDA (and clears the flag) when a bounded in-kernel wait ran out since the last call
 int device_wait_status(exf_sys *s);
+// GMRES + ILU level solver (ilu_gmres.cu)
+int ilu_ready(exf_sys *s, int lev);
+int ilu_apply(exf_sys *s, int lev, const double *c, double *y);
+int gmres_smooth(exf_sys *s, int lev, double eps, int m, double *x, const double *b, double *acc);
 // runs a bounded wait that nothing completes; returns the resulting device_wait_status
 int wait_probe(exf_sys *s);
 template <class T>

@@ -2094,6 +2094,14 @@ int device_wait_status(exf_sys *s) {
 
 template <class T>
 int smooth(exf_sys *s, int lev, const exf_mg_params *p, int nsweeps, T *x, const T *b) {
+  if (p->smoother == EXF_SMOOTH_GMRES_ILU) {  // one level-solver call of nsweeps iterations
+    if constexpr (sizeof(T) == 8) {
+      return gmres_smooth(s, lev, p->eps, nsweeps, x, b, nullptr);
+    } else {
+      set_error("GMRES + ILU smoothing runs in FP64 precision only");
+      return EXF_ERR_UNSUPPORTED;
+    }
+  }
   for (int it = 0; it < nsweeps; it++) {
     if (s->kind == EXF_KIND_T) {
       EXF_TRY(gs_sweep<T>(s, lev, p, x, b));

@@ -415,6 +415,13 @@ class MGSolBase:
         check(self.L.exf_smooth(self.h, lev, C.byref(params), nsweeps, dptr(x), dptr(b)))
         return x
 
+    def ilu_apply(self, lev, c):
+        """ILUPrecond of level lev: (D + U)^-1 D (D + L)^-1 c with LASPACK's ILU(0) factor."""
+        c = np.ascontiguousarray(c, np.float64)
+        y = np.zeros(self.ndof(lev))
+        check(self.L.exf_ilu_apply(self.h, lev, dptr(c), dptr(y)))
+        return y
+
     def coarse_solve(self, b):
         x = np.zeros(self.ndof(0))
         b = np.ascontiguousarray(b, np.float64)

@@ -57,6 +57,8 @@ extern "C" {
 /* smoothers */
 #define EXF_SMOOTH_GS 0          /* multi-colour Gauss-Seidel (scalar systems)      */
 #define EXF_SMOOTH_VANKA 1       /* multi-colour pressure-node Vanka (NS)           */
+#define EXF_SMOOTH_GMRES_ILU 2   /* GMRES(30) + ILU, the reference's default level    */
+                                 /* solver (scalar systems, FP64 precision)          */
 
 /* precision of the V-cycle */
 #define EXF_PREC_FP64 0          /* everything FP64                                 */
@@ -342,6 +344,9 @@ EXF_API int exf_restrict(exf_sys *s, int lev, const double *r_fine, double *b_co
 EXF_API int exf_prolong(exf_sys *s, int lev, const double *x_coarse, double *y_fine);  /* lev = fine   */
 EXF_API int exf_smooth(exf_sys *s, int lev, const exf_mg_params *p, int nsweeps, double *x, const double *b);
 EXF_API int exf_coarse_solve(exf_sys *s, const double *b, double *x);
+/* y = ILUPrecond(c) of level lev (LASPACK's ILU(0) of the level matrix, factored once per
+ * assembly; contrib/laspack/precond.c:75-110, factor.c:25-320), y may be c; scalar systems */
+EXF_API int exf_ilu_apply(exf_sys *s, int lev, const double *c, double *y);
 EXF_API int exf_sys_transpose(exf_sys *s);                      /* A[L] <- A[L]^T, all levels */
 
 /* --- discrete adjoint of the T solve (LinearSolverM::adjoint_solve semantics) ------------

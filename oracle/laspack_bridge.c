@@ -122,3 +122,19 @@ int lpb_sorforw(int n, const int *ptr, const int *col, const double *val, const 
   Q_Destr(&A);
   return rc;
 }
+
+/* y = ILUPrecond(c) (precond.c:75-110) with the ILU(0) factor of A (factor.c:25-320) */
+int lpb_ilu_apply(int n, const int *ptr, const int *col, const double *val, const double *c, double *y) {
+  QMatrix A;
+  QVector C, Y;
+  fill_q(&A, n, ptr, col, val);
+  fill_v(&C, "c", n, c);
+  fill_v(&Y, "y", n, NULL);
+  ILUPrecond(&A, &Y, &C, 1.);
+  get_v(&Y, n, y);
+  int rc = LASResult() == LASOK ? 0 : 1;
+  V_Destr(&C);
+  V_Destr(&Y);
+  Q_Destr(&A);
+  return rc;
+}

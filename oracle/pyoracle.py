@@ -303,6 +303,7 @@ class Laspack:
             L.lpb_sorforw.argtypes = [I, ip, ip, dp, dp, dp, I, C.c_double, C.POINTER(C.c_double)]
             L.lpb_gmres_pc.argtypes = [I, ip, ip, dp, dp, dp, C.c_double, I, I, I, I, C.POINTER(I),
                                        C.POINTER(C.c_double)]
+            L.lpb_ilu_apply.argtypes = [I, ip, ip, dp, dp, dp]
             _LP = L
         self.L = _LP
 
@@ -326,6 +327,14 @@ class Laspack:
         self.L.lpb_gmres_pc(n, rp, col, val, np.ascontiguousarray(b, np.float64), x, tol, maxit, restart,
                             1 if transpose else 0, 1 if ilu else 0, C.byref(it), C.byref(acc))
         return x, it.value, acc.value
+
+    def ilu_apply(self, rp, col, val, c):
+        """ILUPrecond(c): (D + U)^-1 D (D + L)^-1 c with LASPACK's ILU(0) factor of A."""
+        y = np.zeros(len(rp) - 1)
+        rc = self.L.lpb_ilu_apply(len(rp) - 1, rp, col, val, np.ascontiguousarray(c, np.float64), y)
+        if rc:
+            raise RuntimeError("LASPACK ILUPrecond failed")
+        return y
 
     def sorforw(self, rp, col, val, b, x0, nsweeps, omega=1.0):
         x = np.array(x0, np.float64)
