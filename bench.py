@@ -327,6 +327,22 @@ def run_workloads(args, local):
     from exfemus_b200 import _lib, workloads
     L = ex.load()
 
+    def gmres_line(name, t, top, gs=None):
+        """The scalar system t solved from zero with GMRES(30) + ILU smoothing (2 / 2), with
+        the ILU factorisation, one ILUPrecond and one smoother iteration of the top level."""
+        p = ex.mg_params(eps=1e-10, max_cycles=200, smoother=_lib.SMOOTH_GMRES_ILU, nu_pre=2, nu_post=2)
+        t.set_x(np.zeros(t.ntop_dof))
+        st = t.solve(p)
+        tv = C.c_double()
+        out = {"workload": name, "smoother": "gmres30+ilu 2/2", "ndof": t.ntop_dof, "cycles": st.cycles,
+               "rel_res": st.rel_res, "solve_s": st.seconds}
+        for what, key in ((7, "ilu_factor_ms"), (8, "ilu_apply_ms"), (1, "gmres_iteration_ms")):
+            _lib.check(L.exf_time_op(t.h, what, top, C.byref(p), C.byref(t.phys), 3, C.byref(tv)))
+            out[key] = tv.value
+        if gs is not None:
+            out["gs_cycles"], out["gs_solve_s"] = gs
+        print(json.dumps(out), flush=True)
+
     def picard_run(name, precision):
         case = ex.make_case(name, device=local)
         t0 = time.perf_counter()
@@ -348,6 +364,7 @@ def run_workloads(args, local):
     st = t.solve(case["mg_T"])
     print(json.dumps({"workload": "heat2d", "ndof": t.ntop_dof, "cycles": st.cycles, "rel_res": st.rel_res,
                       "solve_s": st.seconds}), flush=True)
+    gmres_line("heat2d", t, case["w"]["nlev"] - 1)
     for name in ("cavity2d", "channel3d"):
         for prec in (_lib.PREC_FP64, _lib.PREC_MIXED):
             _, out = picard_run(name, prec)
@@ -355,6 +372,13 @@ def run_workloads(args, local):
     for prec in (_lib.PREC_FP64, _lib.PREC_MIXED):
         case, out = picard_run("bouss2d", prec)
         print(json.dumps(out), flush=True)
+    # the Boussinesq temperature system at full size with the reference's default level
+    # solver (GMRES + ILU) against its Gauss-Seidel multigrid, same system, from zero
+    tb = case["T"]
+    tb.assemble_all()
+    tb.set_x(np.zeros(tb.ntop_dof))
+    stg = tb.solve(ex.mg_params(eps=1e-10, max_cycles=200, smoother=_lib.SMOOTH_GS, nu_pre=2, nu_post=2))
+    gmres_line("bouss2d_T", tb, case["w"]["nlev"] - 1, gs=(stg.cycles, stg.seconds))
 
     # adjoint2d on the converged Boussinesq velocity (mixed run above): T system with
     # lognormal per-element sources and 64 Legendre modes of left-wall data

@@ -1309,6 +1309,11 @@ int exf_time_op(exf_sys *s, int what, int lev, const exf_mg_params *p, const exf
         k_fma_probe<<<4 * s->nsm, 256, 0, s->stream>>>(1e-3);
         EXF_LAUNCH_CHECK();
         return EXF_OK;
+      case 7:
+        L.ilu_ok = false;
+        return ilu_ready(s, lev);
+      case 8:
+        return ilu_apply(s, lev, L.r.p, L.r.p);
       default:
         set_error("exf_time_op: unknown operation %d", what);
         return EXF_ERR_ARG;

@@ -370,6 +370,8 @@ EXF_API int exf_adjoint_backward(exf_sys *s, const exf_phys *ph, const exf_mg_pa
  *     nothing completes; returns EXF_ERR_CUDA with the run-out message, the status every
  *     bounded in-kernel wait (the BULK smoother's stage barriers) reports, and leaves the
  *     context usable;
+ * 7 = ILU factorisation of level lev (scalar systems; the GMRES + ILU level solver pays it
+ *     once per assembly), 8 = one ILUPrecond application on level lev (in place on r);
  * avg_ms = average duration per launch group over reps, precision per exf_mg_params */
 EXF_API int exf_time_op(exf_sys *s, int what, int lev, const exf_mg_params *p, const exf_phys *ph, int reps,
                 double *avg_ms);

@@ -128,8 +128,9 @@ def test_graph_cache_eviction_keeps_results(gpu_lib):
 
 
 def test_timing_probes_and_refactorisation(heat):
-    """exf_time_op 4 (coarse refactorisation) and 5 (FP64 FMA probe) run on an assembled
-    system; a solve after a refactorisation gives the same bits as before it."""
+    """exf_time_op 4 (coarse refactorisation), 5 (FP64 FMA probe), 7 and 8 (ILU factor and
+    application) run on an assembled system; a solve after them gives the same bits as
+    before."""
     L = _lib.load()
     heat.assemble_all()
     p = ex.mg_params(precision=_lib.PREC_MIXED)
@@ -137,8 +138,8 @@ def test_timing_probes_and_refactorisation(heat):
     heat.solve(p)
     x0 = heat.x()
     tv = C.c_double()
-    for what in (4, 5):
-        _lib.check(L.exf_time_op(heat.h, what, 0, C.byref(p), C.byref(heat.phys), 2, C.byref(tv)))
+    for what, lev in ((4, 0), (5, 0), (7, 2), (8, 2)):  # 7, 8: ILU factorisation and application
+        _lib.check(L.exf_time_op(heat.h, what, lev, C.byref(p), C.byref(heat.phys), 2, C.byref(tv)))
         assert tv.value > 0.0
     heat.set_x(np.zeros(heat.ntop_dof))
     heat.solve(p)
