@@ -237,8 +237,9 @@ struct SysLevel {
   // pivot}; the Krylov vectors, two scratch vectors, the scalars and a control word
   DBuf<double> ilu_f, ilu_inv;
   DBuf<int> ilu_flag, ilu_ctl;
+  DBuf<int> ilu_ord_lo, ilu_ord_up;  // rows by dependency level of the lower / upper solve
   bool ilu_ok = false;
-  int ilu_maxl = 0;
+  int ilu_maxl = 0, ilu_depth[2] = {0, 0};
   DBuf<double> gm_V, gm_w, gm_t, gm_sc, gm_part;
   DBuf<int> gm_ctl;
   // vectors

@@ -15,13 +15,13 @@
 // preconditioner give the reference's bits.
 //
 // The row recurrences run sync-free: a warp takes the next row from a ticket counter
-// (rows in order, descending for the upper solve), waits until the rows it depends on
-// carry the current generation in their flag (bounded, acquire loads), computes, and
-// publishes its row (release store).  A warp only waits on rows with earlier tickets,
-// which running warps hold, so the recurrences always progress; a wait that runs out
-// sets the system's wait flag, which the host reports as EXF_ERR_CUDA.  Time is set by
-// the dependency depth of the ordering (the level-nested numbering: about 770 steps for
-// the 257 x 257 nodes of a 128 x 128 quad9 level), not by bandwidth.
+// (rows by dependency level, see level_order), waits until the rows it depends on carry
+// the current generation in their flag (bounded, acquire loads), computes, and publishes
+// its row (release store).  A warp only waits on rows with earlier tickets, which running
+// warps hold, so the recurrences always progress; a wait that runs out sets the system's
+// wait flag, which the host reports as EXF_ERR_CUDA.  Time is set by the dependency depth
+// of the numbering (the level-nested numbering: about 770 levels for the 257 x 257 nodes
+// of a 128 x 128 quad9 level), not by bandwidth.
 //
 // GMRES (contrib/laspack/itersolv.c:1341-1510): MaxIter = the smoothing count, modified
 // Gram-Schmidt, Givens rotations, the reference's relative-residual test (rtc.c:48-70)
@@ -30,8 +30,10 @@
 // graph can hold.  Vector updates use the reference's rounding (a product, then a sum);
 // inner products and norms are parallel reductions, so GMRES iterates agree with the
 // reference's to rounding, not bitwise.
+#include <algorithm>
 #include <cfloat>
 #include <cmath>
+#include <vector>
 
 #include "exf_internal.h"
 
@@ -90,9 +92,9 @@ __global__ void k_ilu_arm(int *ctl, const int *skip) {
 // one warp per row; MAXL >= the longest lower row + 1; f holds a copy of the matrix on
 // entry and the factor on exit; invd[i] = 1 / the factor's diagonal
 template <int MAXL, int NW>
-__global__ void __launch_bounds__(32 * NW) k_ilu_factor(int N, const int *__restrict__ ptr, const int *__restrict__ col,
-                                                   const int *__restrict__ dpos, double *f, double *invd, int *flag,
-                                                   int *ctl, int *err) {
+__global__ void __launch_bounds__(32 * NW) k_ilu_factor(int N, const int *__restrict__ ord, const int *__restrict__ ptr,
+                                                        const int *__restrict__ col, const int *__restrict__ dpos,
+                                                        double *f, double *invd, int *flag, int *ctl, int *err) {
   constexpr int KU = (MAXL + 31) / 32;
   extern __shared__ double ilu_smem[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -101,10 +103,11 @@ __global__ void __launch_bounds__(32 * NW) k_ilu_factor(int N, const int *__rest
   const int gen = ctl[1];
   auto Lat = [&](int a, int b) -> double & { return Lm[a * (MAXL + 1) + b]; };
   for (;;) {
-    int i = 0;
-    if (lane == 0) i = atomicAdd(ctl, 1);
-    i = __shfl_sync(0xffffffffu, i, 0);
-    if (i >= N) return;
+    int t = 0;
+    if (lane == 0) t = atomicAdd(ctl, 1);
+    t = __shfl_sync(0xffffffffu, t, 0);
+    if (t >= N) return;
+    const int i = ord[t];
     const int k0 = ptr[i], kd = dpos[i], LD = kd - k0 + 1;
     if (LD > MAXL) {  // the host sizes MAXL from the pattern: not reached
       if (lane == 0) atomicExch(err, 1);
@@ -181,7 +184,8 @@ __global__ void __launch_bounds__(32 * NW) k_ilu_factor(int N, const int *__rest
 
 // w = (D + L)^-1 c: Sum = 0, Sum -= l_ik w_k over the row's lower entries in column
 // order, Sum += c_i, w_i = Sum / d_i (as the product with the stored inverse)
-__global__ void __launch_bounds__(128) k_ilu_lower(int N, const int *__restrict__ ptr, const int *__restrict__ col,
+__global__ void __launch_bounds__(128) k_ilu_lower(int N, const int *__restrict__ ord, const int *__restrict__ ptr,
+                                                   const int *__restrict__ col,
                                                    const int *__restrict__ dpos, const double *__restrict__ f,
                                                    const double *__restrict__ invd, const double *c, double *w,
                                                    int *flag, int *ctl, int *err, const int *skip) {
@@ -189,10 +193,11 @@ __global__ void __launch_bounds__(128) k_ilu_lower(int N, const int *__restrict_
   const int lane = threadIdx.x & 31;
   const int gen = ctl[1];
   for (;;) {
-    int i = 0;
-    if (lane == 0) i = atomicAdd(ctl, 1);
-    i = __shfl_sync(0xffffffffu, i, 0);
-    if (i >= N) return;
+    int t = 0;
+    if (lane == 0) t = atomicAdd(ctl, 1);
+    t = __shfl_sync(0xffffffffu, t, 0);
+    if (t >= N) return;
+    const int i = ord[t];
     const int k0 = ptr[i], nl = dpos[i] - k0;
     double s = 0.;
     for (int base = 0; base < nl; base += 32) {
@@ -208,15 +213,15 @@ __global__ void __launch_bounds__(128) k_ilu_lower(int N, const int *__restrict_
     s = __dadd_rn(s, c[i]);
     if (lane == 0) {
       w[i] = __dmul_rn(s, invd[i]);
-      __threadfence();
-      st_rel(flag + i, gen);
+      st_rel(flag + i, gen);  // the release orders the value before the flag
     }
   }
 }
 
-// y = (D + U)^-1 (D w): rows from the last, Sum -= u_ik y_k over the upper entries from
-// the row's end, Sum += d_i w_i, y_i = Sum / d_i
-__global__ void __launch_bounds__(128) k_ilu_upper(int N, const int *__restrict__ ptr, const int *__restrict__ col,
+// y = (D + U)^-1 (D w): Sum -= u_ik y_k over the upper entries from the row's end,
+// Sum += d_i w_i, y_i = Sum / d_i (rows by level of the upper entries)
+__global__ void __launch_bounds__(128) k_ilu_upper(int N, const int *__restrict__ ord, const int *__restrict__ ptr,
+                                                   const int *__restrict__ col,
                                                    const int *__restrict__ dpos, const double *__restrict__ f,
                                                    const double *__restrict__ invd, const double *w, double *y,
                                                    int *flag, int *ctl, int *err, const int *skip) {
@@ -228,7 +233,7 @@ __global__ void __launch_bounds__(128) k_ilu_upper(int N, const int *__restrict_
     if (lane == 0) t0 = atomicAdd(ctl, 1);
     t0 = __shfl_sync(0xffffffffu, t0, 0);
     if (t0 >= N) return;
-    const int i = N - 1 - t0;
+    const int i = ord[t0];
     const int kd = dpos[i], k1 = ptr[i + 1], nu = k1 - 1 - kd;
     double s = 0.;
     for (int base = 0; base < nu; base += 32) {
@@ -245,7 +250,6 @@ __global__ void __launch_bounds__(128) k_ilu_upper(int N, const int *__restrict_
     s = __dadd_rn(s, __dadd_rn(0., __dmul_rn(f[kd], w[i])));  // Mul_QV of the diagonal: 0 + d_i w_i
     if (lane == 0) {
       y[i] = __dmul_rn(s, invd[i]);
-      __threadfence();
       st_rel(flag + i, gen);
     }
   }
@@ -382,10 +386,10 @@ static int ilu_apply_dev(exf_sys *s, int lev, const double *c, double *y, const 
   SysLevel &L = s->L[lev];
   const int N = L.N, G = ilu_grid(s);
   k_ilu_arm<<<1, 1, 0, s->stream>>>(L.ilu_ctl.p, skip);
-  k_ilu_lower<<<G, 128, 0, s->stream>>>(N, L.qq_ptr.p, L.qq_col.p, L.diag_pos.p, L.ilu_f.p, L.ilu_inv.p, c,
+  k_ilu_lower<<<G, 128, 0, s->stream>>>(N, L.ilu_ord_lo.p, L.qq_ptr.p, L.qq_col.p, L.diag_pos.p, L.ilu_f.p, L.ilu_inv.p, c,
                                         L.gm_w.p, L.ilu_flag.p, L.ilu_ctl.p, s->wait_flag.p, skip);
   k_ilu_arm<<<1, 1, 0, s->stream>>>(L.ilu_ctl.p, skip);
-  k_ilu_upper<<<G, 128, 0, s->stream>>>(N, L.qq_ptr.p, L.qq_col.p, L.diag_pos.p, L.ilu_f.p, L.ilu_inv.p, L.gm_w.p,
+  k_ilu_upper<<<G, 128, 0, s->stream>>>(N, L.ilu_ord_up.p, L.qq_ptr.p, L.qq_col.p, L.diag_pos.p, L.ilu_f.p, L.ilu_inv.p, L.gm_w.p,
                                         y, L.ilu_flag.p, L.ilu_ctl.p, s->wait_flag.p, skip);
   EXF_COUNT(4);
   EXF_LAUNCH_CHECK();
@@ -398,11 +402,38 @@ static int launch_factor(exf_sys *s, SysLevel &L) {
   auto kern = k_ilu_factor<MAXL, NW>;
   EXF_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   k_ilu_arm<<<1, 1, 0, s->stream>>>(L.ilu_ctl.p, nullptr);
-  kern<<<s->nsm * 4, 32 * NW, smem, s->stream>>>(L.N, L.qq_ptr.p, L.qq_col.p, L.diag_pos.p, L.ilu_f.p, L.ilu_inv.p,
+  kern<<<s->nsm * 4, 32 * NW, smem, s->stream>>>(L.N, L.ilu_ord_lo.p, L.qq_ptr.p, L.qq_col.p, L.diag_pos.p, L.ilu_f.p, L.ilu_inv.p,
                                                    L.ilu_flag.p, L.ilu_ctl.p, s->wait_flag.p);
   EXF_COUNT(2);
   EXF_LAUNCH_CHECK();
   return EXF_OK;
+}
+
+// The rows in the order their tickets hand them out: by dependency level (the longest
+// chain of lower, or upper, entries leading to the row), index order within a level.
+// Every row depends only on rows of earlier levels, so a warp still waits only on earlier
+// tickets, and the rows of a level run together instead of one index after the other
+// (consecutive rows of the level-nested numbering mostly depend on each other).
+// Returns the number of levels.
+static int level_order(const std::vector<int> &ptr, const std::vector<int> &col, const std::vector<int> &dp,
+                       bool upper, std::vector<int> &ord) {
+  const int N = (int)dp.size();
+  std::vector<int> lv(N, 0);
+  int nl = 0;
+  for (int q = 0; q < N; q++) {
+    const int i = upper ? N - 1 - q : q;
+    int l = 0;
+    const int a = upper ? dp[i] + 1 : ptr[i], e = upper ? ptr[i + 1] : dp[i];
+    for (int k = a; k < e; k++) l = std::max(l, lv[col[k]] + 1);
+    lv[i] = l;
+    nl = std::max(nl, l + 1);
+  }
+  std::vector<int> cnt(nl + 1, 0);
+  for (int i = 0; i < N; i++) cnt[lv[i] + 1]++;
+  for (int l = 0; l < nl; l++) cnt[l + 1] += cnt[l];
+  ord.assign(N, 0);
+  for (int i = 0; i < N; i++) ord[cnt[lv[i]]++] = i;
+  return nl;
 }
 
 // ILUFactor of level lev's matrix, once per assembly (outside graph capture)
@@ -421,14 +452,24 @@ int ilu_ready(exf_sys *s, int lev) {
     return EXF_ERR_STATE;
   }
   const int N = L.N;
-  if (L.ilu_maxl == 0) {  // longest lower row + diagonal, from the pattern (fixed per system)
-    std::vector<int> ptr(N + 1), dp(N);
+  if (L.ilu_maxl == 0) {  // from the pattern, fixed per system
+    std::vector<int> ptr(N + 1), dp(N), col(L.nqq);
     EXF_CUDA(cudaMemcpyAsync(ptr.data(), L.qq_ptr.p, (N + 1) * sizeof(int), cudaMemcpyDeviceToHost, s->stream));
     EXF_CUDA(cudaMemcpyAsync(dp.data(), L.diag_pos.p, N * sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+    EXF_CUDA(cudaMemcpyAsync(col.data(), L.qq_col.p, L.nqq * sizeof(int), cudaMemcpyDeviceToHost, s->stream));
     EXF_CUDA(cudaStreamSynchronize(s->stream));
     int m = 1;
     for (int i = 0; i < N; i++) m = std::max(m, dp[i] - ptr[i] + 1);
+    std::vector<int> lo, up;
+    L.ilu_depth[0] = level_order(ptr, col, dp, false, lo);
+    L.ilu_depth[1] = level_order(ptr, col, dp, true, up);
+    EXF_TRY(L.ilu_ord_lo.alloc(N));
+    EXF_TRY(L.ilu_ord_up.alloc(N));
+    EXF_CUDA(cudaMemcpyAsync(L.ilu_ord_lo.p, lo.data(), N * sizeof(int), cudaMemcpyHostToDevice, s->stream));
+    EXF_CUDA(cudaMemcpyAsync(L.ilu_ord_up.p, up.data(), N * sizeof(int), cudaMemcpyHostToDevice, s->stream));
+    EXF_CUDA(cudaStreamSynchronize(s->stream));
     L.ilu_maxl = m;
+    s->buf_epoch++;
   }
   if (L.ilu_maxl > 128) {
     set_error("ILU: a row of level %d has %d entries left of the diagonal (at most 127 supported)", lev,
