@@ -15,9 +15,10 @@
 // preconditioner give the reference's bits.
 //
 // The row recurrences run sync-free: a warp takes the next row from a ticket counter
-// (rows by dependency level, see level_order), waits until the rows it depends on carry
-// the current generation in their flag (bounded, acquire loads), computes, and publishes
-// its row (release store).  A warp only waits on rows with earlier tickets, which running
+// (rows by dependency level, see level_order), waits until the rows it depends on are
+// published (bounded acquire loads: of a generation flag per row in the factorisation, of
+// the value itself in the triangular solves), computes, and publishes its row (release
+// store).  A warp only waits on rows with earlier tickets, which running
 // warps hold, so the recurrences always progress; a wait that runs out sets the system's
 // wait flag, which the host reports as EXF_ERR_CUDA.  Time is set by the dependency depth
 // of the numbering (the level-nested numbering: about 770 levels for the 257 x 257 nodes
@@ -46,6 +47,31 @@ __device__ __forceinline__ int ld_acq(const int *p) {
 }
 __device__ __forceinline__ void st_rel(int *p, int v) {
   asm volatile("st.release.gpu.global.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// the triangular solves publish each row's value itself: the output vector is filled with
+// this NaN pattern (which arithmetic does not produce) first, and a row's value replaces it
+// with a release store
+constexpr unsigned long long kNotReady = 0x7FF4C0FFEE000001ull;
+__device__ __forceinline__ double ld_acq_f64(const double *p) {
+  unsigned long long v;
+  asm volatile("ld.acquire.gpu.global.b64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return __longlong_as_double((long long)v);
+}
+__device__ __forceinline__ void st_rel_f64(double *p, double v) {
+  asm volatile("st.release.gpu.global.b64 [%0], %1;" ::"l"(p), "l"((unsigned long long)__double_as_longlong(v))
+               : "memory");
+}
+// bounded wait for the published value of row j (0 if the wait ran out; the flag is set)
+__device__ __forceinline__ double wait_val(const double *v, int j, int *err) {
+  for (int t = 0; t < (1 << 20); t++) {
+    const double x = ld_acq_f64(v + j);
+    if ((unsigned long long)__double_as_longlong(x) != kNotReady) return x;
+    if ((t & 255) == 255 && *(volatile int *)err) return 0.;
+    __nanosleep(32);
+  }
+  atomicExch(err, 1);
+  return 0.;
 }
 
 // bounded wait until row j is published in generation gen; false if it ran out (or an
@@ -82,11 +108,18 @@ __device__ __forceinline__ double pick(const double (&a)[KU], int u) {
   return v;
 }
 
-// ctl[0]: ticket, ctl[1]: generation, ctl[2]: zero-pivot row + 1 (factorisation)
+// ctl[0]: ticket, ctl[1]: generation (factorisation), ctl[2]: zero-pivot row + 1
 __global__ void k_ilu_arm(int *ctl, const int *skip) {
   if (skip && *skip) return;
   ctl[0] = 0;
   ctl[1] += 1;
+}
+// before a triangular solve: the output marked unpublished, the ticket reset
+__global__ void k_ilu_prep(double *v, long n, int *ctl, const int *skip) {
+  if (skip && *skip) return;
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i == 0) ctl[0] = 0;
+  if (i < n) v[i] = __longlong_as_double((long long)kNotReady);
 }
 
 // one warp per row; MAXL >= the longest lower row + 1; f holds a copy of the matrix on
@@ -99,7 +132,10 @@ __global__ void __launch_bounds__(32 * NW) k_ilu_factor(int N, const int *__rest
   extern __shared__ double ilu_smem[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   double *Lm = ilu_smem + (size_t)warp * MAXL * (MAXL + 1);
-  int *Sc = reinterpret_cast<int *>(ilu_smem + (size_t)NW * MAXL * (MAXL + 1)) + warp * MAXL;
+  // per warp: S, each S row's first entry and entry count, the offsets of the rows'
+  // entries in the flattened gather, and the position of column i in each S row
+  int *Sc = reinterpret_cast<int *>(ilu_smem + (size_t)NW * MAXL * (MAXL + 1)) + warp * 5 * MAXL;
+  int *Rb = Sc + MAXL, *Off = Rb + MAXL, *Pi = Off + MAXL + 1;  // Off holds MAXL + 1 entries
   const int gen = ctl[1];
   auto Lat = [&](int a, int b) -> double & { return Lm[a * (MAXL + 1) + b]; };
   for (;;) {
@@ -114,20 +150,49 @@ __global__ void __launch_bounds__(32 * NW) k_ilu_factor(int N, const int *__rest
       if (lane == 0) st_rel(flag + i, gen);
       continue;
     }
-    for (int a = lane; a < LD; a += 32) Sc[a] = col[k0 + a];
+    for (int a = lane; a < LD; a += 32) {
+      const int r = col[k0 + a];
+      Sc[a] = r;
+      Rb[a] = ptr[r];
+      Off[a + 1] = ptr[r + 1] - Rb[a];  // the row's entry count, summed below
+      Pi[a] = -1;
+    }
     for (int a = lane; a < LD - 1; a += 32) wait_row(flag, Sc[a], gen, err);
-    __syncwarp();
     for (int t = lane; t < LD * (MAXL + 1); t += 32) Lm[t] = 0.;
     __syncwarp();
-    // the entries (S_a, S_b) of the rows in S, columns <= i
-    for (int a = lane; a < LD; a += 32) {
-      const int r = Sc[a];
-      for (int k = ptr[r]; k < ptr[r + 1]; k++) {
-        const int c = col[k];
-        if (c > i) break;
-        const int b = bsearch_i(Sc, LD, c);
-        if (b >= 0) Lat(a, b) = f[k];
+    if (lane == 0) {
+      Off[0] = 0;
+      for (int a = 0; a < LD; a++) Off[a + 1] += Off[a];
+    }
+    __syncwarp();
+    // the entries (S_a, S_b) of the rows in S, columns <= i, gathered by all lanes over the
+    // rows' concatenated entries, four entries per lane in flight
+    const int T = Off[LD];
+    for (int e0 = 0; e0 < T; e0 += 128) {
+      int kk[4], cc[4], aa[4];
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        const int e = e0 + 32 * q + lane;
+        kk[q] = -1;
+        if (e < T) {
+          int lo = 0, hi = LD - 1;  // the row a with Off[a] <= e < Off[a + 1]
+          while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (Off[mid] <= e) lo = mid;
+            else hi = mid - 1;
+          }
+          aa[q] = lo;
+          kk[q] = Rb[lo] + (e - Off[lo]);
+          cc[q] = col[kk[q]];
+        }
       }
+#pragma unroll
+      for (int q = 0; q < 4; q++)
+        if (kk[q] >= 0 && cc[q] <= i) {
+          const int b = bsearch_i(Sc, LD, cc[q]);
+          if (b >= 0) Lat(aa[q], b) = f[kk[q]];
+          if (cc[q] == i) Pi[aa[q]] = kk[q];
+        }
     }
     __syncwarp();
     const int last = LD - 1;
@@ -166,10 +231,8 @@ __global__ void __launch_bounds__(32 * NW) k_ilu_factor(int N, const int *__rest
       const int k = lane + 32 * u;
       if (k < last) {
         f[k0 + k] = lk[u];
-        const int r = Sc[k];  // entry (S_k, i) of the earlier row S_k
-        const int p = bsearch_i(col + ptr[r], ptr[r + 1] - ptr[r], i);
-        if (p >= 0) f[ptr[r] + p] = uk[u];
-        else atomicExch(err, 1);  // LASILUStructErr: the pattern is symmetric here
+        if (Pi[k] >= 0) f[Pi[k]] = uk[u];  // entry (S_k, i) of the earlier row S_k
+        else atomicExch(err, 1);           // LASILUStructErr: the pattern is symmetric here
       }
     }
     if (lane == 0) {
@@ -188,10 +251,9 @@ __global__ void __launch_bounds__(128) k_ilu_lower(int N, const int *__restrict_
                                                    const int *__restrict__ col,
                                                    const int *__restrict__ dpos, const double *__restrict__ f,
                                                    const double *__restrict__ invd, const double *c, double *w,
-                                                   int *flag, int *ctl, int *err, const int *skip) {
+                                                   int *ctl, int *err, const int *skip) {
   if (skip && *skip) return;
   const int lane = threadIdx.x & 31;
-  const int gen = ctl[1];
   for (;;) {
     int t = 0;
     if (lane == 0) t = atomicAdd(ctl, 1);
@@ -199,22 +261,20 @@ __global__ void __launch_bounds__(128) k_ilu_lower(int N, const int *__restrict_
     if (t >= N) return;
     const int i = ord[t];
     const int k0 = ptr[i], nl = dpos[i] - k0;
+    const double ci = c[i], di = invd[i];  // loaded before the waits, off the critical path
     double s = 0.;
     for (int base = 0; base < nl; base += 32) {
       double p = 0.;
       if (base + lane < nl) {
-        const int j = col[k0 + base + lane];
-        wait_row(flag, j, gen, err);
-        p = __dmul_rn(f[k0 + base + lane], w[j]);
+        const int k = k0 + base + lane;
+        const double fk = f[k];
+        p = __dmul_rn(fk, wait_val(w, col[k], err));
       }
       const int n = min(32, nl - base);
       for (int t = 0; t < n; t++) s = __dsub_rn(s, __shfl_sync(0xffffffffu, p, t));
     }
-    s = __dadd_rn(s, c[i]);
-    if (lane == 0) {
-      w[i] = __dmul_rn(s, invd[i]);
-      st_rel(flag + i, gen);  // the release orders the value before the flag
-    }
+    s = __dadd_rn(s, ci);
+    if (lane == 0) st_rel_f64(w + i, __dmul_rn(s, di));
   }
 }
 
@@ -224,10 +284,9 @@ __global__ void __launch_bounds__(128) k_ilu_upper(int N, const int *__restrict_
                                                    const int *__restrict__ col,
                                                    const int *__restrict__ dpos, const double *__restrict__ f,
                                                    const double *__restrict__ invd, const double *w, double *y,
-                                                   int *flag, int *ctl, int *err, const int *skip) {
+                                                   int *ctl, int *err, const int *skip) {
   if (skip && *skip) return;
   const int lane = threadIdx.x & 31;
-  const int gen = ctl[1];
   for (;;) {
     int t0 = 0;
     if (lane == 0) t0 = atomicAdd(ctl, 1);
@@ -235,23 +294,20 @@ __global__ void __launch_bounds__(128) k_ilu_upper(int N, const int *__restrict_
     if (t0 >= N) return;
     const int i = ord[t0];
     const int kd = dpos[i], k1 = ptr[i + 1], nu = k1 - 1 - kd;
+    const double zi = __dadd_rn(0., __dmul_rn(f[kd], w[i])), di = invd[i];  // Mul_QV of the diagonal: 0 + d_i w_i
     double s = 0.;
     for (int base = 0; base < nu; base += 32) {
       double p = 0.;
       if (base + lane < nu) {
         const int k = k1 - 1 - base - lane;  // from the row's end
-        const int j = col[k];
-        wait_row(flag, j, gen, err);
-        p = __dmul_rn(f[k], y[j]);
+        const double fk = f[k];
+        p = __dmul_rn(fk, wait_val(y, col[k], err));
       }
       const int n = min(32, nu - base);
       for (int t = 0; t < n; t++) s = __dsub_rn(s, __shfl_sync(0xffffffffu, p, t));
     }
-    s = __dadd_rn(s, __dadd_rn(0., __dmul_rn(f[kd], w[i])));  // Mul_QV of the diagonal: 0 + d_i w_i
-    if (lane == 0) {
-      y[i] = __dmul_rn(s, invd[i]);
-      st_rel(flag + i, gen);
-    }
+    s = __dadd_rn(s, zi);
+    if (lane == 0) st_rel_f64(y + i, __dmul_rn(s, di));
   }
 }
 
@@ -385,12 +441,13 @@ static int dot_dev(exf_sys *s, SysLevel &L, const double *a, const double *b, lo
 static int ilu_apply_dev(exf_sys *s, int lev, const double *c, double *y, const int *skip) {
   SysLevel &L = s->L[lev];
   const int N = L.N, G = ilu_grid(s);
-  k_ilu_arm<<<1, 1, 0, s->stream>>>(L.ilu_ctl.p, skip);
-  k_ilu_lower<<<G, 128, 0, s->stream>>>(N, L.ilu_ord_lo.p, L.qq_ptr.p, L.qq_col.p, L.diag_pos.p, L.ilu_f.p, L.ilu_inv.p, c,
-                                        L.gm_w.p, L.ilu_flag.p, L.ilu_ctl.p, s->wait_flag.p, skip);
-  k_ilu_arm<<<1, 1, 0, s->stream>>>(L.ilu_ctl.p, skip);
-  k_ilu_upper<<<G, 128, 0, s->stream>>>(N, L.ilu_ord_up.p, L.qq_ptr.p, L.qq_col.p, L.diag_pos.p, L.ilu_f.p, L.ilu_inv.p, L.gm_w.p,
-                                        y, L.ilu_flag.p, L.ilu_ctl.p, s->wait_flag.p, skip);
+  const unsigned g = (unsigned)((N + 255) / 256);
+  k_ilu_prep<<<g, 256, 0, s->stream>>>(L.gm_w.p, N, L.ilu_ctl.p, skip);
+  k_ilu_lower<<<G, 128, 0, s->stream>>>(N, L.ilu_ord_lo.p, L.qq_ptr.p, L.qq_col.p, L.diag_pos.p, L.ilu_f.p,
+                                        L.ilu_inv.p, c, L.gm_w.p, L.ilu_ctl.p, s->wait_flag.p, skip);
+  k_ilu_prep<<<g, 256, 0, s->stream>>>(y, N, L.ilu_ctl.p, skip);
+  k_ilu_upper<<<G, 128, 0, s->stream>>>(N, L.ilu_ord_up.p, L.qq_ptr.p, L.qq_col.p, L.diag_pos.p, L.ilu_f.p,
+                                        L.ilu_inv.p, L.gm_w.p, y, L.ilu_ctl.p, s->wait_flag.p, skip);
   EXF_COUNT(4);
   EXF_LAUNCH_CHECK();
   return EXF_OK;
@@ -398,7 +455,7 @@ static int ilu_apply_dev(exf_sys *s, int lev, const double *c, double *y, const 
 
 template <int MAXL, int NW>
 static int launch_factor(exf_sys *s, SysLevel &L) {
-  const size_t smem = (size_t)NW * (MAXL * (MAXL + 1) * sizeof(double) + MAXL * sizeof(int));
+  const size_t smem = (size_t)NW * (MAXL * (MAXL + 1) * sizeof(double) + 5 * MAXL * sizeof(int));
   auto kern = k_ilu_factor<MAXL, NW>;
   EXF_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   k_ilu_arm<<<1, 1, 0, s->stream>>>(L.ilu_ctl.p, nullptr);
