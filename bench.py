@@ -56,10 +56,11 @@ def parse():
     ap.add_argument("--vanka-kernel", type=int, default=None,
                     help="profiling modes: EXF_VANKA_* kernel of the Vanka sweeps (default AUTO)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--mode", default="bench", choices=["bench", "vcycle", "step", "workloads"],
+    ap.add_argument("--mode", default="bench", choices=["bench", "vcycle", "step", "workloads", "gmres"],
                     help="vcycle: assemble once and run one mixed and one FP64 V-cycle; step: one Picard "
                          "step (assembly of all levels + mixed solve to 1e-10) -- profiling cases; "
-                         "workloads: every workload at full size, one JSON line each")
+                         "workloads: every workload at full size, one JSON line each; gmres: the "
+                         "Boussinesq temperature system with the GMRES + ILU level solver")
     return ap.parse_args()
 
 
@@ -318,6 +319,43 @@ def top_wall_weights(xyz):
     return w
 
 
+def gmres_line(name, t, top, gs=None):
+    """The scalar system t solved from zero with GMRES(30) + ILU smoothing (2 / 2), with
+    the ILU factorisation, one ILUPrecond and one smoother iteration of the top level."""
+    import ctypes as C
+    import exfemus_b200 as ex
+    from exfemus_b200 import _lib
+    L = ex.load()
+    p = ex.mg_params(eps=1e-10, max_cycles=200, smoother=_lib.SMOOTH_GMRES_ILU, nu_pre=2, nu_post=2)
+    t.set_x(np.zeros(t.ntop_dof))
+    st = t.solve(p)
+    tv = C.c_double()
+    out = {"workload": name, "smoother": "gmres30+ilu 2/2", "ndof": t.ntop_dof, "cycles": st.cycles,
+           "rel_res": st.rel_res, "solve_s": st.seconds}
+    t.set_x(np.zeros(t.ntop_dof))  # the iteration from an unconverged iterate
+    for what, key in ((7, "ilu_factor_ms"), (8, "ilu_apply_ms"), (1, "gmres_iteration_ms")):
+        _lib.check(L.exf_time_op(t.h, what, top, C.byref(p), C.byref(t.phys), 3, C.byref(tv)))
+        out[key] = tv.value
+    if gs is not None:
+        out["gs_cycles"], out["gs_solve_s"] = gs
+    print(json.dumps(out), flush=True)
+
+
+def run_gmres(args, local):
+    """The Boussinesq temperature system at full size (after one mixed Picard step) with the
+    reference's default level solver, GMRES(30) + ILU, against its Gauss-Seidel multigrid
+    on the same system, both from zero (also the profiling case of the ILU kernels)."""
+    import exfemus_b200 as ex
+    from exfemus_b200 import _lib, workloads
+    case = ex.make_case("bouss2d", device=local)
+    workloads.picard(case, 1, precision=_lib.PREC_MIXED)
+    tb = case["T"]
+    tb.assemble_all()
+    tb.set_x(np.zeros(tb.ntop_dof))
+    stg = tb.solve(ex.mg_params(eps=1e-10, max_cycles=200, smoother=_lib.SMOOTH_GS, nu_pre=2, nu_post=2))
+    gmres_line("bouss2d_T", tb, case["w"]["nlev"] - 1, gs=(stg.cycles, stg.seconds))
+
+
 def run_workloads(args, local):
     """Every workload at its full size (one GPU): Picard steps with per-step cycles and
     device seconds; the adjoint gradient's cost against the forward solve and its
@@ -326,23 +364,6 @@ def run_workloads(args, local):
     import exfemus_b200 as ex
     from exfemus_b200 import _lib, workloads
     L = ex.load()
-
-    def gmres_line(name, t, top, gs=None):
-        """The scalar system t solved from zero with GMRES(30) + ILU smoothing (2 / 2), with
-        the ILU factorisation, one ILUPrecond and one smoother iteration of the top level."""
-        p = ex.mg_params(eps=1e-10, max_cycles=200, smoother=_lib.SMOOTH_GMRES_ILU, nu_pre=2, nu_post=2)
-        t.set_x(np.zeros(t.ntop_dof))
-        st = t.solve(p)
-        tv = C.c_double()
-        out = {"workload": name, "smoother": "gmres30+ilu 2/2", "ndof": t.ntop_dof, "cycles": st.cycles,
-               "rel_res": st.rel_res, "solve_s": st.seconds}
-        t.set_x(np.zeros(t.ntop_dof))  # the iteration from an unconverged iterate
-        for what, key in ((7, "ilu_factor_ms"), (8, "ilu_apply_ms"), (1, "gmres_iteration_ms")):
-            _lib.check(L.exf_time_op(t.h, what, top, C.byref(p), C.byref(t.phys), 3, C.byref(tv)))
-            out[key] = tv.value
-        if gs is not None:
-            out["gs_cycles"], out["gs_solve_s"] = gs
-        print(json.dumps(out), flush=True)
 
     def picard_run(name, precision):
         case = ex.make_case(name, device=local)
@@ -445,16 +466,7 @@ def run_workloads(args, local):
                       "backward_rel_res": stb.rel_res, "cost_ratio": bwd_ms / fwd_ms,
                       "fd_rel_err_max": float(max(errs)), "fd_directions": len(errs), "fd_h": h}), flush=True)
 
-    # the Boussinesq temperature system at full size (a fresh copy of the mixed run's last
-    # step) with the reference's default level solver, GMRES(30) + ILU, against its
-    # Gauss-Seidel multigrid on the same system, both from zero
-    case = ex.make_case("bouss2d", device=local)
-    workloads.picard(case, 1, precision=_lib.PREC_MIXED)
-    tb = case["T"]
-    tb.assemble_all()
-    tb.set_x(np.zeros(tb.ntop_dof))
-    stg = tb.solve(ex.mg_params(eps=1e-10, max_cycles=200, smoother=_lib.SMOOTH_GS, nu_pre=2, nu_post=2))
-    gmres_line("bouss2d_T", tb, case["w"]["nlev"] - 1, gs=(stg.cycles, stg.seconds))
+    run_gmres(args, local)
 
 
 def run_ours(args, ws, rank, local):
@@ -468,6 +480,8 @@ def run_ours(args, ws, rank, local):
         return run_step(args, local)
     if args.mode == "workloads":
         return run_workloads(args, local)
+    if args.mode == "gmres":
+        return run_gmres(args, local)
     case = ex.make_case(args.workload, device=local)
     w = case["w"]
     ns = case["NS"]
