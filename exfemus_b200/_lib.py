@@ -79,7 +79,7 @@ class ExfMgParams(C.Structure):
                 ("smoother", C.c_int), ("omega", C.c_double), ("corr_damp", C.c_double),
                 ("cond_corr", C.c_int), ("reverse_colours", C.c_int), ("precision", C.c_int),
                 ("use_graph", C.c_int), ("vanka_kernel", C.c_int), ("stop_test", C.c_int),
-                ("fp32_blocks", C.c_int)]
+                ("fp32_blocks", C.c_int), ("coarse_iters", C.c_int)]
 
 
 class ExfSolveStats(C.Structure):

@@ -240,6 +240,13 @@ static int mg_step(exf_sys *s, int lev, const exf_mg_params *p, bool final_resid
   double *acc = needs_acc(p) ? s->mg_acc.p + 4 * lev : nullptr;
   if (acc) EXF_TRY(norm2<T>(s, b, len, acc));
   if (lev == 0) {
+    if constexpr (sizeof(T) == 8) {
+      if (p->smoother == EXF_SMOOTH_GMRES_ILU && p->coarse_iters > 0) {  // _solver[0]->solve(.., 60)
+        EXF_TRY(gmres_smooth(s, 0, p->eps, p->coarse_iters, x, b, acc ? acc + 2 : nullptr));
+        if (final_resid) EXF_TRY(spmv_resid<T>(s, 0, x, b, r, d_norm_out));
+        return EXF_OK;
+      }
+    }
     EXF_TRY(coarse_apply<T>(s, b, x));
     if (acc) EXF_TRY(spmv_resid<T>(s, 0, x, b, r, acc + 2));
     if (final_resid) EXF_TRY(spmv_resid<T>(s, 0, x, b, r, d_norm_out));
@@ -899,6 +906,12 @@ static unsigned long long params_key(const exf_mg_params *p) {
   mix((unsigned long long)p->cond_corr);
   mix((unsigned long long)p->stop_test);
   mix((unsigned long long)p->fp32_blocks);
+  if (p->smoother == EXF_SMOOTH_GMRES_ILU) {  // the level solver's accuracy test is in its kernels
+    unsigned long long e;
+    memcpy(&e, &p->eps, 8);
+    mix(e);
+    mix((unsigned long long)p->coarse_iters);
+  }
   return h | 1ull;
 }
 
@@ -1069,7 +1082,7 @@ int exf_mg_solve(exf_sys *s, const exf_mg_params *p, exf_solve_stats *st) {
     return EXF_ERR_STATE;
   }
   EXF_TRY(need_transfers(s));
-  if (p->gamma < 1 || p->nu_pre < 0 || p->nu_post < 0 || p->max_cycles < 0 ||
+  if (p->gamma < 1 || p->nu_pre < 0 || p->nu_post < 0 || p->max_cycles < 0 || p->coarse_iters < 0 ||
       (p->stop_test != EXF_STOP_RELRES && p->stop_test != EXF_STOP_REFERENCE))
     return EXF_ERR_ARG;
   if (needs_acc(p) && s->mg_acc.n != (size_t)4 * s->nlev) {
@@ -1085,7 +1098,7 @@ int exf_mg_solve(exf_sys *s, const exf_mg_params *p, exf_solve_stats *st) {
       set_error("GMRES + ILU smoothing runs in FP64 precision only");
       return EXF_ERR_UNSUPPORTED;
     }
-    for (int l = 1; l < s->nlev; l++) EXF_TRY(ilu_ready(s, l));  // ILUFactor once per assembly
+    for (int l = p->coarse_iters > 0 ? 0 : 1; l < s->nlev; l++) EXF_TRY(ilu_ready(s, l));  // once per assembly
   }
   if (!s->coarse_ok) EXF_TRY(coarse_factor(s));
   EXF_CUDA(cudaEventRecord(s->ev0, s->stream));

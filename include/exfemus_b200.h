@@ -120,6 +120,9 @@ typedef struct {
   int fp32_blocks;     /* mixed precision: 1 = the Vanka sweeps read the FP32 velocity */
                        /* blocks (FP32 storage throughout the V-cycle) with the row    */
                        /* kernel; 0 = row-scaled FP16 block records (default)          */
+  int coarse_iters;    /* 0: direct solve on level 0 (default); with the GMRES + ILU   */
+                       /* smoother, n > 0 runs that level solver for n iterations there */
+                       /* instead, as MGStep does (60, src/MGSolverBase.C:222)          */
 } exf_mg_params;
 
 /* stop tests of exf_mg_solve.  A level's accuracy is what the reference's level solver

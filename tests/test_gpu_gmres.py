@@ -79,11 +79,13 @@ def mg_step_here(s, lev, x, b, p, laspack):
     """MGStep (src/MGSolverBase.C:212-289) from the library's unit operations with
     LASPACK's GMRES + ILU as the level solver (corrections added with corr_damp)."""
     top = s.nlev - 1
-    if lev == 0:
-        return s.coarse_solve(b)
-    mul = 2 if (p.double_below_top and lev < top) else 1
     rp, col, val = s.csr(lev)
     rp, col = rp.astype(np.int32), col.astype(np.int32)
+    if lev == 0:
+        if p.coarse_iters > 0:  # _solver[0]->solve(A, x, b, Eps1, 60) from x = 0
+            return laspack.gmres(rp, col, val, b, x0=x, tol=p.eps, maxit=p.coarse_iters, restart=30, ilu=True)[0]
+        return s.coarse_solve(b)
+    mul = 2 if (p.double_below_top and lev < top) else 1
     x, _, _ = laspack.gmres(rp, col, val, b, x0=x, tol=p.eps, maxit=p.nu_pre * mul, restart=30, ilu=True)
     r = s.resid(lev, x, b)
     bc = s.restrict(lev - 1, r)
@@ -106,6 +108,24 @@ def test_one_vcycle_matches_the_composed_reference_cycle(gpu_lib, oracle_mod, la
     xg = s.x()
     xh = mg_step_here(s, top, np.zeros(s.ntop_dof), b, p, laspack)
     assert np.linalg.norm(xg - xh) <= 1e-11 * np.linalg.norm(xh)
+
+
+@pytest.mark.parametrize("name", ["heat2d", "heat3d"])
+def test_one_vcycle_with_the_coarse_level_solver(gpu_lib, oracle_mod, laspack, name):
+    """coarse_iters = 60: level 0 runs the same GMRES + ILU for 60 iterations (or to the
+    accuracy test), as MGStep does, instead of the direct solve."""
+    c = assembled(name, oracle_mod)
+    s = c["gs"]
+    b = s.rhs()
+    p = gmres_params(max_cycles=1, eps=1e-10, use_graph=0, coarse_iters=60)
+    s.set_x(np.zeros(s.ntop_dof))
+    st = s.solve(p)
+    assert st.cycles == 1
+    xh = mg_step_here(s, c["nlev"] - 1, np.zeros(s.ntop_dof), b, p, laspack)
+    assert np.linalg.norm(s.x() - xh) <= 1e-9 * np.linalg.norm(xh)
+    s.set_x(np.zeros(s.ntop_dof))
+    st = s.solve(gmres_params(eps=1e-10, coarse_iters=60))
+    assert st.converged
 
 
 @pytest.mark.parametrize("name", ["heat2d", "heat3d"])
