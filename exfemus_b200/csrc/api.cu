@@ -397,7 +397,7 @@ static int sys_upload_bc(exf_sys *s) {
 }
 
 int exf_sys_create(exf_mesh *m, int kind, exf_sys **out) {
-  if (!m || !out || (kind != EXF_KIND_T && kind != EXF_KIND_NS)) {
+  if (!m || !out || kind < EXF_KIND_T || kind > EXF_KIND_W) {
     set_error("exf_sys_create: bad argument");
     return EXF_ERR_ARG;
   }
@@ -407,8 +407,8 @@ int exf_sys_create(exf_mesh *m, int kind, exf_sys **out) {
   s->kind = kind;
   s->dim = m->dim;
   s->nlev = m->nlev;
-  s->nv2 = kind == EXF_KIND_T ? 1 : m->dim;
-  s->nv1 = kind == EXF_KIND_T ? 0 : 1;
+  s->nv2 = kind == EXF_KIND_NS ? m->dim : 1;  // T, K, W: one quadratic variable
+  s->nv1 = kind == EXF_KIND_NS ? 1 : 0;
   s->nvars = s->nv2 + s->nv1;
   if (cudaDeviceGetAttribute(&s->nsm, cudaDevAttrMultiProcessorCount, m->device) != cudaSuccess ||
       cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess ||
@@ -762,7 +762,34 @@ int exf_sys_couple(exf_sys *s, exf_sys *other) {
     set_error("coupled systems must share the mesh");
     return EXF_ERR_ARG;
   }
-  s->other = other;
+  const bool kw = s->kind == EXF_KIND_K || s->kind == EXF_KIND_W;
+  if (kw && other && (other->kind == EXF_KIND_K || other->kind == EXF_KIND_W)) {
+    if (other->kind == s->kind) {
+      set_error("a kappa (omega) system couples to an omega (kappa) system");
+      return EXF_ERR_ARG;
+    }
+    s->turb = other;  // the other turbulence variable
+  } else {
+    s->other = other;
+  }
+  return EXF_OK;
+}
+
+int exf_sys_set_wall(exf_sys *s, const double *dist, double nu_wall) {
+  CHECK_SYS(s);
+  if (!dist || (s->kind != EXF_KIND_K && s->kind != EXF_KIND_W)) return EXF_ERR_ARG;
+  std::vector<long> off(1, 0);
+  for (int l = 0; l < s->nlev; l++) off.push_back(off.back() + s->mesh->lev[l].nel);
+  for (long e = 0; e < off.back(); e++)
+    if (!(dist[e] > 0.)) {
+      set_error("exf_sys_set_wall: element %ld has wall distance %g", e, dist[e]);
+      return EXF_ERR_ARG;
+    }
+  EXF_TRY(s->wall_dist.ensure(off.back()));
+  EXF_CUDA(cudaMemcpyAsync(s->wall_dist.p, dist, off.back() * sizeof(double), cudaMemcpyHostToDevice, s->stream));
+  EXF_CUDA(cudaStreamSynchronize(s->stream));
+  s->wall_off = off;
+  s->nu_wall = nu_wall;
   return EXF_OK;
 }
 
@@ -822,7 +849,8 @@ int exf_gen_mat_rhs(exf_sys *s, const exf_phys *ph, int lev, int mode) {
   CHECK_LEV(s, lev);
   if (!ph || (mode != 0 && mode != 1)) return EXF_ERR_ARG;
   if (s->kind == EXF_KIND_NS && s->mesh->dim == 3 && s->nv2 != 3) return EXF_ERR_STATE;
-  EXF_TRY(assemble_level(s, ph, lev, mode));
+  if (s->kind == EXF_KIND_K || s->kind == EXF_KIND_W) EXF_TRY(assemble_kw_level(s, ph, lev, mode));
+  else EXF_TRY(assemble_level(s, ph, lev, mode));
   EXF_TRY(sync_fp32(s, lev));
   if (lev == 0) s->coarse_ok = 0;
   s->assembled = 1;
@@ -835,7 +863,11 @@ int exf_assemble_all(exf_sys *s, const exf_phys *ph) {
   CHECK_SYS(s);
   if (!ph) return EXF_ERR_ARG;
   if (s->kind == EXF_KIND_NS && s->mesh->dim == 3 && s->nv2 != 3) return EXF_ERR_STATE;
-  EXF_TRY(assemble_all_levels(s, ph));
+  if (s->kind == EXF_KIND_K || s->kind == EXF_KIND_W) {
+    for (int l = s->nlev - 1; l >= 0; l--) EXF_TRY(assemble_kw_level(s, ph, l, l == s->nlev - 1 ? 1 : 0));
+  } else {
+    EXF_TRY(assemble_all_levels(s, ph));
+  }
   for (int l = 0; l < s->nlev; l++) EXF_TRY(sync_fp32(s, l));
   s->coarse_ok = 0;
   s->assembled = 1;
@@ -1386,7 +1418,7 @@ int exf_level_bytes(exf_sys *s, int lev, int precision, double *spmv_bytes, doub
   const double vec = (double)L.ndof * vb;
   if (spmv_bytes) *spmv_bytes = A + 3. * vec;
   if (sweep_bytes) {
-    if (s->kind == EXF_KIND_T) {
+    if (s->nv1 == 0) {
       *sweep_bytes = A + 3. * vec;
     } else {
       double B = 0.;

@@ -724,4 +724,278 @@ int assemble_level(exf_sys *s, const exf_phys *ph, int lev, int mode) {
   return assemble_dim<3>(s, ph, lev, mode);
 }
 
+// ---------------------------------------------------------------- kappa-omega
+// One variable (var 0 kappa, 1 omega) of MGSolTBK::GenMatRhs, the turbulence template's
+// coupled kappa-omega system (template_appl/turb-ckw/SRC/MGSolverTBKW.C:83-454; its
+// matrix has no kappa-omega blocks, so each variable is its own scalar system), with the
+// template's model (MGSolTBK::f_mu, :484-587, WILCOX and LOWRE, constants of
+// template_appl/turb-ckw/DATA/MGSclass_conf.h:296-356).  Per Gauss point, with the
+// Navier-Stokes velocity v and the kappa, omega fields interpolated from the nodes:
+//   tau = min(1/omega, MAX_TAU), Re_t = clamp(kappa tau / IRe, MU_LOW, MU_TOP),
+//   alpha* = (0.024 + Re_t/6) / (1 + Re_t/6), mu_t = alpha* Re_t,
+//   S = 1e-20 + sum_ij (dv_i/dx_j + dv_j/dx_i)^2, nut2 = kappa / (7 sqrt(alpha* S / 2 / beta*) / 8),
+//   sources and dissipations of the 2006 model with the low-Re factors gamma*, beta*,
+//   cross = max(grad kappa . grad omega, 0) tau / 8, IRe_eff = IRe (1 + sigma alpha* mu_t),
+// then the reference's volume terms (time, advection, upwinded diffusion, dissipation;
+// rhs: x_old / dt, source, cross for omega), its Dirichlet sides (penalty det / dt, the
+// omega wall value 6 nu / (beta* y^2) where the flags ask for it) and its Neumann sides
+// (2 IRe_eff / y with the last Gauss point's IRe_eff, as the reference leaves it).
+constexpr double kKwSigmaK = 0.6, kKwSigmaW = 0.5, kKwBetaStar = 0.09, kKwMaxTau = 100., kKwMuLow = 1.e-6,
+                 kKwMuTop = 1.e+6, kKwUpwind = 1.;
+
+template <int DIM>
+struct KwArgs {
+  const FETab<DIM> *tab;
+  const int *conn, *neigh, *elist;
+  const double *xyz;
+  int ntop, Ntop;
+  const int *bc0, *bc1;
+  const double *kold, *wold, *vel, *dist;
+  const int *qq_ptr;
+  const uint8_t *pos_qq;
+  double *vv, *rhs;
+  double ire, idt, nu_wall;
+  int var;
+  int sides[FE<DIM>::NSIDE][FE<DIM>::NSN];
+};
+
+template <int DIM, int NT>
+__global__ void __launch_bounds__(NT) k_assemble_kw(KwArgs<DIM> A, int mode) {
+  using F = FE<DIM>;
+  constexpr int NEN = F::NEN, NQ = F::NQ;
+  const int tid = threadIdx.x, e = A.elist[blockIdx.x];
+  __shared__ int s_conn[NEN], s_bcv[NEN], s_bcb[NEN];
+  __shared__ double s_xx[DIM][NEN];
+  __shared__ double s_v[DIM][NEN], s_k[NEN], s_w[NEN];
+  __shared__ double s_dphi[NQ][NEN][DIM];
+  __shared__ double s_cM[NQ], s_cA[NQ][DIM], s_cL[NQ][DIM], s_cR[NQ];
+  __shared__ double s_h[DIM], s_ire_last;
+  const FETab<DIM> *t = A.tab;
+  for (int k = tid; k < NEN; k += NT) {
+    const int nd = A.conn[(long)e * NEN + k];
+    s_conn[k] = nd;
+    for (int d = 0; d < DIM; d++) {
+      s_xx[d][k] = A.xyz[nd + (long)d * A.ntop];
+      s_v[d][k] = A.vel ? A.vel[nd + (long)d * A.Ntop] : 0.;
+    }
+    s_bcv[k] = A.bc0[nd];
+    s_bcb[k] = A.bc1[nd];
+    s_k[k] = A.kold[nd];
+    s_w[k] = A.wold[nd];
+  }
+  __syncthreads();
+  if (tid < DIM) {
+    const int v2 = DIM == 2 ? 2 : 6, v3 = DIM == 2 ? 3 : 7;
+    const double h = fabs(s_xx[tid][v2] - s_xx[tid][0]), h1 = fabs(s_xx[tid][v3] - s_xx[tid][1]);
+    s_h[tid] = h < h1 ? h1 : h;
+  }
+  __syncthreads();
+  const int var = A.var;
+  const double IRe = A.ire, idt = A.idt;
+  for (int q = tid; q < NQ; q += NT) {  // one thread per Gauss point
+    double J[DIM][DIM];
+    for (int a = 0; a < DIM; a++)
+      for (int b = 0; b < DIM; b++) {
+        double sum = 0.;
+        for (int k = 0; k < NEN; k++) sum += s_xx[a][k] * t->dphi[q][k][b];
+        J[a][b] = sum;
+      }
+    double det, inv[DIM][DIM];  // inv[b][a] = dxi_b / dx_a
+    if constexpr (DIM == 2) {
+      det = J[0][0] * J[1][1] - J[1][0] * J[0][1];
+      const double id = 1. / det;
+      inv[0][0] = J[1][1] * id;
+      inv[0][1] = -J[0][1] * id;
+      inv[1][0] = -J[1][0] * id;
+      inv[1][1] = J[0][0] * id;
+    } else {
+      const int o = DIM - 1;
+      det = J[0][0] * (J[1][1] * J[o][o] - J[1][o] * J[o][1]) - J[0][1] * (J[1][0] * J[o][o] - J[1][o] * J[o][0]) +
+            J[0][o] * (J[1][0] * J[o][1] - J[1][1] * J[o][0]);
+      const double id = 1. / det;
+      inv[0][0] = (J[1][1] * J[o][o] - J[1][o] * J[o][1]) * id;
+      inv[0][1] = (J[0][o] * J[o][1] - J[0][1] * J[o][o]) * id;
+      inv[0][o] = (J[0][1] * J[1][o] - J[0][o] * J[1][1]) * id;
+      inv[1][0] = (J[1][o] * J[o][0] - J[1][0] * J[o][o]) * id;
+      inv[1][1] = (J[0][0] * J[o][o] - J[0][o] * J[o][0]) * id;
+      inv[1][o] = (J[0][o] * J[1][0] - J[0][0] * J[1][o]) * id;
+      inv[o][0] = (J[1][0] * J[o][1] - J[1][1] * J[o][0]) * id;
+      inv[o][1] = (J[0][1] * J[o][0] - J[0][0] * J[o][1]) * id;
+      inv[o][o] = (J[0][0] * J[1][1] - J[0][1] * J[1][0]) * id;
+    }
+    const double JxW = det * t->w[q];
+    double vg[DIM], g[DIM][DIM], gk[DIM], gw[DIM], kg = 0., wg = 0.;
+    for (int d = 0; d < DIM; d++) {
+      vg[d] = gk[d] = gw[d] = 0.;
+      for (int a = 0; a < DIM; a++) g[a][d] = 0.;
+    }
+    for (int k = 0; k < NEN; k++) {
+      const double ph = t->phi[q][k];
+      kg += ph * s_k[k];
+      wg += ph * s_w[k];
+      for (int d = 0; d < DIM; d++) {
+        double dp = 0.;
+        for (int b = 0; b < DIM; b++) dp += inv[b][d] * t->dphi[q][k][b];
+        s_dphi[q][k][d] = dp;
+        vg[d] += ph * s_v[d][k];
+        gk[d] += s_k[k] * dp;
+        gw[d] += s_w[k] * dp;
+        for (int a = 0; a < DIM; a++) g[a][d] += s_v[a][k] * dp;
+      }
+    }
+    double mod = 1e-20, sP = 1.e-20, chi = 0.;
+    for (int d = 0; d < DIM; d++) mod += vg[d] * vg[d];
+    mod = sqrt(mod);
+    for (int a = 0; a < DIM; a++)
+      for (int b = 0; b < DIM; b++) {
+        const double sss = g[a][b] + g[b][a];
+        sP += sss * sss;
+      }
+    for (int d = 0; d < DIM; d++) chi += gk[d] * gw[d];
+    // f_mu (WILCOX, LOWRE)
+    if (kg < 1.e-20) kg = 1.e-20;
+    double tau = 1. / wg;
+    if (tau > kKwMaxTau) tau = kKwMaxTau;
+    double Re_t = kg * tau / IRe;
+    if (Re_t > kKwMuTop) Re_t = kKwMuTop;
+    if (Re_t < kKwMuLow) Re_t = kKwMuLow;
+    const double astar = (0.024 + 0.166666666667 * Re_t) / (1. + 0.166666666667 * Re_t);
+    const double mu_t = Re_t * astar;
+    const double nut2 = kg / (7. * sqrt(astar * 0.5 * sP / kKwBetaStar) / 8.);
+    double src0, src1;
+    if (mu_t * IRe < nut2) {
+      src0 = 0.5 * mu_t * IRe * sP;
+      src1 = 0.5 * 13. * sP / 25.;
+    } else {
+      src0 = 0.5 * nut2 * sP;
+      src1 = 0.5 * 13. * nut2 * sP / (25. * mu_t * IRe);
+    }
+    const double gstar = (0.111111111111 + 0.338983050847 * Re_t) / (1. + 0.338983050847 * Re_t);
+    const double r4 = Re_t * Re_t * Re_t * Re_t;
+    const double bstar = (0.266666666667 + 0.000244140625 * r4) / (1. + 0.000244140625 * r4);
+    const double diss = var == 0 ? kKwBetaStar / tau * bstar : 0.0708 / tau;
+    const double src = var == 0 ? src0 : src1 * gstar;
+    const double cross = chi > 0 ? chi * tau / 8. : 0.;
+    const double ire = IRe * (1. + (var == 0 ? kKwSigmaK : kKwSigmaW) * astar * mu_t);
+    s_cM[q] = JxW * (idt + diss);
+    s_cR[q] = JxW * ((var == 0 ? kg : wg) * idt + src + cross * var);
+    for (int d = 0; d < DIM; d++) {
+      const double pe = 0.5 * mod * s_h[d] / IRe;
+      const double fu = kKwUpwind * 0.5 * (1. / tanh(pe) - 1. / pe) * s_h[d] / mod;
+      s_cA[q][d] = JxW * vg[d];
+      s_cL[q][d] = JxW * (ire + fu * vg[d] * vg[d]);
+    }
+    if (q == NQ - 1) s_ire_last = ire;
+  }
+  __syncthreads();
+  // volume integrals of the node pairs and the rhs
+  for (int p = tid; p < NEN * NEN; p += NT) {
+    const int i = p / NEN, j = p % NEN;
+    const long blk = A.qq_ptr[s_conn[i]] + A.pos_qq[((long)e * NEN + i) * NEN + j];
+    const double old = A.vv[blk];
+    double K = 0.;
+    for (int q = 0; q < NQ; q++) {
+      const double pi = t->phi[q][i], pj = t->phi[q][j];
+      double adv = 0., lap = 0.;
+      for (int d = 0; d < DIM; d++) {
+        adv += s_cA[q][d] * s_dphi[q][j][d];
+        lap += s_cL[q][d] * s_dphi[q][j][d] * s_dphi[q][i][d];
+      }
+      K += pi * (s_cM[q] * pj + adv) + lap;
+    }
+    A.vv[blk] = old + s_bcv[i] * K;
+  }
+  if (mode == 1)
+    for (int i = tid; i < NEN; i += NT) {
+      double f = 0.;
+      for (int q = 0; q < NQ; q++) f += s_cR[q] * t->phi[q][i];
+      A.rhs[s_conn[i]] += s_bcv[i] * f;
+    }
+  __syncthreads();
+  // boundary sides, one after the other (a node may lie on two of them)
+  const double y = A.dist[e];
+  for (int sd = 0; sd < F::NSIDE; sd++) {
+    if (A.neigh[(long)e * F::NSIDE + sd] != -1) continue;
+    const int *sur = A.sides[sd];
+    const int last = sur[F::NSN - 1];
+    for (int k = tid; k < F::NSN; k += NT) {
+      const int lv = sur[k];
+      const long dblk = A.qq_ptr[s_conn[lv]] + A.pos_qq[((long)e * NEN + lv) * NEN + lv];
+      if (s_bcv[last] == 0) {
+        const double ipen = jac_sur<DIM>(t, F::NSQ - 1, s_xx, sur) * idt;
+        const int bs = s_bcb[lv], bc_rhs = (bs & 2) >> 1, bc_n = bs % 2;
+        const double xo = var == 0 ? s_k[lv] : s_w[lv];
+        const double kw = xo < 1.e-20 ? 1.e-20 : xo;
+        const double wall = 6. * A.nu_wall / (kKwBetaStar * y * y);
+        A.vv[dblk] += ipen;
+        if (mode == 1) A.rhs[s_conn[lv]] += ipen * (bc_n * (1 - bc_rhs) * kw + (1 - bc_n) * bc_rhs * (var * wall));
+      } else if (s_bcb[last] != 0) {
+        const double fac = 2. * s_ire_last * (s_bcv[lv] == 0 ? 0. : 1.) * (s_bcb[lv] % 2) / y;
+        for (int j = 0; j < F::NSN; j++) {
+          double v = 0.;
+          for (int q = 0; q < F::NSQ; q++) v += jac_sur<DIM>(t, q, s_xx, sur) * t->sw[q] * t->sphi[q][j] * t->sphi[q][k];
+          const long bj = A.qq_ptr[s_conn[lv]] + A.pos_qq[((long)e * NEN + lv) * NEN + sur[j]];
+          A.vv[bj] += fac * v;
+        }
+      }
+    }
+    __syncthreads();
+  }
+}
+
+template <int DIM>
+static int assemble_kw_dim(exf_sys *s, const exf_phys *ph, int lev, int mode) {
+  const exf_mesh *m = s->mesh;
+  const int top = s->nlev - 1;
+  SysLevel &L = s->L[lev];
+  const MeshLevel &ml = m->lev[lev];
+  if (!s->turb || s->wall_off.empty() || !(ph->inv_dt > 0.)) {
+    set_error("kappa-omega assembly needs the partner system (exf_sys_couple), the wall distances "
+              "(exf_sys_set_wall) and a time step (phys.inv_dt > 0)");
+    return EXF_ERR_STATE;
+  }
+  KwArgs<DIM> a;
+  memset(&a, 0, sizeof(a));
+  a.tab = reinterpret_cast<const FETab<DIM> *>(m->d_fetab.p);
+  for (int sd = 0; sd < FE<DIM>::NSIDE; sd++)
+    for (int k = 0; k < FE<DIM>::NSN; k++) a.sides[sd][k] = DIM == 2 ? Q9_SIDE[sd][k] : H27_FACE[sd][k];
+  a.conn = ml.d_conn.p;
+  a.neigh = ml.d_neigh.p;
+  a.xyz = m->d_xyz.p;
+  a.ntop = m->ntop;
+  a.Ntop = s->L[top].N;
+  a.bc0 = s->d_bc0.p;
+  a.bc1 = s->d_bc1.p;
+  const exf_sys *kk = s->kind == EXF_KIND_K ? s : s->turb, *ww = s->kind == EXF_KIND_W ? s : s->turb;
+  a.kold = kk->xold.p;
+  a.wold = ww->xold.p;
+  a.vel = (s->other && s->other->kind == EXF_KIND_NS) ? s->other->xold.p : nullptr;
+  a.dist = s->wall_dist.p + s->wall_off[lev];
+  a.qq_ptr = L.qq_ptr.p;
+  a.pos_qq = L.pos_qq.p;
+  a.vv = L.A.vv.p;
+  a.rhs = mode == 1 ? L.b.p : nullptr;
+  a.ire = ph->inv_re;
+  a.idt = ph->inv_dt;
+  a.nu_wall = s->nu_wall;
+  a.var = s->kind == EXF_KIND_K ? 0 : 1;
+  EXF_TRY(L.A.vv.zero(s->stream));
+  if (mode == 1) EXF_TRY(L.b.zero(s->stream));
+  constexpr int NT = DIM == 2 ? 64 : 128;
+  for (int c = 0; c + 1 < (int)ml.ecol_off.size(); c++) {
+    const int n = ml.ecol_off[c + 1] - ml.ecol_off[c];
+    if (n == 0) continue;
+    a.elist = ml.d_elist.p + ml.ecol_off[c];
+    k_assemble_kw<DIM, NT><<<n, NT, 0, s->stream>>>(a, mode);
+    EXF_LAUNCH_CHECK();
+    EXF_COUNT(1);
+  }
+  return EXF_OK;
+}
+
+int assemble_kw_level(exf_sys *s, const exf_phys *ph, int lev, int mode) {
+  if (s->mesh->dim == 2) return assemble_kw_dim<2>(s, ph, lev, mode);
+  return assemble_kw_dim<3>(s, ph, lev, mode);
+}
+
 }  // namespace exf

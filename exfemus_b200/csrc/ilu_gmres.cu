@@ -497,7 +497,7 @@ static int level_order(const std::vector<int> &ptr, const std::vector<int> &col,
 int ilu_ready(exf_sys *s, int lev) {
   SysLevel &L = s->L[lev];
   if (L.ilu_ok) return EXF_OK;
-  if (s->kind != EXF_KIND_T) {
+  if (s->nv1 != 0) {
     set_error("GMRES + ILU smoothing needs a scalar system: the Navier-Stokes pressure block has zero "
               "diagonal entries, on which LASPACK's ILU stops (LASZeroInDiagErr)");
     return EXF_ERR_UNSUPPORTED;

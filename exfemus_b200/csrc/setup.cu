@@ -372,7 +372,7 @@ static int colour_general(exf_sys *s, int l, int nitem, std::vector<int> &col) {
   EXF_CUDA(cudaMemcpy(lp.data(), L.ql_ptr.p, (L.N + 1) * sizeof(int), cudaMemcpyDeviceToHost));
   EXF_CUDA(cudaMemcpy(lc.data(), L.ql_col.p, L.nql * sizeof(int), cudaMemcpyDeviceToHost));
   std::vector<int> cptr(nitem + 1, 0), cidx;
-  if (s->kind == EXF_KIND_T) {
+  if (s->nv1 == 0) {
     cptr.assign(qp.begin(), qp.begin() + nitem + 1);
     cidx.assign(qc.begin(), qc.begin() + qp[nitem]);
   } else {
@@ -399,8 +399,8 @@ int build_colours(exf_sys *s) {
   for (int l = 0; l < s->nlev; l++) {
     SysLevel &L = s->L[l];
     int sl = 1 << (m->nlev - 1 - l);
-    int nitem = s->kind == EXF_KIND_T ? L.N : L.NL;
-    int step = s->kind == EXF_KIND_T ? sl : 2 * sl;
+    int nitem = s->nv1 == 0 ? L.N : L.NL;  // scalar systems colour DOFs, NS pressure nodes
+    int step = s->nv1 == 0 ? sl : 2 * sl;
     EXF_TRY(L.item_colour.alloc(nitem));
     std::vector<int> col(nitem);
     if (m->lattice) {

@@ -2103,7 +2103,7 @@ int smooth(exf_sys *s, int lev, const exf_mg_params *p, int nsweeps, T *x, const
     }
   }
   for (int it = 0; it < nsweeps; it++) {
-    if (s->kind == EXF_KIND_T) {
+    if (s->nv1 == 0) {  // scalar systems (T, kappa, omega)
       EXF_TRY(gs_sweep<T>(s, lev, p, x, b));
     } else if (s->dim == 2) {
       EXF_TRY((vanka_sweep<T, 2>(s, lev, p, x, b)));

@@ -194,7 +194,7 @@ class MGSolBase:
         check(self.L.exf_sys_create(mesh.h, self.kind, C.byref(h)))  # init_dof + pattern (MGDofBcOp)
         self.h = h
         self.nlev = mesh.nlev
-        self.nvars = 1 if self.kind == _lib.KIND_T else mesh.dim + 1
+        self.nvars = mesh.dim + 1 if self.kind == _lib.KIND_NS else 1
         self.phys = phys()
         self._keep = None
 
@@ -267,7 +267,7 @@ class MGSolBase:
         return self._transfer(self.L.exf_sys_get_rest, lev, self.ndof(lev))
 
     def colours(self, lev):
-        nitem = self.mesh.nnodes(lev) if self.kind == _lib.KIND_T else (
+        nitem = self.mesh.nnodes(lev) if self.kind != _lib.KIND_NS else (
             self.mesh.nnodes(lev - 1) if lev > 0 else self.mesh.nvert0)
         out = np.zeros(nitem, np.int32)
         nc = C.c_int()
@@ -440,6 +440,24 @@ class MGSolT(MGSolBase):
 class MGSolNS(MGSolBase):
     """Coupled Navier-Stokes, Taylor-Hood Q2-Q1 (MGSolNS, NS_EQUATIONS==1)."""
     kind = _lib.KIND_NS
+
+
+class MGSolTBK(MGSolBase):
+    """One variable of the turbulence template's coupled kappa-omega system (MGSolTBK,
+    template_appl/turb-ckw/SRC/MGSolverTBKW.C, TBK_EQUATIONS 5): var 0 kappa, 1 omega.
+    Couple it to the Navier-Stokes system (velocity) and to the other variable; the
+    element wall distances come from set_wall."""
+
+    def __init__(self, mesh, var):
+        super().__init__(mesh, _lib.KIND_K if var == 0 else _lib.KIND_W)
+        self.var = var
+
+    def set_wall(self, dist, nu_wall):
+        """dist: the wall distance of every element, level 0's first (_mgmesh._dist);
+        nu_wall = mu / rho of the omega wall value 6 nu_wall / (BETASTAR y^2)."""
+        d = np.ascontiguousarray(dist, np.float64)
+        self._wall = d
+        check(self.L.exf_sys_set_wall(self.h, dptr(d), float(nu_wall)))
 
 
 def timestep_loop(systems, params, nsteps):

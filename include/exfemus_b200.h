@@ -46,6 +46,14 @@ extern "C" {
  * dim quadratic velocity components + one linear pressure) */
 #define EXF_KIND_T 0
 #define EXF_KIND_NS 1
+/* the two variables of the turbulence template's coupled kappa-omega system
+ * (MGSolTBK, template_appl/turb-ckw/SRC/MGSolverTBKW.C, TBK_EQUATIONS 5, Wilcox 2006 with
+ * the low-Reynolds corrections): the system's matrix has no kappa-omega coupling blocks,
+ * so each variable is one scalar system (quadratic, like MGSolT) that reads the other
+ * through exf_sys_couple, the Navier-Stokes velocity likewise, and the element wall
+ * distances of exf_sys_set_wall */
+#define EXF_KIND_K 2
+#define EXF_KIND_W 3
 
 /* boundary-condition presets: the per-node bc_read rules of the workloads */
 #define EXF_BC_HEAT_DIRICHLET 1  /* T = 0 on every wall                              */
@@ -266,6 +274,10 @@ EXF_API int exf_sys_check_pattern(exf_sys *s, int lev, int block, const int dim[
 /* coupling: T reads the NS velocity, NS reads T for buoyancy (get_el_sol of the
  * other equation, src/MGSolverBase.C:336-354) */
 EXF_API int exf_sys_couple(exf_sys *s, exf_sys *other);
+/* kappa / omega systems: the wall distance of every element (_mgmesh._dist: level 0's
+ * elements first, then level 1's, ...) and nu_wall = mu / rho of the omega wall value
+ * 6 nu_wall / (BETASTAR y^2) */
+EXF_API int exf_sys_set_wall(exf_sys *s, const double *dist, double nu_wall);
 
 /* --- fields (host buffers) ---------------------------------------------------------- */
 EXF_API int exf_sys_set_xold(exf_sys *s, const double *xold);   /* x_old[top]             */

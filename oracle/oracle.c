@@ -1209,6 +1209,217 @@ void or_sys_assemble(or_sys *s, int lev, int mode, const or_phys *ph, const doub
   if (lev == 0) s->lu_ok = 0;
 }
 
+/* ------------------------------------------------------------------ k-omega
+ * MGSolTBK::GenMatRhs of the turbulence template (template_appl/turb-ckw/SRC/
+ * MGSolverTBKW.C:83-454) with its configuration (template_appl/turb-ckw/DATA/
+ * MGSclass_conf.h:276-356, Equations_conf.h:40: TBK_EQUATIONS 5, the coupled kappa-omega
+ * system; WILCOX with LOWRE; SIGMA_K 0.6, SIGMA_W 0.5, BETASTAR 0.09, MAX_TAU 100,
+ * MU_LOW 1e-6, MU_TOP 1e6, UP_WIND_K 1) and the model of MGSolTBK::f_mu (:484-587).  The
+ * coupled system's matrix is block diagonal (no kappa-omega coupling entries), so one
+ * variable var (0 kappa, 1 omega) is assembled on a scalar system: its diagonal block and
+ * its rhs.  Fields: vel = the Navier-Stokes x_old [dim][Ntop], kold / wold = the kappa and
+ * omega x_old [Ntop], dist = the element wall distances of this level (_mgmesh._dist),
+ * nu_wall = _muf / _rhof of the omega wall value. */
+#define KW_SIGMA_K 0.6
+#define KW_SIGMA_W 0.5
+#define KW_BETASTAR 0.09
+#define KW_MAX_TAU 100.
+#define KW_MU_LOW 1.e-6
+#define KW_MU_TOP 1.e+6
+#define KW_UP_WIND 1.
+
+typedef struct {
+  double ire[2], src[2], diss[2], cross;
+} kw_coef;
+
+/* MGSolTBK::f_mu, WILCOX + LOWRE (MGSolverTBKW.C:484-587), and the effective
+ * viscosities IRe (1 + sigma_v mu_t) (:243-247); kappa is clamped in place */
+static void kw_model(double *kg, double wg, double sP, double chi, double IRe, kw_coef *c) {
+  if (kg[0] < 1.e-20) kg[0] = 1.e-20;
+  double tau_k = 1. / wg;
+  if (tau_k > KW_MAX_TAU) tau_k = KW_MAX_TAU;
+  double Re_t = kg[0] * tau_k / IRe;
+  if (Re_t > KW_MU_TOP) Re_t = KW_MU_TOP;
+  if (Re_t < KW_MU_LOW) Re_t = KW_MU_LOW;
+  double mu_t = Re_t;
+  const double alpha_star = (0.024 + 0.166666666667 * Re_t) / (1. + 0.166666666667 * Re_t);
+  mu_t *= alpha_star;
+  const double nut2 = kg[0] / (7. * sqrt(alpha_star * 0.5 * sP / KW_BETASTAR) / 8.);
+  if (mu_t * IRe < nut2) {
+    c->src[0] = 0.5 * mu_t * IRe * sP;
+    c->src[1] = 0.5 * 13. * sP / (25.);
+  } else {
+    c->src[0] = 0.5 * nut2 * sP;
+    c->src[1] = 0.5 * 13. * nut2 * sP / (25. * mu_t * IRe);
+  }
+  c->diss[0] = KW_BETASTAR / tau_k;
+  c->diss[1] = 0.0708 / tau_k;
+  c->cross = chi > 0 ? chi * tau_k / 8. : 0.;
+  const double gamma_star = (0.111111111111 + 0.338983050847 * Re_t) / (1. + 0.338983050847 * Re_t);
+  const double beta_star = (0.266666666667 + 0.000244140625 * Re_t * Re_t * Re_t * Re_t) /
+                           (1. + 0.000244140625 * Re_t * Re_t * Re_t * Re_t);
+  c->diss[0] *= beta_star;
+  c->src[1] *= gamma_star;
+  c->ire[0] = IRe * (1. + KW_SIGMA_K * alpha_star * mu_t);
+  c->ire[1] = IRe * (1. + KW_SIGMA_W * alpha_star * mu_t);
+}
+
+static void kw_element(or_sys *s, int lev, int mode, int var, const or_phys *ph, const double *vel,
+                       const double *kold, const double *wold, double y, double nu_wall, const fe_tab *t, int e,
+                       double *Ke, double *Fe, double *rhs) {
+  const or_mesh *m = s->m;
+  int dim = m->dim, nen = m->nen, top = s->nlev - 1, off = m->ntop, Ntop = m->nnodes[top];
+  csr *A = &s->A[lev];
+  int dofs[MAXEN], bcv[MAXEN], bcb[MAXEN];
+  double xx[3 * MAXEN], vo[3][MAXEN], ko[MAXEN], wo[MAXEN];
+  const double IRe = ph->inv_re, idt = ph->inv_dt;
+  const int *c = m->conn[lev] + (long)e * nen;
+  memset(Ke, 0, (size_t)nen * nen * sizeof(double));
+  memset(Fe, 0, nen * sizeof(double));
+  for (int k = 0; k < nen; k++) {
+    for (int d = 0; d < dim; d++) xx[d * nen + k] = m->xyz[c[k] + (long)d * off];
+    dofs[k] = s->node_dof[lev][c[k]];
+    int td = s->node_dof[top][c[k]];
+    bcv[k] = s->bc0[td];
+    bcb[k] = s->bc1[td];
+    for (int d = 0; d < dim; d++) vo[d][k] = vel ? vel[c[k] + d * Ntop] : 0.;
+    ko[k] = kold[c[k]];
+    wo[k] = wold[c[k]];
+  }
+  const double *vold = var == 0 ? ko : wo;
+  double h[3];
+  {
+    int v2 = dim == 2 ? 2 : 6, v3 = dim == 2 ? 3 : 7;
+    for (int d = 0; d < dim; d++) {
+      h[d] = fabs(xx[d * nen + v2] - xx[d * nen + 0]);
+      double h1 = fabs(xx[d * nen + v3] - xx[d * nen + 1]);
+      if (h[d] < h1) h[d] = h1;
+    }
+  }
+  kw_coef cf = {{IRe, IRe}, {0, 0}, {0, 0}, 0};
+  for (int q = 0; q < t->ng; q++) {
+    double ij[9];
+    double det = jac(t, q, xx, nen, ij);
+    double JxW = det * t->w[q];
+    double dphi[MAXEN][3];
+    for (int sh = 0; sh < nen; sh++)
+      for (int i = 0; i < dim; i++) {
+        double sum = 0.;
+        for (int j = 0; j < dim; j++) sum += ij[j + i * dim] * t->dphi[q][sh][j];
+        dphi[sh][i] = sum;
+      }
+    const double *phi = t->phi[q];
+    double vg[3] = {0, 0, 0}, g[9] = {0}, gk[3] = {0, 0, 0}, gw[3] = {0, 0, 0}, kg[2] = {0, 0}, mod = 1e-20;
+    for (int k = 0; k < nen; k++) {
+      kg[0] += phi[k] * ko[k];
+      kg[1] += phi[k] * wo[k];
+      for (int d = 0; d < dim; d++) {
+        vg[d] += phi[k] * vo[d][k];
+        gk[d] += ko[k] * dphi[k][d];
+        gw[d] += wo[k] * dphi[k][d];
+        for (int a = 0; a < dim; a++) g[a * dim + d] += vo[a][k] * dphi[k][d];
+      }
+    }
+    for (int d = 0; d < dim; d++) mod += vg[d] * vg[d];
+    mod = sqrt(mod);
+    double sP = 1.e-20, chi = 0., f[3];
+    for (int a = 0; a < dim; a++)
+      for (int b = 0; b < dim; b++) {
+        const double sss = g[a + b * dim] + g[b + a * dim];
+        sP += sss * sss;
+      }
+    for (int d = 0; d < dim; d++) {
+      f[d] = upwind_f(KW_UP_WIND, 1., mod, h[d], IRe);
+      chi += gk[d] * gw[d];
+    }
+    kw_model(kg, kg[1], sP, chi, IRe, &cf);
+    const double ire = cf.ire[var];
+    for (int i = 0; i < nen; i++) {
+      const double dt = JxW * bcv[i];
+      if (mode == 1) Fe[i] += dt * (kg[var] * phi[i] * idt + cf.src[var] * phi[i] + cf.cross * var * phi[i]);
+      for (int j = 0; j < nen; j++) {
+        double adv = 0., lap = 0.;
+        for (int d = 0; d < dim; d++) {
+          adv += vg[d] * dphi[j][d];
+          lap += (ire + f[d] * vg[d] * vg[d]) * dphi[j][d] * dphi[i][d];
+        }
+        Ke[i * nen + j] += dt * (phi[j] * phi[i] * idt + adv * phi[i] + lap + cf.diss[var] * phi[j] * phi[i]);
+      }
+    }
+  }
+  /* boundary sides (MGSolverTBKW.C:305-412); IRe_eff is the last Gauss point's */
+  for (int sd = 0; sd < m->nsides; sd++) {
+    if (m->neigh[lev][(long)e * m->nsides + sd] != -1) continue;
+    const int *sur = dim == 2 ? Q9_SIDE[sd] : H27_FACE[sd];
+    int nsn = m->nsn;
+    double xb[3 * 9];
+    for (int k = 0; k < nsn; k++)
+      for (int d = 0; d < dim; d++) xb[d * nsn + k] = xx[d * nen + sur[k]];
+    int last = sur[nsn - 1];
+    if (bcv[last] == 0) {
+      const double ipen = jac_sur(t, t->sng - 1, xb, nsn) * idt;
+      const double wall = 6. * nu_wall / (KW_BETASTAR * y * y);
+      for (int k = 0; k < nsn; k++) {
+        int lv = sur[k];
+        int bs = bcb[lv], bc_rhs = (bs & 2) >> 1, bc_n = bs % 2;
+        double kw = vold[lv] < 1.e-20 ? 1.e-20 : vold[lv];
+        if (mode == 1) Fe[lv] += ipen * (bc_n * (1 - bc_rhs) * kw + (1 - bc_n) * bc_rhs * (var * wall));
+        Ke[lv * nen + lv] += ipen;
+      }
+    } else if (bcb[last] != 0) {
+      for (int q = 0; q < t->sng; q++) {
+        double JxW = jac_sur(t, q, xb, nsn) * t->sw[q];
+        for (int i = 0; i < nsn; i++) {
+          int lei = sur[i];
+          double dt = JxW * (bcv[lei] == 0 ? 0 : 1);
+          int bc_n = bcb[lei] % 2;
+          for (int j = 0; j < nsn; j++)
+            Ke[lei * nen + sur[j]] += 2. * cf.ire[var] * dt * t->sphi[q][j] * t->sphi[q][i] * bc_n / y;
+        }
+      }
+    }
+  }
+  for (int i = 0; i < nen; i++) {
+    int gi = dofs[i];
+    if (mode == 1) rhs[gi] += Fe[i];
+    for (int j = 0; j < nen; j++) A->val[find_col(A, gi, dofs[j])] += Ke[i * nen + j];
+  }
+}
+
+/* one level of the variable var of the coupled kappa-omega system on the scalar system
+ * s (kind 0): matrix (and, mode 1, rhs) as or_sys_assemble; dist holds this level's
+ * element wall distances */
+void or_kw_assemble(or_sys *s, int lev, int mode, int var, const or_phys *ph, const double *vel,
+                    const double *kold, const double *wold, const double *dist, double nu_wall) {
+  const or_mesh *m = s->m;
+  int dim = m->dim, nen = m->nen, top = s->nlev - 1;
+  fe_tab t;
+  fe_init(&t, dim);
+  csr *A = &s->A[lev];
+  memset(A->val, 0, (size_t)A->ptr[A->n] * sizeof(double));
+  double *rhs = NULL;
+  if (mode == 1) {
+    rhs = s->b[lev];
+    memset(rhs, 0, s->ndof[lev] * sizeof(double));
+  }
+  const int nel = m->nel[lev], ncol = 1 << dim;
+  for (int c = 0; c < ncol; c++) {
+#pragma omp parallel
+    {
+      double *Ke = (double *)malloc((size_t)nen * nen * sizeof(double));
+      double *Fe = (double *)malloc(nen * sizeof(double));
+#pragma omp for schedule(dynamic, 4)
+      for (int e = 0; e < nel; e++)
+        if (m->ecol[lev][e] == c)
+          kw_element(s, lev, mode, var, ph, vel, kold, wold, dist[e], nu_wall, &t, e, Ke, Fe, rhs);
+      free(Ke);
+      free(Fe);
+    }
+  }
+  if (mode == 1 && lev == top) memcpy(s->rhs, rhs, s->ndof[lev] * sizeof(double));
+  if (lev == 0) s->lu_ok = 0;
+}
+
 void or_sys_get_matrix(const or_sys *s, int lev, double *val) {
   memcpy(val, s->A[lev].val, (size_t)or_sys_nnz(s, lev) * sizeof(double));
 }

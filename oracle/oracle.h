@@ -100,6 +100,10 @@ void or_sys_colours(const or_sys *s, int lev, int *ncol, int *colour_of_item);
 void or_sys_assemble(or_sys *s, int lev, int mode, const or_phys *ph,
                      const double *xold, const double *vel, const double *temp,
                      const double *qe);
+/* one level of variable var (0 kappa, 1 omega) of the coupled kappa-omega system of the
+ * turbulence template on a scalar system (MGSolTBK::GenMatRhs) */
+void or_kw_assemble(or_sys *s, int lev, int mode, int var, const or_phys *ph, const double *vel,
+                    const double *kold, const double *wold, const double *dist, double nu_wall);
 void or_sys_get_matrix(const or_sys *s, int lev, double *val);
 void or_sys_set_matrix(or_sys *s, int lev, const double *val);
 void or_sys_get_rhs(const or_sys *s, double *rhs);

@@ -76,6 +76,7 @@ def oracle_lib():
         L.or_sys_rest.argtypes = [P, I, ip, ip, dp]
         L.or_sys_colours.argtypes = [P, I, C.POINTER(C.c_int), ip]
         L.or_sys_assemble.argtypes = [P, I, I, C.POINTER(OrPhys), P, P, P, P]
+        L.or_kw_assemble.argtypes = [P, I, I, I, C.POINTER(OrPhys), P, P, P, P, C.c_double]
         L.or_sys_get_matrix.argtypes = [P, I, dp]
         L.or_sys_set_matrix.argtypes = [P, I, dp]
         L.or_sys_get_rhs.argtypes = [P, dp]
@@ -224,6 +225,13 @@ class OrSys:
     def assemble(self, lev, mode, phys, xold=None, vel=None, temp=None, qe=None):
         keep = [None if a is None else np.ascontiguousarray(a, np.float64) for a in (xold, vel, temp, qe)]
         self.L.or_sys_assemble(self.h, lev, mode, C.byref(phys), *[_ptr(a) for a in keep])
+
+    def kw_assemble(self, lev, mode, var, phys, vel, kold, wold, dist, nu_wall):
+        """Level lev of variable var (0 kappa, 1 omega) of the turbulence template's
+        kappa-omega system on this scalar system; dist: this level's element wall
+        distances."""
+        keep = [None if a is None else np.ascontiguousarray(a, np.float64) for a in (vel, kold, wold, dist)]
+        self.L.or_kw_assemble(self.h, lev, mode, var, C.byref(phys), *[_ptr(a) for a in keep], float(nu_wall))
 
     def assemble_all(self, phys, xold=None, vel=None, temp=None, qe=None):
         top = self.mesh.nlev - 1
