@@ -763,7 +763,9 @@ int exf_sys_couple(exf_sys *s, exf_sys *other) {
     return EXF_ERR_ARG;
   }
   const bool kw = s->kind == EXF_KIND_K || s->kind == EXF_KIND_W;
-  if (kw && other && (other->kind == EXF_KIND_K || other->kind == EXF_KIND_W)) {
+  if (s->kind == EXF_KIND_NS && other && (other->kind == EXF_KIND_K || other->kind == EXF_KIND_W)) {
+    (other->kind == EXF_KIND_K ? s->ns_k : s->ns_w) = other;  // the eddy viscosity's fields
+  } else if (kw && other && (other->kind == EXF_KIND_K || other->kind == EXF_KIND_W)) {
     if (other->kind == s->kind) {
       set_error("a kappa (omega) system couples to an omega (kappa) system");
       return EXF_ERR_ARG;

@@ -151,6 +151,7 @@ struct AsmArgs {
   const double *vel;     // coupled NS x_old (top) for T, or null
   int vel_Ntop;
   const double *temp;    // coupled T x_old (top) for NS buoyancy, or null
+  const double *kold, *wold;  // NS: kappa, omega x_old (top) of the eddy viscosity, or null
   const double *qe;      // per top element source (T), or null
   const int *qq_ptr, *ql_ptr;
   const uint8_t *pos_qq, *pos_ql;
@@ -222,6 +223,7 @@ __device__ __forceinline__ void assemble_element(const AsmArgs<DIM> &A, const in
   __shared__ double s_h[DIM];
   __shared__ double s_J[NQ][DIM * DIM];  // Jacobian entries per Gauss point
   __shared__ double s_vg[NQ][DIM + 1];   // velocity (and temperature) at each Gauss point
+  __shared__ double s_kt[NEN], s_wt[NEN];  // NS with the eddy viscosity: kappa, omega
 
   const FETab<DIM> *t = A.tab;
   // ---- element data (get_el_dof_bc, get_el_sol)
@@ -247,6 +249,10 @@ __device__ __forceinline__ void assemble_element(const AsmArgs<DIM> &A, const in
     }
     if (ns) s_told[k] = A.temp ? A.temp[nd] : 0.;
     else s_told[k] = s_uold[0][k];
+    if (ns && A.kold) {
+      s_kt[k] = A.kold[nd];
+      s_wt[k] = A.wold[nd];
+    }
   }
   for (int i = tid; i < NQ * NEN; i += NT) (&s_phi[0][0])[i] = (&t->phi[0][0])[i];
   for (int i = tid; i < NQ * NVX; i += NT) (&s_psi[0][0])[i] = (&t->psi[0][0])[i];
@@ -359,6 +365,43 @@ __device__ __forceinline__ void assemble_element(const AsmArgs<DIM> &A, const in
     }
   }
   __syncthreads();
+  if (ns && A.kold) {
+    // the turbulence template's momentum equation (template_appl/turb-ckw/SRC/
+    // MGSolverNS.C:256-293, f_mu :685-760): IRe_eff = IRe (1 + mu_t) in the viscous terms,
+    // the upwind Peclet number keeps IRe; kappa-omega, WILCOX and LOWRE: tau = 1/omega,
+    // Re_t = kappa tau / IRe, mu_t = alpha* Re_t capped by nut2 / IRe, then clamped
+    for (int q = tid; q < NQ; q += NT) {
+      double g[DIM][DIM], kg = 0., wg = 0.;
+      for (int a = 0; a < DIM; a++)
+        for (int d = 0; d < DIM; d++) g[a][d] = 0.;
+      for (int k = 0; k < NEN; k++) {
+        kg += s_phi[q][k] * s_kt[k];
+        wg += s_phi[q][k] * s_wt[k];
+        for (int a = 0; a < DIM; a++)
+          for (int d = 0; d < DIM; d++) g[a][d] += s_uold[a][k] * s_dphi[q][k][d];
+      }
+      double sP = 1.e-20;
+      for (int a = 0; a < DIM; a++)
+        for (int b = 0; b < DIM; b++) {
+          const double sss = g[a][b] + g[b][a];
+          sP += sss * sss;
+        }
+      if (kg < 1.e-20) kg = 1.e-20;
+      if (wg < 1.e-20) wg = 1.e-20;
+      const double IRe = ph.inv_re, Re_t = kg * (1. / wg) / IRe;
+      const double astar = (0.024 + 0.166666666667 * Re_t) / (1. + 0.166666666667 * Re_t);
+      double mu_t = Re_t * astar;
+      const double nut2 = kg / (7. * sqrt(astar * 0.5 * sP / 0.09) / 8.);
+      if (mu_t * IRe > nut2) mu_t = nut2 / IRe;
+      mu_t = fmin(fmax(mu_t, 1.e-6), 1.e+6);
+      const double add = s_JxW[q] * ph.rho * IRe * mu_t;
+      for (int a = 0; a < DIM; a++) {
+        s_cL[q][a] += add;
+        for (int b = 0; b < DIM; b++) s_cT[q][a * DIM + b] += add;
+      }
+    }
+    __syncthreads();
+  }
 
   // ---- volume integrals, node pairs (i,j)
   const int *qq_ptr = A.qq_ptr;
@@ -623,6 +666,11 @@ static int level_args(exf_sys *s, const exf_phys *ph, int lev, int mode, AsmArgs
     a.vel_Ntop = s->other->L[top].N;
   }
   if (s->other && s->kind == EXF_KIND_NS && s->other->kind == EXF_KIND_T) a.temp = s->other->xold.p;
+  a.kold = a.wold = nullptr;
+  if (s->kind == EXF_KIND_NS && s->ns_k && s->ns_w) {
+    a.kold = s->ns_k->xold.p;
+    a.wold = s->ns_w->xold.p;
+  }
   a.qe = (lev == top && s->kind == EXF_KIND_T) ? s->src_qe.p : nullptr;
   a.qq_ptr = L.qq_ptr.p;
   a.ql_ptr = L.ql_ptr.p;

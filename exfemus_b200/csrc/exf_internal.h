@@ -293,6 +293,7 @@ struct exf_sys {
   int transposed = 0;
   exf_sys *other = nullptr;                 // coupled system (T <- NS velocity, NS <- T)
   exf_sys *turb = nullptr;                  // kappa <-> omega partner of a K / W system
+  exf_sys *ns_k = nullptr, *ns_w = nullptr; // NS: the kappa and omega systems of the eddy viscosity
   exf::DBuf<double> wall_dist;              // K / W: element wall distances, all levels
   std::vector<long> wall_off;               // first element of each level in wall_dist
   double nu_wall = 0.;

@@ -434,6 +434,7 @@ struct or_sys {
   int *ncolour;
   int **col_items;  /* per level: items grouped by colour, ascending within a colour */
   int **col_off;    /* per level: [ncolour+1] offsets into col_items */
+  const double *turb_k, *turb_w; /* NS: kappa, omega x_old [Ntop] of the turbulence model */
 };
 
 static void csr_alloc(csr *c, int n, long nnz) {
@@ -952,6 +953,56 @@ static void side_normal(int dim, const double *xb, int nsn, double *nrm) {
   for (int d = 0; d < dim; d++) nrm[d] /= mm;
 }
 
+/* the turbulence template's model constants (template_appl/turb-ckw/DATA/
+ * MGSclass_conf.h:296-356: WILCOX, LOWRE) */
+#define KW_SIGMA_K 0.6
+#define KW_SIGMA_W 0.5
+#define KW_BETASTAR 0.09
+#define KW_MAX_TAU 100.
+#define KW_MU_LOW 1.e-6
+#define KW_MU_TOP 1.e+6
+#define KW_UP_WIND 1.
+
+/* IRe_eff = IRe (1 + mu_t) of the turbulence template's Navier-Stokes equation
+ * (template_appl/turb-ckw/SRC/MGSolverNS.C:256-293) with its kappa-omega f_mu (:685-760:
+ * tau = 1/omega, Re_t = kappa tau / IRe, WILCOX with LOWRE: mu_t = alpha* Re_t, capped by
+ * nut2 / IRe, clamped to [MU_LOW, MU_TOP]) at one Gauss point; S from the velocity
+ * gradients of the NS x_old */
+static double ns_eddy_viscosity(const or_sys *s, const or_phys *ph, const int *c, double (*uold)[MAXEN],
+                                double (*dphi)[3], const double *phi, int nen, int dim) {
+  const double IRe = ph->inv_re;
+  double g[9] = {0}, kg = 0., wg = 0.;
+  for (int k = 0; k < nen; k++) {
+    kg += phi[k] * s->turb_k[c[k]];
+    wg += phi[k] * s->turb_w[c[k]];
+    for (int a = 0; a < dim; a++)
+      for (int d = 0; d < dim; d++) g[a * dim + d] += uold[a][k] * dphi[k][d];
+  }
+  double sP = 1.e-20;
+  for (int a = 0; a < dim; a++)
+    for (int b = 0; b < dim; b++) {
+      const double sss = g[a + b * dim] + g[b + a * dim];
+      sP += sss * sss;
+    }
+  if (kg < 1.e-20) kg = 1.e-20;
+  if (wg < 1.e-20) wg = 1.e-20;
+  const double tau_k = 1. / wg;
+  const double Re_t = kg * tau_k / IRe;
+  double mu_t = Re_t;
+  const double alpha_star = (0.024 + 0.166666666667 * Re_t) / (1. + 0.166666666667 * Re_t);
+  mu_t *= alpha_star;
+  const double nut2 = kg / (7. * sqrt(alpha_star * 0.5 * sP / KW_BETASTAR) / 8.);
+  if (mu_t * IRe > nut2) mu_t = nut2 / IRe;
+  if (mu_t > KW_MU_TOP) mu_t = KW_MU_TOP;
+  if (mu_t < KW_MU_LOW) mu_t = KW_MU_LOW;
+  return IRe * (1. + mu_t);
+}
+
+void or_sys_set_turb(or_sys *s, const double *kold, const double *wold) {
+  s->turb_k = kold;
+  s->turb_w = wold;
+}
+
 /* One element of MGSolT::GenMatRhs (template_appl/nse/SRC/MGSolverT.C:93-525) or
  * MGSolNS::GenMatRhs (template_appl/nse/SRC/MGSolverNS.C:108-717): local matrix and rhs,
  * boundary sides, scatter into the level matrix (A[Level]->add_matrix) and rhs. */
@@ -1047,6 +1098,7 @@ static void asm_element(or_sys *s, int lev, int mode, const or_phys *ph, const d
       for (int k = 0; k < nen; k++) tg += phi[k] * told[k];
       const double *psi = t->psi[q];
       double nu = ph->inv_re, rho = ph->rho;
+      if (s->turb_k && s->turb_w) nu = ns_eddy_viscosity(s, ph, c, uold, dphi, phi, nen, dim);
       for (int i = 0; i < nen; i++) {
         for (int a = 0; a < dim; a++) {
           int row = a * nen + i;
@@ -1220,13 +1272,6 @@ void or_sys_assemble(or_sys *s, int lev, int mode, const or_phys *ph, const doub
  * its rhs.  Fields: vel = the Navier-Stokes x_old [dim][Ntop], kold / wold = the kappa and
  * omega x_old [Ntop], dist = the element wall distances of this level (_mgmesh._dist),
  * nu_wall = _muf / _rhof of the omega wall value. */
-#define KW_SIGMA_K 0.6
-#define KW_SIGMA_W 0.5
-#define KW_BETASTAR 0.09
-#define KW_MAX_TAU 100.
-#define KW_MU_LOW 1.e-6
-#define KW_MU_TOP 1.e+6
-#define KW_UP_WIND 1.
 
 typedef struct {
   double ire[2], src[2], diss[2], cross;

@@ -100,6 +100,9 @@ void or_sys_colours(const or_sys *s, int lev, int *ncol, int *colour_of_item);
 void or_sys_assemble(or_sys *s, int lev, int mode, const or_phys *ph,
                      const double *xold, const double *vel, const double *temp,
                      const double *qe);
+/* Navier-Stokes systems: kappa and omega x_old [Ntop] of the turbulence model, whose eddy
+ * viscosity then enters the momentum equation (NULL: laminar) */
+void or_sys_set_turb(or_sys *s, const double *kold, const double *wold);
 /* one level of variable var (0 kappa, 1 omega) of the coupled kappa-omega system of the
  * turbulence template on a scalar system (MGSolTBK::GenMatRhs) */
 void or_kw_assemble(or_sys *s, int lev, int mode, int var, const or_phys *ph, const double *vel,

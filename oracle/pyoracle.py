@@ -77,6 +77,7 @@ def oracle_lib():
         L.or_sys_colours.argtypes = [P, I, C.POINTER(C.c_int), ip]
         L.or_sys_assemble.argtypes = [P, I, I, C.POINTER(OrPhys), P, P, P, P]
         L.or_kw_assemble.argtypes = [P, I, I, I, C.POINTER(OrPhys), P, P, P, P, C.c_double]
+        L.or_sys_set_turb.argtypes = [P, P, P]
         L.or_sys_get_matrix.argtypes = [P, I, dp]
         L.or_sys_set_matrix.argtypes = [P, I, dp]
         L.or_sys_get_rhs.argtypes = [P, dp]
@@ -225,6 +226,11 @@ class OrSys:
     def assemble(self, lev, mode, phys, xold=None, vel=None, temp=None, qe=None):
         keep = [None if a is None else np.ascontiguousarray(a, np.float64) for a in (xold, vel, temp, qe)]
         self.L.or_sys_assemble(self.h, lev, mode, C.byref(phys), *[_ptr(a) for a in keep])
+
+    def set_turb(self, kold, wold):
+        """NS: the kappa, omega fields of the eddy viscosity (kept alive here)."""
+        self._turb = [np.ascontiguousarray(a, np.float64) for a in (kold, wold)]
+        self.L.or_sys_set_turb(self.h, *[_ptr(a) for a in self._turb])
 
     def kw_assemble(self, lev, mode, var, phys, vel, kold, wold, dist, nu_wall):
         """Level lev of variable var (0 kappa, 1 omega) of the turbulence template's

@@ -132,3 +132,41 @@ def test_kappa_omega_needs_partner_and_wall(gpu_lib):
     with pytest.raises(_lib.ExfError) as e:
         s.set_wall(np.zeros(m.nel(0) + m.nel(1)), 1e-3)  # distances must be positive
     assert e.value.code == _lib.EXF_ERR_ARG
+
+
+def test_eddy_viscosity_in_the_momentum_equation_matches_the_oracle(gpu_lib, oracle_mod, kw_case):
+    """The NS system coupled to the kappa and omega systems assembles the turbulence
+    template's momentum equation (IRe_eff = IRe (1 + mu_t)) on every level, as the
+    oracle does with the same fields; without them it stays laminar."""
+    m, nlev = kw_case["mesh"], kw_case["nlev"]
+    xyz = m.xyz()
+    u, v, k, w = fields(xyz)
+    N = m.ntop
+    ph = ex.phys(inv_re=0.01, inv_dt=10.0)
+
+    def gpu_ns(turb):
+        ns = ex.MGSolNS(m)
+        ns.GenBc(_lib.BC_CHANNEL)
+        x = np.zeros(ns.ntop_dof)
+        x[:N], x[N:2 * N] = u, v
+        ns.set_xold(x)
+        ns.phys = ph
+        if turb:
+            for s in kw_case["sys"]:
+                ns.couple(s)
+        ns.assemble_all()
+        return ns, x
+
+    ns, x = gpu_ns(True)
+    lam, _ = gpu_ns(False)
+    om = oracle_mod.OrMesh(2, nlev, (4, 2), BOX)
+    o = oracle_mod.OrSys(om, 1)
+    o.bc_preset(_lib.BC_CHANNEL)
+    o.set_turb(k, w)
+    o.assemble_all(or_phys(oracle_mod, inv_re=0.01, inv_dt=10.0), xold=x)
+    for lev in range(nlev):
+        _, _, val = ns.csr(lev)
+        _, _, oval = o.csr(lev)
+        assert rel(val, oval) <= 1e-12, lev
+        assert rel(lam.csr(lev)[2], val) > 1e-6  # the eddy viscosity changed the operator
+    assert rel(ns.rhs(), o.rhs()) <= 1e-12
