@@ -272,7 +272,10 @@ EXF_API int exf_sys_get_transfer(exf_sys *s, int lev, int kind, int block, int d
  * EXF_ERR_ARG with the first differing row otherwise */
 EXF_API int exf_sys_check_pattern(exf_sys *s, int lev, int block, const int dim[2], const int *len, const int *pos);
 /* coupling: T reads the NS velocity, NS reads T for buoyancy (get_el_sol of the
- * other equation, src/MGSolverBase.C:336-354) */
+ * other equation, src/MGSolverBase.C:336-354); a kappa / omega system reads the NS
+ * velocity and the other turbulence variable; NS coupled to both kappa and omega
+ * systems takes the eddy viscosity IRe (1 + mu_t) of the turbulence template
+ * (template_appl/turb-ckw/SRC/MGSolverNS.C:256-293) */
 EXF_API int exf_sys_couple(exf_sys *s, exf_sys *other);
 /* kappa / omega systems: the wall distance of every element (_mgmesh._dist: level 0's
  * elements first, then level 1's, ...) and nu_wall = mu / rho of the omega wall value
