@@ -356,6 +356,64 @@ def run_gmres(args, local):
     gmres_line("bouss2d_T", tb, case["w"]["nlev"] - 1, gs=(stg.cycles, stg.seconds))
 
 
+def run_kw(args, local):
+    """The turbulence template's kappa-omega equations on a 2D channel (0,2) x (0,1),
+    128 x 64 quad9, 6 levels: a parabolic Navier-Stokes velocity, kappa and omega systems
+    (no-slip walls with omega's wall value, inlet on the old value, Neumann outlet,
+    element-centroid wall distances), the NS system with their eddy viscosity; the
+    device time of each assembly of all levels and of the kappa and omega solves to
+    1e-10 (multigrid, Gauss-Seidel 2/2)."""
+    import ctypes as C
+    import exfemus_b200 as ex
+    from exfemus_b200 import _lib
+    L = ex.load()
+    nlev, n0, box = 6, (4, 2), (0.0, 2.0, 0.0, 1.0)
+    m = ex.Mesh(2, nlev, n0, box, device=local)
+    x, y = m.xyz()
+    N = m.ntop
+    ph = ex.phys(inv_re=0.01, inv_dt=10.0)
+    ns = ex.MGSolNS(m)
+    ns.GenBc(_lib.BC_CHANNEL)
+    xns = np.zeros(ns.ntop_dof)
+    xns[:N] = 4.0 * y * (1.0 - y)
+    ns.set_xold(xns)
+    ns.phys = ph
+    b0, b1 = np.ones(N, np.int32), np.zeros(N, np.int32)
+    b1[np.abs(x - box[1]) < 1e-12] = 1
+    inl = np.abs(x - box[0]) < 1e-12
+    b0[inl], b1[inl] = 0, 1
+    wall = (np.abs(y - box[2]) < 1e-12) | (np.abs(y - box[3]) < 1e-12)
+    b0[wall], b1[wall] = 0, 2
+    dist = np.concatenate([np.minimum(y[c].mean(axis=1) - box[2], box[3] - y[c].mean(axis=1))
+                           for c in (m.conn(l)[0] for l in range(nlev))])
+    tk = []
+    for var, old in ((0, 0.01 + 0.02 * y * (1.0 - y)), (1, 40.0 + 30.0 * (y - 0.5) ** 2)):
+        s = ex.MGSolTBK(m, var)
+        s.set_bc(b0, b1)
+        s.set_xold(old)
+        s.set_wall(dist, 0.01)
+        s.phys = ph
+        tk.append(s)
+    for s, o in ((tk[0], tk[1]), (tk[1], tk[0])):
+        s.couple(ns)
+        s.couple(o)
+        ns.couple(s)
+    ms = C.c_double()
+    out = {"workload": "channel2d_kw", "mesh": "128x64 quad9, 6 levels", "ndof_per_variable": tk[0].ntop_dof}
+    for name, s in (("kappa", tk[0]), ("omega", tk[1]), ("ns_eddy", ns)):
+        for rep in range(2):  # the second call is timed
+            _lib.check(L.exf_event_record(s.h, 0))
+            s.assemble_all()
+            _lib.check(L.exf_event_record(s.h, 1))
+            _lib.check(L.exf_event_elapsed(s.h, 0, 1, C.byref(ms)))
+        out[name + "_assembly_ms"] = ms.value
+    for name, s in (("kappa", tk[0]), ("omega", tk[1])):
+        s.set_x(np.zeros(s.ntop_dof))
+        st = s.solve(ex.mg_params(eps=1e-10, max_cycles=200, smoother=_lib.SMOOTH_GS))
+        out[name + "_cycles"], out[name + "_solve_s"], out[name + "_rel_res"] = st.cycles, st.seconds, st.rel_res
+    print(json.dumps(out), flush=True)
+
+
 def run_workloads(args, local):
     """Every workload at its full size (one GPU): Picard steps with per-step cycles and
     device seconds; the adjoint gradient's cost against the forward solve and its
@@ -467,6 +525,7 @@ def run_workloads(args, local):
                       "fd_rel_err_max": float(max(errs)), "fd_directions": len(errs), "fd_h": h}), flush=True)
 
     run_gmres(args, local)
+    run_kw(args, local)
 
 
 def run_ours(args, ws, rank, local):
