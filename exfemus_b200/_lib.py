@@ -126,6 +126,7 @@ SIGNATURES = [
     ("exf_sys_get_colours", _I, [_P, _I, _IP, _IP]),
     ("exf_sys_couple", _I, [_P, _P]),
     ("exf_sys_set_wall", _I, [_P, _DP, C.c_double]),
+    ("exf_mesh_wall_dist", _I, [_P, _IP, _DP]),
     ("exf_sys_set_xold", _I, [_P, _DP]),
     ("exf_sys_get_xold", _I, [_P, _DP]),
     ("exf_sys_set_x", _I, [_P, _DP]),

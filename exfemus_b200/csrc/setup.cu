@@ -826,4 +826,71 @@ int update_rmask(exf_sys *s) {
   return EXF_OK;
 }
 
+// ---------------------------------------------------------------- wall distances
+// MGMesh::B_dist (src/MGMesh.C:1285-1350): per element of a level, the distance from its
+// centre (the mean of its Q2 nodes) to the nearest centre (the mean of the side's nodes) of
+// a wall side of the same level; one thread per element, the sides' centres in order
+__global__ void k_wall_dist(int nel, int nen, const int *__restrict__ conn, const double *__restrict__ xyz, int ntop,
+                            int dim, const double *__restrict__ wc, int nw, double *__restrict__ dist) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= nel) return;
+  double xm[3] = {0., 0., 0.};
+  for (int d = 0; d < dim; d++) {
+    for (int k = 0; k < nen; k++) xm[d] += xyz[conn[(long)e * nen + k] + (long)d * ntop];
+    xm[d] /= nen;
+  }
+  double dmin = 1.e+20;
+  for (int w = 0; w < nw; w++) {
+    double dq = 0.;
+    for (int d = 0; d < dim; d++) {
+      const double t = xm[d] - wc[(long)w * 3 + d];
+      dq += t * t;
+    }
+    if (dq < dmin) dmin = dq;
+  }
+  dist[e] = sqrt(dmin);
+}
+
 }  // namespace exf
+
+using namespace exf;
+
+int exf_mesh_wall_dist(const exf_mesh *m, const int *wall_node, double *dist) {
+  if (!m || !wall_node || !dist) {
+    set_error("exf_mesh_wall_dist: bad argument");
+    return EXF_ERR_ARG;
+  }
+  EXF_CUDA(cudaSetDevice(m->device));
+  const int dim = m->dim, nen = m->nen, nsn = m->nsn, nside = m->nsides;
+  long off = 0;
+  for (int l = 0; l < m->nlev; l++) {
+    const MeshLevel &ml = m->lev[l];
+    // the level's wall sides: boundary sides whose nodes are all wall nodes, centres as
+    // the mean of the side's nodes (the boundary element's NDOF_FEMB nodes)
+    std::vector<double> wc;
+    for (int e = 0; e < ml.nel; e++)
+      for (int sd = 0; sd < nside; sd++) {
+        if (ml.neigh[(size_t)e * nside + sd] != -1) continue;
+        bool wall = true;
+        double c[3] = {0., 0., 0.};
+        for (int k = 0; k < nsn; k++) {
+          const int n = ml.conn[(size_t)e * nen + (dim == 2 ? Q9_SIDE[sd][k] : H27_FACE[sd][k])];
+          wall = wall && wall_node[n] != 0;
+          for (int d = 0; d < dim; d++) c[d] += m->xyz[(size_t)n + (size_t)d * m->ntop];
+        }
+        if (!wall) continue;
+        for (int d = 0; d < 3; d++) wc.push_back(d < dim ? c[d] / nsn : 0.);
+      }
+    DBuf<double> d_wc, d_dist;
+    EXF_TRY(d_wc.alloc(std::max<size_t>(1, wc.size())));
+    EXF_TRY(d_dist.alloc(ml.nel));
+    if (!wc.empty()) EXF_CUDA(cudaMemcpy(d_wc.p, wc.data(), wc.size() * sizeof(double), cudaMemcpyHostToDevice));
+    k_wall_dist<<<(ml.nel + 127) / 128, 128>>>(ml.nel, nen, ml.d_conn.p, m->d_xyz.p, m->ntop, dim, d_wc.p,
+                                               (int)(wc.size() / 3), d_dist.p);
+    EXF_LAUNCH_CHECK();
+    EXF_COUNT(1);
+    EXF_CUDA(cudaMemcpy(dist + off, d_dist.p, ml.nel * sizeof(double), cudaMemcpyDeviceToHost));
+    off += ml.nel;
+  }
+  return EXF_OK;
+}

@@ -134,6 +134,15 @@ class Mesh:
                     neigh=[neigh[off[l]:off[l + 1]] for l in range(nlev)],
                     parent=[None] + [parent[off[l] - off[1]:off[l + 1] - off[1]] for l in range(1, nlev)])
 
+    def wall_dist(self, wall_node):
+        """MGMesh::B_dist: per element of every level (level 0's first) the distance from
+        its centre to the nearest wall-side centre of its level; wall_node [ntop] marks
+        the wall nodes."""
+        w = np.ascontiguousarray(wall_node, np.int32)
+        out = np.zeros(sum(self.nel(l) for l in range(self.nlev)))
+        check(self.L.exf_mesh_wall_dist(self.h, iptr(w), dptr(out)))
+        return out
+
     def close(self):
         if getattr(self, "h", None):
             self.L.exf_mesh_destroy(self.h)

@@ -281,6 +281,11 @@ EXF_API int exf_sys_couple(exf_sys *s, exf_sys *other);
  * elements first, then level 1's, ...) and nu_wall = mu / rho of the omega wall value
  * 6 nu_wall / (BETASTAR y^2) */
 EXF_API int exf_sys_set_wall(exf_sys *s, const double *dist, double nu_wall);
+/* MGMesh::B_dist (src/MGMesh.C:1285-1350): for every element of every level (level 0's
+ * first), the distance from its centre (mean of its nodes) to the nearest centre (mean of
+ * the side's nodes) of a wall side of its level; a boundary side is a wall when all its
+ * nodes have wall_node[n] != 0 (wall_node: [ntop], the reference's user predicate) */
+EXF_API int exf_mesh_wall_dist(const exf_mesh *m, const int *wall_node, double *dist);
 
 /* --- fields (host buffers) ---------------------------------------------------------- */
 EXF_API int exf_sys_set_xold(exf_sys *s, const double *xold);   /* x_old[top]             */

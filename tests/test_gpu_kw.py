@@ -170,3 +170,32 @@ def test_eddy_viscosity_in_the_momentum_equation_matches_the_oracle(gpu_lib, ora
         assert rel(val, oval) <= 1e-12, lev
         assert rel(lam.csr(lev)[2], val) > 1e-6  # the eddy viscosity changed the operator
     assert rel(ns.rhs(), o.rhs()) <= 1e-12
+
+
+def b_dist_here(m, wall_node):
+    """MGMesh::B_dist restated: element centre to the nearest wall-side centre."""
+    xyz = m.xyz()
+    side = [(0, 1, 4), (1, 2, 5), (2, 3, 6), (3, 0, 7)]
+    out = []
+    for lev in range(m.nlev):
+        conn, neigh = m.conn(lev)[:2]
+        wc = []
+        for e in range(conn.shape[0]):
+            for sd in range(4):
+                if neigh[e, sd] == -1 and all(wall_node[conn[e, k]] for k in side[sd]):
+                    wc.append(xyz[:, conn[e, list(side[sd])]].sum(axis=1) / 3)
+        wc = np.array(wc)
+        xm = xyz[:, conn].sum(axis=2) / conn.shape[1]
+        d2 = ((xm.T[:, None, :] - wc[None, :, :]) ** 2).sum(axis=2)
+        out.append(np.sqrt(d2.min(axis=1)))
+    return np.concatenate(out)
+
+
+def test_wall_distances_are_b_dist(gpu_lib, kw_case):
+    m = kw_case["mesh"]
+    x, y = m.xyz()
+    wall = ((np.abs(y) < 1e-12) | (np.abs(y - 1.0) < 1e-12)).astype(np.int32)
+    d = m.wall_dist(wall)
+    assert d.size == sum(m.nel(l) for l in range(m.nlev))
+    assert np.allclose(d, b_dist_here(m, wall), rtol=1e-14, atol=0)
+    assert np.all(d > 0)
