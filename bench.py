@@ -360,7 +360,7 @@ def run_kw(args, local):
     """The turbulence template's kappa-omega equations on a 2D channel (0,2) x (0,1),
     128 x 64 quad9, 6 levels: a parabolic Navier-Stokes velocity, kappa and omega systems
     (no-slip walls with omega's wall value, inlet on the old value, Neumann outlet,
-    element-centroid wall distances), the NS system with their eddy viscosity; the
+    B_dist wall distances), the NS system with their eddy viscosity; the
     device time of each assembly of all levels and of the kappa and omega solves to
     1e-10 (multigrid, Gauss-Seidel 2/2)."""
     import ctypes as C
@@ -384,8 +384,7 @@ def run_kw(args, local):
     b0[inl], b1[inl] = 0, 1
     wall = (np.abs(y - box[2]) < 1e-12) | (np.abs(y - box[3]) < 1e-12)
     b0[wall], b1[wall] = 0, 2
-    dist = np.concatenate([np.minimum(y[c].mean(axis=1) - box[2], box[3] - y[c].mean(axis=1))
-                           for c in (m.conn(l)[0] for l in range(nlev))])
+    dist = m.wall_dist(wall.astype(np.int32))  # MGMesh::B_dist to the no-slip walls
     tk = []
     for var, old in ((0, 0.01 + 0.02 * y * (1.0 - y)), (1, 40.0 + 30.0 * (y - 0.5) ** 2)):
         s = ex.MGSolTBK(m, var)
