@@ -14,54 +14,67 @@ from conftest import or_mg, or_phys, rel
 
 pytestmark = pytest.mark.gpu
 
-BOX = (0.0, 2.0, 0.0, 1.0)
 NU_WALL = 0.01
+# dim: box, levels, level-0 elements (walls: the y and z faces)
+CASES = {2: ((0.0, 2.0, 0.0, 1.0), 3, (4, 2)), 3: ((0.0, 2.0, 0.0, 1.0, 0.0, 1.0), 2, (2, 1, 1))}
+
+
+def on_wall(xyz):
+    w = (np.abs(xyz[1]) < 1e-12) | (np.abs(xyz[1] - 1.0) < 1e-12)
+    if len(xyz) == 3:
+        w |= (np.abs(xyz[2]) < 1e-12) | (np.abs(xyz[2] - 1.0) < 1e-12)
+    return w
 
 
 def flags(xyz):
-    """(bc0, bc1) per node: walls y = 0, 1 Dirichlet (bc1 2: omega's wall value, kappa
-    0), inlet x = 0 Dirichlet on the old value (bc1 1), outlet x = 2 Neumann (bc0 1,
-    bc1 1), interior (1, 0)."""
-    x, y = xyz
+    """(bc0, bc1) per node: walls Dirichlet (bc1 2: omega's wall value, kappa 0), inlet
+    x = 0 Dirichlet on the old value (bc1 1), outlet x = 2 Neumann (bc0 1, bc1 1),
+    interior (1, 0)."""
+    x = xyz[0]
     n = x.size
     b0, b1 = np.ones(n, np.int32), np.zeros(n, np.int32)
-    out = np.abs(x - BOX[1]) < 1e-12
-    b1[out] = 1
-    inl = np.abs(x - BOX[0]) < 1e-12
+    b1[np.abs(x - 2.0) < 1e-12] = 1
+    inl = np.abs(x) < 1e-12
     b0[inl], b1[inl] = 0, 1
-    wall = (np.abs(y - BOX[2]) < 1e-12) | (np.abs(y - BOX[3]) < 1e-12)
+    wall = on_wall(xyz)
     b0[wall], b1[wall] = 0, 2
     return b0, b1
 
 
 def fields(xyz):
-    x, y = xyz
-    u = 4.0 * y * (1.0 - y) * (1.0 + 0.1 * np.sin(2.0 * x))
-    v = 0.05 * np.sin(np.pi * y) * x
+    """Velocity components, kappa, omega at the nodes."""
+    x, y = xyz[0], xyz[1]
+    zf = 4.0 * xyz[2] * (1.0 - xyz[2]) if len(xyz) == 3 else 1.0
+    u = 4.0 * y * (1.0 - y) * zf * (1.0 + 0.1 * np.sin(2.0 * x))
+    vel = [u, 0.05 * np.sin(np.pi * y) * x]
+    if len(xyz) == 3:
+        vel.append(0.03 * np.sin(np.pi * xyz[2]) * y)
     k = 0.01 + 0.02 * y * (1.0 - y) * (1.0 + 0.2 * x)
     w = 40.0 + 30.0 * (y - 0.5) ** 2 + 2.0 * x
-    return u, v, k, w
+    return vel, k, w
 
 
 def wall_dist(conns, xyz):
-    """Centroid distance of every element to the nearest wall, level after level."""
+    """Centroid distance of every element to the nearest wall plane, level after level."""
     d = []
     for c in conns:
-        yc = xyz[1][c].mean(axis=1)
-        d.append(np.minimum(yc - BOX[2], BOX[3] - yc))
+        cen = [xyz[a][c].mean(axis=1) for a in range(1, len(xyz))]
+        d.append(np.min([np.minimum(q, 1.0 - q) for q in cen], axis=0))
     return np.concatenate(d)
 
 
-@pytest.fixture(scope="module")
-def kw_case(oracle_mod):
-    nlev, n0 = 3, (4, 2)
-    m = ex.Mesh(2, nlev, n0, BOX)
+@pytest.fixture(scope="module", params=[2, 3])
+def kw_case(oracle_mod, request):
+    dim = request.param
+    box, nlev, n0 = CASES[dim]
+    m = ex.Mesh(dim, nlev, n0, box)
     xyz = m.xyz()
     N = m.ntop
-    u, v, k, w = fields(xyz)
+    vel, k, w = fields(xyz)
     ns = ex.MGSolNS(m)
     xns = np.zeros(ns.ntop_dof)
-    xns[:N], xns[N:2 * N] = u, v
+    for a in range(dim):
+        xns[a * N:(a + 1) * N] = vel[a]
     ns.set_xold(xns)
     ph = ex.phys(inv_re=0.01, inv_dt=10.0)
     conns = [m.conn(l)[0] for l in range(nlev)]
@@ -78,7 +91,7 @@ def kw_case(oracle_mod):
     for s, other in ((sys[0], sys[1]), (sys[1], sys[0])):
         s.couple(ns)
         s.couple(other)
-    om = oracle_mod.OrMesh(2, nlev, n0, BOX)
+    om = oracle_mod.OrMesh(dim, nlev, n0, box)
     osys = []
     oph = or_phys(oracle_mod, inv_re=0.01, inv_dt=10.0)
     off = np.cumsum([0] + [c.shape[0] for c in conns])
@@ -86,10 +99,10 @@ def kw_case(oracle_mod):
         o = oracle_mod.OrSys(om, 0)
         o.set_bc(b0, b1)
         for lev in range(nlev):
-            o.kw_assemble(lev, 1 if lev == nlev - 1 else 0, var, oph, xns[:2 * N], k, w,
+            o.kw_assemble(lev, 1 if lev == nlev - 1 else 0, var, oph, xns[:dim * N], k, w,
                           dist[off[lev]:off[lev + 1]], NU_WALL)
         osys.append(o)
-    return dict(mesh=m, ns=ns, sys=sys, osys=osys, nlev=nlev)
+    return dict(mesh=m, ns=ns, sys=sys, osys=osys, nlev=nlev, dim=dim, box=box, n0=n0)
 
 
 def test_kappa_omega_assembly_matches_the_oracle(gpu_lib, kw_case):
@@ -112,10 +125,8 @@ def test_kappa_omega_solves_match_the_oracle(gpu_lib, oracle_mod, kw_case):
         xo, sto = o.mg_solve(or_mg(oracle_mod, eps=1e-11, max_cycles=100))
         assert st.converged and sto.converged
         assert rel(s.x(), xo) <= 1e-9, s.var
-    xk, xw = kw_case["sys"][0].x(), kw_case["sys"][1].x()
-    xyz = kw_case["mesh"].xyz()
-    wall = (np.abs(xyz[1]) < 1e-12) | (np.abs(xyz[1] - 1.0) < 1e-12)
-    assert np.abs(xk[wall]).max() < 1e-10  # kappa = 0 on the no-slip walls
+    xk = kw_case["sys"][0].x()
+    assert np.abs(xk[on_wall(kw_case["mesh"].xyz())]).max() < 1e-10  # kappa = 0 on the walls
 
 
 def test_kappa_omega_needs_partner_and_wall(gpu_lib):
@@ -138,9 +149,9 @@ def test_eddy_viscosity_in_the_momentum_equation_matches_the_oracle(gpu_lib, ora
     """The NS system coupled to the kappa and omega systems assembles the turbulence
     template's momentum equation (IRe_eff = IRe (1 + mu_t)) on every level, as the
     oracle does with the same fields; without them it stays laminar."""
-    m, nlev = kw_case["mesh"], kw_case["nlev"]
+    m, nlev, dim = kw_case["mesh"], kw_case["nlev"], kw_case["dim"]
     xyz = m.xyz()
-    u, v, k, w = fields(xyz)
+    vel, k, w = fields(xyz)
     N = m.ntop
     ph = ex.phys(inv_re=0.01, inv_dt=10.0)
 
@@ -148,7 +159,8 @@ def test_eddy_viscosity_in_the_momentum_equation_matches_the_oracle(gpu_lib, ora
         ns = ex.MGSolNS(m)
         ns.GenBc(_lib.BC_CHANNEL)
         x = np.zeros(ns.ntop_dof)
-        x[:N], x[N:2 * N] = u, v
+        for a in range(dim):
+            x[a * N:(a + 1) * N] = vel[a]
         ns.set_xold(x)
         ns.phys = ph
         if turb:
@@ -159,7 +171,7 @@ def test_eddy_viscosity_in_the_momentum_equation_matches_the_oracle(gpu_lib, ora
 
     ns, x = gpu_ns(True)
     lam, _ = gpu_ns(False)
-    om = oracle_mod.OrMesh(2, nlev, (4, 2), BOX)
+    om = oracle_mod.OrMesh(dim, nlev, kw_case["n0"], kw_case["box"])
     o = oracle_mod.OrSys(om, 1)
     o.bc_preset(_lib.BC_CHANNEL)
     o.set_turb(k, w)
@@ -192,9 +204,10 @@ def b_dist_here(m, wall_node):
 
 
 def test_wall_distances_are_b_dist(gpu_lib, kw_case):
+    if kw_case["dim"] != 2:
+        pytest.skip("the restatement here walks quad9 sides")
     m = kw_case["mesh"]
-    x, y = m.xyz()
-    wall = ((np.abs(y) < 1e-12) | (np.abs(y - 1.0) < 1e-12)).astype(np.int32)
+    wall = on_wall(m.xyz()).astype(np.int32)
     d = m.wall_dist(wall)
     assert d.size == sum(m.nel(l) for l in range(m.nlev))
     assert np.allclose(d, b_dist_here(m, wall), rtol=1e-14, atol=0)
