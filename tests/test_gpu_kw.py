@@ -212,3 +212,61 @@ def test_wall_distances_are_b_dist(gpu_lib, kw_case):
     assert d.size == sum(m.nel(l) for l in range(m.nlev))
     assert np.allclose(d, b_dist_here(m, wall), rtol=1e-14, atol=0)
     assert np.all(d > 0)
+
+
+def channel_kw_systems(nlev=3):
+    """NS (parabolic start), kappa and omega on the 2D channel, all coupled, eddy
+    viscosity on."""
+    box, _, n0 = CASES[2]
+    m = ex.Mesh(2, nlev, n0, box)
+    xyz = m.xyz()
+    N = m.ntop
+    vel, k, w = fields(xyz)
+    ph = ex.phys(inv_re=0.01, inv_dt=10.0)
+    ns = ex.MGSolNS(m)
+    ns.GenBc(_lib.BC_CHANNEL)
+    x = np.zeros(ns.ntop_dof)
+    x[:N], x[N:2 * N] = vel[0], vel[1]
+    ns.set_xold(x)
+    ns.set_x(x)
+    ns.phys = ph
+    b0, b1 = flags(xyz)
+    dist = m.wall_dist(on_wall(xyz).astype(np.int32))
+    tk = []
+    for var, old in ((0, k), (1, w)):
+        s = ex.MGSolTBK(m, var)
+        s.set_bc(b0, b1)
+        s.set_xold(old)
+        s.set_wall(dist, NU_WALL)
+        s.phys = ph
+        tk.append(s)
+    for s, o in ((tk[0], tk[1]), (tk[1], tk[0])):
+        s.couple(ns)
+        s.couple(o)
+        ns.couple(s)
+    params = [ex.mg_params(eps=1e-10, max_cycles=200, smoother=_lib.SMOOTH_VANKA, nu_pre=3, nu_post=3, omega=0.4)]
+    params += [ex.mg_params(eps=1e-10, max_cycles=200, smoother=_lib.SMOOTH_GS) for _ in tk]
+    return m, [ns] + tk, params
+
+
+def test_turbulent_channel_time_loop_matches_the_host_loop(gpu_lib):
+    """exf_timestep_loop over NS (with the eddy viscosity), kappa and omega gives the bits
+    of the same MGTimeStep sequence driven from here, with the same cycle counts."""
+    _, a, pa = channel_kw_systems()
+    _, b, pb = channel_kw_systems()
+    nsteps = 3
+    host = []
+    for _ in range(nsteps):
+        row = []
+        for s, p in zip(a, pa):
+            s.assemble_all()
+            st = s.solve(p)
+            assert st.converged
+            s.xold_update()
+            row.append(st.cycles)
+        host.append(row)
+    cyc, sec = ex.timestep_loop(b, pb, nsteps)
+    assert cyc.tolist() == host
+    for sa, sb in zip(a, b):
+        assert np.array_equal(sa.x(), sb.x())
+    assert np.all(np.isfinite(b[1].x())) and b[2].x().min() > 0  # omega stays positive
