@@ -185,17 +185,22 @@ def test_eddy_viscosity_in_the_momentum_equation_matches_the_oracle(gpu_lib, ora
 
 
 def b_dist_here(m, wall_node):
-    """MGMesh::B_dist restated: element centre to the nearest wall-side centre."""
+    """MGMesh::B_dist restated: element centre to the nearest wall-side centre; the sides
+    are the reference's _surf_top (tests/golden/mggeomel.json)."""
+    import json
+    import os
+    gold = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "mggeomel.json")))
+    t = gold["quad9_surf_top" if m.dim == 2 else "hex27_surf_top"]
+    side = np.array(t["data"], dtype=int).reshape(t["shape"])
     xyz = m.xyz()
-    side = [(0, 1, 4), (1, 2, 5), (2, 3, 6), (3, 0, 7)]
     out = []
     for lev in range(m.nlev):
         conn, neigh = m.conn(lev)[:2]
         wc = []
         for e in range(conn.shape[0]):
-            for sd in range(4):
+            for sd in range(side.shape[0]):
                 if neigh[e, sd] == -1 and all(wall_node[conn[e, k]] for k in side[sd]):
-                    wc.append(xyz[:, conn[e, list(side[sd])]].sum(axis=1) / 3)
+                    wc.append(xyz[:, conn[e, side[sd]]].sum(axis=1) / side.shape[1])
         wc = np.array(wc)
         xm = xyz[:, conn].sum(axis=2) / conn.shape[1]
         d2 = ((xm.T[:, None, :] - wc[None, :, :]) ** 2).sum(axis=2)
@@ -204,8 +209,6 @@ def b_dist_here(m, wall_node):
 
 
 def test_wall_distances_are_b_dist(gpu_lib, kw_case):
-    if kw_case["dim"] != 2:
-        pytest.skip("the restatement here walks quad9 sides")
     m = kw_case["mesh"]
     wall = on_wall(m.xyz()).astype(np.int32)
     d = m.wall_dist(wall)
