@@ -167,6 +167,8 @@ SIGNATURES = [
     ("exf_sys_check_pattern", _I, [_P, _I, _I, _IP, _IP, _IP]),
     ("exf_write_xdmf", _I, [C.POINTER(ExfNodeFields), C.POINTER(ExfSolnOut)]),
     ("exf_print_soln", _I, [C.POINTER(_P), _I, C.POINTER(C.c_char_p), _DP, C.POINTER(ExfSolnOut)]),
+    ("exf_write_xdmf_case", _I, [C.POINTER(ExfNodeFields), C.POINTER(ExfSolnOut)]),
+    ("exf_print_case", _I, [C.POINTER(_P), _I, C.POINTER(C.c_char_p), _DP, C.POINTER(ExfSolnOut)]),
 ]
 
 

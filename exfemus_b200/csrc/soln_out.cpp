@@ -117,11 +117,15 @@ int write_file(const std::string &path, const std::vector<const void *> &parts, 
 
 using namespace exf;
 
-int exf_write_xdmf(const exf_node_fields *f, const exf_soln_out *o) {
+namespace {
+
+// one XDMF step (case_file: MGEquationsSystem::print_case_xmf, src/MGEquationsSystem.C:
+// 872-935: no <Time>, the coordinates of the base mesh file <basemesh>.bin)
+int write_xdmf_step(const exf_node_fields *f, const exf_soln_out *o, bool case_file) {
   if (!f || !o || (f->dim != 2 && f->dim != 3) || f->nnodes < 1 || f->nel < 1 || !f->xyz || !f->conn ||
       f->nvars < 0 || (f->nvars > 0 && (!f->names || !f->order || !f->vals)) || !o->basesol || !o->basemesh ||
       !o->connlin || o->ndigits < 1 || o->ndigits > 9 || o->t_step < 0) {
-    set_error("exf_write_xdmf: bad argument");
+    set_error(case_file ? "exf_write_xdmf_case: bad argument" : "exf_write_xdmf: bad argument");
     return EXF_ERR_ARG;
   }
   const int dim = f->dim, nen = dim == 2 ? 9 : 27, nvx = 1 << dim, nsub = 1 << dim;
@@ -145,7 +149,7 @@ int exf_write_xdmf(const exf_node_fields *f, const exf_soln_out *o) {
   }
   const std::string step = step_str(o->t_step, o->ndigits);
   const std::string conn_name = std::string(o->basemesh) + o->connlin + ".bin";
-  const std::string coord_name = std::string(o->basemesh) + "." + step + ".bin";
+  const std::string coord_name = std::string(o->basemesh) + (case_file ? "" : "." + step) + ".bin";
   const std::string sol_name = std::string(o->basesol) + "." + step + ".bin";
   const std::string xmf_name = std::string(o->basesol) + "." + step + ".xmf";
 
@@ -197,8 +201,10 @@ int exf_write_xdmf(const exf_node_fields *f, const exf_soln_out *o) {
     x += file + "\n</" + tag + ">\n";
   };
   x += "<?xml version=\"1.0\" ?>\n<Xdmf>\n<Domain>\n<Grid Name=\"Mesh\">\n";
-  snprintf(b, sizeof(b), "<Time Value=\"%.17g\" />\n", o->time);
-  x += b;
+  if (!case_file) {
+    snprintf(b, sizeof(b), "<Time Value=\"%.17g\" />\n", o->time);
+    x += b;
+  }
   snprintf(b, sizeof(b), "<Topology Type=\"%s\" Dimensions=\"%zu\">\n", dim == 2 ? "Quadrilateral" : "Hexahedron",
            nsc);
   x += b;
@@ -215,6 +221,11 @@ int exf_write_xdmf(const exf_node_fields *f, const exf_soln_out *o) {
   x += "</Grid>\n</Domain>\n</Xdmf>\n";
   return write_file(join(o->dir, xmf_name), {x.data()}, {x.size()});
 }
+
+}  // namespace
+
+int exf_write_xdmf(const exf_node_fields *f, const exf_soln_out *o) { return write_xdmf_step(f, o, false); }
+int exf_write_xdmf_case(const exf_node_fields *f, const exf_soln_out *o) { return write_xdmf_step(f, o, true); }
 
 int exf_print_soln(exf_sys *const *sys, int nsys, const char *const *names, const double *refvalue,
                    const exf_soln_out *o) {
@@ -248,7 +259,7 @@ int exf_print_soln(exf_sys *const *sys, int nsys, const char *const *names, cons
       } else if (s->kind == EXF_KIND_NS) {
         nm.push_back(v < s->nv2 ? ns_names[v] : "p");
       } else {
-        nm.push_back(s->nvars == 1 ? "T" : "T" + std::to_string(v));
+        nm.push_back(s->kind == EXF_KIND_K ? "kt" : s->kind == EXF_KIND_W ? "wt" : "T");
       }
       order.push_back(v < s->nv2 ? 2 : 1);
       const double ref = refvalue ? refvalue[var] : 1.;
@@ -274,4 +285,101 @@ int exf_print_soln(exf_sys *const *sys, int nsys, const char *const *names, cons
   f.order = order.data();
   f.vals = vals.data();
   return exf_write_xdmf(&f, o);
+}
+
+// MGEquationsSystem::print_case (src/MGEquationsSystem.C:814-935): the initial state of
+// every variable (x_old, MGSolDA::print_u) with its boundary flags (MGSolDA::print_bc,
+// src/MGSolverDA.C:1418-1520): <name>bd = bc[1] and <name>vl = bc[0] at every node; for a
+// linear variable the vertex flags are carried to the other nodes by the element's linear
+// map and stored as integers (truncated), as print_bc's int buffer does.
+int exf_print_case(exf_sys *const *sys, int nsys, const char *const *names, const double *refvalue,
+                   const exf_soln_out *o) {
+  if (!sys || nsys < 1 || !o) {
+    set_error("exf_print_case: bad argument");
+    return EXF_ERR_ARG;
+  }
+  const exf_mesh *m = nullptr;
+  for (int k = 0; k < nsys; k++) {
+    CHECK_SYS(sys[k]);
+    if (!m) m = sys[k]->mesh;
+    if (sys[k]->mesh != m) {
+      set_error("exf_print_case: system %d lives on another mesh", k);
+      return EXF_ERR_ARG;
+    }
+  }
+  const size_t nn = (size_t)m->ntop;
+  const exf::MeshLevel &T = m->lev[m->nlev - 1];
+  const int nen = m->nen, nvx = m->nvx;
+  const int(*ABC)[3] = m->dim == 2 ? Q9_ABC : H27_ABC;
+  // linear basis of vertex j at node k (0, 1/2, 1 products), as linear_to_nodes
+  std::vector<double> w((size_t)nen * nvx);
+  for (int k = 0; k < nen; k++)
+    for (int j = 0; j < nvx; j++) {
+      double x = 1.;
+      for (int d = 0; d < m->dim; d++) {
+        const int a = ABC[k][d], b = ABC[j][d] / 2;
+        x *= a == 1 ? 0.5 : (a / 2 == b ? 1. : 0.);
+      }
+      w[(size_t)k * nvx + j] = x;
+    }
+  std::vector<std::string> nm;
+  std::vector<int> order;
+  std::vector<double> vals;
+  int var = 0;
+  for (int k = 0; k < nsys; k++) {
+    exf_sys *s = sys[k];
+    std::vector<double> xo(s->L[s->nlev - 1].ndof);
+    EXF_TRY(exf_sys_get_xold(s, xo.data()));
+    const std::vector<int> &nd = s->node_dof[s->nlev - 1];
+    for (int v = 0; v < s->nvars; v++, var++) {
+      static const char *ns_names[4] = {"u", "v", "w", "p"};
+      std::string name;
+      if (names) name = names[var] ? names[var] : "";
+      else if (s->kind == EXF_KIND_NS) name = v < s->nv2 ? ns_names[v] : "p";
+      else name = s->kind == EXF_KIND_K ? "kt" : s->kind == EXF_KIND_W ? "wt" : "T";
+      const bool quad = v < s->nv2;
+      const double ref = refvalue ? refvalue[var] : 1.;
+      std::vector<double> val(nn, 0.), bd(nn, 0.), vl(nn, 0.);
+      for (size_t i = 0; i < nn; i++) {
+        const int d = nd[i + (size_t)v * nn];
+        if (d < 0) continue;
+        val[i] = xo[d] * ref;
+        bd[i] = s->bc1[d];
+        vl[i] = s->bc0[d];
+      }
+      if (!quad)  // the flags of the other nodes from the vertices, truncated to integers
+        for (int e = 0; e < T.nel; e++) {
+          const int *c = &T.conn[(size_t)e * nen];
+          for (double *f : {bd.data(), vl.data()}) {
+            double fc[8];
+            for (int j = 0; j < nvx; j++) fc[j] = f[c[j]];
+            for (int kk = 0; kk < nen; kk++) {
+              double sum = 0.;
+              for (int j = 0; j < nvx; j++) sum += w[(size_t)kk * nvx + j] * fc[j];
+              f[c[kk]] = (double)(int)sum;
+            }
+          }
+        }
+      const std::string names3[3] = {name, name + "bd", name + "vl"};
+      const std::vector<double> *data3[3] = {&val, &bd, &vl};
+      for (int q = 0; q < 3; q++) {
+        nm.push_back(names3[q]);
+        order.push_back(q == 0 && !quad ? 1 : 2);
+        vals.insert(vals.end(), data3[q]->begin(), data3[q]->end());
+      }
+    }
+  }
+  std::vector<const char *> np;
+  for (const std::string &n : nm) np.push_back(n.c_str());
+  exf_node_fields f;
+  f.dim = m->dim;
+  f.nnodes = m->ntop;
+  f.xyz = m->xyz.data();
+  f.nel = T.nel;
+  f.conn = T.conn.data();
+  f.nvars = (int)nm.size();
+  f.names = np.data();
+  f.order = order.data();
+  f.vals = vals.data();
+  return exf_write_xdmf_case(&f, o);
 }

@@ -1,8 +1,10 @@
-"""Solution output: MGEquationsSystem::print_soln (src/MGEquationsSystem.C:606-721) over
-the C ABI, XDMF text over raw binary datasets in place of HDF5 (not installed here).
+"""Solution output: MGEquationsSystem::print_soln (src/MGEquationsSystem.C:606-721) and
+print_case (src/MGEquationsSystem.C:814-935) over the C ABI, XDMF text over raw binary
+datasets in place of HDF5 (not installed here).
 
 print_soln(systems, t_step, time, ...) writes the top level of one or more systems on
-one mesh; write_xdmf(...) writes node fields given as host arrays; read_xdmf(path) loads
+one mesh; print_case(systems, t_step, ...) writes their initial state with the boundary
+flags; write_xdmf(...) writes node fields given as host arrays; read_xdmf(path) loads
 a written step back (coordinates, sub-cell connectivity, node fields) by following the
 XDMF file's Seek offsets, for checks and for restarting from output.
 """
@@ -52,12 +54,33 @@ def print_soln(systems, t_step, time, out_dir="", basesol="sol", basemesh="mesh"
     return xmf_path(t_step, out_dir, basesol, ndigits)
 
 
+def print_case(systems, t_step=0, out_dir="", basecase="case", basemesh="mesh", connlin="_conn_lin",
+               ndigits=4, names=None, refvalue=None):
+    """The initial state (x_old) of every variable of every system with its boundary
+    flags, three node fields per variable: <name> (scaled by refvalue), <name>bd (bc[1],
+    the Dirichlet flag) and <name>vl (bc[0], the value flag); the coordinates are those
+    of <basemesh>.bin and the file has no <Time>.  Returns the XDMF file's path."""
+    L = _lib.load()
+    n = len(systems)
+    hs = (C.c_void_p * n)(*[s.h for s in systems])
+    nm = None
+    if names is not None:
+        nm = (C.c_char_p * len(names))(*[x.encode() for x in names])
+    rv = None
+    if refvalue is not None:
+        rv = np.ascontiguousarray(refvalue, dtype=np.float64)
+    o = _out(t_step, 0.0, out_dir, basecase, basemesh, connlin, ndigits)
+    check(L.exf_print_case(hs, n, nm, None if rv is None else _lib.dptr(rv), C.byref(o)))
+    return xmf_path(t_step, out_dir, basecase, ndigits)
+
+
 def write_xdmf(dim, xyz, conn, fields, t_step=0, time=0.0, out_dir="", basesol="sol", basemesh="mesh",
-               connlin="_conn_lin", ndigits=4):
+               connlin="_conn_lin", ndigits=4, case=False):
     """Node fields on a quad9 / hex27 mesh given as host arrays: xyz [dim][nnodes], conn
     [nel][9 | 27], fields a list of (name, order, values[nnodes]) with order 2 for a
-    quadratic variable and 1 for a linear one (read at the element vertices).  Returns
-    the XDMF file's path."""
+    quadratic variable and 1 for a linear one (read at the element vertices).  case=True
+    writes a case file (the coordinates as <basemesh>.bin, no <Time>).  Returns the XDMF
+    file's path."""
     L = _lib.load()
     xyz = np.ascontiguousarray(xyz, dtype=np.float64)
     conn = np.ascontiguousarray(conn, dtype=np.int32)
@@ -71,7 +94,7 @@ def write_xdmf(dim, xyz, conn, fields, t_step=0, time=0.0, out_dir="", basesol="
     nf.names = names
     nf.order, nf.vals = order.ctypes.data, vals.ctypes.data
     o = _out(t_step, time, out_dir, basesol, basemesh, connlin, ndigits)
-    check(L.exf_write_xdmf(C.byref(nf), C.byref(o)))
+    check((L.exf_write_xdmf_case if case else L.exf_write_xdmf)(C.byref(nf), C.byref(o)))
     return xmf_path(t_step, out_dir, basesol, ndigits)
 
 
@@ -90,14 +113,14 @@ def _item(el, base):
 
 
 def read_xdmf(path):
-    """A written step: {"time", "cell_type", "cells" [nsub][4 | 8], "xyz" [3][nnodes],
-    "fields" {name: [nnodes]}}."""
+    """A written step: {"time" (None for a case file), "cell_type", "cells" [nsub][4 | 8],
+    "xyz" [3][nnodes], "fields" {name: [nnodes]}}."""
     base = os.path.dirname(path)
     grid = ET.parse(path).getroot().find("Domain").find("Grid")
     topo = grid.find("Topology")
     geo = grid.find("Geometry")
     out = {
-        "time": float(grid.find("Time").get("Value")),
+        "time": None if grid.find("Time") is None else float(grid.find("Time").get("Value")),
         "cell_type": topo.get("Type"),
         "cells": _item(topo.find("DataStructure"), base),
         "xyz": np.stack([_item(d, base)[:, 0] for d in geo.findall("DataStructure")]),

@@ -360,6 +360,14 @@ EXF_API int exf_write_xdmf(const exf_node_fields *f, const exf_soln_out *o);
  * refvalue[var] (NULL: 1), from x of the top level. */
 EXF_API int exf_print_soln(exf_sys *const *sys, int nsys, const char *const *names, const double *refvalue,
                            const exf_soln_out *o);
+/* MGEquationsSystem::print_case (src/MGEquationsSystem.C:814-935): the initial state
+ * (x_old) of every variable with its boundary flags <name>bd (bc1) and <name>vl (bc0)
+ * (MGSolDA::print_bc, src/MGSolverDA.C:1418-1520), three node attributes per variable, in
+ * <dir>/<basesol>.<step>.xmf/.bin (basesol as BASECASE) over the base mesh coordinates
+ * <basemesh>.bin, without <Time>; exf_write_xdmf_case writes given node fields so */
+EXF_API int exf_print_case(exf_sys *const *sys, int nsys, const char *const *names, const double *refvalue,
+                           const exf_soln_out *o);
+EXF_API int exf_write_xdmf_case(const exf_node_fields *f, const exf_soln_out *o);
 /* unit-level operations on host buffers (NumericVectorM::resid / matrix_mult);
  * exf_resid with b == NULL returns r = A x */
 EXF_API int exf_resid(exf_sys *s, int lev, const double *x, const double *b, double *r);

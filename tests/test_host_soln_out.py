@@ -123,3 +123,24 @@ def test_bad_output_arguments(tmp_path):
         ex.write_xdmf(2, xyz, conn, [("u", 2, np.zeros(nn))], out_dir=str(tmp_path / "missing"))
     assert e.value.code == _lib.EXF_ERR_IO
     assert b"cannot open" in _lib.load().exf_last_error()
+
+
+def test_case_file(tmp_path):
+    """The case file of print_case_xmf (src/MGEquationsSystem.C:872-935): the base mesh
+    coordinates <basemesh>.bin and no <Time>."""
+    xyz, conn = top_mesh(3, 2)
+    nn = xyz.shape[1]
+    f = np.arange(nn, dtype=float)
+    path = ex.write_xdmf(3, xyz, conn, [("T", 2, f), ("Tbd", 2, f % 2), ("Tvl", 2, f % 3)], t_step=0,
+                         out_dir=str(tmp_path), basesol="case", basemesh="grid", case=True)
+    assert os.path.basename(path) == "case.0000.xmf"
+    assert sorted(os.listdir(tmp_path)) == ["case.0000.bin", "case.0000.xmf", "grid.bin", "grid_conn_lin.bin"]
+    root = ET.parse(path).getroot()
+    grid = root.find("Domain").find("Grid")
+    assert grid.find("Time") is None
+    assert all(g.text.strip() == "grid.bin" for g in grid.find("Geometry").findall("DataStructure"))
+    d = ex.read_xdmf(path)
+    assert d["time"] is None
+    assert np.array_equal(d["xyz"], xyz)
+    assert [a.get("Name") for a in grid.findall("Attribute")] == ["T", "Tbd", "Tvl"]
+    assert np.array_equal(d["fields"]["Tvl"], f % 3)
