@@ -7,6 +7,6 @@ first call raises.
 """
 from . import _lib  # noqa: F401
 from ._lib import ExfError, load  # noqa: F401
-from .mgsolver import MGSolBase, MGSolNS, MGSolT, MGSolTBK, Mesh, mg_params, phys, timestep_loop  # noqa: F401
+from .mgsolver import MGSolBase, MGSolDS, MGSolNS, MGSolT, MGSolTBK, Mesh, mg_params, phys, timestep_loop  # noqa: F401
 from .soln_out import print_case, print_soln, read_xdmf, write_xdmf  # noqa: F401
 from .workloads import WORKLOADS, make_case  # noqa: F401

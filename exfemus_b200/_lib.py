@@ -22,6 +22,7 @@ KIND_T = 0
 KIND_NS = 1
 KIND_K = 2
 KIND_W = 3
+KIND_DS = 4
 BC_HEAT_DIRICHLET = 1
 BC_CAVITY = 2
 BC_CHANNEL = 3
@@ -126,6 +127,7 @@ SIGNATURES = [
     ("exf_sys_get_colours", _I, [_P, _I, _IP, _IP]),
     ("exf_sys_couple", _I, [_P, _P]),
     ("exf_sys_set_wall", _I, [_P, _DP, C.c_double]),
+    ("exf_sys_set_ds", _I, [_P, _I, C.c_double, _DP, _DP]),
     ("exf_mesh_wall_dist", _I, [_P, _IP, _DP]),
     ("exf_sys_set_xold", _I, [_P, _DP]),
     ("exf_sys_get_xold", _I, [_P, _DP]),

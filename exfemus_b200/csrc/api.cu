@@ -397,7 +397,7 @@ static int sys_upload_bc(exf_sys *s) {
 }
 
 int exf_sys_create(exf_mesh *m, int kind, exf_sys **out) {
-  if (!m || !out || kind < EXF_KIND_T || kind > EXF_KIND_W) {
+  if (!m || !out || kind < EXF_KIND_T || kind > EXF_KIND_DS) {
     set_error("exf_sys_create: bad argument");
     return EXF_ERR_ARG;
   }
@@ -407,7 +407,7 @@ int exf_sys_create(exf_mesh *m, int kind, exf_sys **out) {
   s->kind = kind;
   s->dim = m->dim;
   s->nlev = m->nlev;
-  s->nv2 = kind == EXF_KIND_NS ? m->dim : 1;  // T, K, W: one quadratic variable
+  s->nv2 = kind == EXF_KIND_NS ? m->dim : 1;  // T, K, W, DS: one quadratic variable
   s->nv1 = kind == EXF_KIND_NS ? 1 : 0;
   s->nvars = s->nv2 + s->nv1;
   if (cudaDeviceGetAttribute(&s->nsm, cudaDevAttrMultiProcessorCount, m->device) != cudaSuccess ||
@@ -795,6 +795,23 @@ int exf_sys_set_wall(exf_sys *s, const double *dist, double nu_wall) {
   return EXF_OK;
 }
 
+int exf_sys_set_ds(exf_sys *s, int dir, double dt, const double *u_fsi, const double *d_old) {
+  CHECK_SYS(s);
+  if (s->kind != EXF_KIND_DS || dir < 0 || dir >= s->mesh->dim || !(dt > 0.) || !u_fsi || !d_old) {
+    set_error("exf_sys_set_ds: needs a displacement system, 0 <= dir < dim, dt > 0 and both fields");
+    return EXF_ERR_ARG;
+  }
+  const size_t n = (size_t)s->mesh->dim * s->mesh->ntop;
+  EXF_TRY(s->ds_u.ensure(n));
+  EXF_TRY(s->ds_d.ensure(n));
+  EXF_CUDA(cudaMemcpyAsync(s->ds_u.p, u_fsi, n * sizeof(double), cudaMemcpyHostToDevice, s->stream));
+  EXF_CUDA(cudaMemcpyAsync(s->ds_d.p, d_old, n * sizeof(double), cudaMemcpyHostToDevice, s->stream));
+  EXF_CUDA(cudaStreamSynchronize(s->stream));
+  s->ds_dir = dir;
+  s->ds_dt = dt;
+  return EXF_OK;
+}
+
 static int h2d(exf_sys *s, double *d, const double *h, size_t n) {
   if (!h) return EXF_ERR_ARG;
   EXF_CUDA(cudaMemcpyAsync(d, h, n * sizeof(double), cudaMemcpyHostToDevice, s->stream));
@@ -852,6 +869,7 @@ int exf_gen_mat_rhs(exf_sys *s, const exf_phys *ph, int lev, int mode) {
   if (!ph || (mode != 0 && mode != 1)) return EXF_ERR_ARG;
   if (s->kind == EXF_KIND_NS && s->mesh->dim == 3 && s->nv2 != 3) return EXF_ERR_STATE;
   if (s->kind == EXF_KIND_K || s->kind == EXF_KIND_W) EXF_TRY(assemble_kw_level(s, ph, lev, mode));
+  else if (s->kind == EXF_KIND_DS) EXF_TRY(assemble_ds_level(s, lev, mode));
   else EXF_TRY(assemble_level(s, ph, lev, mode));
   EXF_TRY(sync_fp32(s, lev));
   if (lev == 0) s->coarse_ok = 0;
@@ -859,17 +877,24 @@ int exf_gen_mat_rhs(exf_sys *s, const exf_phys *ph, int lev, int mode) {
   return EXF_OK;
 }
 
-// GenMatRhs of every level (the top one with its rhs), the levels' elements of one colour
-// in one launch
+// GenMatRhs of every level (the top one with its rhs); for T and NS the levels' elements
+// of one colour in one launch
+static int assemble_every_level(exf_sys *s, const exf_phys *ph) {
+  if (s->kind == EXF_KIND_K || s->kind == EXF_KIND_W) {
+    for (int l = s->nlev - 1; l >= 0; l--) EXF_TRY(assemble_kw_level(s, ph, l, l == s->nlev - 1 ? 1 : 0));
+  } else if (s->kind == EXF_KIND_DS) {
+    for (int l = s->nlev - 1; l >= 0; l--) EXF_TRY(assemble_ds_level(s, l, l == s->nlev - 1 ? 1 : 0));
+  } else {
+    EXF_TRY(assemble_all_levels(s, ph));
+  }
+  return EXF_OK;
+}
+
 int exf_assemble_all(exf_sys *s, const exf_phys *ph) {
   CHECK_SYS(s);
   if (!ph) return EXF_ERR_ARG;
   if (s->kind == EXF_KIND_NS && s->mesh->dim == 3 && s->nv2 != 3) return EXF_ERR_STATE;
-  if (s->kind == EXF_KIND_K || s->kind == EXF_KIND_W) {
-    for (int l = s->nlev - 1; l >= 0; l--) EXF_TRY(assemble_kw_level(s, ph, l, l == s->nlev - 1 ? 1 : 0));
-  } else {
-    EXF_TRY(assemble_all_levels(s, ph));
-  }
+  EXF_TRY(assemble_every_level(s, ph));
   for (int l = 0; l < s->nlev; l++) EXF_TRY(sync_fp32(s, l));
   s->coarse_ok = 0;
   s->assembled = 1;
@@ -1338,7 +1363,7 @@ int exf_time_op(exf_sys *s, int what, int lev, const exf_mg_params *p, const exf
       case 1:
         return f32 ? smooth<float>(s, lev, p, 1, L.x32.p, L.b32.p) : smooth<double>(s, lev, p, 1, L.x.p, L.b.p);
       case 2:
-        EXF_TRY(assemble_all_levels(s, ph));  // the exf_assemble_all path
+        EXF_TRY(assemble_every_level(s, ph));  // the exf_assemble_all path
         for (int l = 0; l < s->nlev; l++) s->L[l].ilu_ok = false;
         return EXF_OK;
       case 3: {

@@ -1046,4 +1046,172 @@ int assemble_kw_level(exf_sys *s, const exf_phys *ph, int lev, int mode) {
   return assemble_kw_dim<3>(s, ph, lev, mode);
 }
 
+// ---- the fluid-structure template's mesh displacement, one direction ------------------
+// MGSolDS::GenMatRhs (template_appl/fsi/SRC/MGSolverDS.C:321-700, ALE_MOVING): phase from
+// the element centre's bc0 (< 2 fluid); fluid rows K_ij = sum_q JxW (bc0_i % 2) fl_i dt
+// (100 grad phi_j . grad phi_i), fl_i = 0 on interface nodes (bc0 > 3), rhs 0; boundary
+// sides whose last node has an even bc0: K_ii += fl_i det_side(last Gauss point) / dt,
+// rhs fl_i (bc1_last % 2) det/dt (u_fsi_x dt + d_old_x); solid rows K_ii = 1, rhs
+// u_fsi_dir dt + d_old_dir.  One CTA per element, the elements of one colour per launch.
+template <int DIM>
+struct DsArgs {
+  const FETab<DIM> *tab;
+  const int *conn, *neigh, *elist;
+  const double *xyz;
+  int ntop, Ntop;
+  const int *bc0, *bc1;
+  const double *u, *d;  // [DIM][Ntop]
+  const int *qq_ptr;
+  const uint8_t *pos_qq;
+  double *vv, *rhs;
+  double dt;
+  int dir;
+  int sides[FE<DIM>::NSIDE][FE<DIM>::NSN];
+};
+
+template <int DIM, int NT>
+__global__ void __launch_bounds__(NT) k_assemble_ds(DsArgs<DIM> A, int mode) {
+  using F = FE<DIM>;
+  constexpr int NEN = F::NEN, NQ = F::NQ;
+  const int tid = threadIdx.x, e = A.elist[blockIdx.x];
+  __shared__ int s_conn[NEN], s_bcv[NEN];
+  __shared__ double s_xx[DIM][NEN];
+  __shared__ double s_dphi[NQ][NEN][DIM];
+  __shared__ double s_jxw[NQ];
+  const FETab<DIM> *t = A.tab;
+  for (int k = tid; k < NEN; k += NT) {
+    const int nd = A.conn[(long)e * NEN + k];
+    s_conn[k] = nd;
+    for (int d = 0; d < DIM; d++) s_xx[d][k] = A.xyz[nd + (long)d * A.ntop];
+    s_bcv[k] = A.bc0[nd];
+  }
+  __syncthreads();
+  const double dt = A.dt;
+  if (s_bcv[NEN - 1] >= 2) {  // solid: the displacement follows the FSI velocity
+    for (int i = tid; i < NEN; i += NT) {
+      const int nd = s_conn[i];
+      A.vv[A.qq_ptr[nd] + A.pos_qq[((long)e * NEN + i) * NEN + i]] += 1.;
+      if (mode == 1) A.rhs[nd] += A.u[nd + (long)A.dir * A.Ntop] * dt + A.d[nd + (long)A.dir * A.Ntop];
+    }
+    return;
+  }
+  for (int q = tid; q < NQ; q += NT) {  // one thread per Gauss point
+    double J[DIM][DIM];
+    for (int a = 0; a < DIM; a++)
+      for (int b = 0; b < DIM; b++) {
+        double sum = 0.;
+        for (int k = 0; k < NEN; k++) sum += s_xx[a][k] * t->dphi[q][k][b];
+        J[a][b] = sum;
+      }
+    double det, inv[DIM][DIM];  // inv[b][a] = dxi_b / dx_a
+    if constexpr (DIM == 2) {
+      det = J[0][0] * J[1][1] - J[1][0] * J[0][1];
+      const double id = 1. / det;
+      inv[0][0] = J[1][1] * id;
+      inv[0][1] = -J[0][1] * id;
+      inv[1][0] = -J[1][0] * id;
+      inv[1][1] = J[0][0] * id;
+    } else {
+      const int o = DIM - 1;
+      det = J[0][0] * (J[1][1] * J[o][o] - J[1][o] * J[o][1]) - J[0][1] * (J[1][0] * J[o][o] - J[1][o] * J[o][0]) +
+            J[0][o] * (J[1][0] * J[o][1] - J[1][1] * J[o][0]);
+      const double id = 1. / det;
+      inv[0][0] = (J[1][1] * J[o][o] - J[1][o] * J[o][1]) * id;
+      inv[0][1] = (J[0][o] * J[o][1] - J[0][1] * J[o][o]) * id;
+      inv[0][o] = (J[0][1] * J[1][o] - J[0][o] * J[1][1]) * id;
+      inv[1][0] = (J[1][o] * J[o][0] - J[1][0] * J[o][o]) * id;
+      inv[1][1] = (J[0][0] * J[o][o] - J[0][o] * J[o][0]) * id;
+      inv[1][o] = (J[0][o] * J[1][0] - J[0][0] * J[1][o]) * id;
+      inv[o][0] = (J[1][0] * J[o][1] - J[1][1] * J[o][0]) * id;
+      inv[o][1] = (J[0][1] * J[o][0] - J[0][0] * J[o][1]) * id;
+      inv[o][o] = (J[0][0] * J[1][1] - J[0][1] * J[1][0]) * id;
+    }
+    s_jxw[q] = det * t->w[q];
+    for (int k = 0; k < NEN; k++)
+      for (int d = 0; d < DIM; d++) {
+        double dp = 0.;
+        for (int b = 0; b < DIM; b++) dp += inv[b][d] * t->dphi[q][k][b];
+        s_dphi[q][k][d] = dp;
+      }
+  }
+  __syncthreads();
+  for (int p = tid; p < NEN * NEN; p += NT) {
+    const int i = p / NEN, j = p % NEN;
+    const int bv = s_bcv[i];
+    if (bv % 2 == 0 || bv > 3) continue;  // a zero row factor
+    double K = 0.;
+    for (int q = 0; q < NQ; q++) {
+      double lap = 0.;
+      for (int d = 0; d < DIM; d++) lap += s_dphi[q][j][d] * s_dphi[q][i][d];
+      K += s_jxw[q] * dt * (100. * lap);
+    }
+    A.vv[A.qq_ptr[s_conn[i]] + A.pos_qq[((long)e * NEN + i) * NEN + j]] += K;
+  }
+  __syncthreads();
+  // boundary sides, one after the other (a node may lie on two of them)
+  for (int sd = 0; sd < F::NSIDE; sd++) {
+    if (A.neigh[(long)e * F::NSIDE + sd] != -1) continue;
+    const int *sur = A.sides[sd];
+    const int last = sur[F::NSN - 1];
+    if (s_bcv[last] % 2 != 0) continue;
+    const int bc_var = A.bc1[s_conn[last]] % 2;
+    for (int k = tid; k < F::NSN; k += NT) {
+      const int lv = sur[k], nd = s_conn[lv];
+      if (s_bcv[lv] > 3) continue;  // interface node
+      const double ipen = jac_sur<DIM>(t, F::NSQ - 1, s_xx, sur) / dt;
+      A.vv[A.qq_ptr[nd] + A.pos_qq[((long)e * NEN + lv) * NEN + lv]] += ipen;
+      if (mode == 1 && bc_var) A.rhs[nd] += ipen * (A.u[nd] * dt + A.d[nd]);
+    }
+    __syncthreads();
+  }
+}
+
+template <int DIM>
+static int assemble_ds_dim(exf_sys *s, int lev, int mode) {
+  const exf_mesh *m = s->mesh;
+  SysLevel &L = s->L[lev];
+  const MeshLevel &ml = m->lev[lev];
+  if (s->ds_dir < 0) {
+    set_error("displacement assembly needs its direction, dt and fields (exf_sys_set_ds)");
+    return EXF_ERR_STATE;
+  }
+  DsArgs<DIM> a;
+  memset(&a, 0, sizeof(a));
+  a.tab = reinterpret_cast<const FETab<DIM> *>(m->d_fetab.p);
+  for (int sd = 0; sd < FE<DIM>::NSIDE; sd++)
+    for (int k = 0; k < FE<DIM>::NSN; k++) a.sides[sd][k] = DIM == 2 ? Q9_SIDE[sd][k] : H27_FACE[sd][k];
+  a.conn = ml.d_conn.p;
+  a.neigh = ml.d_neigh.p;
+  a.xyz = m->d_xyz.p;
+  a.ntop = m->ntop;
+  a.Ntop = m->ntop;  // the [dim][ntop] fields of exf_sys_set_ds
+  a.bc0 = s->d_bc0.p;
+  a.bc1 = s->d_bc1.p;
+  a.u = s->ds_u.p;
+  a.d = s->ds_d.p;
+  a.qq_ptr = L.qq_ptr.p;
+  a.pos_qq = L.pos_qq.p;
+  a.vv = L.A.vv.p;
+  a.rhs = mode == 1 ? L.b.p : nullptr;
+  a.dt = s->ds_dt;
+  a.dir = s->ds_dir;
+  EXF_TRY(L.A.vv.zero(s->stream));
+  if (mode == 1) EXF_TRY(L.b.zero(s->stream));
+  constexpr int NT = DIM == 2 ? 64 : 128;
+  for (int c = 0; c + 1 < (int)ml.ecol_off.size(); c++) {
+    const int n = ml.ecol_off[c + 1] - ml.ecol_off[c];
+    if (n == 0) continue;
+    a.elist = ml.d_elist.p + ml.ecol_off[c];
+    k_assemble_ds<DIM, NT><<<n, NT, 0, s->stream>>>(a, mode);
+    EXF_LAUNCH_CHECK();
+    EXF_COUNT(1);
+  }
+  return EXF_OK;
+}
+
+int assemble_ds_level(exf_sys *s, int lev, int mode) {
+  if (s->mesh->dim == 2) return assemble_ds_dim<2>(s, lev, mode);
+  return assemble_ds_dim<3>(s, lev, mode);
+}
+
 }  // namespace exf

@@ -297,6 +297,9 @@ struct exf_sys {
   exf::DBuf<double> wall_dist;              // K / W: element wall distances, all levels
   std::vector<long> wall_off;               // first element of each level in wall_dist
   double nu_wall = 0.;
+  exf::DBuf<double> ds_u, ds_d;             // DS: u_fsi and d_old, [dim][ntop] node fields
+  int ds_dir = -1;                          // DS: the direction (-1: exf_sys_set_ds not called)
+  double ds_dt = 0.;
   exf::Partials red;
   exf::DBuf<int> wait_flag;                 // set by a bounded in-kernel wait that ran out
   // per level {||b_L||^2, r^2 before the last pre-smoothing sweep, r^2 before the last
@@ -378,7 +381,8 @@ int update_rmask(exf_sys *s);
 int build_colours(exf_sys *s);
 int assemble_level(exf_sys *s, const exf_phys *ph, int lev, int mode);
 int assemble_all_levels(exf_sys *s, const exf_phys *ph);
-int assemble_kw_level(exf_sys *s, const exf_phys *ph, int lev, int mode);  // K / W systems  // every level, one launch per colour
+int assemble_kw_level(exf_sys *s, const exf_phys *ph, int lev, int mode);
+int assemble_ds_level(exf_sys *s, int lev, int mode);  // DS systems  // K / W systems  // every level, one launch per colour
 int sync_fp32(exf_sys *s, int lev);  // FP32 copy + smoother coefficients after a matrix change
 int vanka_prep(exf_sys *s, int lev);
 int csr_values(exf_sys *s, int lev, double *d_out);         // NB -> CSR order (device)

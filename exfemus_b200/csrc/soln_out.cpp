@@ -119,6 +119,9 @@ using namespace exf;
 
 namespace {
 
+// a displacement system's variable name (MGSolDS: dx, dy, dz)
+const char *ds_name(const exf_sys *s) { return s->ds_dir == 1 ? "dy" : s->ds_dir == 2 ? "dz" : "dx"; }
+
 // one XDMF step (case_file: MGEquationsSystem::print_case_xmf, src/MGEquationsSystem.C:
 // 872-935: no <Time>, the coordinates of the base mesh file <basemesh>.bin)
 int write_xdmf_step(const exf_node_fields *f, const exf_soln_out *o, bool case_file) {
@@ -259,7 +262,7 @@ int exf_print_soln(exf_sys *const *sys, int nsys, const char *const *names, cons
       } else if (s->kind == EXF_KIND_NS) {
         nm.push_back(v < s->nv2 ? ns_names[v] : "p");
       } else {
-        nm.push_back(s->kind == EXF_KIND_K ? "kt" : s->kind == EXF_KIND_W ? "wt" : "T");
+        nm.push_back(s->kind == EXF_KIND_K ? "kt" : s->kind == EXF_KIND_W ? "wt" : s->kind == EXF_KIND_DS ? ds_name(s) : "T");
       }
       order.push_back(v < s->nv2 ? 2 : 1);
       const double ref = refvalue ? refvalue[var] : 1.;
@@ -336,7 +339,7 @@ int exf_print_case(exf_sys *const *sys, int nsys, const char *const *names, cons
       std::string name;
       if (names) name = names[var] ? names[var] : "";
       else if (s->kind == EXF_KIND_NS) name = v < s->nv2 ? ns_names[v] : "p";
-      else name = s->kind == EXF_KIND_K ? "kt" : s->kind == EXF_KIND_W ? "wt" : "T";
+      else name = s->kind == EXF_KIND_K ? "kt" : s->kind == EXF_KIND_W ? "wt" : s->kind == EXF_KIND_DS ? ds_name(s) : "T";
       const bool quad = v < s->nv2;
       const double ref = refvalue ? refvalue[var] : 1.;
       std::vector<double> val(nn, 0.), bd(nn, 0.), vl(nn, 0.);

@@ -469,6 +469,25 @@ class MGSolTBK(MGSolBase):
         check(self.L.exf_sys_set_wall(self.h, dptr(d), float(nu_wall)))
 
 
+class MGSolDS(MGSolBase):
+    """One direction of the fluid-structure template's mesh displacement (MGSolDS,
+    template_appl/fsi/SRC/MGSolverDS.C, ALE_MOVING): direction 0 dx, 1 dy, 2 dz.  Its
+    element matrices read the FSI velocity and the old displacements given to set_fields;
+    bc0 carries the reference's volume flags (element phase from the centre node: < 2
+    fluid, else solid; > 3 on interface nodes) and bc1 the boundary flags."""
+
+    def __init__(self, mesh, direction):
+        super().__init__(mesh, _lib.KIND_DS)
+        self.direction = direction
+
+    def set_fields(self, dt, u_fsi, d_old):
+        """u_fsi, d_old: [dim][ntop] node fields (the FSI velocity, the old displacement
+        of every direction); dt the time step."""
+        u = np.ascontiguousarray(u_fsi, np.float64)
+        d = np.ascontiguousarray(d_old, np.float64)
+        check(self.L.exf_sys_set_ds(self.h, int(self.direction), float(dt), dptr(u), dptr(d)))
+
+
 def timestep_loop(systems, params, nsteps):
     """MGEquationsSystem::eqnmap_timestep_loop (src/MGEquationsSystem.C:422-432) in the
     library: nsteps times the MGTimeStep of every system in order (assembly, solve,

@@ -54,6 +54,10 @@ extern "C" {
  * distances of exf_sys_set_wall */
 #define EXF_KIND_K 2
 #define EXF_KIND_W 3
+/* one direction of the fluid-structure template's mesh displacement (MGSolDS,
+ * template_appl/fsi/SRC/MGSolverDS.C:321-700 with ALE_MOVING): one quadratic variable,
+ * assembled from the FSI velocity and the old displacements of exf_sys_set_ds */
+#define EXF_KIND_DS 4
 
 /* boundary-condition presets: the per-node bc_read rules of the workloads */
 #define EXF_BC_HEAT_DIRICHLET 1  /* T = 0 on every wall                              */
@@ -281,6 +285,16 @@ EXF_API int exf_sys_couple(exf_sys *s, exf_sys *other);
  * elements first, then level 1's, ...) and nu_wall = mu / rho of the omega wall value
  * 6 nu_wall / (BETASTAR y^2) */
 EXF_API int exf_sys_set_wall(exf_sys *s, const double *dist, double nu_wall);
+/* displacement systems (EXF_KIND_DS): the direction dir (0 = dx, 1 = dy, 2 = dz, the
+ * reference's _dir), the time step dt, and the top-level node fields [dim][ntop] the
+ * element matrices read: u_fsi, the FSI velocity, and d_old, the old displacement of every
+ * direction.  Elements whose centre node has bc0 >= 2 are solid (displacement row
+ * d = u_fsi dt + d_old of the direction), the rest fluid (100 dt times the Laplacian,
+ * masked by bc0 % 2 and zero on interface nodes, bc0 > 3); a boundary side whose last
+ * node has an even bc0 gets the penalty det_side / dt with the rhs
+ * bc1 % 2 (u_fsi dt + d_old) of direction 0, as the reference writes it for every
+ * direction (MGSolverDS.C:610-650) */
+EXF_API int exf_sys_set_ds(exf_sys *s, int dir, double dt, const double *u_fsi, const double *d_old);
 /* MGMesh::B_dist (src/MGMesh.C:1285-1350): for every element of every level (level 0's
  * first), the distance from its centre (mean of its nodes) to the nearest centre (mean of
  * the side's nodes) of a wall side of its level; a boundary side is a wall when all its

@@ -1465,6 +1465,115 @@ void or_kw_assemble(or_sys *s, int lev, int mode, int var, const or_phys *ph, co
   if (lev == 0) s->lu_ok = 0;
 }
 
+/* MGSolDS::GenMatRhs with ALE_MOVING (template_appl/fsi/SRC/MGSolverDS.C:321-700), one
+ * element: fluid (centre bc_vol < 1.5) rows dt JxW (bc_vol_i % 2) fl_int_i (100 Lap_ij) over
+ * the Gauss points (:446-480), the boundary penalty det/_dt of sides whose last node has an
+ * even bc_vol with the rhs of the x components, fsi_idx and disp_idx without _dir
+ * (:600-650); solid rows KeM(i,i) = 1, FeM(i) = u_fsi[_dir] dt + d_old[_dir] (:664-671) */
+static void ds_element(or_sys *s, int lev, int mode, int dir, double dt, const double *u, const double *dd,
+                       const fe_tab *t, int e, double *Ke, double *Fe, double *rhs) {
+  const or_mesh *m = s->m;
+  int dim = m->dim, nen = m->nen, top = s->nlev - 1, off = m->ntop, Ntop = m->nnodes[top];
+  csr *A = &s->A[lev];
+  int dofs[MAXEN], bcv[MAXEN], bcb[MAXEN];
+  double xx[3 * MAXEN];
+  const int *c = m->conn[lev] + (long)e * nen;
+  memset(Ke, 0, (size_t)nen * nen * sizeof(double));
+  memset(Fe, 0, nen * sizeof(double));
+  for (int k = 0; k < nen; k++) {
+    for (int d = 0; d < dim; d++) xx[d * nen + k] = m->xyz[c[k] + (long)d * off];
+    dofs[k] = s->node_dof[lev][c[k]];
+    int td = s->node_dof[top][c[k]];
+    bcv[k] = s->bc0[td];
+    bcb[k] = s->bc1[td];
+  }
+  const int phase = bcv[nen - 1] < 1.5 ? 0 : 1;
+  if (phase == 0) {
+    for (int q = 0; q < t->ng; q++) {
+      double ij[9];
+      double det = jac(t, q, xx, nen, ij);
+      double JxW = det * t->w[q];
+      double dphi[MAXEN][3];
+      for (int sh = 0; sh < nen; sh++)
+        for (int i = 0; i < dim; i++) {
+          double sum = 0.;
+          for (int j = 0; j < dim; j++) sum += ij[j + i * dim] * t->dphi[q][sh][j];
+          dphi[sh][i] = sum;
+        }
+      for (int i = 0; i < nen; i++) {
+        int fl_int = bcv[i] > 3.5 ? 0 : 1;
+        double dtxJxW = JxW * (bcv[i] % 2) * fl_int * dt;
+        Fe[i] = 0.;
+        for (int j = 0; j < nen; j++) {
+          double lap = 0.;
+          for (int d = 0; d < dim; d++) lap += dphi[j][d] * dphi[i][d];
+          Ke[i * nen + j] += dtxJxW * (100 * lap);
+        }
+      }
+    }
+    for (int sd = 0; sd < m->nsides; sd++) {
+      if (m->neigh[lev][(long)e * m->nsides + sd] != -1) continue;
+      const int *sur = dim == 2 ? Q9_SIDE[sd] : H27_FACE[sd];
+      int nsn = m->nsn;
+      double xb[3 * 9];
+      for (int k = 0; k < nsn; k++)
+        for (int d = 0; d < dim; d++) xb[d * nsn + k] = xx[d * nen + sur[k]];
+      int last = sur[nsn - 1];
+      if (bcv[last] % 2 != 0) continue;
+      int bc_var = bcb[last] % 2;
+      double ipen = jac_sur(t, t->sng - 1, xb, nsn) / dt;
+      for (int k = 0; k < nsn; k++) {
+        int lv = sur[k];
+        int fl_int = bcv[lv] > 3.5 ? 0 : 1;
+        if (mode == 1) Fe[lv] += fl_int * bc_var * ipen * (u[c[lv]] * dt + dd[c[lv]]);
+        Ke[lv * nen + lv] += fl_int * ipen;
+      }
+    }
+  } else {
+    for (int i = 0; i < nen; i++) {
+      Fe[i] = u[c[i] + (long)dir * Ntop] * dt + dd[c[i] + (long)dir * Ntop];
+      Ke[i * nen + i] = 1.;
+    }
+  }
+  for (int i = 0; i < nen; i++) {
+    int gi = dofs[i];
+    if (mode == 1) rhs[gi] += Fe[i];
+    for (int j = 0; j < nen; j++) A->val[find_col(A, gi, dofs[j])] += Ke[i * nen + j];
+  }
+}
+
+/* one level of the displacement direction dir on the scalar system s (kind 0): matrix
+ * (and, mode 1, rhs) as or_sys_assemble; u (the FSI velocity) and d (the old
+ * displacements) are [dim][ntop] node fields */
+void or_ds_assemble(or_sys *s, int lev, int mode, int dir, double dt, const double *u, const double *d) {
+  const or_mesh *m = s->m;
+  int dim = m->dim, nen = m->nen, top = s->nlev - 1;
+  fe_tab t;
+  fe_init(&t, dim);
+  csr *A = &s->A[lev];
+  memset(A->val, 0, (size_t)A->ptr[A->n] * sizeof(double));
+  double *rhs = NULL;
+  if (mode == 1) {
+    rhs = s->b[lev];
+    memset(rhs, 0, s->ndof[lev] * sizeof(double));
+  }
+  const int nel = m->nel[lev], ncol = 1 << dim;
+  for (int c = 0; c < ncol; c++) {
+#pragma omp parallel
+    {
+      double *Ke = (double *)malloc((size_t)nen * nen * sizeof(double));
+      double *Fe = (double *)malloc(nen * sizeof(double));
+#pragma omp for schedule(dynamic, 4)
+      for (int e = 0; e < nel; e++)
+        if (m->ecol[lev][e] == c) ds_element(s, lev, mode, dir, dt, u, d, &t, e, Ke, Fe, rhs);
+      free(Ke);
+      free(Fe);
+    }
+  }
+  if (mode == 1 && lev == top) memcpy(s->rhs, rhs, s->ndof[lev] * sizeof(double));
+  if (lev == 0) s->lu_ok = 0;
+}
+
 void or_sys_get_matrix(const or_sys *s, int lev, double *val) {
   memcpy(val, s->A[lev].val, (size_t)or_sys_nnz(s, lev) * sizeof(double));
 }

@@ -107,6 +107,7 @@ void or_sys_set_turb(or_sys *s, const double *kold, const double *wold);
  * turbulence template on a scalar system (MGSolTBK::GenMatRhs) */
 void or_kw_assemble(or_sys *s, int lev, int mode, int var, const or_phys *ph, const double *vel,
                     const double *kold, const double *wold, const double *dist, double nu_wall);
+void or_ds_assemble(or_sys *s, int lev, int mode, int dir, double dt, const double *u, const double *d);
 void or_sys_get_matrix(const or_sys *s, int lev, double *val);
 void or_sys_set_matrix(or_sys *s, int lev, const double *val);
 void or_sys_get_rhs(const or_sys *s, double *rhs);

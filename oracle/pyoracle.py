@@ -78,6 +78,7 @@ def oracle_lib():
         L.or_sys_assemble.argtypes = [P, I, I, C.POINTER(OrPhys), P, P, P, P]
         L.or_kw_assemble.argtypes = [P, I, I, I, C.POINTER(OrPhys), P, P, P, P, C.c_double]
         L.or_sys_set_turb.argtypes = [P, P, P]
+        L.or_ds_assemble.argtypes = [P, I, I, I, C.c_double, P, P]
         L.or_sys_get_matrix.argtypes = [P, I, dp]
         L.or_sys_set_matrix.argtypes = [P, I, dp]
         L.or_sys_get_rhs.argtypes = [P, dp]
@@ -238,6 +239,12 @@ class OrSys:
         distances."""
         keep = [None if a is None else np.ascontiguousarray(a, np.float64) for a in (vel, kold, wold, dist)]
         self.L.or_kw_assemble(self.h, lev, mode, var, C.byref(phys), *[_ptr(a) for a in keep], float(nu_wall))
+
+    def ds_assemble(self, lev, mode, direction, dt, u_fsi, d_old):
+        """Level lev of the fluid-structure template's displacement direction on this
+        scalar system; u_fsi, d_old: [dim][ntop] node fields."""
+        keep = [np.ascontiguousarray(a, np.float64) for a in (u_fsi, d_old)]
+        self.L.or_ds_assemble(self.h, lev, mode, direction, float(dt), *[_ptr(a) for a in keep])
 
     def assemble_all(self, phys, xold=None, vel=None, temp=None, qe=None):
         top = self.mesh.nlev - 1
