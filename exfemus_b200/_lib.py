@@ -128,6 +128,7 @@ SIGNATURES = [
     ("exf_sys_couple", _I, [_P, _P]),
     ("exf_sys_set_wall", _I, [_P, _DP, C.c_double]),
     ("exf_sys_set_ds", _I, [_P, _I, C.c_double, _DP, _DP]),
+    ("exf_sys_set_mesh_motion", _I, [_P, _I]),
     ("exf_mesh_wall_dist", _I, [_P, _IP, _DP]),
     ("exf_sys_set_xold", _I, [_P, _DP]),
     ("exf_sys_get_xold", _I, [_P, _DP]),

@@ -358,6 +358,7 @@ int exf_mesh_info(const exf_mesh *m, int lev, int *nnodes, int *nel, int *nvert0
 
 int exf_mesh_get_xyz(const exf_mesh *m, double *xyz) {
   if (!m || !xyz) return EXF_ERR_ARG;
+  EXF_TRY(mesh_pull_xyz(const_cast<exf_mesh *>(m)));
   memcpy(xyz, m->xyz.data(), m->xyz.size() * sizeof(double));
   return EXF_OK;
 }
@@ -763,7 +764,9 @@ int exf_sys_couple(exf_sys *s, exf_sys *other) {
     return EXF_ERR_ARG;
   }
   const bool kw = s->kind == EXF_KIND_K || s->kind == EXF_KIND_W;
-  if (s->kind == EXF_KIND_NS && other && (other->kind == EXF_KIND_K || other->kind == EXF_KIND_W)) {
+  if (s->kind == EXF_KIND_DS && other && other->kind == EXF_KIND_DS) {
+    s->ds_x = other;  // the x displacement the boundary rows read
+  } else if (s->kind == EXF_KIND_NS && other && (other->kind == EXF_KIND_K || other->kind == EXF_KIND_W)) {
     (other->kind == EXF_KIND_K ? s->ns_k : s->ns_w) = other;  // the eddy viscosity's fields
   } else if (kw && other && (other->kind == EXF_KIND_K || other->kind == EXF_KIND_W)) {
     if (other->kind == s->kind) {
@@ -797,18 +800,36 @@ int exf_sys_set_wall(exf_sys *s, const double *dist, double nu_wall) {
 
 int exf_sys_set_ds(exf_sys *s, int dir, double dt, const double *u_fsi, const double *d_old) {
   CHECK_SYS(s);
-  if (s->kind != EXF_KIND_DS || dir < 0 || dir >= s->mesh->dim || !(dt > 0.) || !u_fsi || !d_old) {
-    set_error("exf_sys_set_ds: needs a displacement system, 0 <= dir < dim, dt > 0 and both fields");
+  if (s->kind != EXF_KIND_DS || dir < 0 || dir >= s->mesh->dim || !(dt > 0.) || (!u_fsi != !d_old)) {
+    set_error("exf_sys_set_ds: needs a displacement system, 0 <= dir < dim, dt > 0 and both fields or none");
     return EXF_ERR_ARG;
   }
+  s->ds_dir = dir;
+  s->ds_dt = dt;
+  s->ds_host = u_fsi != nullptr;
+  if (!u_fsi) return EXF_OK;  // coupled: the fields are the systems' x_old on the device
   const size_t n = (size_t)s->mesh->dim * s->mesh->ntop;
   EXF_TRY(s->ds_u.ensure(n));
   EXF_TRY(s->ds_d.ensure(n));
   EXF_CUDA(cudaMemcpyAsync(s->ds_u.p, u_fsi, n * sizeof(double), cudaMemcpyHostToDevice, s->stream));
   EXF_CUDA(cudaMemcpyAsync(s->ds_d.p, d_old, n * sizeof(double), cudaMemcpyHostToDevice, s->stream));
   EXF_CUDA(cudaStreamSynchronize(s->stream));
-  s->ds_dir = dir;
-  s->ds_dt = dt;
+  return EXF_OK;
+}
+
+int exf_sys_set_mesh_motion(exf_sys *s, int moving) {
+  CHECK_SYS(s);
+  if (s->kind != EXF_KIND_DS) return EXF_ERR_ARG;
+  s->ds_move = moving != 0;
+  return EXF_OK;
+}
+
+int mesh_pull_xyz(exf_mesh *m) {
+  if (!m->xyz_moved) return EXF_OK;
+  EXF_CUDA(cudaSetDevice(m->device));
+  EXF_CUDA(cudaDeviceSynchronize());
+  EXF_CUDA(cudaMemcpy(m->xyz.data(), m->d_xyz.p, m->xyz.size() * sizeof(double), cudaMemcpyDeviceToHost));
+  m->xyz_moved = false;
   return EXF_OK;
 }
 
@@ -846,7 +867,10 @@ int exf_sys_get_x(exf_sys *s, double *x) {
 int exf_sys_xold_update(exf_sys *s) {
   CHECK_SYS(s);
   SysLevel &T = s->L[s->nlev - 1];
+  if (s->kind == EXF_KIND_DS && s->ds_move) EXF_TRY(ds_move_mesh(s));  // FINE_MOVEMENT
   EXF_CUDA(cudaMemcpyAsync(s->xold.p, T.x.p, T.ndof * sizeof(double), cudaMemcpyDeviceToDevice, s->stream));
+  // coupled systems read this x_old (and the moved mesh) from their own streams
+  EXF_CUDA(cudaStreamSynchronize(s->stream));
   return EXF_OK;
 }
 int exf_sys_set_source(exf_sys *s, const double *qe) {

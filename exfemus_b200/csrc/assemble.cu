@@ -1060,12 +1060,11 @@ struct DsArgs {
   const double *xyz;
   int ntop, Ntop;
   const int *bc0, *bc1;
-  const double *u, *d;  // [DIM][Ntop]
+  const double *ux, *ud, *dx, *dd;  // [Ntop]: u_fsi and d_old, direction 0 and direction dir
   const int *qq_ptr;
   const uint8_t *pos_qq;
   double *vv, *rhs;
   double dt;
-  int dir;
   int sides[FE<DIM>::NSIDE][FE<DIM>::NSN];
 };
 
@@ -1091,7 +1090,7 @@ __global__ void __launch_bounds__(NT) k_assemble_ds(DsArgs<DIM> A, int mode) {
     for (int i = tid; i < NEN; i += NT) {
       const int nd = s_conn[i];
       A.vv[A.qq_ptr[nd] + A.pos_qq[((long)e * NEN + i) * NEN + i]] += 1.;
-      if (mode == 1) A.rhs[nd] += A.u[nd + (long)A.dir * A.Ntop] * dt + A.d[nd + (long)A.dir * A.Ntop];
+      if (mode == 1) A.rhs[nd] += A.ud[nd] * dt + A.dd[nd];
     }
     return;
   }
@@ -1160,7 +1159,7 @@ __global__ void __launch_bounds__(NT) k_assemble_ds(DsArgs<DIM> A, int mode) {
       if (s_bcv[lv] > 3) continue;  // interface node
       const double ipen = jac_sur<DIM>(t, F::NSQ - 1, s_xx, sur) / dt;
       A.vv[A.qq_ptr[nd] + A.pos_qq[((long)e * NEN + lv) * NEN + lv]] += ipen;
-      if (mode == 1 && bc_var) A.rhs[nd] += ipen * (A.u[nd] * dt + A.d[nd]);
+      if (mode == 1 && bc_var) A.rhs[nd] += ipen * (A.ux[nd] * dt + A.dx[nd]);
     }
     __syncthreads();
   }
@@ -1184,17 +1183,31 @@ static int assemble_ds_dim(exf_sys *s, int lev, int mode) {
   a.neigh = ml.d_neigh.p;
   a.xyz = m->d_xyz.p;
   a.ntop = m->ntop;
-  a.Ntop = m->ntop;  // the [dim][ntop] fields of exf_sys_set_ds
+  a.Ntop = m->ntop;
   a.bc0 = s->d_bc0.p;
   a.bc1 = s->d_bc1.p;
-  a.u = s->ds_u.p;
-  a.d = s->ds_d.p;
+  const long off = (long)s->ds_dir * m->ntop;
+  if (s->ds_host) {  // the [dim][ntop] fields of exf_sys_set_ds
+    a.ux = s->ds_u.p;
+    a.ud = s->ds_u.p + off;
+    a.dx = s->ds_d.p;
+    a.dd = s->ds_d.p + off;
+  } else {  // coupled: the velocity system's x_old ([dim][ntop] first), the DS systems' x_old
+    const exf_sys *v = s->other, *x0 = s->ds_dir == 0 ? s : s->ds_x;
+    if (!v || v->kind != EXF_KIND_NS || !x0 || x0->kind != EXF_KIND_DS || x0->ds_dir != 0) {
+      set_error("a coupled displacement system needs the velocity system and the dx system (exf_sys_couple)");
+      return EXF_ERR_STATE;
+    }
+    a.ux = v->xold.p;
+    a.ud = v->xold.p + off;
+    a.dx = x0->xold.p;
+    a.dd = s->xold.p;
+  }
   a.qq_ptr = L.qq_ptr.p;
   a.pos_qq = L.pos_qq.p;
   a.vv = L.A.vv.p;
   a.rhs = mode == 1 ? L.b.p : nullptr;
   a.dt = s->ds_dt;
-  a.dir = s->ds_dir;
   EXF_TRY(L.A.vv.zero(s->stream));
   if (mode == 1) EXF_TRY(L.b.zero(s->stream));
   constexpr int NT = DIM == 2 ? 64 : 128;
@@ -1212,6 +1225,27 @@ static int assemble_ds_dim(exf_sys *s, int lev, int mode) {
 int assemble_ds_level(exf_sys *s, int lev, int mode) {
   if (s->mesh->dim == 2) return assemble_ds_dim<2>(s, lev, mode);
   return assemble_ds_dim<3>(s, lev, mode);
+}
+
+// MGSolDS::MGTimeStep with moving_mesh and FINE_MOVEMENT (MGSolverDS.C:724-744): the node
+// coordinates of the direction move by the step's displacement increment
+__global__ void k_ds_move(double *xyz, const double *x, const double *xold, int n) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) xyz[i] += x[i] - xold[i];
+}
+
+int ds_move_mesh(exf_sys *s) {
+  exf_mesh *m = s->mesh;
+  const int n = m->ntop;
+  if (s->ds_dir < 0 || s->L[s->nlev - 1].ndof != n) {
+    set_error("mesh motion needs the displacement system's direction (exf_sys_set_ds)");
+    return EXF_ERR_STATE;
+  }
+  const int nb = (n + 255) / 256 < 148 * 8 ? (n + 255) / 256 : 148 * 8;
+  k_ds_move<<<nb, 256, 0, s->stream>>>(m->d_xyz.p + (long)s->ds_dir * n, s->L[s->nlev - 1].x.p, s->xold.p, n);
+  EXF_LAUNCH_CHECK();
+  EXF_COUNT(1);
+  m->xyz_moved = true;
+  return EXF_OK;
 }
 
 }  // namespace exf

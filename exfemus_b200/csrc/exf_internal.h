@@ -151,6 +151,7 @@ struct exf_mesh {
   std::vector<double> xyz;    // [dim*ntop]
   std::vector<exf::MeshLevel> lev;
   exf::DBuf<double> d_xyz;
+  bool xyz_moved = false;  // d_xyz moved on the device (displacement mesh motion): xyz is stale
   exf::DBuf<int> d_lat;
   // FE tables of the assembly (Gauss points, shape values and derivatives, surface
   // rules) on the mesh's device: written once in exf_mesh_create, read-only after
@@ -300,6 +301,9 @@ struct exf_sys {
   exf::DBuf<double> ds_u, ds_d;             // DS: u_fsi and d_old, [dim][ntop] node fields
   int ds_dir = -1;                          // DS: the direction (-1: exf_sys_set_ds not called)
   double ds_dt = 0.;
+  bool ds_host = false;                     // DS: fields from ds_u / ds_d, else from couplings
+  bool ds_move = false;                     // DS: move the mesh at each x_old update
+  exf_sys *ds_x = nullptr;                  // DS: the dx system (old x displacement)
   exf::Partials red;
   exf::DBuf<int> wait_flag;                 // set by a bounded in-kernel wait that ran out
   // per level {||b_L||^2, r^2 before the last pre-smoothing sweep, r^2 before the last
@@ -380,9 +384,11 @@ bool transfers_ready(const exf_sys *s);
 int update_rmask(exf_sys *s);
 int build_colours(exf_sys *s);
 int assemble_level(exf_sys *s, const exf_phys *ph, int lev, int mode);
-int assemble_all_levels(exf_sys *s, const exf_phys *ph);
-int assemble_kw_level(exf_sys *s, const exf_phys *ph, int lev, int mode);
-int assemble_ds_level(exf_sys *s, int lev, int mode);  // DS systems  // K / W systems  // every level, one launch per colour
+int assemble_all_levels(exf_sys *s, const exf_phys *ph);  // every level, one launch per colour
+int assemble_kw_level(exf_sys *s, const exf_phys *ph, int lev, int mode);  // K / W systems
+int assemble_ds_level(exf_sys *s, int lev, int mode);  // DS systems
+int ds_move_mesh(exf_sys *s);       // DS: xyz[dir] += x - x_old on the device
+int mesh_pull_xyz(exf_mesh *m);     // refresh the host xyz after device mesh motion
 int sync_fp32(exf_sys *s, int lev);  // FP32 copy + smoother coefficients after a matrix change
 int vanka_prep(exf_sys *s, int lev);
 int csr_values(exf_sys *s, int lev, double *d_out);         // NB -> CSR order (device)

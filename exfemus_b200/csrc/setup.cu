@@ -861,6 +861,7 @@ int exf_mesh_wall_dist(const exf_mesh *m, const int *wall_node, double *dist) {
     return EXF_ERR_ARG;
   }
   EXF_CUDA(cudaSetDevice(m->device));
+  EXF_TRY(mesh_pull_xyz(const_cast<exf_mesh *>(m)));
   const int dim = m->dim, nen = m->nen, nsn = m->nsn, nside = m->nsides;
   long off = 0;
   for (int l = 0; l < m->nlev; l++) {

@@ -245,6 +245,7 @@ int exf_print_soln(exf_sys *const *sys, int nsys, const char *const *names, cons
       return EXF_ERR_ARG;
     }
   }
+  EXF_TRY(mesh_pull_xyz(const_cast<exf_mesh *>(m)));  // coordinates after mesh motion
   const size_t nn = (size_t)m->ntop;
   std::vector<std::string> nm;
   std::vector<int> order;
@@ -310,6 +311,7 @@ int exf_print_case(exf_sys *const *sys, int nsys, const char *const *names, cons
       return EXF_ERR_ARG;
     }
   }
+  EXF_TRY(mesh_pull_xyz(const_cast<exf_mesh *>(m)));  // coordinates after mesh motion
   const size_t nn = (size_t)m->ntop;
   const exf::MeshLevel &T = m->lev[m->nlev - 1];
   const int nen = m->nen, nvx = m->nvx;

@@ -480,12 +480,22 @@ class MGSolDS(MGSolBase):
         super().__init__(mesh, _lib.KIND_DS)
         self.direction = direction
 
-    def set_fields(self, dt, u_fsi, d_old):
+    def set_fields(self, dt, u_fsi=None, d_old=None):
         """u_fsi, d_old: [dim][ntop] node fields (the FSI velocity, the old displacement
-        of every direction); dt the time step."""
+        of every direction); dt the time step.  Without fields the element matrices read
+        the coupled systems' x_old on the device: the velocity of the coupled NS system,
+        this system's own x_old and the coupled dx system's."""
+        if u_fsi is None and d_old is None:
+            check(self.L.exf_sys_set_ds(self.h, int(self.direction), float(dt), None, None))
+            return
         u = np.ascontiguousarray(u_fsi, np.float64)
         d = np.ascontiguousarray(d_old, np.float64)
         check(self.L.exf_sys_set_ds(self.h, int(self.direction), float(dt), dptr(u), dptr(d)))
+
+    def set_mesh_motion(self, moving=True):
+        """moving_mesh with FINE_MOVEMENT: each x_old update moves the mesh's coordinates
+        of this direction by x - x_old."""
+        check(self.L.exf_sys_set_mesh_motion(self.h, int(bool(moving))))
 
 
 def timestep_loop(systems, params, nsteps):

@@ -295,6 +295,15 @@ EXF_API int exf_sys_set_wall(exf_sys *s, const double *dist, double nu_wall);
  * bc1 % 2 (u_fsi dt + d_old) of direction 0, as the reference writes it for every
  * direction (MGSolverDS.C:610-650) */
 EXF_API int exf_sys_set_ds(exf_sys *s, int dir, double dt, const double *u_fsi, const double *d_old);
+/* u_fsi = d_old = NULL: the fields stay on the device as the reference's _data_eq x_old
+ * views: u_fsi the velocity components of the NS system coupled with exf_sys_couple
+ * (x_old's first dim*ntop entries), d_old of direction dir the system's own x_old and of
+ * direction 0 the dx system coupled with exf_sys_couple (itself when dir = 0) */
+/* moving_mesh with FINE_MOVEMENT (MGSolverDS.C:724-744): at each exf_sys_xold_update
+ * (and so in exf_timestep_loop) the mesh's node coordinates of direction dir move by
+ * x - x_old on the device; every later assembly reads the moved mesh, and
+ * exf_mesh_get_xyz, the output and exf_mesh_wall_dist the moved coordinates */
+EXF_API int exf_sys_set_mesh_motion(exf_sys *s, int moving);
 /* MGMesh::B_dist (src/MGMesh.C:1285-1350): for every element of every level (level 0's
  * first), the distance from its centre (mean of its nodes) to the nearest centre (mean of
  * the side's nodes) of a wall side of its level; a boundary side is a wall when all its

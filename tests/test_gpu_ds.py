@@ -115,3 +115,91 @@ def test_displacement_needs_its_fields(gpu_lib):
     with pytest.raises(_lib.ExfError) as e:
         _lib.check(t.L.exf_sys_set_ds(t.h, 0, DT, _lib.dptr(np.ascontiguousarray(u)), _lib.dptr(np.ascontiguousarray(u))))
     assert e.value.code == _lib.EXF_ERR_ARG
+
+
+def coupled_systems(dim, moving):
+    """A fresh mesh with the velocity system (x_old = u_fsi, not stepped) and the
+    displacement systems in coupled mode (their fields are the systems' x_old)."""
+    box, nlev, n0 = CASES[dim]
+    m = ex.Mesh(dim, nlev, n0, box)
+    xyz = m.xyz()
+    N = m.ntop
+    b0, b1 = flags(xyz)
+    u, d = fields(xyz)
+    ns = ex.MGSolNS(m)
+    xns = np.zeros(ns.ntop_dof)
+    xns[:dim * N] = u.reshape(-1)
+    ns.set_xold(xns)
+    ds = []
+    for a in range(dim):
+        s = ex.MGSolDS(m, a)
+        s.set_bc(b0, b1)
+        s.set_xold(d[a])
+        s.set_fields(DT)
+        s.couple(ns)
+        if moving:
+            s.set_mesh_motion(True)
+        ds.append(s)
+    for s in ds[1:]:
+        s.couple(ds[0])
+    params = [ex.mg_params(eps=1e-11, max_cycles=100, smoother=_lib.SMOOTH_GS) for _ in ds]
+    return m, ds, params
+
+
+def test_coupled_fields_give_the_host_field_operators_bitwise(gpu_lib, ds_case):
+    """The coupled mode reads the velocity system's and the displacement systems' x_old
+    in place of the node fields: the same matrices and rhs, bit for bit."""
+    _, ds, _ = coupled_systems(ds_case["dim"], False)
+    for s, h in zip(ds, ds_case["sys"]):
+        s.assemble_all()
+        h.assemble_all()
+        for lev in range(ds_case["nlev"]):
+            assert np.array_equal(s.csr(lev)[2], h.csr(lev)[2]), (s.direction, lev)
+        assert np.array_equal(s.rhs(), h.rhs())
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+def test_time_loop_moves_the_mesh_as_the_host_loop(gpu_lib, dim):
+    """exf_timestep_loop over the displacement systems with mesh motion gives the bits,
+    cycle counts and node coordinates of the same MGTimeStep sequence driven from here;
+    each update moves the direction's coordinates by x - x_old."""
+    ma, a, pa = coupled_systems(dim, True)
+    mb, b, pb = coupled_systems(dim, True)
+    nsteps = 2
+    host = []
+    for _ in range(nsteps):
+        row = []
+        for s, p in zip(a, pa):
+            s.assemble_all()
+            st = s.solve(p)
+            assert st.converged
+            before, xo, x = ma.xyz(), s.xold(), s.x()
+            s.xold_update()
+            after = ma.xyz()
+            k = s.direction
+            assert np.array_equal(after[k], before[k] + (x - xo))
+            assert np.array_equal(np.delete(after, k, 0), np.delete(before, k, 0))
+            row.append(st.cycles)
+        host.append(row)
+    cyc, _ = ex.timestep_loop(b, pb, nsteps)
+    assert cyc.tolist() == host
+    for sa, sb in zip(a, b):
+        assert np.array_equal(sa.x(), sb.x())
+    assert np.array_equal(ma.xyz(), mb.xyz())
+    assert not np.array_equal(mb.xyz(), ex.Mesh(dim, *CASES[dim][1:], CASES[dim][0]).xyz())
+
+
+def test_coupled_mode_needs_its_partners(gpu_lib):
+    m = ex.Mesh(2, 2, (2, 2), (0, 1, 0, 1))
+    s = ex.MGSolDS(m, 1)
+    s.set_fields(DT)
+    with pytest.raises(_lib.ExfError) as e:
+        s.assemble_all()  # no velocity system, no dx system
+    assert e.value.code == _lib.EXF_ERR_STATE
+    s.couple(ex.MGSolNS(m))
+    with pytest.raises(_lib.ExfError) as e:
+        s.assemble_all()  # still no dx system
+    assert e.value.code == _lib.EXF_ERR_STATE
+    with pytest.raises(_lib.ExfError) as e:
+        _lib.check(s.L.exf_sys_set_ds(s.h, 1, DT, _lib.dptr(np.zeros(2 * m.ntop)), None))  # one field only
+    assert e.value.code == _lib.EXF_ERR_ARG
