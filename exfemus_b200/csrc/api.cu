@@ -824,14 +824,6 @@ int exf_sys_set_mesh_motion(exf_sys *s, int moving) {
   return EXF_OK;
 }
 
-int mesh_pull_xyz(exf_mesh *m) {
-  if (!m->xyz_moved) return EXF_OK;
-  EXF_CUDA(cudaSetDevice(m->device));
-  EXF_CUDA(cudaDeviceSynchronize());
-  EXF_CUDA(cudaMemcpy(m->xyz.data(), m->d_xyz.p, m->xyz.size() * sizeof(double), cudaMemcpyDeviceToHost));
-  m->xyz_moved = false;
-  return EXF_OK;
-}
 
 static int h2d(exf_sys *s, double *d, const double *h, size_t n) {
   if (!h) return EXF_ERR_ARG;

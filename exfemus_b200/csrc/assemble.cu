@@ -1248,4 +1248,13 @@ int ds_move_mesh(exf_sys *s) {
   return EXF_OK;
 }
 
+int mesh_pull_xyz(exf_mesh *m) {
+  if (!m->xyz_moved) return EXF_OK;
+  EXF_CUDA(cudaSetDevice(m->device));
+  EXF_CUDA(cudaDeviceSynchronize());
+  EXF_CUDA(cudaMemcpy(m->xyz.data(), m->d_xyz.p, m->xyz.size() * sizeof(double), cudaMemcpyDeviceToHost));
+  m->xyz_moved = false;
+  return EXF_OK;
+}
+
 }  // namespace exf
