@@ -453,12 +453,32 @@ int exf_sys_create(exf_mesh *m, int kind, exf_sys **out) {
     exf_sys_destroy(s);
     return rc;
   }
+  {
+    std::lock_guard<std::mutex> g(m->sys_mu);
+    m->systems.push_back(s);
+  }
   *out = s;
   return EXF_OK;
 }
 
 int exf_sys_destroy(exf_sys *s) {
   if (!s) return EXF_OK;
+  {  // no partner keeps a pointer to s (their next assembly reports the missing coupling)
+    exf_mesh *m = s->mesh;
+    std::lock_guard<std::mutex> g(m->sys_mu);
+    for (exf_sys *o : m->systems) {
+      if (o->other == s) o->other = nullptr;
+      if (o->turb == s) o->turb = nullptr;
+      if (o->ns_k == s) o->ns_k = nullptr;
+      if (o->ns_w == s) o->ns_w = nullptr;
+      if (o->ds_x == s) o->ds_x = nullptr;
+    }
+    for (size_t k = 0; k < m->systems.size(); k++)
+      if (m->systems[k] == s) {
+        m->systems.erase(m->systems.begin() + k);
+        break;
+      }
+  }
   cudaSetDevice(s->mesh->device);
   for (int k = 0; k < exf_sys::kGraphSlots; k++) {
     if (s->cyc_slot[k].exec) cudaGraphExecDestroy(s->cyc_slot[k].exec);

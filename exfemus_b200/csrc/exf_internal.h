@@ -18,6 +18,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -152,6 +153,9 @@ struct exf_mesh {
   std::vector<exf::MeshLevel> lev;
   exf::DBuf<double> d_xyz;
   bool xyz_moved = false;  // d_xyz moved on the device (displacement mesh motion): xyz is stale
+  // the live systems on this mesh: a destroyed system is cleared from its partners' couplings
+  std::mutex sys_mu;
+  std::vector<exf_sys *> systems;
   exf::DBuf<int> d_lat;
   // FE tables of the assembly (Gauss points, shape values and derivatives, surface
   // rules) on the mesh's device: written once in exf_mesh_create, read-only after

@@ -143,13 +143,13 @@ def coupled_systems(dim, moving):
     for s in ds[1:]:
         s.couple(ds[0])
     params = [ex.mg_params(eps=1e-11, max_cycles=100, smoother=_lib.SMOOTH_GS) for _ in ds]
-    return m, ds, params
+    return m, ds, params, ns
 
 
 def test_coupled_fields_give_the_host_field_operators_bitwise(gpu_lib, ds_case):
     """The coupled mode reads the velocity system's and the displacement systems' x_old
     in place of the node fields: the same matrices and rhs, bit for bit."""
-    _, ds, _ = coupled_systems(ds_case["dim"], False)
+    _, ds, _, _ns = coupled_systems(ds_case["dim"], False)
     for s, h in zip(ds, ds_case["sys"]):
         s.assemble_all()
         h.assemble_all()
@@ -163,8 +163,8 @@ def test_time_loop_moves_the_mesh_as_the_host_loop(gpu_lib, dim):
     """exf_timestep_loop over the displacement systems with mesh motion gives the bits,
     cycle counts and node coordinates of the same MGTimeStep sequence driven from here;
     each update moves the direction's coordinates by x - x_old."""
-    ma, a, pa = coupled_systems(dim, True)
-    mb, b, pb = coupled_systems(dim, True)
+    ma, a, pa, _nsa = coupled_systems(dim, True)
+    mb, b, pb, _nsb = coupled_systems(dim, True)
     nsteps = 2
     host = []
     for _ in range(nsteps):
@@ -203,3 +203,20 @@ def test_coupled_mode_needs_its_partners(gpu_lib):
     with pytest.raises(_lib.ExfError) as e:
         _lib.check(s.L.exf_sys_set_ds(s.h, 1, DT, _lib.dptr(np.zeros(2 * m.ntop)), None))  # one field only
     assert e.value.code == _lib.EXF_ERR_ARG
+
+
+def test_a_closed_partner_leaves_no_coupling(gpu_lib):
+    """Closing a coupled system clears it from its partners: their next assembly reports
+    the missing coupling instead of reading a destroyed system."""
+    m, ds, _, ns = coupled_systems(2, False)
+    ds[1].assemble_all()
+    ns.close()
+    for s in ds:
+        with pytest.raises(_lib.ExfError) as e:
+            s.assemble_all()
+        assert e.value.code == _lib.EXF_ERR_STATE
+    m2, ds2, _, ns2 = coupled_systems(2, False)
+    ds2[0].close()
+    with pytest.raises(_lib.ExfError) as e:
+        ds2[1].assemble_all()  # its dx system is gone
+    assert e.value.code == _lib.EXF_ERR_STATE
