@@ -340,7 +340,15 @@ int exf_mesh_create(const exf_mesh_desc *desc, exf_mesh **out) {
 }
 
 int exf_mesh_destroy(exf_mesh *m) {
-  if (m) cudaSetDevice(m->device);
+  if (!m) return EXF_OK;
+  {
+    std::lock_guard<std::mutex> g(m->sys_mu);
+    if (!m->systems.empty()) {  // the last exf_sys_destroy frees it
+      m->orphaned = true;
+      return EXF_OK;
+    }
+  }
+  cudaSetDevice(m->device);
   delete m;
   return EXF_OK;
 }
@@ -463,8 +471,9 @@ int exf_sys_create(exf_mesh *m, int kind, exf_sys **out) {
 
 int exf_sys_destroy(exf_sys *s) {
   if (!s) return EXF_OK;
+  exf_mesh *const m = s->mesh;
+  bool drop_mesh = false;
   {  // no partner keeps a pointer to s (their next assembly reports the missing coupling)
-    exf_mesh *m = s->mesh;
     std::lock_guard<std::mutex> g(m->sys_mu);
     for (exf_sys *o : m->systems) {
       if (o->other == s) o->other = nullptr;
@@ -478,6 +487,7 @@ int exf_sys_destroy(exf_sys *s) {
         m->systems.erase(m->systems.begin() + k);
         break;
       }
+    drop_mesh = m->orphaned && m->systems.empty();
   }
   cudaSetDevice(s->mesh->device);
   for (int k = 0; k < exf_sys::kGraphSlots; k++) {
@@ -492,6 +502,10 @@ int exf_sys_destroy(exf_sys *s) {
   if (s->ev1) cudaEventDestroy(s->ev1);
   if (s->stream) cudaStreamDestroy(s->stream);
   delete s;
+  if (drop_mesh) {  // exf_mesh_destroy came first
+    cudaSetDevice(m->device);
+    delete m;
+  }
   return EXF_OK;
 }
 

@@ -156,6 +156,7 @@ struct exf_mesh {
   // the live systems on this mesh: a destroyed system is cleared from its partners' couplings
   std::mutex sys_mu;
   std::vector<exf_sys *> systems;
+  bool orphaned = false;  // exf_mesh_destroy called while systems lived: freed with the last
   exf::DBuf<int> d_lat;
   // FE tables of the assembly (Gauss points, shape values and derivatives, surface
   // rules) on the mesh's device: written once in exf_mesh_create, read-only after

@@ -311,11 +311,9 @@ class MGSolBase:
         return self.L.exf_sys_check_pattern(self.h, lev, block, iptr(a), iptr(b), iptr(c))
 
     def couple(self, other):
-        """exf_sys_couple; the partner is kept alive as long as this system (the library
-        clears the coupling of a partner that is closed)."""
+        """exf_sys_couple; keep the partner open while this system assembles (closing it
+        clears the coupling, and the next assembly that needs it fails)."""
         check(self.L.exf_sys_couple(self.h, other.h if other is not None else None))
-        if other is not None:
-            self._partners = getattr(self, "_partners", []) + [other]
 
     # ---- fields
     def set_xold(self, x):
