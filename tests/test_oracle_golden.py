@@ -379,3 +379,42 @@ def test_face0_normal_follows_the_reference_side_order(oracle_mod):
     s.assemble(0, 1, or_phys(oracle_mod, inv_re=0.1, traction=1.0), xold=xold)
     r = s.rhs()[2 * N:3 * N]
     assert r[bottom].sum() < 0 and abs(r[bottom].sum() + 1.0) < 1e-13  # -n_z int p = -(+1)(1)
+
+
+def _ds_oracle(oracle_mod, dim, direction):
+    """The oracle's displacement system (MGSolverDS.C:321-700) on the box of the GPU
+    displacement tests, assembled on every level."""
+    import test_gpu_ds as T
+    box, nlev, n0 = T.CASES[dim]
+    om = oracle_mod.OrMesh(dim, nlev, n0, box)
+    xyz = om.xyz()
+    b0, b1 = T.flags(xyz)
+    u, d = T.fields(xyz)
+    o = oracle_mod.OrSys(om, 0)
+    o.set_bc(b0, b1)
+    for lev in range(nlev):
+        o.ds_assemble(lev, 1 if lev == nlev - 1 else 0, direction, T.DT, u, d)
+    return o, xyz, b0, b1, u, d, T.DT
+
+
+@pytest.mark.parametrize("dim,direction", [(2, 0), (2, 1), (3, 2)])
+def test_displacement_restatement_known_answers(oracle_mod, dim, direction):
+    """Fixed answers of MGSolDS's element rules: solid and interface rows solve to
+    u_fsi dt + d_old of the direction (:664-671); the Dirichlet moving wall takes the x
+    components (:640, fsi_idx and disp_idx without _dir); the fixed inlet (bc1 0) is 0
+    away from the corners; fluid interior rows are 100 dt times a Laplacian, whose rows
+    sum to zero."""
+    o, xyz, b0, b1, u, d, dt = _ds_oracle(oracle_mod, dim, direction)
+    x, st = o.mg_solve(or_mg(oracle_mod, eps=1e-12, max_cycles=100))
+    assert st.converged
+    solid = b0 >= 2
+    assert np.abs(x[solid] - (u[direction][solid] * dt + d[direction][solid])).max() <= 1e-15
+    top = (np.abs(xyz[1] - 1.0) < 1e-12) & (b0 == 0) & (b1 == 1)
+    assert top.any() and np.abs(x[top] - (u[0][top] * dt + d[0][top])).max() <= 1e-14
+    inlet = (np.abs(xyz[0]) < 1e-12) & (np.abs(xyz[1]) > 1e-12) & (np.abs(xyz[1] - 1.0) > 1e-12)
+    assert np.abs(x[inlet]).max() <= 1e-14
+    rp, col, val = o.csr(o.mesh.nlev - 1)
+    interior = np.flatnonzero(b0 == 1)
+    for i in interior[:: max(1, interior.size // 40)]:
+        row = val[rp[i]:rp[i + 1]]
+        assert abs(row.sum()) <= 1e-12 * np.abs(row).max(), i
