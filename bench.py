@@ -56,11 +56,12 @@ def parse():
     ap.add_argument("--vanka-kernel", type=int, default=None,
                     help="profiling modes: EXF_VANKA_* kernel of the Vanka sweeps (default AUTO)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--mode", default="bench", choices=["bench", "vcycle", "step", "workloads", "gmres"],
+    ap.add_argument("--mode", default="bench", choices=["bench", "vcycle", "step", "workloads", "gmres", "ds"],
                     help="vcycle: assemble once and run one mixed and one FP64 V-cycle; step: one Picard "
                          "step (assembly of all levels + mixed solve to 1e-10) -- profiling cases; "
                          "workloads: every workload at full size, one JSON line each; gmres: the "
-                         "Boussinesq temperature system with the GMRES + ILU level solver")
+                         "Boussinesq temperature system with the GMRES + ILU level solver; ds: the FSI "
+                         "mesh displacement (dx, dy) with mesh motion in the time loop")
     return ap.parse_args()
 
 
@@ -525,6 +526,68 @@ def run_workloads(args, local):
 
     run_gmres(args, local)
     run_kw(args, local)
+    run_ds(args, local)
+
+
+def run_ds(args, local):
+    """The fluid-structure template's mesh displacement (dx, dy) on a 2D box (0,2) x
+    (0,1), 128 x 64 quad9, 6 levels, solid for x >= 1: fluid inlet fixed, top wall moving
+    with the structure, bottom natural, interface at x = 1; the velocity system's x_old a
+    smooth field; coupled on the device with mesh motion.  Device time of each assembly of
+    all levels, the solves to 1e-10 (multigrid, Gauss-Seidel 2/2), and the time loop's
+    seconds per step (assembly, solve, x_old update and mesh motion of both directions)."""
+    import ctypes as C
+    import exfemus_b200 as ex
+    from exfemus_b200 import _lib
+    L = ex.load()
+    nlev, n0, box = 6, (4, 2), (0.0, 2.0, 0.0, 1.0)
+    m = ex.Mesh(2, nlev, n0, box, device=local)
+    x, y = m.xyz()
+    N = m.ntop
+    ns = ex.MGSolNS(m)
+    xns = np.zeros(ns.ntop_dof)
+    xns[:N] = 0.3 * np.sin(1.5 * x) * (0.5 + y)
+    xns[N:2 * N] = 0.3 * np.sin(1.5 * x + 1.0) * (0.5 + y) + 0.1
+    ns.set_xold(xns)
+    b0, b1 = np.ones(N, np.int32), np.zeros(N, np.int32)
+    top = np.abs(y - 1.0) < 1e-12
+    b0[top], b1[top] = 0, 1
+    inl = np.abs(x) < 1e-12
+    b0[inl], b1[inl] = 0, 0
+    b0[x > 1.0 + 1e-12] = 2
+    b0[np.abs(x - 1.0) < 1e-12] = 4
+    ds = []
+    for a in range(2):
+        s = ex.MGSolDS(m, a)
+        s.set_bc(b0, b1)
+        s.set_xold(0.02 * np.cos(x + 2.0 * y + a))
+        s.set_fields(0.05)
+        s.couple(ns)
+        ds.append(s)
+    ds[1].couple(ds[0])
+    ms = C.c_double()
+    out = {"workload": "fsi2d_ds", "mesh": "128x64 quad9, 6 levels", "ndof_per_direction": ds[0].ntop_dof}
+    p = ex.mg_params(eps=1e-10, max_cycles=200, smoother=_lib.SMOOTH_GS)
+    for name, s in (("dx", ds[0]), ("dy", ds[1])):
+        for rep in range(2):  # the second call is timed
+            _lib.check(L.exf_event_record(s.h, 0))
+            s.assemble_all()
+            _lib.check(L.exf_event_record(s.h, 1))
+            _lib.check(L.exf_event_elapsed(s.h, 0, 1, C.byref(ms)))
+        out[name + "_assembly_ms"] = ms.value
+        s.set_x(np.zeros(s.ntop_dof))
+        st = s.solve(p)
+        out[name + "_cycles"], out[name + "_solve_s"], out[name + "_rel_res"] = st.cycles, st.seconds, st.rel_res
+    for s in ds:
+        s.set_mesh_motion(True)
+    steps = 4
+    cyc, sec = ex.timestep_loop(ds, [p, p], 1)  # warm-up step
+    t0 = time.perf_counter()
+    cyc, sec = ex.timestep_loop(ds, [p, p], steps)
+    out["loop_s_per_step"] = (time.perf_counter() - t0) / steps
+    out["loop_cycles"] = cyc.tolist()
+    out["mesh_moved_max"] = float(np.abs(m.xyz() - np.stack([x, y])).max())
+    print(json.dumps(out), flush=True)
 
 
 def run_ours(args, ws, rank, local):
@@ -540,6 +603,8 @@ def run_ours(args, ws, rank, local):
         return run_workloads(args, local)
     if args.mode == "gmres":
         return run_gmres(args, local)
+    if args.mode == "ds":
+        return run_ds(args, local)
     case = ex.make_case(args.workload, device=local)
     w = case["w"]
     ns = case["NS"]
