@@ -583,11 +583,11 @@ def run_ds(args, local):
         s.set_mesh_motion(True)
     steps = 4
     pl = ex.mg_params(eps=1e-6, max_cycles=40, smoother=_lib.SMOOTH_GS)  # MGTimeStep's MGSolve(1.e-6, 40)
-    cyc, sec = ex.timestep_loop(ds, [pl, pl], 1)  # warm-up step
+    cyc, sec = ex.timestep_loop(ds, [pl, pl], 1, strict=False)  # warm-up step
     t0 = time.perf_counter()
-    cyc, sec = ex.timestep_loop(ds, [pl, pl], steps)
+    cyc, sec = ex.timestep_loop(ds, [pl, pl], steps, strict=False)
     out["loop_s_per_step"] = (time.perf_counter() - t0) / steps
-    out["loop_cycles"] = cyc.tolist()
+    out["loop_cycles"] = cyc.tolist()  # 40 = MGSolve's cycle limit reached above 1e-6
     out["mesh_moved_max"] = float(np.abs(m.xyz() - np.stack([x, y])).max())
     print(json.dumps(out), flush=True)
 

@@ -1520,6 +1520,7 @@ int exf_timestep_loop(exf_sys *const *sys, int nsys, const exf_phys *phys, const
       set_error("exf_timestep_loop: system %d is NULL", k);
       return EXF_ERR_ARG;
     }
+  bool missed = false;
   for (int step = 0; step < nsteps; step++) {
     for (int k = 0; k < nsys; k++) {
       exf_solve_stats st;
@@ -1527,9 +1528,14 @@ int exf_timestep_loop(exf_sys *const *sys, int nsys, const exf_phys *phys, const
       const int rc = exf_mg_solve(sys[k], &params[k], &st);
       if (cycles) cycles[(long)step * nsys + k] = st.cycles;
       if (seconds) seconds[(long)step * nsys + k] = st.seconds;
-      if (rc != EXF_OK) return rc;
+      if (rc == EXF_ERR_NOT_CONVERGED) missed = true;
+      else if (rc != EXF_OK) return rc;
       EXF_TRY(exf_sys_xold_update(sys[k]));
     }
+  }
+  if (missed) {
+    set_error("exf_timestep_loop: a solve ended above its tolerance (cycles per step and system returned)");
+    return EXF_ERR_NOT_CONVERGED;
   }
   return EXF_OK;
 }

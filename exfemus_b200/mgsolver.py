@@ -500,11 +500,13 @@ class MGSolDS(MGSolBase):
         check(self.L.exf_sys_set_mesh_motion(self.h, int(bool(moving))))
 
 
-def timestep_loop(systems, params, nsteps):
+def timestep_loop(systems, params, nsteps, strict=True):
     """MGEquationsSystem::eqnmap_timestep_loop (src/MGEquationsSystem.C:422-432) in the
     library: nsteps times the MGTimeStep of every system in order (assembly, solve,
     x_old update) without returning here between them.  params: one exf_mg_params per
-    system.  Returns (cycles, seconds), arrays [nsteps, len(systems)]."""
+    system.  Returns (cycles, seconds), arrays [nsteps, len(systems)].  Every step runs
+    even when a solve ends above its tolerance; that raises EXF_ERR_NOT_CONVERGED at the
+    end unless strict is False."""
     L = _lib.load()
     n = len(systems)
     hs = (C.c_void_p * n)(*[s.h for s in systems])
@@ -512,6 +514,8 @@ def timestep_loop(systems, params, nsteps):
     ps = (_lib.ExfMgParams * n)(*params)
     cyc = np.zeros((nsteps, n), dtype=np.int32)
     sec = np.zeros((nsteps, n))
-    check(L.exf_timestep_loop(hs, n, phs, ps, nsteps, iptr(cyc), dptr(sec)))
+    rc = L.exf_timestep_loop(hs, n, phs, ps, nsteps, iptr(cyc), dptr(sec))
+    if strict or rc != _lib.EXF_ERR_NOT_CONVERGED:
+        check(rc)
     return cyc, sec
 

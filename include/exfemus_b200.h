@@ -335,8 +335,10 @@ EXF_API int exf_mg_solve(exf_sys *s, const exf_mg_params *p, exf_solve_stats *st
  * its MGTimeStep (MGSolverNS.C:722-750, MGSolverT.C:530-561): assemble every level with
  * phys[k], solve with params[k], x_old = x.  Coupled systems see each other's x_old as
  * updated within the step.  Per (step, system) the cycles and device seconds of the solve
- * go to cycles[step*nsys + k] and seconds[...] when those are not NULL.  Stops at the first
- * failing solve and returns its status. */
+ * go to cycles[step*nsys + k] and seconds[...] when those are not NULL.  A solve that ends
+ * at its cycle limit above its tolerance does not stop the loop (MGSolve does not stop
+ * MGTimeStep): every step runs, and the loop then returns EXF_ERR_NOT_CONVERGED; any
+ * other failure stops the loop and returns its status. */
 EXF_API int exf_timestep_loop(exf_sys *const *sys, int nsys, const exf_phys *phys, const exf_mg_params *params,
                               int nsteps, int *cycles, double *seconds);
 

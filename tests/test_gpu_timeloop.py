@@ -51,3 +51,24 @@ def test_timestep_loop_matches_oracle_segregated_picard(oracle_mod, gpu_lib):
         x_t_old = x_t
     assert rel(xg_ns, x_ns) < 1e-9
     assert rel(xg_t, x_t) < 1e-9
+
+
+def test_unconverged_solves_do_not_stop_the_loop(gpu_lib):
+    """MGSolve ending at its cycle limit does not stop MGTimeStep: every step runs (one
+    cycle each here), x_old follows x, and the loop reports EXF_ERR_NOT_CONVERGED at the
+    end (strict) or returns the cycle counts (strict=False)."""
+    over = dict(nlev=3, n0=(4, 4))
+    nsteps = 3
+    for strict in (True, False):
+        case = workloads.make_case("bouss2d", **over)
+        ns, t = case["NS"], case["T"]
+        p = [ex.mg_params(eps=1e-30, max_cycles=1, smoother=s, omega=workloads.VANKA_OMEGA)
+             for s in (_lib.SMOOTH_VANKA, _lib.SMOOTH_GS)]
+        if strict:
+            with pytest.raises(_lib.ExfError) as e:
+                ex.timestep_loop([ns, t], p, nsteps)
+            assert e.value.code == _lib.EXF_ERR_NOT_CONVERGED
+        else:
+            cyc, _ = ex.timestep_loop([ns, t], p, nsteps, strict=False)
+            assert cyc.tolist() == [[1, 1]] * nsteps
+        assert np.array_equal(t.xold(), t.x()) and np.array_equal(ns.xold(), ns.x())
