@@ -279,7 +279,10 @@ EXF_API int exf_sys_check_pattern(exf_sys *s, int lev, int block, const int dim[
  * other equation, src/MGSolverBase.C:336-354); a kappa / omega system reads the NS
  * velocity and the other turbulence variable; NS coupled to both kappa and omega
  * systems takes the eddy viscosity IRe (1 + mu_t) of the turbulence template
- * (template_appl/turb-ckw/SRC/MGSolverNS.C:256-293) */
+ * (template_appl/turb-ckw/SRC/MGSolverNS.C:256-293); a displacement system reads the
+ * velocity of an NS system and, for dy / dz, the dx system's x_old.  The library keeps
+ * a pointer to other: destroying other clears the coupling (the next assembly that
+ * needs it returns EXF_ERR_STATE) */
 EXF_API int exf_sys_couple(exf_sys *s, exf_sys *other);
 /* kappa / omega systems: the wall distance of every element (_mgmesh._dist: level 0's
  * elements first, then level 1's, ...) and nu_wall = mu / rho of the omega wall value
